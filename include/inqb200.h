@@ -1,0 +1,139 @@
+/*
+ * inqb200.h — C ABI of libinqb200, the B200 (sm_100a) implementation of INQ's
+ * Kohn-Sham Hamiltonian application H|psi> and the real-time propagators built
+ * on it.
+ *
+ * Conventions (identical to INQ; paths relative to the reference project root):
+ *   - An orbital block is [N][ld] interleaved complex, orbital index fastest:
+ *     element (point p, orbital m) at psi[p*ld + m], p = (ix*ny + iy)*nz + iz
+ *     (src/basis/field_set.hpp:51, :188-194).  complex128 for INQB_FP64,
+ *     complex64 for INQB_MIXED.  Device pointers are caller owned and 16-byte
+ *     aligned; ld >= M.
+ *   - The lattice is given as 9 doubles, row i = lattice vector a_i in bohr.
+ *   - Vectors called "cov" are covariant components (k . a_i), as INQ stores
+ *     the k-point plus vector potential (src/hamiltonian/self_consistency.hpp:152-160).
+ *   - Every function returns an inqb_status; inqb_last_error() describes the
+ *     last failure of the calling thread.  Functions taking a `stream`
+ *     (a cudaStream_t, NULL = legacy default stream) are asynchronous unless
+ *     stated otherwise.
+ */
+#ifndef INQB200_H
+#define INQB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct inqb_ctx inqb_ctx;
+
+enum inqb_status {
+  INQB_OK = 0,
+  INQB_ERR_INVALID = 1,       /* bad argument or call order */
+  INQB_ERR_UNSUPPORTED = 2,   /* grid size / projector count not compiled in */
+  INQB_ERR_CUDA = 3,          /* CUDA runtime error */
+  INQB_ERR_NOMEM = 4,         /* device allocation failed */
+  INQB_ERR_NONFINITE = 5,     /* NaN or Inf found in an input */
+  INQB_ERR_NOT_POSITIVE_DEFINITE = 6, /* overlap matrix failed Cholesky */
+  INQB_ERR_TIMEOUT = 7        /* a bounded device-side wait gave up */
+};
+
+enum inqb_precision {
+  INQB_FP64 = 0,   /* complex128 storage, FP64 arithmetic */
+  INQB_MIXED = 1   /* complex64 storage and FFT/pointwise, FP64 reductions */
+};
+
+/* ---------------------------------------------------------------- library */
+int inqb_version(void);
+const char* inqb_status_string(int status);
+const char* inqb_last_error(void);
+/* 1 if an (nx, ny, nz) grid has compiled kernels for `precision`, else 0. */
+int inqb_grid_supported(int nx, int ny, int nz, int precision);
+
+/* ---------------------------------------------------------------- context
+ * Replaces the construction of basis::real_space + hamiltonian::ks_hamiltonian
+ * (src/basis/real_space.hpp:29-32, src/hamiltonian/ks_hamiltonian.hpp:79-90).
+ * The grid is given explicitly (INQ derives it as round(|a_i| / spacing)). */
+int inqb_ctx_create(const double lattice[9], int nx, int ny, int nz, int precision, int device,
+                    inqb_ctx** out);
+int inqb_ctx_destroy(inqb_ctx* ctx);
+/* Allocates the device workspace for blocks of up to M orbitals, so that the
+ * later calls with M' <= M allocate nothing (INQ allocates per call from its
+ * caching pool, external_libs/gpurun/include/gpu/array.hpp:66-116). */
+int inqb_ctx_reserve(inqb_ctx* ctx, int M);
+/* volume element dV = V_cell / N (src/basis/real_space.hpp:150-152) */
+double inqb_volume_element(const inqb_ctx* ctx);
+/* cartesian -> covariant components (src/systems/cell.hpp:185-187) */
+int inqb_cart_to_cov(const inqb_ctx* ctx, const double cart[3], double cov[3]);
+
+/* ---------------------------------------------------------------- Hamiltonian state
+ * ks_hamiltonian::scalar_potential() (src/hamiltonian/ks_hamiltonian.hpp:200-204):
+ * V[N] on the host, copied to the device. */
+int inqb_set_local_potential(inqb_ctx* ctx, const double* V);
+/* ks_hamiltonian::uniform_vector_potential() plus the k-point, covariant
+ * (src/hamiltonian/ks_hamiltonian.hpp:214-221, used as phi.kpoint() + A). */
+int inqb_set_vector_potential(inqb_ctx* ctx, const double kA_cov[3]);
+
+/* ---------------------------------------------------------------- projector setup
+ * Setup helpers; they need no context and no GPU.
+ * basis::spherical_grid (src/basis/spherical_grid.hpp:59-158): the grid points
+ * within `radius` of `center` (cartesian) including periodic replicas, with the
+ * float distance and float contravariant relative position INQ stores.
+ * inqb_sphere_points fills coords[npts][3], distance[npts], relpos[npts][3]. */
+int inqb_sphere_size(const double lattice[9], const int nr[3], const double center[3], double radius,
+                     int* npts);
+int inqb_sphere_points(const double lattice[9], const int nr[3], const double center[3], double radius,
+                       int npts, int* coords, float* distance, float* relpos);
+/* projector::build (src/hamiltonian/projector.hpp:29-50) for Gaussian KB
+ * projectors: beta[lm][p], lm = (s, p_-1, p_0, p_+1), radial r^l exp(-r^2/2s^2)
+ * times real Y_lm of the relative position. */
+int inqb_gaussian_kb_beta(const double lattice[9], int npts, const float* distance, const float* relpos,
+                          double sigma, double* beta);
+/* projector_all constructor (src/hamiltonian/projector_all.hpp:27-73): per-atom
+ * tables padded to smax points: counts[nproj], coords[nproj][smax][3],
+ * relpos[nproj][smax][3] (float), beta[nproj][L][smax], coeff[nproj][L]. */
+int inqb_set_projectors(inqb_ctx* ctx, int nproj, int L, int smax, const int* counts, const int* coords,
+                        const float* relpos, const double* beta, const double* coeff);
+
+/* ---------------------------------------------------------------- H|psi>
+ * ks_hamiltonian::operator()(orbital_set<real_space, complex> const&)
+ * (src/hamiltonian/ks_hamiltonian.hpp:132-152):
+ *   hpsi = IFFT(1/2|G+k+A|^2 FFT psi) + V psi + sum_a beta_a E_a beta_a^T dV psi
+ * with projector phases exp(+-i (k+A).r).  hpsi may alias psi. */
+int inqb_apply_h(inqb_ctx* ctx, const void* psi, void* hpsi, int M, int ld, void* stream);
+/* The same on HOST buffers ([N][M], ld = M): copies in, applies, copies out,
+ * synchronous.  This is the call an INQ host-memory orbital_set would use. */
+int inqb_apply_h_host(inqb_ctx* ctx, const void* psi_host, void* hpsi_host, int M);
+/* operations::transform::to_fourier / to_real (src/operations/transform.hpp:337-400):
+ * forward unnormalised sign -1, backward sign +1 then 1/N.  out may alias in. */
+int inqb_fft_forward(inqb_ctx* ctx, const void* in, void* out, int M, int ld, void* stream);
+int inqb_fft_backward(inqb_ctx* ctx, const void* in, void* out, int M, int ld, void* stream);
+
+/* ---------------------------------------------------------------- propagation
+ * operations::exponential_in_place (src/operations/exponential.hpp:21-34):
+ * psi <- sum_{k<=order} (f H)^k / k! psi, f = f_re + i f_im, in place. */
+int inqb_exponential(inqb_ctx* ctx, void* psi, int M, int ld, double f_re, double f_im, int order,
+                     void* stream);
+/* real_time::etrs (src/real_time/etrs.hpp:22-82) for a density-independent H:
+ * psi <- T4(i dt/2 H(kA_tdt)) T4(i dt/2 H(kA_t)) psi, in place.  Leaves the
+ * context's vector potential at kA_tdt, as self_consistency does. */
+int inqb_etrs_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                   const double kA_tdt_cov[3], void* stream);
+
+/* ---------------------------------------------------------------- observables
+ * observables::density::calculate (src/observables/density.hpp:23-33,77-95):
+ * rho[p] = sum_m occ[m] |psi[p][m]|^2; occ and rho are FP64 device arrays. */
+int inqb_density(inqb_ctx* ctx, const void* psi, int M, int ld, const double* occ, double* rho,
+                 void* stream);
+/* observables::dipole(density) (src/observables/dipole.hpp:23-40):
+ * out = dV sum_p r_p rho[p] with symmetric-range r; rho on device, out on
+ * host; synchronous. */
+int inqb_dipole(inqb_ctx* ctx, const double* rho, double out[3], void* stream);
+/* operations::orthogonalize (src/operations/orthogonalize.hpp:25-32): FP64
+ * overlap S = dV psi^H psi, Cholesky S = U^H U, psi <- psi U^-1; synchronous. */
+int inqb_orthonormalize(inqb_ctx* ctx, void* psi, int M, int ld, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* INQB200_H */

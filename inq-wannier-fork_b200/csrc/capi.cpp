@@ -1,0 +1,457 @@
+// extern "C" entry points of libinqb200 (declared in include/inqb200.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "inqb_internal.h"
+#include "observables.h"
+#include "plan.h"
+
+namespace inqb {
+const char* last_error();
+void twiddle_table(int n, int n1, int n2, std::vector<double>& re, std::vector<double>& im);
+int split_of(int n, int* n1, int* n2);
+int build_proj_tables(const inqb_ctx& ctx, int nproj, int L, int smax, const int* counts, const int* coords,
+                      const float* relpos, const double* beta, const double* coeff, ProjTables& t);
+int upload_proj_tables(const inqb_ctx& ctx, ProjTables& t);
+int sphere_points(const CellGeom& cell, const int nr[3], const double center[3], double radius, int npts, int* coords,
+                  float* dist, float* relpos, int* count_out);
+int gaussian_kb_beta(const CellGeom& cell, int npts, const float* dist, const float* relpos, double sigma,
+                     double* beta);
+constexpr int kMaxL = 4;
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  int status = INQB_OK;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev && cudaSetDevice(dev) != cudaSuccess) status = fail(INQB_ERR_CUDA, "cudaSetDevice failed");
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+#define INQB_CHECK_CTX(ctx)                                                   \
+  do {                                                                        \
+    if (!(ctx)) return ::inqb::fail(INQB_ERR_INVALID, "null context");        \
+  } while (0)
+
+#define INQB_GUARD(ctx)                  \
+  DeviceGuard guard_((ctx)->device);     \
+  if (guard_.status != INQB_OK) return guard_.status
+
+template <typename T>
+ProjView<T> proj_view(inqb_ctx* ctx) {
+  ProjView<T> v{};
+  const ProjTables& t = ctx->proj;
+  v.nproj = t.nproj;
+  v.L = t.L;
+  v.seg_ptr = t.d_seg_ptr.as<int>();
+  v.seg_atom = t.d_seg_atom.as<int>();
+  v.seg_ent = t.d_seg_ent.as<int>();
+  v.ent_off = t.d_ent_off.as<int>();
+  v.ent_atom = t.d_ent_atom.as<int>();
+  v.pt_ptr = t.d_pt_ptr.as<int>();
+  v.pt_ent = t.d_pt_ent.as<int>();
+  v.ent_beta = t.d_ent_beta.as<T>();
+  v.ent_phase = t.d_ent_phase.ptr;
+  v.scale = t.d_scale.as<double>();
+  v.proj = ctx->d_projacc.as<double2>();
+  return v;
+}
+
+int check_block(const inqb_ctx* ctx, const void* a, int M, long ld) {
+  if (M <= 0) return fail(INQB_ERR_INVALID, "M must be positive");
+  if (ld < M) return fail(INQB_ERR_INVALID, "ld must be >= M");
+  if (!a) return fail(INQB_ERR_INVALID, "null orbital pointer");
+  if (((uintptr_t)a) % 16 != 0) return fail(INQB_ERR_INVALID, "orbital pointer must be 16-byte aligned");
+  (void)ctx;
+  return INQB_OK;
+}
+
+int reserve(inqb_ctx* ctx, int M) {
+  const int G = ctx->plan->G;
+  const size_t groups = (size_t)(M + G - 1) / G;
+  INQB_TRY(ctx->d_tmp.ensure(groups * G * (size_t)ctx->N * ctx->elem_bytes()));
+  if (ctx->proj.nproj > 0) INQB_TRY(ctx->d_projacc.ensure(sizeof(double2) * (size_t)ctx->proj.nproj * ctx->proj.L * M));
+  return INQB_OK;
+}
+
+int update_phases(inqb_ctx* ctx, void* stream) {
+  if (ctx->proj.nproj == 0 || ctx->proj.nent == 0) return INQB_OK;
+  return launch_phases(ctx->precision, ctx->proj.nent, ctx->proj.d_ent_relpos.as<float>(), ctx->kA_cov,
+                       ctx->proj.d_ent_phase.ptr, stream);
+}
+
+int set_kA(inqb_ctx* ctx, const double kA[3], void* stream) {
+  bool same = true;
+  for (int d = 0; d < 3; d++) same = same && (ctx->kA_cov[d] == kA[d]);
+  for (int d = 0; d < 3; d++) ctx->kA_cov[d] = kA[d];
+  if (same && ctx->proj_phases_valid) return INQB_OK;
+  INQB_TRY(update_phases(ctx, stream));
+  ctx->proj_phases_valid = true;
+  return INQB_OK;
+}
+
+// One H application: out = alpha * H in + beta * base.
+int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long ld_out, int M, const void* base,
+          long ld_base, const double alpha[2], const double beta[2], void* stream) {
+  INQB_TRY(reserve(ctx, M));
+  if (!ctx->proj_phases_valid) {
+    INQB_TRY(update_phases(ctx, stream));
+    ctx->proj_phases_valid = true;
+  }
+  LaunchArgs a;
+  a.mode = mode;
+  a.in = in;
+  a.ld_in = ld_in;
+  a.out = out;
+  a.ld_out = ld_out;
+  a.M = M;
+  a.tmp = ctx->d_tmp.ptr;
+  a.tw = ctx->d_tw.ptr;
+  a.V = ctx->d_V.ptr;
+  a.base = base;
+  a.ld_base = ld_base;
+  a.alpha[0] = alpha[0];
+  a.alpha[1] = alpha[1];
+  a.beta[0] = beta[0];
+  a.beta[1] = beta[1];
+  a.stream = stream;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) a.rlat[i][j] = ctx->cell.rlat[i][j];
+  ctx->cell.cov_to_cart(ctx->kA_cov, a.kA_cart);
+  ProjView<double> v64;
+  ProjView<float> v32;
+  if (ctx->precision == INQB_FP64) {
+    v64 = proj_view<double>(ctx);
+    a.proj_view = &v64;
+  } else {
+    v32 = proj_view<float>(ctx);
+    a.proj_view = &v32;
+  }
+  return ctx->plan->launch(a);
+}
+
+// psi <- sum_{k <= order} (f H)^k / k! psi by Horner's rule:
+// y = psi; for k = order..1: y = psi + (f/k) H y.  (exponential.hpp:21-34)
+int exponential(inqb_ctx* ctx, void* psi, int M, long ld, double fre, double fim, int order, void* stream) {
+  if (order < 1) return INQB_OK;
+  INQB_TRY(ctx->d_work.ensure((size_t)ctx->N * M * ctx->elem_bytes()));
+  void* y = ctx->d_work.ptr;
+  const double one[2] = {1.0, 0.0};
+  for (int k = order; k >= 1; k--) {
+    const double alpha[2] = {fre / k, fim / k};
+    const void* in = (k == order) ? psi : y;
+    const long ldi = (k == order) ? ld : M;
+    void* out = (k == 1) ? psi : y;
+    const long ldo = (k == 1) ? ld : M;
+    INQB_TRY(apply(ctx, LaunchArgs::H, in, ldi, out, ldo, M, psi, ld, alpha, one, stream));
+  }
+  return INQB_OK;
+}
+
+}  // namespace
+}  // namespace inqb
+
+using namespace inqb;
+
+extern "C" {
+
+int inqb_version(void) { return 1; }
+
+const char* inqb_status_string(int status) {
+  switch (status) {
+    case INQB_OK: return "ok";
+    case INQB_ERR_INVALID: return "invalid argument";
+    case INQB_ERR_UNSUPPORTED: return "unsupported configuration";
+    case INQB_ERR_CUDA: return "CUDA error";
+    case INQB_ERR_NOMEM: return "out of device memory";
+    case INQB_ERR_NONFINITE: return "non-finite input";
+    case INQB_ERR_NOT_POSITIVE_DEFINITE: return "matrix not positive definite";
+    case INQB_ERR_TIMEOUT: return "device wait timed out";
+    default: return "unknown status";
+  }
+}
+
+const char* inqb_last_error(void) { return inqb::last_error(); }
+
+int inqb_grid_supported(int nx, int ny, int nz, int precision) {
+  return find_plan(nx, ny, nz, precision) != nullptr ? 1 : 0;
+}
+
+int inqb_ctx_create(const double lattice[9], int nx, int ny, int nz, int precision, int device, inqb_ctx** out) {
+  if (!out || !lattice) return fail(INQB_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (precision != INQB_FP64 && precision != INQB_MIXED) return fail(INQB_ERR_INVALID, "unknown precision");
+  const Plan* plan = find_plan(nx, ny, nz, precision);
+  if (!plan)
+    return fail(INQB_ERR_UNSUPPORTED, "no kernels compiled for grid " + std::to_string(nx) + "x" +
+                                          std::to_string(ny) + "x" + std::to_string(nz));
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(INQB_ERR_CUDA, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(INQB_ERR_INVALID, "device index out of range");
+  DeviceGuard guard(device);
+  if (guard.status != INQB_OK) return guard.status;
+
+  auto* ctx = new inqb_ctx();
+  ctx->device = device;
+  ctx->precision = precision;
+  ctx->nr[0] = nx;
+  ctx->nr[1] = ny;
+  ctx->nr[2] = nz;
+  ctx->N = (long)nx * ny * nz;
+  ctx->cell.init(lattice);
+  if (!(ctx->cell.volume > 1e-10)) {
+    delete ctx;
+    return fail(INQB_ERR_INVALID, "lattice volume is not positive");
+  }
+  ctx->dV = ctx->cell.volume / (double)ctx->N;
+  ctx->plan = plan;
+
+  // twiddles x | y | z in context precision
+  std::vector<double> tw;
+  for (int d = 0; d < 3; d++) {
+    int n1, n2;
+    split_of(ctx->nr[d], &n1, &n2);
+    std::vector<double> re, im;
+    twiddle_table(ctx->nr[d], n1, n2, re, im);
+    for (int i = 0; i < ctx->nr[d]; i++) {
+      tw.push_back(re[i]);
+      tw.push_back(im[i]);
+    }
+  }
+  int st = INQB_OK;
+  if (precision == INQB_FP64) {
+    st = ctx->d_tw.ensure(sizeof(double) * tw.size());
+    if (st == INQB_OK && cudaMemcpy(ctx->d_tw.ptr, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      st = fail(INQB_ERR_CUDA, "twiddle upload failed");
+  } else {
+    std::vector<float> twf(tw.begin(), tw.end());
+    st = ctx->d_tw.ensure(sizeof(float) * twf.size());
+    if (st == INQB_OK && cudaMemcpy(ctx->d_tw.ptr, twf.data(), sizeof(float) * twf.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      st = fail(INQB_ERR_CUDA, "twiddle upload failed");
+  }
+  if (st == INQB_OK) {
+    ctx->V_host.assign(ctx->N, 0.0);
+    st = ctx->d_V.ensure(ctx->N * (precision == INQB_FP64 ? sizeof(double) : sizeof(float)));
+    if (st == INQB_OK && cudaMemset(ctx->d_V.ptr, 0, ctx->d_V.bytes) != cudaSuccess)
+      st = fail(INQB_ERR_CUDA, "potential init failed");
+  }
+  if (st != INQB_OK) {
+    delete ctx;
+    return st;
+  }
+  *out = ctx;
+  return INQB_OK;
+}
+
+int inqb_ctx_destroy(inqb_ctx* ctx) {
+  if (!ctx) return INQB_OK;
+  DeviceGuard guard(ctx->device);
+  cudaDeviceSynchronize();
+  delete ctx;
+  return INQB_OK;
+}
+
+int inqb_ctx_reserve(inqb_ctx* ctx, int M) {
+  INQB_CHECK_CTX(ctx);
+  INQB_GUARD(ctx);
+  if (M <= 0) return fail(INQB_ERR_INVALID, "M must be positive");
+  INQB_TRY(reserve(ctx, M));
+  INQB_TRY(ctx->d_work.ensure((size_t)ctx->N * M * ctx->elem_bytes()));
+  return INQB_OK;
+}
+
+double inqb_volume_element(const inqb_ctx* ctx) { return ctx ? ctx->dV : 0.0; }
+
+int inqb_cart_to_cov(const inqb_ctx* ctx, const double cart[3], double cov[3]) {
+  INQB_CHECK_CTX(ctx);
+  if (!cart || !cov) return fail(INQB_ERR_INVALID, "null vector");
+  ctx->cell.cart_to_cov(cart, cov);
+  return INQB_OK;
+}
+
+int inqb_set_local_potential(inqb_ctx* ctx, const double* V) {
+  INQB_CHECK_CTX(ctx);
+  if (!V) return fail(INQB_ERR_INVALID, "null potential");
+  INQB_GUARD(ctx);
+  for (long p = 0; p < ctx->N; p++)
+    if (!std::isfinite(V[p])) return fail(INQB_ERR_NONFINITE, "potential has a non-finite value");
+  ctx->V_host.assign(V, V + ctx->N);
+  if (ctx->precision == INQB_FP64) {
+    INQB_CUDA_TRY(cudaMemcpy(ctx->d_V.ptr, V, sizeof(double) * ctx->N, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> vf(V, V + ctx->N);
+    INQB_CUDA_TRY(cudaMemcpy(ctx->d_V.ptr, vf.data(), sizeof(float) * ctx->N, cudaMemcpyHostToDevice));
+  }
+  return INQB_OK;
+}
+
+int inqb_set_vector_potential(inqb_ctx* ctx, const double kA_cov[3]) {
+  INQB_CHECK_CTX(ctx);
+  if (!kA_cov) return fail(INQB_ERR_INVALID, "null vector");
+  for (int d = 0; d < 3; d++)
+    if (!std::isfinite(kA_cov[d])) return fail(INQB_ERR_NONFINITE, "vector potential is not finite");
+  INQB_GUARD(ctx);
+  INQB_TRY(set_kA(ctx, kA_cov, nullptr));
+  INQB_CUDA_TRY(cudaStreamSynchronize(nullptr));
+  return INQB_OK;
+}
+
+int inqb_sphere_size(const double lattice[9], const int nr[3], const double center[3], double radius, int* npts) {
+  if (!lattice || !nr || !center || !npts || !(radius >= 0.0)) return fail(INQB_ERR_INVALID, "bad sphere arguments");
+  if (nr[0] <= 0 || nr[1] <= 0 || nr[2] <= 0) return fail(INQB_ERR_INVALID, "grid sizes must be positive");
+  CellGeom cell;
+  cell.init(lattice);
+  return sphere_points(cell, nr, center, radius, 0, nullptr, nullptr, nullptr, npts);
+}
+
+int inqb_sphere_points(const double lattice[9], const int nr[3], const double center[3], double radius, int npts,
+                       int* coords, float* distance, float* relpos) {
+  if (!lattice || !nr || !center || !coords || !distance || !relpos || !(radius >= 0.0))
+    return fail(INQB_ERR_INVALID, "bad sphere arguments");
+  if (nr[0] <= 0 || nr[1] <= 0 || nr[2] <= 0) return fail(INQB_ERR_INVALID, "grid sizes must be positive");
+  CellGeom cell;
+  cell.init(lattice);
+  return sphere_points(cell, nr, center, radius, npts, coords, distance, relpos, nullptr);
+}
+
+int inqb_gaussian_kb_beta(const double lattice[9], int npts, const float* distance, const float* relpos, double sigma,
+                          double* beta) {
+  if (!lattice || npts < 0 || (npts > 0 && (!distance || !relpos || !beta)))
+    return fail(INQB_ERR_INVALID, "bad arguments");
+  CellGeom cell;
+  cell.init(lattice);
+  return gaussian_kb_beta(cell, npts, distance, relpos, sigma, beta);
+}
+
+int inqb_set_projectors(inqb_ctx* ctx, int nproj, int L, int smax, const int* counts, const int* coords,
+                        const float* relpos, const double* beta, const double* coeff) {
+  INQB_CHECK_CTX(ctx);
+  INQB_GUARD(ctx);
+  if (nproj < 0 || smax < 0 || L < 0) return fail(INQB_ERR_INVALID, "negative size");
+  if (nproj > 0 && (L == 0 || L > kMaxL))
+    return fail(INQB_ERR_UNSUPPORTED, "projectors per atom must be 1.." + std::to_string(kMaxL));
+  if (nproj > 0 && (!counts || !coords || !relpos || !beta || !coeff)) return fail(INQB_ERR_INVALID, "null table");
+  ProjTables fresh;
+  if (nproj > 0) {
+    INQB_TRY(build_proj_tables(*ctx, nproj, L, smax, counts, coords, relpos, beta, coeff, fresh));
+    for (double b : fresh.ent_beta)
+      if (!std::isfinite(b)) return fail(INQB_ERR_NONFINITE, "projector table has a non-finite value");
+    INQB_TRY(upload_proj_tables(*ctx, fresh));
+  }
+  INQB_CUDA_TRY(cudaDeviceSynchronize());
+  ctx->proj = std::move(fresh);
+  ctx->proj_phases_valid = false;
+  INQB_TRY(update_phases(ctx, nullptr));
+  INQB_CUDA_TRY(cudaStreamSynchronize(nullptr));
+  ctx->proj_phases_valid = true;
+  return INQB_OK;
+}
+
+int inqb_apply_h(inqb_ctx* ctx, const void* psi, void* hpsi, int M, int ld, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  INQB_TRY(check_block(ctx, hpsi, M, ld));
+  INQB_GUARD(ctx);
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  return apply(ctx, LaunchArgs::H, psi, ld, hpsi, ld, M, nullptr, 0, one, zero, stream);
+}
+
+int inqb_apply_h_host(inqb_ctx* ctx, const void* psi_host, void* hpsi_host, int M) {
+  INQB_CHECK_CTX(ctx);
+  if (!psi_host || !hpsi_host || M <= 0) return fail(INQB_ERR_INVALID, "bad host buffers");
+  INQB_GUARD(ctx);
+  const size_t bytes = (size_t)ctx->N * M * ctx->elem_bytes();
+  INQB_TRY(ctx->d_work2.ensure(bytes));
+  cudaStream_t st = nullptr;
+  INQB_CUDA_TRY(cudaMemcpyAsync(ctx->d_work2.ptr, psi_host, bytes, cudaMemcpyHostToDevice, st));
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  INQB_TRY(apply(ctx, LaunchArgs::H, ctx->d_work2.ptr, M, ctx->d_work2.ptr, M, M, nullptr, 0, one, zero, st));
+  INQB_CUDA_TRY(cudaMemcpyAsync(hpsi_host, ctx->d_work2.ptr, bytes, cudaMemcpyDeviceToHost, st));
+  INQB_CUDA_TRY(cudaStreamSynchronize(st));
+  return INQB_OK;
+}
+
+int inqb_fft_forward(inqb_ctx* ctx, const void* in, void* out, int M, int ld, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, in, M, ld));
+  INQB_TRY(check_block(ctx, out, M, ld));
+  INQB_GUARD(ctx);
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  return apply(ctx, LaunchArgs::FFT_FWD, in, ld, out, ld, M, nullptr, 0, one, zero, stream);
+}
+
+int inqb_fft_backward(inqb_ctx* ctx, const void* in, void* out, int M, int ld, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, in, M, ld));
+  INQB_TRY(check_block(ctx, out, M, ld));
+  INQB_GUARD(ctx);
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  return apply(ctx, LaunchArgs::FFT_BWD, in, ld, out, ld, M, nullptr, 0, one, zero, stream);
+}
+
+int inqb_exponential(inqb_ctx* ctx, void* psi, int M, int ld, double f_re, double f_im, int order, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (order < 0 || order > 64) return fail(INQB_ERR_INVALID, "order out of range");
+  INQB_GUARD(ctx);
+  return exponential(ctx, psi, M, ld, f_re, f_im, order, stream);
+}
+
+int inqb_etrs_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                   const double kA_tdt_cov[3], void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!kA_t_cov || !kA_tdt_cov || !std::isfinite(dt)) return fail(INQB_ERR_INVALID, "bad step arguments");
+  INQB_GUARD(ctx);
+  INQB_TRY(set_kA(ctx, kA_t_cov, stream));
+  INQB_TRY(exponential(ctx, psi, M, ld, 0.0, dt / 2.0, 4, stream));
+  INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
+  INQB_TRY(exponential(ctx, psi, M, ld, 0.0, dt / 2.0, 4, stream));
+  return INQB_OK;
+}
+
+int inqb_density(inqb_ctx* ctx, const void* psi, int M, int ld, const double* occ, double* rho, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!occ || !rho) return fail(INQB_ERR_INVALID, "null occupation or density");
+  INQB_GUARD(ctx);
+  return launch_density(ctx->precision, psi, ld, M, ctx->N, occ, rho, stream);
+}
+
+int inqb_dipole(inqb_ctx* ctx, const double* rho, double out[3], void* stream) {
+  INQB_CHECK_CTX(ctx);
+  if (!rho || !out) return fail(INQB_ERR_INVALID, "null argument");
+  INQB_GUARD(ctx);
+  INQB_TRY(ctx->d_red.ensure(256));
+  double* d = ctx->d_red.as<double>();
+  INQB_TRY(launch_dipole(rho, ctx->N, ctx->cell.lat, ctx->nr, d, stream));
+  double h[3];
+  INQB_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  INQB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  for (int k = 0; k < 3; k++) out[k] = ctx->dV * h[k];
+  return INQB_OK;
+}
+
+int inqb_orthonormalize(inqb_ctx* ctx, void* psi, int M, int ld, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  INQB_GUARD(ctx);
+  DevBuf S, X, info;
+  INQB_TRY(S.ensure(sizeof(double2) * (size_t)M * M));
+  INQB_TRY(X.ensure(sizeof(double2) * (size_t)M * M));
+  INQB_TRY(info.ensure(sizeof(int)));
+  return launch_orthonormalize(ctx->precision, psi, ld, M, ctx->N, ctx->dV, S.as<double2>(), X.as<double2>(),
+                               info.as<int>(), stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,134 @@
+// Internal state of libinqb200: the context that backs the C ABI in
+// include/inqb200.h.  Host-only declarations plus the POD views that kernels get.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/inqb200.h"
+
+namespace inqb {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+
+#define INQB_CUDA_TRY(expr)                                                            \
+  do {                                                                                 \
+    cudaError_t err_ = (expr);                                                         \
+    if (err_ != cudaSuccess)                                                           \
+      return ::inqb::fail(INQB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(err_)); \
+  } while (0)
+
+#define INQB_TRY(expr)        \
+  do {                        \
+    int st_ = (expr);         \
+    if (st_ != INQB_OK) return st_; \
+  } while (0)
+
+// ---------------------------------------------------------------- cell
+struct CellGeom {
+  double lat[3][3];   // lat[i] = lattice vector a_i (cartesian, bohr)
+  double rlat[3][3];  // reciprocal vectors b_i with a_i . b_j = 2 pi delta_ij
+  double volume;
+  void init(const double* lattice);
+  void contra_to_cart(const double c[3], double out[3]) const;
+  void cov_to_cart(const double c[3], double out[3]) const;
+  void cart_to_contra(const double v[3], double out[3]) const;
+  void cart_to_cov(const double v[3], double out[3]) const;
+};
+
+// ---------------------------------------------------------------- device buffer
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes) {
+    o.ptr = nullptr;
+    o.bytes = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      ptr = o.ptr;
+      bytes = o.bytes;
+      o.ptr = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
+  int ensure(size_t nbytes);  // grows, never shrinks; contents not preserved
+  void release();
+  ~DevBuf() { release(); }
+  template <typename P>
+  P* as() const { return reinterpret_cast<P*>(ptr); }
+};
+
+// Projector tables in the layout the fused H kernels read (built on the host
+// from projector_all-style per-atom sphere tables, then uploaded).
+struct ProjTables {
+  int nproj = 0, L = 0;
+  int nent = 0, nseg = 0;
+  // host copies
+  std::vector<int> seg_ptr, seg_atom, seg_ent, ent_off, ent_atom, pt_ptr, pt_ent;
+  std::vector<double> ent_beta;     // [nent][L]
+  std::vector<float> ent_relpos;    // [nent][3] contravariant, float as the reference stores it
+  std::vector<double> scale;        // [nproj][L] = dV * kb coefficient
+  // device copies
+  DevBuf d_seg_ptr, d_seg_atom, d_seg_ent, d_ent_off, d_ent_atom, d_pt_ptr, d_pt_ent;
+  DevBuf d_ent_beta;                // [nent][L] in the context precision
+  DevBuf d_ent_relpos;              // [nent][3] float
+  DevBuf d_ent_phase;               // [nent] complex, exp(+i (k+A).r), context precision
+  DevBuf d_scale;                   // [nproj][L] double
+};
+
+// Kernel view of the projector tables (T = float or double).
+template <typename T>
+struct ProjView {
+  int nproj, L;
+  const int* seg_ptr;
+  const int* seg_atom;
+  const int* seg_ent;
+  const int* ent_off;
+  const int* ent_atom;
+  const int* pt_ptr;
+  const int* pt_ent;
+  const T* ent_beta;
+  const void* ent_phase;  // cplx<T>*
+  const double* scale;
+  double2* proj;          // [nproj][L][M] accumulators (FP64 in both precisions)
+};
+
+struct Plan;  // kernel launch plan for one (precision, grid) pair
+
+}  // namespace inqb
+
+struct inqb_ctx {
+  int device = 0;
+  int precision = INQB_FP64;
+  int nr[3] = {0, 0, 0};
+  long N = 0;
+  inqb::CellGeom cell;
+  double dV = 0.0;
+  double kA_cov[3] = {0, 0, 0};
+  const inqb::Plan* plan = nullptr;
+  bool proj_phases_valid = false;  // device phases match kA_cov
+
+  std::vector<double> V_host;
+  inqb::DevBuf d_V;       // [N] in context precision
+  inqb::DevBuf d_tw;      // twiddles for x, y, z (context precision), N_d entries each
+  inqb::ProjTables proj;
+
+  // workspace (grown on demand)
+  inqb::DevBuf d_tmp;     // Fourier-space intermediate, [groups][N][G]
+  inqb::DevBuf d_projacc; // projection accumulators
+  inqb::DevBuf d_work;    // one orbital block for propagators
+  inqb::DevBuf d_work2;
+  inqb::DevBuf d_red;     // small reduction buffers
+  size_t elem_bytes() const { return precision == INQB_FP64 ? 16 : 8; }
+};

@@ -1,0 +1,263 @@
+// Observables and FP64 orbital linear algebra on the device:
+//   density   rho[p] = sum_m occ[m] |psi[p][m]|^2       (src/observables/density.hpp:23-33)
+//   dipole    dV sum_p r_p rho[p]                         (src/observables/dipole.hpp:23-40)
+//   overlap   S = dV psi^H psi, FP64 accumulation         (src/operations/overlap.hpp:41)
+//   cholesky  S = U^H U, U upper                          (src/matrix/cholesky.hpp:28-89)
+//   rotate    psi <- psi U^-1                             (src/operations/rotate.hpp:147-157)
+// Input orbitals may be complex64 (mixed) or complex128; every sum is FP64.
+#include <cuda_runtime.h>
+
+#include "dft.cuh"
+#include "inqb_internal.h"
+#include "observables.h"
+
+namespace inqb {
+
+template <typename T>
+__global__ void k_density(const cplx<T>* __restrict__ psi, long ld, int M, long N, const double* __restrict__ occ,
+                          double* __restrict__ rho) {
+  const int lane = threadIdx.x & 31;
+  const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+  for (long p = warp; p < N; p += nwarps) {
+    double acc = 0.0;
+    for (int m = lane; m < M; m += 32) {
+      const cplx<T> v = psi[p * ld + m];
+      acc += occ[m] * ((double)v.x * (double)v.x + (double)v.y * (double)v.y);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) rho[p] = acc;
+  }
+}
+
+struct LatticeView {
+  double lat[3][3];
+  int nr[3];
+};
+
+__device__ __forceinline__ void rvector(const LatticeView& g, long p, double r[3]) {
+  const int nyz = g.nr[1] * g.nr[2];
+  int ii[3] = {(int)(p / nyz), (int)((p / g.nr[2]) % g.nr[1]), (int)(p % g.nr[2])};
+  double c[3];
+  for (int d = 0; d < 3; d++) {
+    int s = (ii[d] >= (g.nr[d] + 1) / 2) ? ii[d] - g.nr[d] : ii[d];
+    c[d] = s * (1.0 / g.nr[d]);
+  }
+  for (int k = 0; k < 3; k++) r[k] = g.lat[0][k] * c[0] + g.lat[1][k] * c[1] + g.lat[2][k] * c[2];
+}
+
+__global__ void k_dipole(const double* __restrict__ rho, long N, LatticeView g, double* __restrict__ out) {
+  double acc[3] = {0, 0, 0};
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (long)gridDim.x * blockDim.x) {
+    double r[3];
+    rvector(g, p, r);
+    const double d = rho[p];
+    for (int k = 0; k < 3; k++) acc[k] += r[k] * d;
+  }
+  __shared__ double red[3][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = 0; k < 3; k++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if (lane == 0) red[k][warp] = acc[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    for (int k = 0; k < 3; k++) {
+      double v = lane < nw ? red[k][lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) atomicAdd(&out[k], v);
+    }
+  }
+}
+
+// S[i][j] += dV sum_{p in chunk} conj(psi[p][i]) psi[p][j] ; 32x32 tile per CTA.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_overlap(const cplx<T>* __restrict__ psi, long ld, int M, long N,
+                                                  long chunk, double dV, double2* __restrict__ S) {
+  constexpr int TP = 32;  // points staged per round
+  __shared__ double2 a[TP][33], b[TP][33];
+  const int ti = threadIdx.y, tj = threadIdx.x;
+  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+  const long p0 = (long)blockIdx.z * chunk, p1 = min(N, p0 + chunk);
+  double re = 0.0, im = 0.0;
+  for (long pb = p0; pb < p1; pb += TP) {
+    // thread (ti, tj) loads point pb+ti, orbital i0+tj / j0+tj
+    const long p = pb + ti;
+    double2 va = make_double2(0, 0), vb = make_double2(0, 0);
+    if (p < p1) {
+      if (i0 + tj < M) {
+        cplx<T> v = psi[p * ld + i0 + tj];
+        va = make_double2(v.x, v.y);
+      }
+      if (j0 + tj < M) {
+        cplx<T> v = psi[p * ld + j0 + tj];
+        vb = make_double2(v.x, v.y);
+      }
+    }
+    a[ti][tj] = va;
+    b[ti][tj] = vb;
+    __syncthreads();
+#pragma unroll 8
+    for (int q = 0; q < TP; q++) {
+      const double2 x = a[q][ti], y = b[q][tj];
+      re += x.x * y.x + x.y * y.y;
+      im += x.x * y.y - x.y * y.x;
+    }
+    __syncthreads();
+  }
+  if (i0 + ti < M && j0 + tj < M) {
+    atomicAdd(&S[(long)(i0 + ti) * M + j0 + tj].x, dV * re);
+    atomicAdd(&S[(long)(i0 + ti) * M + j0 + tj].y, dV * im);
+  }
+}
+
+// In-place Cholesky of the Hermitian S (upper triangle used): on exit the upper
+// triangle holds U with S = U^H U.  One CTA; info[0] = first failing pivot + 1.
+__global__ void __launch_bounds__(1024) k_cholesky(double2* __restrict__ S, int M, int* __restrict__ info) {
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  for (int k = 0; k < M; k++) {
+    __syncthreads();
+    const double d = S[(long)k * M + k].x;
+    if (!(d > 0.0)) {
+      if (threadIdx.x == 0) {
+        bad = 1;
+        info[0] = k + 1;
+      }
+      __syncthreads();
+      return;
+    }
+    const double u = sqrt(d);
+    __syncthreads();
+    for (int j = k + threadIdx.x; j < M; j += blockDim.x) {
+      double2 v = S[(long)k * M + j];
+      S[(long)k * M + j] = j == k ? make_double2(u, 0.0) : make_double2(v.x / u, v.y / u);
+    }
+    __syncthreads();
+    // trailing update: S[i][j] -= conj(U[k][i]) U[k][j], k < i <= j
+    const int n = M - k - 1;
+    for (long t = threadIdx.x; t < (long)n * n; t += blockDim.x) {
+      const int i = k + 1 + (int)(t / n), j = k + 1 + (int)(t % n);
+      if (j < i) continue;
+      const double2 ui = S[(long)k * M + i], uj = S[(long)k * M + j];
+      double2 s = S[(long)i * M + j];
+      s.x -= ui.x * uj.x + ui.y * uj.y;
+      s.y -= ui.x * uj.y - ui.y * uj.x;
+      S[(long)i * M + j] = s;
+    }
+  }
+  (void)bad;
+}
+
+// X = U^-1 (upper triangular), one thread per column j, back substitution.
+__global__ void k_triangular_inverse(const double2* __restrict__ U, int M, double2* __restrict__ X) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= M) return;
+  for (int i = 0; i < M; i++) X[(long)i * M + j] = make_double2(0, 0);
+  for (int i = j; i >= 0; i--) {
+    double2 s = make_double2(i == j ? 1.0 : 0.0, 0.0);
+    for (int k = i + 1; k <= j; k++) {
+      const double2 u = U[(long)i * M + k], x = X[(long)k * M + j];
+      s.x -= u.x * x.x - u.y * x.y;
+      s.y -= u.x * x.y + u.y * x.x;
+    }
+    const double uii = U[(long)i * M + i].x;
+    X[(long)i * M + j] = make_double2(s.x / uii, s.y / uii);
+  }
+}
+
+// psi[p][:] <- psi[p][:] X  (X upper triangular), FP64 arithmetic, in place.
+template <typename T>
+__global__ void k_rotate_upper(cplx<T>* __restrict__ psi, long ld, int M, long N, const double2* __restrict__ X) {
+  extern __shared__ double2 row[];
+  for (long p = blockIdx.x; p < N; p += gridDim.x) {
+    __syncthreads();
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+      const cplx<T> v = psi[p * ld + m];
+      row[m] = make_double2(v.x, v.y);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < M; j += blockDim.x) {
+      double re = 0.0, im = 0.0;
+      for (int i = 0; i <= j; i++) {
+        const double2 a = row[i], x = X[(long)i * M + j];
+        re += a.x * x.x - a.y * x.y;
+        im += a.x * x.y + a.y * x.x;
+      }
+      psi[p * ld + j] = mk<T>((T)re, (T)im);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- launchers
+template <typename T>
+static int density_impl(const void* psi, long ld, int M, long N, const double* occ, double* rho, cudaStream_t st) {
+  const int blocks = (int)std::min<long>((N * 32 + 255) / 256, 148L * 16);
+  k_density<T><<<blocks, 256, 0, st>>>((const cplx<T>*)psi, ld, M, N, occ, rho);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_density(int precision, const void* psi, long ld, int M, long N, const double* occ, double* rho,
+                   void* stream) {
+  return precision == INQB_FP64 ? density_impl<double>(psi, ld, M, N, occ, rho, (cudaStream_t)stream)
+                                : density_impl<float>(psi, ld, M, N, occ, rho, (cudaStream_t)stream);
+}
+
+int launch_dipole(const double* rho, long N, const double lat[3][3], const int nr[3], double* out_dev,
+                  void* stream) {
+  LatticeView g;
+  for (int i = 0; i < 3; i++) {
+    g.nr[i] = nr[i];
+    for (int j = 0; j < 3; j++) g.lat[i][j] = lat[i][j];
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  INQB_CUDA_TRY(cudaMemsetAsync(out_dev, 0, 3 * sizeof(double), st));
+  const int blocks = (int)std::min<long>((N + 255) / 256, 148L * 4);
+  k_dipole<<<blocks, 256, 0, st>>>(rho, N, g, out_dev);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+template <typename T>
+static int orthonormalize_impl(void* psi, long ld, int M, long N, double dV, double2* S, double2* X, int* info,
+                               cudaStream_t st) {
+  INQB_CUDA_TRY(cudaMemsetAsync(S, 0, sizeof(double2) * (size_t)M * M, st));
+  INQB_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
+  const int tiles = (M + 31) / 32;
+  long nchunks = std::max<long>(1, std::min<long>(N / 1024, (148L * 8) / (tiles * tiles) + 1));
+  const long chunk = (N + nchunks - 1) / nchunks;
+  nchunks = (N + chunk - 1) / chunk;
+  k_overlap<T><<<dim3(tiles, tiles, (unsigned)nchunks), dim3(32, 32), 0, st>>>((const cplx<T>*)psi, ld, M, N, chunk,
+                                                                              dV, S);
+  INQB_CUDA_TRY(cudaGetLastError());
+  k_cholesky<<<1, 1024, 0, st>>>(S, M, info);
+  INQB_CUDA_TRY(cudaGetLastError());
+  int h_info = 0;
+  INQB_CUDA_TRY(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+  INQB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h_info != 0)
+    return fail(INQB_ERR_NOT_POSITIVE_DEFINITE,
+                "overlap matrix is not positive definite at pivot " + std::to_string(h_info - 1));
+  k_triangular_inverse<<<(M + 127) / 128, 128, 0, st>>>(S, M, X);
+  INQB_CUDA_TRY(cudaGetLastError());
+  const int blocks = (int)std::min<long>(N, 148L * 16);
+  k_rotate_upper<T><<<blocks, 128, sizeof(double2) * M, st>>>((cplx<T>*)psi, ld, M, N, X);
+  INQB_CUDA_TRY(cudaGetLastError());
+  INQB_CUDA_TRY(cudaStreamSynchronize(st));
+  return INQB_OK;
+}
+
+int launch_orthonormalize(int precision, void* psi, long ld, int M, long N, double dV, double2* S, double2* X,
+                          int* info, void* stream) {
+  return precision == INQB_FP64
+             ? orthonormalize_impl<double>(psi, ld, M, N, dV, S, X, info, (cudaStream_t)stream)
+             : orthonormalize_impl<float>(psi, ld, M, N, dV, S, X, info, (cudaStream_t)stream);
+}
+
+}  // namespace inqb

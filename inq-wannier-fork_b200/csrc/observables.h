@@ -1,0 +1,14 @@
+// Launchers of the observable and orbital linear-algebra kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace inqb {
+
+int launch_density(int precision, const void* psi, long ld, int M, long N, const double* occ, double* rho,
+                   void* stream);
+int launch_dipole(const double* rho, long N, const double lat[3][3], const int nr[3], double* out_dev, void* stream);
+int launch_orthonormalize(int precision, void* psi, long ld, int M, long N, double dV, double2* S, double2* X,
+                          int* info, void* stream);
+
+}  // namespace inqb

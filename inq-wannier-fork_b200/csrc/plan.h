@@ -1,0 +1,35 @@
+// Launch plan: the compiled kernel set for one (grid, precision) pair.
+#pragma once
+
+namespace inqb {
+
+struct LaunchArgs {
+  enum Mode { H = 0, FFT_FWD = 1, FFT_BWD = 2 };
+  int mode = H;
+  const void* in = nullptr;
+  long ld_in = 0;
+  void* out = nullptr;
+  long ld_out = 0;
+  int M = 0;
+  void* tmp = nullptr;              // Fourier workspace, [groups][N][G]
+  const void* tw = nullptr;         // twiddles x | y | z
+  const void* proj_view = nullptr;  // ProjView<T>*
+  const void* V = nullptr;          // [N] local potential (T)
+  double rlat[3][3] = {};           // reciprocal vectors (rows)
+  double kA_cart[3] = {};           // cartesian k + A
+  const void* base = nullptr;       // optional epilogue base (out = alpha H in + beta base)
+  long ld_base = 0;
+  double alpha[2] = {1.0, 0.0};
+  double beta[2] = {0.0, 0.0};
+  void* stream = nullptr;
+};
+
+struct Plan {
+  int G = 1;  // orbitals per tile
+  int (*launch)(const LaunchArgs&) = nullptr;
+};
+
+const Plan* find_plan(int nx, int ny, int nz, int precision);
+int launch_phases(int precision, int nent, const float* relpos, const double kA[3], void* phase, void* stream);
+
+}  // namespace inqb

@@ -1,0 +1,238 @@
+"""Python face of libinqb200, mirroring INQ's ``hamiltonian::ks_hamiltonian``.
+
+Device memory comes from torch (CUDA tensors shaped ``[N, M]``, orbital index
+fastest, as INQ's ``orbital_set``); every computation runs in the library's CUDA
+kernels through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import FP64, MIXED, call, dptr, fptr, iptr
+
+
+def _precision(p) -> int:
+    if p in (FP64, "fp64", "double", torch.complex128):
+        return FP64
+    if p in (MIXED, "mixed", "fp32", torch.complex64):
+        return MIXED
+    raise ValueError(f"unknown precision {p!r}")
+
+
+def _lattice(lattice) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(lattice, dtype=np.float64).reshape(9))
+
+
+# ------------------------------------------------------------------ setup helpers (no GPU)
+def sphere(lattice, nr, center, radius):
+    """Atom sphere of INQ's spherical_grid: (coords [n,3] int32, distance [n] float32, relpos [n,3] float32)."""
+    lat = _lattice(lattice)
+    n = np.ascontiguousarray(np.asarray(nr, dtype=np.int32).reshape(3))
+    c = np.ascontiguousarray(np.asarray(center, dtype=np.float64).reshape(3))
+    cnt = ctypes.c_int(0)
+    call("inqb_sphere_size", dptr(lat), iptr(n), dptr(c), float(radius), ctypes.byref(cnt))
+    npts = cnt.value
+    coords = np.zeros((npts, 3), np.int32)
+    dist = np.zeros(npts, np.float32)
+    rel = np.zeros((npts, 3), np.float32)
+    if npts:
+        call("inqb_sphere_points", dptr(lat), iptr(n), dptr(c), float(radius), npts, iptr(coords), fptr(dist),
+             fptr(rel))
+    return coords, dist, rel
+
+
+def gaussian_beta(lattice, dist, relpos, sigma=1.0):
+    """KB tables beta[4][n] for (s, p-1, p0, p+1) Gaussian projectors."""
+    lat = _lattice(lattice)
+    dist = np.ascontiguousarray(dist, np.float32)
+    relpos = np.ascontiguousarray(relpos, np.float32)
+    beta = np.zeros((4, len(dist)))
+    if len(dist):
+        call("inqb_gaussian_kb_beta", dptr(lat), len(dist), fptr(dist), fptr(relpos), float(sigma), dptr(beta))
+    return beta
+
+
+def build_gaussian_kb(lattice, nr, positions, radius=3.0, sigma=1.0, ekb_s=1.5, ekb_p=-0.7):
+    """projector_all-style tables for Gaussian s+p KB projectors on every atom."""
+    spheres = [sphere(lattice, nr, p, radius) for p in np.asarray(positions, float).reshape(-1, 3)]
+    nproj = len(spheres)
+    smax = max([len(s[1]) for s in spheres] + [0])
+    counts = np.array([len(s[1]) for s in spheres], np.int32)
+    coords = -np.ones((nproj, smax, 3), np.int32)
+    relpos = np.zeros((nproj, smax, 3), np.float32)
+    beta = np.zeros((nproj, 4, smax))
+    for a, (c, d, r) in enumerate(spheres):
+        n = len(d)
+        coords[a, :n] = c
+        relpos[a, :n] = r
+        beta[a, :, :n] = gaussian_beta(lattice, d, r, sigma)
+    coeff = np.tile(np.array([ekb_s, ekb_p, ekb_p, ekb_p]), (nproj, 1))
+    return dict(counts=counts, coords=coords, relpos=relpos, beta=beta, coeff=coeff, smax=smax, L=4)
+
+
+def grid_supported(nr, precision="fp64") -> bool:
+    return bool(_lib.lib().inqb_grid_supported(int(nr[0]), int(nr[1]), int(nr[2]), _precision(precision)))
+
+
+# ------------------------------------------------------------------ the Hamiltonian
+class KSHamiltonian:
+    """H|psi> and propagators for one cell/grid on one GPU (drop-in for ks_hamiltonian)."""
+
+    def __init__(self, lattice, nr, precision="fp64", device: int = 0):
+        self.lattice = _lattice(lattice).reshape(3, 3).copy()
+        self.nr = tuple(int(n) for n in nr)
+        self.N = int(np.prod(self.nr))
+        self.precision = _precision(precision)
+        self.dtype = torch.complex128 if self.precision == FP64 else torch.complex64
+        self.device = torch.device("cuda", device)
+        h = ctypes.c_void_p()
+        call("inqb_ctx_create", dptr(_lattice(lattice)), self.nr[0], self.nr[1], self.nr[2], self.precision,
+             int(device), ctypes.byref(h))
+        self._h = h
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _lib.lib().inqb_ctx_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state
+    @property
+    def volume_element(self) -> float:
+        return float(_lib.lib().inqb_volume_element(self._h))
+
+    def cart_to_cov(self, v):
+        v = np.ascontiguousarray(v, np.float64).reshape(3)
+        out = np.zeros(3)
+        call("inqb_cart_to_cov", self._h, dptr(v), dptr(out))
+        return out
+
+    def set_scalar_potential(self, V):
+        V = np.ascontiguousarray(torch.as_tensor(V).detach().cpu().numpy() if torch.is_tensor(V) else V,
+                                 dtype=np.float64).reshape(self.N)
+        call("inqb_set_local_potential", self._h, dptr(V))
+
+    def set_vector_potential_cov(self, kA_cov):
+        kA = np.ascontiguousarray(kA_cov, np.float64).reshape(3)
+        call("inqb_set_vector_potential", self._h, dptr(kA))
+
+    def set_uniform_vector_potential(self, A_cart, kpoint_cart=(0.0, 0.0, 0.0)):
+        self.set_vector_potential_cov(self.cart_to_cov(np.asarray(A_cart, float) + np.asarray(kpoint_cart, float)))
+
+    def set_projectors(self, kb):
+        nproj = len(kb["counts"])
+        counts = np.ascontiguousarray(kb["counts"], np.int32)
+        coords = np.ascontiguousarray(kb["coords"], np.int32)
+        relpos = np.ascontiguousarray(kb["relpos"], np.float32)
+        beta = np.ascontiguousarray(kb["beta"], np.float64)
+        coeff = np.ascontiguousarray(kb["coeff"], np.float64)
+        call("inqb_set_projectors", self._h, nproj, int(kb["L"]), int(kb["smax"]), iptr(counts), iptr(coords),
+             fptr(relpos), dptr(beta), dptr(coeff))
+
+    def set_gaussian_projectors(self, positions, radius=3.0, sigma=1.0, ekb_s=1.5, ekb_p=-0.7):
+        kb = build_gaussian_kb(self.lattice, self.nr, positions, radius, sigma, ekb_s, ekb_p)
+        self.set_projectors(kb)
+        return kb
+
+    def reserve(self, M: int):
+        call("inqb_ctx_reserve", self._h, int(M))
+
+    # -- helpers
+    def _check(self, psi: torch.Tensor) -> torch.Tensor:
+        if not torch.is_tensor(psi) or psi.device.type != "cuda":
+            raise TypeError("orbitals must be a CUDA tensor")
+        if psi.dtype != self.dtype:
+            raise TypeError(f"orbitals must be {self.dtype} for this precision, got {psi.dtype}")
+        if psi.dim() != 2 or psi.shape[0] != self.N or psi.stride(1) != 1:
+            raise ValueError(f"orbitals must be [N={self.N}, M] with unit orbital stride")
+        return psi
+
+    @staticmethod
+    def _stream():
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def empty(self, M: int) -> torch.Tensor:
+        return torch.empty((self.N, M), dtype=self.dtype, device=self.device)
+
+    # -- operations
+    def apply(self, psi: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        """out = H psi  (ks_hamiltonian::operator(); out may be psi)."""
+        psi = self._check(psi)
+        if out is None:
+            out = torch.empty_like(psi)
+        self._check(out)
+        call("inqb_apply_h", self._h, psi.data_ptr(), out.data_ptr(), psi.shape[1], psi.stride(0), self._stream())
+        return out
+
+    __call__ = apply
+
+    def apply_host(self, psi_host: np.ndarray | torch.Tensor, out: np.ndarray | torch.Tensor | None = None):
+        """H psi on host memory (copies in and out inside the call)."""
+        if torch.is_tensor(psi_host):
+            src = psi_host
+            if out is None:
+                out = torch.empty_like(src)
+            call("inqb_apply_h_host", self._h, src.data_ptr(), out.data_ptr(), src.shape[1])
+            return out
+        src = np.ascontiguousarray(psi_host)
+        if out is None:
+            out = np.empty_like(src)
+        call("inqb_apply_h_host", self._h, src.ctypes.data, out.ctypes.data, src.shape[1])
+        return out
+
+    def to_fourier(self, psi, out=None):
+        psi = self._check(psi)
+        out = torch.empty_like(psi) if out is None else self._check(out)
+        call("inqb_fft_forward", self._h, psi.data_ptr(), out.data_ptr(), psi.shape[1], psi.stride(0), self._stream())
+        return out
+
+    def to_real(self, psi, out=None):
+        psi = self._check(psi)
+        out = torch.empty_like(psi) if out is None else self._check(out)
+        call("inqb_fft_backward", self._h, psi.data_ptr(), out.data_ptr(), psi.shape[1], psi.stride(0), self._stream())
+        return out
+
+    def exponential_(self, psi, factor, order=4):
+        """psi <- sum_k (factor H)^k / k! psi (in place)."""
+        psi = self._check(psi)
+        f = complex(factor)
+        call("inqb_exponential", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), f.real, f.imag, int(order),
+             self._stream())
+        return psi
+
+    def etrs_step_(self, psi, dt, kA_t_cov, kA_tdt_cov):
+        psi = self._check(psi)
+        a = np.ascontiguousarray(kA_t_cov, np.float64).reshape(3)
+        b = np.ascontiguousarray(kA_tdt_cov, np.float64).reshape(3)
+        call("inqb_etrs_step", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), float(dt), dptr(a), dptr(b),
+             self._stream())
+        return psi
+
+    def density(self, psi, occ) -> torch.Tensor:
+        psi = self._check(psi)
+        occ_t = torch.as_tensor(occ, dtype=torch.float64, device=self.device).contiguous()
+        rho = torch.empty(self.N, dtype=torch.float64, device=self.device)
+        call("inqb_density", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), occ_t.data_ptr(), rho.data_ptr(),
+             self._stream())
+        return rho
+
+    def dipole(self, rho: torch.Tensor) -> np.ndarray:
+        rho = rho.contiguous()
+        out = np.zeros(3)
+        call("inqb_dipole", self._h, rho.data_ptr(), dptr(out), self._stream())
+        return out
+
+    def orthonormalize_(self, psi):
+        psi = self._check(psi)
+        call("inqb_orthonormalize", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), self._stream())
+        return psi

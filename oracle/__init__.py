@@ -1,0 +1,224 @@
+"""ORACLE — test infrastructure only.
+
+ctypes wrapper around ``oracle/liboracle.so``, the CPU FP64 restatement of INQ's
+Kohn-Sham Hamiltonian hot path (``oracle/oracle.cpp`` lists, for every routine,
+the reference file and lines it follows).  Only ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg import this
+module; the product (``inq-wannier-fork_b200``) never does.
+
+Parity: pinned against the golden values of the reference's unit tests (see
+``tests/test_oracle_golden.py``); the projector tables and the ETRS/CN steps are
+parity-unpinned conventions because the reference's own tests for them are empty
+or need the absent pseudopod library.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the committed Makefile (g++, OpenMP)."""
+    src = os.path.join(_HERE, "oracle.cpp")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_create.restype = ctypes.c_void_p
+        L.orc_create.argtypes = [_dp, _ip]
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_volume_element.restype = ctypes.c_double
+        L.orc_volume_element.argtypes = [ctypes.c_void_p]
+        L.orc_set_potential.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_set_vector_potential_cov.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_cart_to_cov.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_sphere.restype = ctypes.c_int
+        L.orc_sphere.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, _ip, _fp, _fp]
+        L.orc_gaussian_beta.argtypes = [ctypes.c_void_p, ctypes.c_int, _fp, _fp, ctypes.c_double, _dp]
+        L.orc_set_projectors.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         _ip, _ip, _fp, _dp, _dp]
+        L.orc_apply_h.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.orc_fft3d.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int, ctypes.c_int]
+        L.orc_exponential_in_place.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
+                                               ctypes.c_double, _dp, ctypes.c_int]
+        L.orc_etrs_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
+        L.orc_density.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]
+        L.orc_dipole.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_rvectors.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_orthonormalize.restype = ctypes.c_int
+        L.orc_orthonormalize.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.orc_num_threads.restype = ctypes.c_int
+        L.orc_set_num_threads.argtypes = [ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+def _f(a):
+    return a.ctypes.data_as(_fp)
+
+
+def set_num_threads(n: int) -> None:
+    lib().orc_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())
+
+
+class System:
+    """FP64 Hamiltonian state on one cell/grid (mirrors ks_hamiltonian's members)."""
+
+    def __init__(self, lattice, nr):
+        self.lattice = np.ascontiguousarray(np.asarray(lattice, dtype=np.float64).reshape(3, 3))
+        self.nr = np.ascontiguousarray(np.asarray(nr, dtype=np.int32).reshape(3))
+        self.N = int(np.prod(self.nr))
+        self._h = lib().orc_create(_d(self.lattice), _i(self.nr))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.orc_destroy(h)
+            self._h = None
+
+    @property
+    def volume_element(self) -> float:
+        return float(lib().orc_volume_element(self._h))
+
+    def set_potential(self, V):
+        V = np.ascontiguousarray(V, dtype=np.float64).reshape(self.N)
+        lib().orc_set_potential(self._h, _d(V))
+
+    def set_vector_potential_cov(self, kA):
+        kA = np.ascontiguousarray(kA, dtype=np.float64).reshape(3)
+        lib().orc_set_vector_potential_cov(self._h, _d(kA))
+
+    def cart_to_cov(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(3)
+        out = np.zeros(3)
+        lib().orc_cart_to_cov(self._h, _d(v), _d(out))
+        return out
+
+    def sphere(self, center, radius):
+        c = np.ascontiguousarray(center, dtype=np.float64).reshape(3)
+        n = lib().orc_sphere(self._h, _d(c), float(radius), None, None, None)
+        coords = np.zeros((n, 3), np.int32)
+        dist = np.zeros(n, np.float32)
+        relpos = np.zeros((n, 3), np.float32)
+        lib().orc_sphere(self._h, _d(c), float(radius), _i(coords), _f(dist), _f(relpos))
+        return coords, dist, relpos
+
+    def gaussian_beta(self, dist, relpos, sigma=1.0):
+        n = len(dist)
+        dist = np.ascontiguousarray(dist, np.float32)
+        relpos = np.ascontiguousarray(relpos, np.float32)
+        beta = np.zeros((4, n))
+        lib().orc_gaussian_beta(self._h, n, _f(dist), _f(relpos), float(sigma), _d(beta))
+        return beta
+
+    def build_gaussian_kb(self, positions, radius=3.0, sigma=1.0, ekb_s=1.5, ekb_p=-0.7):
+        """Per-atom spheres + beta tables padded to the largest sphere (projector_all layout)."""
+        spheres = [self.sphere(p, radius) for p in np.asarray(positions, float).reshape(-1, 3)]
+        nproj = len(spheres)
+        smax = max([len(s[1]) for s in spheres] + [0])
+        counts = np.array([len(s[1]) for s in spheres], np.int32)
+        coords = -np.ones((nproj, smax, 3), np.int32)
+        relpos = np.zeros((nproj, smax, 3), np.float32)
+        beta = np.zeros((nproj, 4, smax))
+        for a, (c, d, r) in enumerate(spheres):
+            n = len(d)
+            coords[a, :n] = c
+            relpos[a, :n] = r
+            beta[a, :, :n] = self.gaussian_beta(d, r, sigma)
+        coeff = np.tile(np.array([ekb_s, ekb_p, ekb_p, ekb_p]), (nproj, 1))
+        return dict(counts=counts, coords=coords, relpos=relpos, beta=beta, coeff=coeff, smax=smax, L=4)
+
+    def set_projectors(self, kb):
+        nproj = len(kb["counts"])
+        self._kb = {k: np.ascontiguousarray(v) if isinstance(v, np.ndarray) else v for k, v in kb.items()}
+        k = self._kb
+        lib().orc_set_projectors(self._h, nproj, int(k["L"]), int(k["smax"]),
+                                 _i(k["counts"].astype(np.int32)), _i(k["coords"].astype(np.int32)),
+                                 _f(k["relpos"].astype(np.float32)), _d(k["beta"].astype(np.float64)),
+                                 _d(k["coeff"].astype(np.float64)))
+
+    def _psi(self, psi):
+        psi = np.ascontiguousarray(psi, dtype=np.complex128)
+        assert psi.ndim == 2 and psi.shape[0] == self.N
+        return psi
+
+    def apply_h(self, psi):
+        psi = self._psi(psi)
+        out = np.zeros_like(psi)
+        lib().orc_apply_h(self._h, psi.shape[1], _d(psi.view(np.float64)), _d(out.view(np.float64)))
+        return out
+
+    def fft3d(self, psi, sign=-1, normalize=False):
+        psi = self._psi(psi)
+        out = np.zeros_like(psi)
+        lib().orc_fft3d(self._h, psi.shape[1], _d(psi.view(np.float64)), _d(out.view(np.float64)),
+                        int(sign), int(bool(normalize)))
+        return out
+
+    def exponential(self, factor, psi, order=4):
+        out = self._psi(psi).copy()
+        lib().orc_exponential_in_place(self._h, out.shape[1], float(np.real(factor)), float(np.imag(factor)),
+                                       _d(out.view(np.float64)), int(order))
+        return out
+
+    def etrs_step(self, psi, dt, kA_t, kA_tdt):
+        out = self._psi(psi).copy()
+        a = np.ascontiguousarray(kA_t, np.float64).reshape(3)
+        b = np.ascontiguousarray(kA_tdt, np.float64).reshape(3)
+        lib().orc_etrs_step(self._h, out.shape[1], float(dt), _d(a), _d(b), _d(out.view(np.float64)))
+        return out
+
+    def density(self, psi, occ):
+        psi = self._psi(psi)
+        occ = np.ascontiguousarray(occ, np.float64).reshape(psi.shape[1])
+        rho = np.zeros(self.N)
+        lib().orc_density(self._h, psi.shape[1], _d(psi.view(np.float64)), _d(occ), _d(rho))
+        return rho
+
+    def dipole(self, rho):
+        rho = np.ascontiguousarray(rho, np.float64).reshape(self.N)
+        out = np.zeros(3)
+        lib().orc_dipole(self._h, _d(rho), _d(out))
+        return out
+
+    def rvectors(self):
+        out = np.zeros((self.N, 3))
+        lib().orc_rvectors(self._h, _d(out))
+        return out
+
+    def orthonormalize(self, psi):
+        out = self._psi(psi).copy()
+        info = lib().orc_orthonormalize(self._h, out.shape[1], _d(out.view(np.float64)))
+        if info != 0:
+            raise ArithmeticError(f"overlap matrix not positive definite at pivot {info - 1}")
+        return out
