@@ -1,0 +1,413 @@
+#!/usr/bin/env python
+"""Benchmark of the KS-Hamiltonian hot path on B200.
+
+Workload (one "step"): H|psi> on the 64-atom diamond supercell -- cubic
+a = 20.52 bohr, 64^3 grid, 128 orbitals, 256 Gaussian KB projectors -- in mixed
+precision (complex64 FFT/pointwise, FP64 projection accumulators).  Reported
+beside it: the same apply in FP64, ETRS steps/s on the same system, and the
+error of the mixed result against the FP64 path and the CPU FP64 oracle.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun: every rank applies H to its own 128 orbitals (the
+path is independent per orbital, no data-path collective: weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "inq-wannier-fork_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "orbital H-applies/s"
+UNIT = "orbital-applies/s"
+WORKLOAD = ("64-atom diamond supercell: cubic a=20.52 bohr, 64^3 grid, 128 orbitals, 256 Gaussian KB "
+            "projectors (s+p, radius 3 bohr), Gamma point; one step = one H|psi> on all 128 orbitals")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--orbitals", type=int, default=128)
+    ap.add_argument("--etrs-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample length")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ distributed plumbing
+def dist_setup(ngpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_pg(world, local):
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180), device_id=torch.device("cuda", local))
+    return dist if world > 1 else None
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        busy = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ inputs
+def build_inputs(M, seed=0):
+    from pinq_b200 import systems
+
+    lattice = systems.cubic(20.52)
+    nr = (64, 64, 64)
+    pos = systems.diamond_positions(10.26, 2)
+    V = systems.gaussian_potential(lattice, nr, pos)
+    psi = systems.random_orbitals(lattice, nr, M, 25.0, seed)
+    return lattice, nr, pos, V, psi
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), float(d.get("bf16_tflops", 1590.0)), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of each kernel from the committed ncu summaries:
+    lines 'traffic <kernel> <bytes_per_launch>' in profiles/*.txt."""
+    out = {}
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return out
+    for f in sorted(os.listdir(pdir)):
+        if not f.endswith(".txt"):
+            continue
+        for line in open(os.path.join(pdir, f)):
+            parts = line.split()
+            if len(parts) == 3 and parts[0] == "traffic":
+                try:
+                    out[parts[1]] = float(parts[2])
+                except ValueError:
+                    pass
+    return out
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle)
+def cpu_baseline(lattice, nr, pos, V, seconds, steps=None, warmup=0):
+    """The oracle's FP64 H|psi> (C++, OpenMP over orbitals, all host threads) on a
+    bounded sample of the same workload: as many orbitals as threads."""
+    import oracle
+
+    oracle.build()
+    threads = oracle.num_threads()
+    from pinq_b200 import systems
+
+    Ms = max(1, min(128, threads))
+    psi = systems.random_orbitals(lattice, nr, Ms, 25.0, 7)
+    o = oracle.System(lattice, nr)
+    o.set_potential(V)
+    o.set_projectors(o.build_gaussian_kb(pos))
+    for _ in range(warmup):
+        o.apply_h(psi)
+    times = []
+    t_end = time.perf_counter() + seconds
+    n = 0
+    while True:
+        t0 = time.perf_counter()
+        o.apply_h(psi)
+        times.append(time.perf_counter() - t0)
+        n += 1
+        if (steps is not None and n >= steps) or (steps is None and time.perf_counter() > t_end):
+            break
+    total = sum(times)
+    return {"value": Ms * n / total, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"oracle FP64 H|psi> on {Ms} of the 128 orbitals of the same 64^3 / 64-atom system, "
+                      f"{n} applies ({total:.1f} s)"}, times
+
+
+def run_reference(args):
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return 0
+    lattice, nr, pos, V, _ = build_inputs(2, 0)
+    res, times = cpu_baseline(lattice, nr, pos, V, seconds=args.cpu_seconds, steps=args.steps,
+                              warmup=args.warmup)
+    total = sum(times)
+    line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "precision": "fp64", "sample_orbitals_per_step":
+                       int(round(res["value"] * total / len(times)))},
+            "impl": "reference", "cpu_baseline": res,
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_setup(args.gpus)
+    dist = make_pg(world, local)
+    import pinq_b200 as pb
+
+    M = args.orbitals
+    lattice, nr, pos, V, psi64 = build_inputs(M, seed=rank)
+    N = int(np.prod(nr))
+
+    h32 = pb.KSHamiltonian(lattice, nr, "mixed", device=local)
+    h64 = pb.KSHamiltonian(lattice, nr, "fp64", device=local)
+    for h in (h32, h64):
+        h.set_scalar_potential(V)
+        kb = h.set_gaussian_projectors(pos, 3.0, 1.0, 1.5, -0.7)
+        h.reserve(M)
+    nent = int(kb["counts"].sum())
+    x64 = torch.as_tensor(psi64).to("cuda")
+    x32 = x64.to(torch.complex64)
+    y32 = torch.empty_like(x32)
+    y64 = torch.empty_like(x64)
+
+    # -- error of the mixed path against the FP64 path and the oracle (first orbitals)
+    h32.apply(x32, y32)
+    h64.apply(x64, y64)
+    torch.cuda.synchronize()
+    err_fp64 = float((y32.to(torch.complex128) - y64).norm() / y64.norm())
+    err_oracle = None
+    if rank == 0:
+        import oracle
+
+        o = oracle.System(lattice, nr)
+        o.set_potential(V)
+        o.set_projectors(o.build_gaussian_kb(pos))
+        sub = np.ascontiguousarray(psi64[:, :4])
+        ref = o.apply_h(sub)
+        mixed = y32[:, :4].cpu().numpy().astype(np.complex128)
+        fp64 = y64[:, :4].cpu().numpy()
+        err_oracle = {"mixed_rel_norm": float(np.linalg.norm(mixed - ref) / np.linalg.norm(ref)),
+                      "fp64_rel_max": float(np.abs(fp64 - ref).max() / np.abs(ref).max()),
+                      "orbitals_checked": 4}
+
+    def timed(fn, K, W):
+        for _ in range(W):
+            fn()
+        barrier(dist)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(K):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        barrier(dist)
+        return max_over_ranks(dist, s.elapsed_time(e))
+
+    K, W = args.steps, max(3, args.warmup)
+    # -- headline: mixed H|psi>, device-resident inputs (268 MB > L2), live per-pass events
+    clocks = ClockSampler(local)
+    for _ in range(W):  # warm-up, untimed
+        h32.apply(x32, y32)
+    clocks.start()
+    h32.timing_start(K)  # CUDA events around the three passes of each timed apply
+    barrier(dist)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(K):
+        h32.apply(x32, y32)
+    e.record()
+    torch.cuda.synchronize()
+    barrier(dist)
+    ms = max_over_ranks(dist, s.elapsed_time(e))
+    clk = clocks.stop()
+    pass_ms, napplies = h32.timing_stop()
+
+    # -- FP64 H|psi>
+    ms64 = timed(lambda: h64.apply(x64, y64), max(3, K // 2), W)
+    k64 = max(3, K // 2)
+    # -- ETRS steps (mixed and FP64) on the same system, A_x changing every step
+    amps = np.random.default_rng(5).normal(0.0, 0.01, args.etrs_steps + W + 2)
+    xe32 = x32.clone()
+    xe64 = x64.clone()
+    cov = [h32.cart_to_cov(np.array([a, 0.0, 0.0])) for a in amps]
+    it = {"n": 0}
+
+    def etrs(h, x):
+        n = it["n"] % (len(cov) - 1)
+        h.etrs_step_(x, 0.05, cov[n], cov[n + 1])
+        it["n"] += 1
+
+    ms_etrs32 = timed(lambda: etrs(h32, xe32), args.etrs_steps, W)
+    ms_etrs64 = timed(lambda: etrs(h64, xe64), args.etrs_steps, W)
+
+    # -- e2e through the host-buffer C-ABI call (pinned host memory, copies in the timed region)
+    xh = x32.cpu().pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    Ke = max(3, K // 4)
+    for _ in range(2):
+        h32.apply_host(xh, yh)
+    barrier(dist)
+    t0 = time.perf_counter()
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record()
+    for _ in range(Ke):
+        h32.apply_host(xh, yh)
+    e2.record()
+    torch.cuda.synchronize()
+    barrier(dist)
+    ms_e2e = max_over_ranks(dist, s2.elapsed_time(e2))
+    wall_e2e = time.perf_counter() - t0
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    hbm, bf16, peak_kind = peaks()
+    b = 8  # bytes per complex64
+    bT = 4
+    L = 4
+    alg = {  # algorithmic bytes per launch
+        "plane_fwd": 2 * N * M * b + nent * (L * bT + b + 4),
+        "line_x": 2 * N * M * b,
+        "plane_inv": 3 * N * M * b + N * bT + 4 * (N + 1) + nent * (4 + 4 + L * bT + b),
+    }
+    per_launch_ms = {k: pass_ms[i] / max(1, napplies) for i, k in enumerate(["plane_fwd", "line_x", "plane_inv"])}
+    kernels = {}
+    traffic = profiled_traffic()
+    for k in alg:
+        t = per_launch_ms[k] * 1e-3
+        gbs = alg[k] / t / 1e9 if t > 0 else 0.0
+        kernels[k] = {"ms_per_launch": per_launch_ms[k], "algorithmic_bytes": alg[k], "achieved_gbs": gbs,
+                      "frac": gbs / hbm, "traffic": traffic.get(k)}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_per_launch"])
+    d = kernels[dom]
+    B_H = 2 * N * M * b + N * bT + nent * L * bT
+    apply_ms = ms / K
+    value = world * M * K / (ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": apply_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded Gaussian orbitals, Gaussian local potential and KB projectors)",
+        "config": {"workload": WORKLOAD, "precision": "mixed: complex64 FFT/pointwise, FP64 projection sums",
+                   "grid": list(nr), "orbitals_per_gpu": M, "atoms": len(pos), "projectors": 4 * len(pos),
+                   "sphere_points": nent, "l2": "inputs larger than L2 (268 MB orbital block > 126 MB L2)",
+                   "parallelism": f"orbital replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": d["achieved_gbs"], "peak": hbm, "unit": "GB/s",
+                     "frac": d["frac"], "traffic": d["traffic"], "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": d["algorithmic_bytes"]},
+        "roofline_apply": {"B_H_bytes": B_H, "achieved_gbs": B_H / (apply_ms * 1e-3) / 1e9,
+                           "frac": B_H / (apply_ms * 1e-3) / 1e9 / hbm},
+        "kernels": kernels,
+        "e2e": {"value": world * M * Ke / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": N * M * b,
+                "d2h_bytes_per_step": N * M * b, "wall_s": wall_e2e, "call": "inqb_apply_h_host"},
+        "gpu_launches": 3 * K,
+        "clocks": clk,
+        "fp64": {"value": world * M * k64 / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64 / k64,
+                 "speedup_mixed_over_fp64": (ms64 / k64) / apply_ms},
+        "etrs": {"mixed_steps_per_s": world * args.etrs_steps / (ms_etrs32 * 1e-3),
+                 "fp64_steps_per_s": world * args.etrs_steps / (ms_etrs64 * 1e-3),
+                 "H_applies_per_step": 8, "dt": 0.05},
+        "error": {"mixed_vs_fp64_gpu_rel_norm": err_fp64, "vs_oracle": err_oracle},
+    }
+    if world == 1:
+        try:
+            res, _ = cpu_baseline(lattice, nr, pos, V, seconds=args.cpu_seconds)
+            line["cpu_baseline"] = res
+        except Exception as ex:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "error": str(ex)}
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

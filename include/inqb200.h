@@ -132,6 +132,16 @@ int inqb_dipole(inqb_ctx* ctx, const double* rho, double out[3], void* stream);
  * overlap S = dV psi^H psi, Cholesky S = U^H U, psi <- psi U^-1; synchronous. */
 int inqb_orthonormalize(inqb_ctx* ctx, void* psi, int M, int ld, void* stream);
 
+/* ---------------------------------------------------------------- profiling
+ * Per-pass CUDA-event timing of the next max_applies H applications, recorded
+ * on the stream the kernels run on; the counterpart of INQ's scoped timers
+ * (CALI_CXX_MARK_SCOPE, src/utils/profiling.hpp:12, external_libs/kalimotxo/cali.h).
+ * inqb_timing_stop waits for the recorded events and returns the summed
+ * milliseconds of the three passes (plane forward + projection, x lines +
+ * kinetic, plane inverse + potential/nonlocal epilogue). */
+int inqb_timing_start(inqb_ctx* ctx, int max_applies);
+int inqb_timing_stop(inqb_ctx* ctx, double ms_per_pass[3], int* napplies);
+
 #ifdef __cplusplus
 }
 #endif

@@ -128,6 +128,10 @@ int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long l
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) a.rlat[i][j] = ctx->cell.rlat[i][j];
   ctx->cell.cov_to_cart(ctx->kA_cov, a.kA_cart);
+  if (ctx->timing_on && mode == LaunchArgs::H && ctx->timing_count < ctx->timing_capacity) {
+    for (int i = 0; i < 4; i++) a.events[i] = ctx->timing_events[4 * ctx->timing_count + i];
+    ctx->timing_count++;
+  }
   ProjView<double> v64;
   ProjView<float> v32;
   if (ctx->precision == INQB_FP64) {
@@ -257,7 +261,42 @@ int inqb_ctx_destroy(inqb_ctx* ctx) {
   if (!ctx) return INQB_OK;
   DeviceGuard guard(ctx->device);
   cudaDeviceSynchronize();
+  for (cudaEvent_t e : ctx->timing_events) cudaEventDestroy(e);
   delete ctx;
+  return INQB_OK;
+}
+
+int inqb_timing_start(inqb_ctx* ctx, int max_applies) {
+  INQB_CHECK_CTX(ctx);
+  INQB_GUARD(ctx);
+  if (max_applies <= 0) return fail(INQB_ERR_INVALID, "max_applies must be positive");
+  while ((int)ctx->timing_events.size() < 4 * max_applies) {
+    cudaEvent_t e;
+    INQB_CUDA_TRY(cudaEventCreate(&e));
+    ctx->timing_events.push_back(e);
+  }
+  ctx->timing_capacity = max_applies;
+  ctx->timing_count = 0;
+  ctx->timing_on = true;
+  return INQB_OK;
+}
+
+int inqb_timing_stop(inqb_ctx* ctx, double ms_per_pass[3], int* napplies) {
+  INQB_CHECK_CTX(ctx);
+  INQB_GUARD(ctx);
+  if (!ms_per_pass || !napplies) return fail(INQB_ERR_INVALID, "null output");
+  ctx->timing_on = false;
+  for (int k = 0; k < 3; k++) ms_per_pass[k] = 0.0;
+  *napplies = ctx->timing_count;
+  for (int i = 0; i < ctx->timing_count; i++) {
+    INQB_CUDA_TRY(cudaEventSynchronize(ctx->timing_events[4 * i + 3]));
+    for (int k = 0; k < 3; k++) {
+      float ms = 0.f;
+      INQB_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->timing_events[4 * i + k], ctx->timing_events[4 * i + k + 1]));
+      ms_per_pass[k] += ms;
+    }
+  }
+  ctx->timing_count = 0;
   return INQB_OK;
 }
 

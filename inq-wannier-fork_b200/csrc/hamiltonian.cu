@@ -493,10 +493,13 @@ static int launch_h_impl(const LaunchArgs& a) {
   if (a.mode == LaunchArgs::H) {
     if (pj.nproj > 0)
       INQB_CUDA_TRY(cudaMemsetAsync(pj.proj, 0, sizeof(double2) * (size_t)pj.nproj * pj.L * a.M, st));
+    if (a.events[0]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[0], st));
     k_plane_fwd<T, NY, NZ, G><<<gplane, kThreads, K::plane_smem, st>>>(
         (const cplx<T>*)a.in, a.ld_in, a.M, tmp, NX, twy, twz, pj, 1);
+    if (a.events[1]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[1], st));
     k_line_x<T, NX, G, K::CX, 0><<<gline, kThreads, K::line_smem, st>>>(tmp, nullptr, nullptr, 0, a.M, NY, NZ,
                                                                         twx, kp);
+    if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
     EpiParams<T> ep;
     ep.V = (const T*)a.V;
     ep.base = (const cplx<T>*)a.base;
@@ -505,6 +508,7 @@ static int launch_h_impl(const LaunchArgs& a) {
     ep.beta = mk<T>((T)a.beta[0], (T)a.beta[1]);
     k_plane_inv<T, NY, NZ, G, 1><<<gplane, kThreads, K::plane_smem, st>>>(
         tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, NX, twy, twz, pj, ep);
+    if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
   } else if (a.mode == LaunchArgs::FFT_FWD) {
     k_plane_fwd<T, NY, NZ, G><<<gplane, kThreads, K::plane_smem, st>>>(
         (const cplx<T>*)a.in, a.ld_in, a.M, tmp, NX, twy, twz, pj, 0);

@@ -131,4 +131,9 @@ struct inqb_ctx {
   inqb::DevBuf d_work2;
   inqb::DevBuf d_red;     // small reduction buffers
   size_t elem_bytes() const { return precision == INQB_FP64 ? 16 : 8; }
+
+  // optional per-pass CUDA-event timing of H applications
+  std::vector<cudaEvent_t> timing_events;  // 4 per recorded application
+  int timing_capacity = 0, timing_count = 0;
+  bool timing_on = false;
 };

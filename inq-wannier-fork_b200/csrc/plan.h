@@ -22,6 +22,7 @@ struct LaunchArgs {
   double alpha[2] = {1.0, 0.0};
   double beta[2] = {0.0, 0.0};
   void* stream = nullptr;
+  void* events[4] = {nullptr, nullptr, nullptr, nullptr};  // optional cudaEvent_t around the passes
 };
 
 struct Plan {

@@ -232,6 +232,17 @@ class KSHamiltonian:
         call("inqb_dipole", self._h, rho.data_ptr(), dptr(out), self._stream())
         return out
 
+    def timing_start(self, max_applies: int):
+        """Record CUDA events around the three passes of the next max_applies H applies."""
+        call("inqb_timing_start", self._h, int(max_applies))
+
+    def timing_stop(self):
+        """(summed ms of [plane_fwd, line_x, plane_inv], number of timed applies)."""
+        ms = np.zeros(3)
+        n = ctypes.c_int(0)
+        call("inqb_timing_stop", self._h, dptr(ms), ctypes.byref(n))
+        return ms, n.value
+
     def orthonormalize_(self, psi):
         psi = self._check(psi)
         call("inqb_orthonormalize", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), self._stream())

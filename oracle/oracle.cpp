@@ -214,7 +214,8 @@ struct Plan1D {
     for (int i = 0; i < len; i++) y[i] = tmp[i];
   }
   void exec(const cd *x, long xs, cd *y, int sign) const {
-    std::vector<cd> tmp(n);
+    thread_local std::vector<cd> tmp;
+    if ((int)tmp.size() < n) tmp.resize(n);
     rec(x, xs, y, n, 0, sign, tmp.data());
   }
 };
