@@ -43,17 +43,45 @@ struct Split;
 INQB_FFT_SIZES(INQB_SPLIT)
 #undef INQB_SPLIT
 
-template <int N>
-using PadAxis = Axis<Split<N>::N1, Split<N>::N2>;  // contiguous (z or x) axis
-template <int N>
-using RowAxis = Axis<Split<N>::N1, Split<N>::N2, 0>;  // strided (y) axis
+// Line split per precision: FP32 lines up to 64 points and FP64 lines up to 32
+// points are transformed by one thread in registers (N2 = 1); longer lines use
+// the four-step team split of the size table.
+template <typename T, int N>
+struct LineSplit {
+  static constexpr bool single = (sizeof(T) == 4 && N <= 64) || (sizeof(T) == 8 && N <= 32);
+  static constexpr int N1 = single ? N : Split<N>::N1;
+  static constexpr int N2 = single ? 1 : Split<N>::N2;
+};
+template <typename T, int N>
+using PadAxis = Axis<LineSplit<T, N>::N1, LineSplit<T, N>::N2>;  // contiguous (z or x) axis
+template <typename T, int N>
+using RowAxis = Axis<LineSplit<T, N>::N1, LineSplit<T, N>::N2, 0>;  // strided (y) axis
 
-// Orbitals per plane tile: largest power of two <= 8 whose tile fits ~76 KB.
+// Geometry of a plane tile: G orbitals x NY rows x ZP z-slots.  Single-thread z
+// lines get an odd row stride (conflict-free row walks); team lines keep the
+// padded-slot layout whose row stride is 8 mod 16.
 template <typename T, int NY, int NZ>
-constexpr int plane_group() {
-  constexpr int bytes1 = NY * PadAxis<NZ>::SLOTS * (int)sizeof(cplx<T>);
-  return (bytes1 * 8 <= 77824) ? 8 : (bytes1 * 4 <= 77824) ? 4 : (bytes1 * 2 <= 77824) ? 2 : 1;
-}
+struct PlaneGeom {
+  using AY = RowAxis<T, NY>;
+  using AZ = PadAxis<T, NZ>;
+  static constexpr int ZP = (AZ::N2 == 1) ? (NZ % 2 == 0 ? NZ + 1 : NZ) : AZ::SLOTS;
+  static constexpr int PLANE = NY * ZP;
+  static constexpr int BYTES1 = PLANE * (int)sizeof(cplx<T>);
+  static constexpr int G = (BYTES1 * 8 <= 77824) ? 8 : (BYTES1 * 4 <= 77824) ? 4 : (BYTES1 * 2 <= 77824) ? 2 : 1;
+  static constexpr int LINES = G * (NY > NZ ? NY : NZ);
+  static constexpr int THREADS =
+      (AZ::N2 == 1 && AY::N2 == 1) ? (LINES < 64 ? 64 : LINES > 512 ? 512 : ((LINES + 31) / 32) * 32) : 256;
+  static constexpr size_t SMEM = sizeof(cplx<T>) * ((size_t)G * PLANE + NY + NZ);
+};
+
+// x-line tile: C columns x NX x G orbitals; column stride CS = G (mod 16) words.
+template <typename T, int NX>
+struct LineGeom {
+  using AX = Axis<Split<NX>::N1, Split<NX>::N2>;  // team split: 256 short-register threads
+  static constexpr int XP = AX::SLOTS;
+  template <int G>
+  static constexpr int cs() { return XP * G + ((XP % 2 == 0) ? G : 0); }
+};
 
 // ---------------------------------------------------------------- kernel params
 template <typename T>
@@ -81,12 +109,48 @@ struct EpiParams {
   cplx<T> alpha, beta;      // out = alpha * H in + beta * base
 };
 
+// G consecutive complex values of one grid point: 16-byte vector accesses when
+// the caller proved alignment (vec), element accesses otherwise.
+template <typename T, int G>
+__device__ __forceinline__ void load_group(const cplx<T>* __restrict__ src, cplx<T> (&v)[G], int gcount, bool vec) {
+  constexpr int PER16 = 16 / (int)sizeof(cplx<T>);  // complex values per 16 bytes
+  if (vec && G % PER16 == 0) {
+#pragma unroll
+    for (int k = 0; k < G / PER16; ++k) {
+      const float4 w = reinterpret_cast<const float4*>(src)[k];
+      memcpy(&v[k * PER16], &w, 16);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < G; ++j) v[j] = (j < gcount) ? src[j] : mk<T>(0, 0);
+  }
+}
+
+template <typename T, int G>
+__device__ __forceinline__ void store_group(cplx<T>* __restrict__ dst, const cplx<T> (&v)[G], int gcount, bool vec) {
+  constexpr int PER16 = 16 / (int)sizeof(cplx<T>);
+  if (vec && G % PER16 == 0) {
+#pragma unroll
+    for (int k = 0; k < G / PER16; ++k) {
+      float4 w;
+      memcpy(&w, &v[k * PER16], 16);
+      reinterpret_cast<float4*>(dst)[k] = w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < G; ++j)
+      if (j < gcount) dst[j] = v[j];
+  }
+}
+
 // ---------------------------------------------------------------- projection (pass 1)
 // Sum over the sphere entries of plane ix:  proj[a][l][m] += scale[a][l] *
 // sum_e beta_e[l] exp(+i (k+A).r_e) psi(r_e)[m]   (projector_all.hpp:104-165).
-template <typename T, int G, int ZP, int PLANE, typename AZ>
-__device__ __forceinline__ void project_plane(const cplx<T>* S, int NZ, int ix, int m0, int gcount, int M,
+template <typename T, int G, typename PG>
+__device__ __forceinline__ void project_plane(const cplx<T>* S, int ix, int m0, int gcount, int M,
                                               const ProjView<T>& pj) {
+  using AZ = typename PG::AZ;
+  constexpr int NZ = AZ::N;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int s0 = pj.seg_ptr[ix], s1 = pj.seg_ptr[ix + 1];
   const cplx<T>* phase = (const cplx<T>*)pj.ent_phase;
@@ -100,14 +164,14 @@ __device__ __forceinline__ void project_plane(const cplx<T>* S, int NZ, int ix, 
       for (int j = 0; j < G; ++j) acc[l][j] = mk<T>(0, 0);
     for (int e = e0 + lane; e < e1; e += 32) {
       const int off = pj.ent_off[e];
-      const int sl = (off / NZ) * ZP + AZ::slot(off % NZ);
+      const int sl = (off / NZ) * PG::ZP + AZ::slot(off % NZ);
       const cplx<T> ph = phase[e];
       T b[LMAX];
 #pragma unroll
       for (int l = 0; l < LMAX; ++l) b[l] = (l < pj.L) ? pj.ent_beta[(long)e * pj.L + l] : (T)0;
 #pragma unroll
       for (int j = 0; j < G; ++j) {
-        cplx<T> x = ph * S[j * PLANE + sl];
+        cplx<T> x = ph * S[j * PG::PLANE + sl];
 #pragma unroll
         for (int l = 0; l < LMAX; ++l) {
           acc[l][j].x = fma(b[l], x.x, acc[l][j].x);
@@ -138,40 +202,105 @@ __device__ __forceinline__ void project_plane(const cplx<T>* S, int NZ, int ix, 
   }
 }
 
+// Nonlocal scatter of plane ix into the real-space tile (pass 3):
+// S(r_e) += conj(exp(i (k+A).r_e)) sum_l beta_e[l] proj[a][l][m]
+// (projector_all.hpp:182-232).  One warp per atom segment; the atom's
+// projections are read once; shared-memory atomics merge overlapping spheres.
+template <typename T, int G, typename PG>
+__device__ __forceinline__ void nonlocal_plane(cplx<T>* S, int ix, int m0, int gcount, int M,
+                                               const ProjView<T>& pj) {
+  using AY = typename PG::AY;
+  using AZ = typename PG::AZ;
+  constexpr int NZ = AZ::N;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int s0 = pj.seg_ptr[ix], s1 = pj.seg_ptr[ix + 1];
+  const cplx<T>* phase = (const cplx<T>*)pj.ent_phase;
+  for (int s = s0 + warp; s < s1; s += nw) {
+    const int a = pj.seg_atom[s];
+    const int e0 = pj.seg_ent[s], e1 = pj.seg_ent[s + 1];
+    cplx<T> P[LMAX][G];
+#pragma unroll
+    for (int l = 0; l < LMAX; ++l)
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        P[l][j] = mk<T>(0, 0);
+        if (l < pj.L && j < gcount) {
+          const double2 pr = pj.proj[((long)a * pj.L + l) * M + m0 + j];
+          P[l][j] = mk<T>((T)pr.x, (T)pr.y);
+        }
+      }
+    for (int e = e0 + lane; e < e1; e += 32) {
+      const int off = pj.ent_off[e];
+      const int iy = off / NZ, iz = off - iy * NZ;
+      const int sl = AY::slot_of_freq(iy) * PG::ZP + AZ::slot_of_freq(iz);
+      const cplx<T> ph = phase[e];
+      T b[LMAX];
+#pragma unroll
+      for (int l = 0; l < LMAX; ++l) b[l] = (l < pj.L) ? pj.ent_beta[(long)e * pj.L + l] : (T)0;
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        cplx<T> t = mk<T>(0, 0);
+#pragma unroll
+        for (int l = 0; l < LMAX; ++l) {
+          t.x = fma(b[l], P[l][j].x, t.x);
+          t.y = fma(b[l], P[l][j].y, t.y);
+        }
+        const cplx<T> c = mul_conj(t, ph);
+        atomicAdd(&S[j * PG::PLANE + sl].x, c.x);
+        atomicAdd(&S[j * PG::PLANE + sl].y, c.y);
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------- pass 1: plane forward
-// MODE_H: H apply (projection on); MODE_FFT: plain forward FFT.
-template <typename T, int NY, int NZ, int G>
-__global__ void __launch_bounds__(kThreads) k_plane_fwd(const cplx<T>* __restrict__ in, long ld, int M,
-                                                        cplx<T>* __restrict__ tmp, int nx,
-                                                        const cplx<T>* __restrict__ tw_y,
-                                                        const cplx<T>* __restrict__ tw_z, ProjView<T> pj,
-                                                        int do_proj) {
-  using AY = RowAxis<NY>;
-  using AZ = PadAxis<NZ>;
-  constexpr int ZP = AZ::SLOTS;
-  constexpr int PLANE = NY * ZP;
+// do_proj = 1: H apply (projection on); 0: plain forward FFT.
+template <typename T, int NY, int NZ>
+__global__ void __launch_bounds__(PlaneGeom<T, NY, NZ>::THREADS)
+    k_plane_fwd(const cplx<T>* __restrict__ in, long ld, int M, cplx<T>* __restrict__ tmp, int nx,
+                const cplx<T>* __restrict__ tw_y, const cplx<T>* __restrict__ tw_z, ProjView<T> pj, int do_proj,
+                int vec) {
+  using PG = PlaneGeom<T, NY, NZ>;
+  using AY = typename PG::AY;
+  using AZ = typename PG::AZ;
+  constexpr int G = PG::G, ZP = PG::ZP, PLANE = PG::PLANE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* twy = S + G * PLANE;
   cplx<T>* twz = twy + NY;
 
-  const int ix = blockIdx.x, grp = blockIdx.y;
+  // orbital group fastest: the CTAs of one plane run together and share the
+  // plane's projector tables and the 32-byte sectors of psi in L2
+  const int grp = blockIdx.x, ix = blockIdx.y;
   const int m0 = grp * G;
   const int gcount = min(G, M - m0);
+  const bool v = vec && gcount == G;
   for (int i = threadIdx.x; i < NY; i += blockDim.x) twy[i] = tw_y[i];
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = tw_z[i];
 
   const long pbase = (long)ix * NY * NZ;
-  for (int q = threadIdx.x; q < NY * NZ; q += blockDim.x) {
-    const int iy = q / NZ, iz = q - iy * NZ;
-    const cplx<T>* src = in + (pbase + q) * ld + m0;
-    const int sl = iy * ZP + AZ::slot(iz);
+  constexpr int B = 8;  // points per batch of independent loads
+  for (int q0 = threadIdx.x; q0 < NY * NZ; q0 += B * blockDim.x) {
+    cplx<T> vals[B][G];
 #pragma unroll
-    for (int j = 0; j < G; ++j) S[j * PLANE + sl] = (j < gcount) ? src[j] : mk<T>(0, 0);
+    for (int b = 0; b < B; ++b) {
+      const int q = q0 + b * blockDim.x;
+      if (q < NY * NZ) load_group<T, G>(in + (pbase + q) * ld + m0, vals[b], gcount, v);
+    }
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      const int q = q0 + b * blockDim.x;
+      if (q < NY * NZ) {
+        const int iy = q / NZ, iz = q - iy * NZ;
+        const int sl = iy * ZP + AZ::slot(iz);
+#pragma unroll
+        for (int j = 0; j < G; ++j) S[j * PLANE + sl] = vals[b][j];
+      }
+    }
   }
   __syncthreads();
   if (do_proj && pj.nproj > 0) {
-    project_plane<T, G, ZP, PLANE, AZ>(S, NZ, ix, m0, gcount, M, pj);
+    project_plane<T, G, PG>(S, ix, m0, gcount, M, pj);
     __syncthreads();
   }
   // z lines: (j, iy), contiguous
@@ -181,12 +310,14 @@ __global__ void __launch_bounds__(kThreads) k_plane_fwd(const cplx<T>* __restric
     es = 1;
   });
   __syncthreads();
-  step2<AZ, false>(S, G * NY * AZ::N1, [](int it, int& base, int& es, int& k1) {
-    k1 = it % AZ::N1;
-    base = (it / AZ::N1) * ZP;
-    es = 1;
-  });
-  __syncthreads();
+  if (AZ::N2 > 1) {
+    step2<AZ, false>(S, G * NY * AZ::N1, [](int it, int& base, int& es, int& k1) {
+      k1 = it % AZ::N1;
+      base = (it / AZ::N1) * ZP;
+      es = 1;
+    });
+    __syncthreads();
+  }
   // y lines: (j, iz), stride ZP; threads run along z
   step1<AY, false>(S, G * NZ * AY::N2, twy, [](int it, int& base, int& es, int& j2) {
     const int iz = it % NZ, r = it / NZ;
@@ -195,21 +326,24 @@ __global__ void __launch_bounds__(kThreads) k_plane_fwd(const cplx<T>* __restric
     es = ZP;
   });
   __syncthreads();
-  step2<AY, false>(S, G * NZ * AY::N1, [](int it, int& base, int& es, int& k1) {
-    const int iz = it % NZ, r = it / NZ;
-    k1 = r % AY::N1;
-    base = (r / AY::N1) * PLANE + AZ::slot(iz);
-    es = ZP;
-  });
-  __syncthreads();
+  if (AY::N2 > 1) {
+    step2<AY, false>(S, G * NZ * AY::N1, [](int it, int& base, int& es, int& k1) {
+      const int iz = it % NZ, r = it / NZ;
+      k1 = r % AY::N1;
+      base = (r / AY::N1) * PLANE + AZ::slot(iz);
+      es = ZP;
+    });
+    __syncthreads();
+  }
   // store natural (ky, kz) to tmp[grp][yz][ix][j]
   const long NYZ = (long)NY * NZ;
   for (int q = threadIdx.x; q < NY * NZ; q += blockDim.x) {
     const int ky = q / NZ, kz = q - ky * NZ;
     const int sl = AY::slot_of_freq(ky) * ZP + AZ::slot_of_freq(kz);
-    cplx<T>* dst = tmp + (((long)grp * NYZ + q) * nx + ix) * G;
+    cplx<T> vals[G];
 #pragma unroll
-    for (int j = 0; j < G; ++j) dst[j] = S[j * PLANE + sl];
+    for (int j = 0; j < G; ++j) vals[j] = S[j * PLANE + sl];
+    store_group<T, G>(tmp + (((long)grp * NYZ + q) * nx + ix) * G, vals, G, vec);
   }
 }
 
@@ -220,10 +354,10 @@ __global__ void __launch_bounds__(kThreads) k_plane_fwd(const cplx<T>* __restric
 template <typename T, int NX, int G, int C, int MODE>
 __global__ void __launch_bounds__(kThreads) k_line_x(cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ ext_in,
                                                      cplx<T>* __restrict__ ext_out, long ld, int M, int ny, int nz,
-                                                     const cplx<T>* __restrict__ tw_x, KinParams<T> kp) {
-  using AX = PadAxis<NX>;
-  constexpr int XP = AX::SLOTS;
-  constexpr int CS = XP * G;
+                                                     const cplx<T>* __restrict__ tw_x, KinParams<T> kp, int vec) {
+  using LG = LineGeom<T, NX>;
+  using AX = typename LG::AX;
+  constexpr int CS = LG::template cs<G>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* twx = S + C * CS;
@@ -238,18 +372,48 @@ __global__ void __launch_bounds__(kThreads) k_line_x(cplx<T>* __restrict__ tmp, 
 
   // load
   if (MODE == 2) {
+    const bool v = vec && gcount == G;
     for (int q = threadIdx.x; q < C * NX; q += blockDim.x) {
       const int c = q % C, x = q / C;  // consecutive threads: consecutive yz
-      const cplx<T>* src = ext_in + ((long)x * NYZ + yz0 + c) * ld + m0;
+      cplx<T> vals[G];
+      if (c < ncol) {
+        load_group<T, G>(ext_in + ((long)x * NYZ + yz0 + c) * ld + m0, vals, gcount, v);
+      } else {
 #pragma unroll
-      for (int j = 0; j < G; ++j)
-        S[c * CS + AX::slot(x) * G + j] = (c < ncol && j < gcount) ? src[j] : mk<T>(0, 0);
+        for (int j = 0; j < G; ++j) vals[j] = mk<T>(0, 0);
+      }
+#pragma unroll
+      for (int j = 0; j < G; ++j) S[c * CS + AX::slot(x) * G + j] = vals[j];
     }
   } else {
+    // contiguous [C][NX][G] block of tmp: 16-byte loads, batched
     const cplx<T>* src = tmp + ((long)grp * NYZ + yz0) * NX * G;
-    for (int q = threadIdx.x; q < C * NX * G; q += blockDim.x) {
-      const int j = q % G, r = q / G, x = r % NX, c = r / NX;
-      S[c * CS + AX::slot(x) * G + j] = (c < ncol) ? src[q] : mk<T>(0, 0);
+    constexpr int P = 16 / (int)sizeof(cplx<T>);  // complex values per 16 bytes
+    constexpr int NV = C * NX * G / P;
+    static_assert((C * NX * G) % P == 0, "tile not a whole number of 16-byte vectors");
+    const int nv = ncol * NX * G / P;
+    constexpr int B = 4;
+    for (int q0 = threadIdx.x; q0 < NV; q0 += B * blockDim.x) {
+      float4 w[B];
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const int q = q0 + b * blockDim.x;
+        w[b] = (q < nv) ? reinterpret_cast<const float4*>(src)[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const int q = q0 + b * blockDim.x;
+        if (q < NV) {
+          cplx<T> vals[P];
+          memcpy(vals, &w[b], 16);
+#pragma unroll
+          for (int k = 0; k < P; ++k) {
+            const int e = q * P + k;
+            const int j = e % G, r = e / G, x = r % NX, c = r / NX;
+            S[c * CS + AX::slot(x) * G + j] = vals[k];
+          }
+        }
+      }
     }
   }
   __syncthreads();
@@ -268,39 +432,81 @@ __global__ void __launch_bounds__(kThreads) k_line_x(cplx<T>* __restrict__ tmp, 
   };
 
   if (MODE == 0) {
-    step1<AX, false>(S, C * G * AX::N2, twx, map1);
-    __syncthreads();
-    step2_fwd_op_inv<AX>(S, C * G * AX::N1, twx, map2, [&](int it, int kx, cplx<T> v) {
-      const int c = (it / G) / AX::N1;
-      const int yz = yz0 + c;
-      const int ky = yz / nz, kz = yz - ky * nz;
-      const T k = kinetic(kp, sym_freq(kx, NX), sym_freq(ky, ny), sym_freq(kz, nz));
-      return k * v;
-    });
-    __syncthreads();
-    step1_inv_transposed<AX>(S, C * G * AX::N2, map1);
+    if (AX::N2 == 1) {
+      // whole line in registers: forward, kinetic, inverse
+      for (int it = threadIdx.x; it < C * G; it += blockDim.x) {
+        const int j = it % G, c = it / G;
+        const int yz = yz0 + c;
+        const int ky = sym_freq(yz / nz, ny), kz = sym_freq(yz % nz, nz);
+        T gp[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) gp[d] = (T)ky * kp.b[1][d] + (T)kz * kp.b[2][d] + kp.kA[d];
+        cplx<T> v[NX];
+        const int base = c * CS + j;
+#pragma unroll
+        for (int x = 0; x < NX; ++x) v[x] = S[base + x * G];
+        DFT<NX, false, T>::run(v);
+#pragma unroll
+        for (int x = 0; x < NX; ++x) {
+          const T kx = (T)sym_freq(x, NX);
+          const T g0 = kx * kp.b[0][0] + gp[0], g1 = kx * kp.b[0][1] + gp[1], g2 = kx * kp.b[0][2] + gp[2];
+          v[x] = ((T)0.5 * kp.scale * (g0 * g0 + g1 * g1 + g2 * g2)) * v[x];
+        }
+        DFT<NX, true, T>::run(v);
+#pragma unroll
+        for (int x = 0; x < NX; ++x) S[base + x * G] = v[x];
+      }
+    } else {
+      step1<AX, false>(S, C * G * AX::N2, twx, map1);
+      __syncthreads();
+      step2_fwd_op_inv<AX>(S, C * G * AX::N1, twx, map2, [&](int it, int kx, cplx<T> v) {
+        const int c = (it / G) / AX::N1;
+        const int yz = yz0 + c;
+        const int ky = yz / nz, kz = yz - ky * nz;
+        const T k = kinetic(kp, sym_freq(kx, NX), sym_freq(ky, ny), sym_freq(kz, nz));
+        return k * v;
+      });
+      __syncthreads();
+      step1_inv_transposed<AX>(S, C * G * AX::N2, map1);
+    }
     __syncthreads();
     cplx<T>* dst = tmp + ((long)grp * NYZ + yz0) * NX * G;
-    for (int q = threadIdx.x; q < ncol * NX * G; q += blockDim.x) {
-      const int j = q % G, r = q / G, x = r % NX, c = r / NX;
-      dst[q] = S[c * CS + AX::slot(x) * G + j];
+    constexpr int P = 16 / (int)sizeof(cplx<T>);
+    const int nv = ncol * NX * G / P;
+    for (int q = threadIdx.x; q < nv; q += blockDim.x) {
+      cplx<T> vals[P];
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        const int e = q * P + k;
+        const int j = e % G, r = e / G, x = r % NX, c = r / NX;
+        vals[k] = S[c * CS + AX::slot(x) * G + j];
+      }
+      float4 w;
+      memcpy(&w, vals, 16);
+      reinterpret_cast<float4*>(dst)[q] = w;
     }
   } else if (MODE == 1) {
     step1<AX, false>(S, C * G * AX::N2, twx, map1);
     __syncthreads();
-    step2<AX, false>(S, C * G * AX::N1, map2);
-    __syncthreads();
+    if (AX::N2 > 1) {
+      step2<AX, false>(S, C * G * AX::N1, map2);
+      __syncthreads();
+    }
     for (int q = threadIdx.x; q < C * NX; q += blockDim.x) {
       const int c = q % C, kx = q / C;
       if (c >= ncol) continue;
-      cplx<T>* dst = ext_out + ((long)kx * NYZ + yz0 + c) * ld + m0;
-      for (int j = 0; j < gcount; ++j) dst[j] = S[c * CS + AX::slot_of_freq(kx) * G + j];
+      cplx<T> vals[G];
+#pragma unroll
+      for (int j = 0; j < G; ++j) vals[j] = S[c * CS + AX::slot_of_freq(kx) * G + j];
+      store_group<T, G>(ext_out + ((long)kx * NYZ + yz0 + c) * ld + m0, vals, gcount, vec && gcount == G);
     }
   } else {
     step1<AX, true>(S, C * G * AX::N2, twx, map1);
     __syncthreads();
-    step2<AX, true>(S, C * G * AX::N1, map2);
-    __syncthreads();
+    if (AX::N2 > 1) {
+      step2<AX, true>(S, C * G * AX::N1, map2);
+      __syncthreads();
+    }
     cplx<T>* dst = tmp + ((long)grp * NYZ + yz0) * NX * G;
     for (int q = threadIdx.x; q < ncol * NX * G; q += blockDim.x) {
       const int j = q % G, r = q / G, x = r % NX, c = r / NX;
@@ -311,35 +517,46 @@ __global__ void __launch_bounds__(kThreads) k_line_x(cplx<T>* __restrict__ tmp, 
 
 // ---------------------------------------------------------------- pass 3: plane inverse + epilogue
 // MODE_H = 1: H epilogue; 0: plain copy (to_real).
-template <typename T, int NY, int NZ, int G, int MODE_H>
-__global__ void __launch_bounds__(kThreads) k_plane_inv(const cplx<T>* __restrict__ tmp,
-                                                        const cplx<T>* __restrict__ in, long ld_in,
-                                                        cplx<T>* __restrict__ out, long ld_out, int M, int nx,
-                                                        const cplx<T>* __restrict__ tw_y,
-                                                        const cplx<T>* __restrict__ tw_z, ProjView<T> pj,
-                                                        EpiParams<T> ep) {
-  using AY = RowAxis<NY>;
-  using AZ = PadAxis<NZ>;
-  constexpr int ZP = AZ::SLOTS;
-  constexpr int PLANE = NY * ZP;
+template <typename T, int NY, int NZ, int MODE_H>
+__global__ void __launch_bounds__(PlaneGeom<T, NY, NZ>::THREADS)
+    k_plane_inv(const cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ in, long ld_in,
+                cplx<T>* __restrict__ out, long ld_out, int M, int nx, const cplx<T>* __restrict__ tw_y,
+                const cplx<T>* __restrict__ tw_z, ProjView<T> pj, EpiParams<T> ep, int vec) {
+  using PG = PlaneGeom<T, NY, NZ>;
+  using AY = typename PG::AY;
+  using AZ = typename PG::AZ;
+  constexpr int G = PG::G, ZP = PG::ZP, PLANE = PG::PLANE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* twy = S + G * PLANE;
   cplx<T>* twz = twy + NY;
 
-  const int ix = blockIdx.x, grp = blockIdx.y;
+  const int grp = blockIdx.x, ix = blockIdx.y;
   const int m0 = grp * G;
   const int gcount = min(G, M - m0);
+  const bool v = vec && gcount == G;
   for (int i = threadIdx.x; i < NY; i += blockDim.x) twy[i] = tw_y[i];
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = tw_z[i];
 
   const long NYZ = (long)NY * NZ;
-  for (int q = threadIdx.x; q < NY * NZ; q += blockDim.x) {
-    const int iy = q / NZ, iz = q - iy * NZ;
-    const cplx<T>* src = tmp + (((long)grp * NYZ + q) * nx + ix) * G;
-    const int sl = iy * ZP + AZ::slot(iz);
+  constexpr int B = 8;  // points per batch of independent loads
+  for (int q0 = threadIdx.x; q0 < NY * NZ; q0 += B * blockDim.x) {
+    cplx<T> vals[B][G];
 #pragma unroll
-    for (int j = 0; j < G; ++j) S[j * PLANE + sl] = src[j];
+    for (int b = 0; b < B; ++b) {
+      const int q = q0 + b * blockDim.x;
+      if (q < NY * NZ) load_group<T, G>(tmp + (((long)grp * NYZ + q) * nx + ix) * G, vals[b], G, vec);
+    }
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      const int q = q0 + b * blockDim.x;
+      if (q < NY * NZ) {
+        const int iy = q / NZ, iz = q - iy * NZ;
+        const int sl = iy * ZP + AZ::slot(iz);
+#pragma unroll
+        for (int j = 0; j < G; ++j) S[j * PLANE + sl] = vals[b][j];
+      }
+    }
   }
   __syncthreads();
   step1<AY, true>(S, G * NZ * AY::N2, twy, [](int it, int& base, int& es, int& j2) {
@@ -349,83 +566,71 @@ __global__ void __launch_bounds__(kThreads) k_plane_inv(const cplx<T>* __restric
     es = ZP;
   });
   __syncthreads();
-  step2<AY, true>(S, G * NZ * AY::N1, [](int it, int& base, int& es, int& k1) {
-    const int iz = it % NZ, r = it / NZ;
-    k1 = r % AY::N1;
-    base = (r / AY::N1) * PLANE + AZ::slot(iz);
-    es = ZP;
-  });
-  __syncthreads();
+  if (AY::N2 > 1) {
+    step2<AY, true>(S, G * NZ * AY::N1, [](int it, int& base, int& es, int& k1) {
+      const int iz = it % NZ, r = it / NZ;
+      k1 = r % AY::N1;
+      base = (r / AY::N1) * PLANE + AZ::slot(iz);
+      es = ZP;
+    });
+    __syncthreads();
+  }
   step1<AZ, true>(S, G * NY * AZ::N2, twz, [](int it, int& base, int& es, int& j2) {
     j2 = it % AZ::N2;
     base = (it / AZ::N2) * ZP;
     es = 1;
   });
   __syncthreads();
-  step2<AZ, true>(S, G * NY * AZ::N1, [](int it, int& base, int& es, int& k1) {
-    k1 = it % AZ::N1;
-    base = (it / AZ::N1) * ZP;
-    es = 1;
-  });
-  __syncthreads();
+  if (AZ::N2 > 1) {
+    step2<AZ, true>(S, G * NY * AZ::N1, [](int it, int& base, int& es, int& k1) {
+      k1 = it % AZ::N1;
+      base = (it / AZ::N1) * ZP;
+      es = 1;
+    });
+    __syncthreads();
+  }
+  if (MODE_H && pj.nproj > 0) {
+    nonlocal_plane<T, G, PG>(S, ix, m0, gcount, M, pj);
+    __syncthreads();
+  }
 
   const long pbase = (long)ix * NYZ;
-  const cplx<T>* phase = (const cplx<T>*)pj.ent_phase;
-  for (int q = threadIdx.x; q < NY * NZ; q += blockDim.x) {
-    const int iy = q / NZ, iz = q - iy * NZ;
-    const int sl = AY::slot_of_freq(iy) * ZP + AZ::slot_of_freq(iz);
-    const long p = pbase + q;
-    cplx<T> h[G];
-#pragma unroll
-    for (int j = 0; j < G; ++j) h[j] = S[j * PLANE + sl];
+  constexpr int BE = 4;  // points per batch in the epilogue
+  for (int q0 = threadIdx.x; q0 < NY * NZ; q0 += BE * blockDim.x) {
+    cplx<T> x[BE][G], bb[BE][G];
+    T vp[BE];
     if (MODE_H) {
-      const T v = ep.V[p];
-      const cplx<T>* src = in + p * ld_in + m0;
 #pragma unroll
-      for (int j = 0; j < G; ++j)
-        if (j < gcount) {
-          const cplx<T> x = src[j];
-          h[j].x = fma(v, x.x, h[j].x);
-          h[j].y = fma(v, x.y, h[j].y);
-        }
-      if (pj.nproj > 0) {
-        const int e0 = pj.pt_ptr[p], e1 = pj.pt_ptr[p + 1];
-        for (int ei = e0; ei < e1; ++ei) {
-          const int e = pj.pt_ent[ei];
-          const int a = pj.ent_atom[e];
-          const cplx<T> ph = phase[e];
-          T b[LMAX];
-#pragma unroll
-          for (int l = 0; l < LMAX; ++l) b[l] = (l < pj.L) ? pj.ent_beta[(long)e * pj.L + l] : (T)0;
-#pragma unroll
-          for (int j = 0; j < G; ++j) {
-            if (j >= gcount) continue;
-            cplx<T> s = mk<T>(0, 0);
-#pragma unroll
-            for (int l = 0; l < LMAX; ++l) {
-              if (l >= pj.L) continue;
-              const double2 pr = pj.proj[((long)a * pj.L + l) * M + m0 + j];
-              s.x = fma(b[l], (T)pr.x, s.x);
-              s.y = fma(b[l], (T)pr.y, s.y);
-            }
-            h[j] = h[j] + mul_conj(s, ph);
-          }
+      for (int b = 0; b < BE; ++b) {
+        const int q = q0 + b * blockDim.x;
+        if (q < NY * NZ) {
+          const long p = pbase + q;
+          vp[b] = ep.V[p];
+          load_group<T, G>(in + p * ld_in + m0, x[b], gcount, v);
+          if (ep.base) load_group<T, G>(ep.base + p * ep.ld_base + m0, bb[b], gcount, v);
         }
       }
-      cplx<T>* dst = out + p * ld_out + m0;
-      const cplx<T>* bsrc = ep.base ? ep.base + p * ep.ld_base + m0 : nullptr;
+    }
 #pragma unroll
-      for (int j = 0; j < G; ++j)
-        if (j < gcount) {
-          cplx<T> r = ep.alpha * h[j];
-          if (bsrc) r = r + ep.beta * bsrc[j];
-          dst[j] = r;
+    for (int b = 0; b < BE; ++b) {
+      const int q = q0 + b * blockDim.x;
+      if (q >= NY * NZ) continue;
+      const int iy = q / NZ, iz = q - iy * NZ;
+      const int sl = AY::slot_of_freq(iy) * ZP + AZ::slot_of_freq(iz);
+      const long p = pbase + q;
+      cplx<T> h[G];
+#pragma unroll
+      for (int j = 0; j < G; ++j) h[j] = S[j * PLANE + sl];
+      if (MODE_H) {
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+          h[j].x = fma(vp[b], x[b][j].x, h[j].x);
+          h[j].y = fma(vp[b], x[b][j].y, h[j].y);
+          h[j] = ep.alpha * h[j];
+          if (ep.base) h[j] = h[j] + ep.beta * bb[b][j];
         }
-    } else {
-      cplx<T>* dst = out + p * ld_out + m0;
-#pragma unroll
-      for (int j = 0; j < G; ++j)
-        if (j < gcount) dst[j] = h[j];
+      }
+      store_group<T, G>(out + p * ld_out + m0, h, gcount, v);
     }
   }
 }
@@ -445,32 +650,42 @@ __global__ void k_phases(int nent, const float* __restrict__ relpos, double k0, 
 // ---------------------------------------------------------------- plan instantiation
 template <typename T, int NX, int NY, int NZ>
 struct Kernels {
-  static constexpr int G = plane_group<T, NY, NZ>();
-  static constexpr int CX = (kThreads / (G * Split<NX>::N2) > 0) ? (kThreads / (G * Split<NX>::N2)) : 1;
-  static constexpr size_t plane_smem =
-      sizeof(cplx<T>) * ((size_t)G * NY * PadAxis<NZ>::SLOTS + NY + NZ);
-  static constexpr size_t line_smem = sizeof(cplx<T>) * ((size_t)CX * PadAxis<NX>::SLOTS * G + NX);
+  using PG = PlaneGeom<T, NY, NZ>;
+  using LG = LineGeom<T, NX>;
+  static constexpr int G = PG::G;
+  static constexpr int CS = LG::template cs<G>();
+  // x-line tile: 128 register lines (single-thread split) or 256 team items per CTA
+  static constexpr int LINE_THREADS = (LG::AX::N2 == 1) ? 128 : kThreads;
+  static constexpr int CX = (LINE_THREADS / (G * LG::AX::N2) > 0) ? (LINE_THREADS / (G * LG::AX::N2)) : 1;
+  static constexpr size_t line_smem = sizeof(cplx<T>) * ((size_t)CX * CS + NX);
 };
+
+static bool aligned16(const void* p, long ld, size_t esz) {
+  return ((uintptr_t)p % 16 == 0) && ((ld * (long)esz) % 16 == 0);
+}
 
 template <typename T, int NX, int NY, int NZ>
 static int launch_h_impl(const LaunchArgs& a) {
   using K = Kernels<T, NX, NY, NZ>;
+  using PG = typename K::PG;
   constexpr int G = K::G;
-  static bool attr_done = false;
-  if (!attr_done) {
-    INQB_CUDA_TRY(cudaFuncSetAttribute(k_plane_fwd<T, NY, NZ, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)K::plane_smem));
-    INQB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inv<T, NY, NZ, G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)K::plane_smem));
-    INQB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inv<T, NY, NZ, G, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)K::plane_smem));
+  static bool attr_done[64] = {};
+  int dev = 0;
+  INQB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 64 && !attr_done[dev]) {
+    INQB_CUDA_TRY(cudaFuncSetAttribute(k_plane_fwd<T, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)PG::SMEM));
+    INQB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inv<T, NY, NZ, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)PG::SMEM));
+    INQB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inv<T, NY, NZ, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)PG::SMEM));
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_line_x<T, NX, G, K::CX, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)K::line_smem));
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_line_x<T, NX, G, K::CX, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)K::line_smem));
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_line_x<T, NX, G, K::CX, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)K::line_smem));
-    attr_done = true;
+    attr_done[dev] = true;
   }
   const int groups = (a.M + G - 1) / G;
   const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(a.tw);
@@ -479,6 +694,11 @@ static int launch_h_impl(const LaunchArgs& a) {
   const cplx<T>* twz = tw + NX + NY;
   cplx<T>* tmp = reinterpret_cast<cplx<T>*>(a.tmp);
   cudaStream_t st = (cudaStream_t)a.stream;
+  const size_t esz = sizeof(cplx<T>);
+  const bool gvec = (G * esz) % 16 == 0;
+  const int vin = gvec && aligned16(a.in, a.ld_in, esz) && aligned16(tmp, 0, esz);
+  const int vout = gvec && aligned16(a.out, a.ld_out, esz) && (a.base == nullptr || aligned16(a.base, a.ld_base, esz)) &&
+                   (a.mode != LaunchArgs::H || aligned16(a.in, a.ld_in, esz));
 
   ProjView<T> pj = *reinterpret_cast<const ProjView<T>*>(a.proj_view);
   KinParams<T> kp;
@@ -488,17 +708,17 @@ static int launch_h_impl(const LaunchArgs& a) {
   }
   kp.scale = (T)(1.0 / ((double)NX * NY * NZ));
 
-  const dim3 gplane(NX, groups);
+  const dim3 gplane(groups, NX);
   const dim3 gline((NY * NZ + K::CX - 1) / K::CX, groups);
   if (a.mode == LaunchArgs::H) {
     if (pj.nproj > 0)
       INQB_CUDA_TRY(cudaMemsetAsync(pj.proj, 0, sizeof(double2) * (size_t)pj.nproj * pj.L * a.M, st));
     if (a.events[0]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[0], st));
-    k_plane_fwd<T, NY, NZ, G><<<gplane, kThreads, K::plane_smem, st>>>(
-        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, NX, twy, twz, pj, 1);
+    k_plane_fwd<T, NY, NZ><<<gplane, PG::THREADS, PG::SMEM, st>>>((const cplx<T>*)a.in, a.ld_in, a.M, tmp, NX, twy,
+                                                                 twz, pj, 1, vin);
     if (a.events[1]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[1], st));
-    k_line_x<T, NX, G, K::CX, 0><<<gline, kThreads, K::line_smem, st>>>(tmp, nullptr, nullptr, 0, a.M, NY, NZ,
-                                                                        twx, kp);
+    k_line_x<T, NX, G, K::CX, 0><<<gline, K::LINE_THREADS, K::line_smem, st>>>(tmp, nullptr, nullptr, 0, a.M, NY, NZ,
+                                                                        twx, kp, 1);
     if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
     EpiParams<T> ep;
     ep.V = (const T*)a.V;
@@ -506,20 +726,20 @@ static int launch_h_impl(const LaunchArgs& a) {
     ep.ld_base = a.ld_base;
     ep.alpha = mk<T>((T)a.alpha[0], (T)a.alpha[1]);
     ep.beta = mk<T>((T)a.beta[0], (T)a.beta[1]);
-    k_plane_inv<T, NY, NZ, G, 1><<<gplane, kThreads, K::plane_smem, st>>>(
-        tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, NX, twy, twz, pj, ep);
+    k_plane_inv<T, NY, NZ, 1><<<gplane, PG::THREADS, PG::SMEM, st>>>(
+        tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, NX, twy, twz, pj, ep, vout);
     if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
   } else if (a.mode == LaunchArgs::FFT_FWD) {
-    k_plane_fwd<T, NY, NZ, G><<<gplane, kThreads, K::plane_smem, st>>>(
-        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, NX, twy, twz, pj, 0);
-    k_line_x<T, NX, G, K::CX, 1><<<gline, kThreads, K::line_smem, st>>>(tmp, nullptr, (cplx<T>*)a.out, a.ld_out,
-                                                                        a.M, NY, NZ, twx, kp);
+    k_plane_fwd<T, NY, NZ><<<gplane, PG::THREADS, PG::SMEM, st>>>((const cplx<T>*)a.in, a.ld_in, a.M, tmp, NX, twy,
+                                                                 twz, pj, 0, vin);
+    k_line_x<T, NX, G, K::CX, 1><<<gline, K::LINE_THREADS, K::line_smem, st>>>(tmp, nullptr, (cplx<T>*)a.out, a.ld_out,
+                                                                        a.M, NY, NZ, twx, kp, vout);
   } else {
-    k_line_x<T, NX, G, K::CX, 2><<<gline, kThreads, K::line_smem, st>>>(tmp, (const cplx<T>*)a.in, nullptr,
-                                                                        a.ld_in, a.M, NY, NZ, twx, kp);
+    k_line_x<T, NX, G, K::CX, 2><<<gline, K::LINE_THREADS, K::line_smem, st>>>(tmp, (const cplx<T>*)a.in, nullptr,
+                                                                        a.ld_in, a.M, NY, NZ, twx, kp, vin);
     EpiParams<T> ep{};
-    k_plane_inv<T, NY, NZ, G, 0><<<gplane, kThreads, K::plane_smem, st>>>(
-        tmp, nullptr, 0, (cplx<T>*)a.out, a.ld_out, a.M, NX, twy, twz, pj, ep);
+    k_plane_inv<T, NY, NZ, 0><<<gplane, PG::THREADS, PG::SMEM, st>>>(tmp, nullptr, 0, (cplx<T>*)a.out, a.ld_out,
+                                                                     a.M, NX, twy, twz, pj, ep, vout);
   }
   INQB_CUDA_TRY(cudaGetLastError());
   return INQB_OK;

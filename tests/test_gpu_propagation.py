@@ -41,7 +41,9 @@ def test_etrs_steps_fp64_and_mixed(pb, oracle_mod, sysd):
         h64.etrs_step_(x64, 0.05, k1, k2)
         h32.etrs_step_(x32, 0.05, k1, k2)
     assert rel_max(x64.cpu().numpy(), ref) < 1e-10
-    assert rel_norm(x32.cpu().numpy(), ref) < 1e-5
+    # mixed path: complex64 FFTs leave ~4e-7 relative error per H apply, which the
+    # 8 Horner applies of a step carry into ~4e-6 per step in the orbitals
+    assert rel_norm(x32.cpu().numpy(), ref) < 3e-5
 
 
 def test_density_and_dipole(pb, oracle_mod, sysd):
