@@ -132,6 +132,27 @@ int inqb_dipole(inqb_ctx* ctx, const double* rho, double out[3], void* stream);
  * overlap S = dV psi^H psi, Cholesky S = U^H U, psi <- psi U^-1; synchronous. */
 int inqb_orthonormalize(inqb_ctx* ctx, void* psi, int M, int ld, void* stream);
 
+/* ---------------------------------------------------------------- adjoint building blocks
+ * The reverse-mode pieces of the ETRS step (the reference has no adjoint; these
+ * differentiate real_time::etrs, src/real_time/etrs.hpp:22-82).  Orbital blocks
+ * follow the layout above; gradients are FP64 device arrays accumulated in place.
+ * y <- a x + b y  (operations::shift generalised, src/operations/shift.hpp:33-44) */
+int inqb_axpby(inqb_ctx* ctx, int M, double a_re, double a_im, const void* x, int ldx, double b_re, double b_im,
+               void* y, int ldy, void* stream);
+/* out[p][m] = scale * occ[m] * r_dir(p) * psi[p][m], r the symmetric-range
+ * cartesian position of dipole.hpp:23-30: the derivative of the dipole with
+ * respect to conj(psi) for scale = dV. */
+int inqb_position_scale(inqb_ctx* ctx, const void* psi, int ld, void* out, int ldo, int M, int dir,
+                        const double* occ, double scale, void* stream);
+/* gV[p] += Re(c sum_m conj(u[p][m]) w[p][m]) = Re(c <u| dH/dV(p) |w>) */
+int inqb_accum_potential_gradient(inqb_ctx* ctx, const void* u, const void* w, int M, int ld, double c_re,
+                                  double c_im, double* gV, void* stream);
+/* gA[d] += Re(c <u| dH/dA_d |w>), d = x, y, z cartesian, at the context's current
+ * k + A: the kinetic term (G + k + A)_d and the nonlocal position commutator of
+ * projector_all::position_commutator (src/hamiltonian/projector_all.hpp:319-403). */
+int inqb_accum_vector_potential_gradient(inqb_ctx* ctx, const void* u, const void* w, int M, int ld, double c_re,
+                                         double c_im, double* gA, void* stream);
+
 /* ---------------------------------------------------------------- profiling
  * Per-pass CUDA-event timing of the next max_applies H applications, recorded
  * on the stream the kernels run on; the counterpart of INQ's scoped timers

@@ -1,0 +1,17 @@
+// Launchers of the adjoint building blocks (adjoint.cu).
+#pragma once
+
+struct inqb_ctx;
+
+namespace inqb {
+
+int launch_axpby(int precision, long N, int M, const double a[2], const void* x, long ldx, const double b[2], void* y,
+                 long ldy, void* stream);
+int launch_position_scale(int precision, const inqb_ctx& ctx, const void* psi, long ld, void* out, long ldo, int M,
+                          int dir, const double* occ, double s, void* stream);
+int launch_vgrad(int precision, long N, int M, const void* u, const void* w, long ld, double cre, double cim,
+                 double* gV, void* stream);
+int launch_agrad(const inqb_ctx& ctx, const void* U, const void* W, const void* u, const void* w, long ld, int M,
+                 double* acc, double cre, double cim, double* gA, void* stream);
+
+}  // namespace inqb

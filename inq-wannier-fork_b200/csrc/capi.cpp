@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "inqb_internal.h"
+#include "adjoint.h"
 #include "observables.h"
 #include "plan.h"
 
@@ -491,6 +492,54 @@ int inqb_orthonormalize(inqb_ctx* ctx, void* psi, int M, int ld, void* stream) {
   INQB_TRY(info.ensure(sizeof(int)));
   return launch_orthonormalize(ctx->precision, psi, ld, M, ctx->N, ctx->dV, S.as<double2>(), X.as<double2>(),
                                info.as<int>(), stream);
+}
+
+int inqb_axpby(inqb_ctx* ctx, int M, double a_re, double a_im, const void* x, int ldx, double b_re, double b_im,
+               void* y, int ldy, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, x, M, ldx));
+  INQB_TRY(check_block(ctx, y, M, ldy));
+  INQB_GUARD(ctx);
+  const double a[2] = {a_re, a_im}, b[2] = {b_re, b_im};
+  return launch_axpby(ctx->precision, ctx->N, M, a, x, ldx, b, y, ldy, stream);
+}
+
+int inqb_position_scale(inqb_ctx* ctx, const void* psi, int ld, void* out, int ldo, int M, int dir,
+                        const double* occ, double scale, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  INQB_TRY(check_block(ctx, out, M, ldo));
+  if (dir < 0 || dir > 2 || !occ) return fail(INQB_ERR_INVALID, "bad direction or occupations");
+  INQB_GUARD(ctx);
+  return launch_position_scale(ctx->precision, *ctx, psi, ld, out, ldo, M, dir, occ, scale, stream);
+}
+
+int inqb_accum_potential_gradient(inqb_ctx* ctx, const void* u, const void* w, int M, int ld, double c_re,
+                                  double c_im, double* gV, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, u, M, ld));
+  INQB_TRY(check_block(ctx, w, M, ld));
+  if (!gV) return fail(INQB_ERR_INVALID, "null gradient");
+  INQB_GUARD(ctx);
+  return launch_vgrad(ctx->precision, ctx->N, M, u, w, ld, c_re, c_im, gV, stream);
+}
+
+int inqb_accum_vector_potential_gradient(inqb_ctx* ctx, const void* u, const void* w, int M, int ld, double c_re,
+                                         double c_im, double* gA, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, u, M, ld));
+  INQB_TRY(check_block(ctx, w, M, ld));
+  if (!gA) return fail(INQB_ERR_INVALID, "null gradient");
+  INQB_GUARD(ctx);
+  const size_t bytes = (size_t)ctx->N * M * ctx->elem_bytes();
+  INQB_TRY(ctx->d_adjU.ensure(bytes));
+  INQB_TRY(ctx->d_adjW.ensure(bytes));
+  INQB_TRY(ctx->d_red.ensure(256));
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  INQB_TRY(apply(ctx, LaunchArgs::FFT_FWD, u, ld, ctx->d_adjU.ptr, M, M, nullptr, 0, one, zero, stream));
+  INQB_TRY(apply(ctx, LaunchArgs::FFT_FWD, w, ld, ctx->d_adjW.ptr, M, M, nullptr, 0, one, zero, stream));
+  return launch_agrad(*ctx, ctx->d_adjU.ptr, ctx->d_adjW.ptr, u, w, ld, M, ctx->d_red.as<double>(), c_re, c_im, gA,
+                      stream);
 }
 
 }  // extern "C"

@@ -79,12 +79,16 @@ struct ProjTables {
   std::vector<double> ent_beta;     // [nent][L]
   std::vector<float> ent_relpos;    // [nent][3] contravariant, float as the reference stores it
   std::vector<double> scale;        // [nproj][L] = dV * kb coefficient
+  // atom-major view used by the derivative kernels of the adjoint
+  std::vector<int> atom_ptr, atom_ent, ent_pt;  // [nproj+1], [nent], [nent] linear grid point
+  std::vector<double> ent_xyz;      // [nent][3] cartesian relative position
   // device copies
   DevBuf d_seg_ptr, d_seg_atom, d_seg_ent, d_ent_off, d_ent_atom, d_pt_ptr, d_pt_ent;
   DevBuf d_ent_beta;                // [nent][L] in the context precision
   DevBuf d_ent_relpos;              // [nent][3] float
   DevBuf d_ent_phase;               // [nent] complex, exp(+i (k+A).r), context precision
   DevBuf d_scale;                   // [nproj][L] double
+  DevBuf d_atom_ptr, d_atom_ent, d_ent_pt, d_ent_xyz;
 };
 
 // Kernel view of the projector tables (T = float or double).
@@ -130,6 +134,7 @@ struct inqb_ctx {
   inqb::DevBuf d_work;    // one orbital block for propagators
   inqb::DevBuf d_work2;
   inqb::DevBuf d_red;     // small reduction buffers
+  inqb::DevBuf d_adjU, d_adjW;  // Fourier transforms for the dH/dA inner products
   size_t elem_bytes() const { return precision == INQB_FP64 ? 16 : 8; }
 
   // optional per-pass CUDA-event timing of H applications

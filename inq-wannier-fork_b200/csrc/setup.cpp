@@ -277,6 +277,23 @@ int build_proj_tables(const inqb_ctx& ctx, int nproj, int L, int smax, const int
     // order inside a point: by atom then sphere point, i.e. plane-bucket order
     for (long i = 0; i < total; i++) t.pt_ent[fill[pt_of[i]]++] = (int)i;
   }
+  // atom-major entry lists, grid points and cartesian relative positions
+  t.ent_pt.resize(total);
+  t.ent_xyz.resize(total * 3);
+  for (long i = 0; i < total; i++) {
+    t.ent_pt[i] = (int)pt_of[i];
+    const double rc[3] = {(double)t.ent_relpos[3 * i], (double)t.ent_relpos[3 * i + 1],
+                          (double)t.ent_relpos[3 * i + 2]};
+    ctx.cell.contra_to_cart(rc, &t.ent_xyz[3 * i]);
+  }
+  t.atom_ptr.assign(nproj + 1, 0);
+  for (long i = 0; i < total; i++) t.atom_ptr[t.ent_atom[i] + 1]++;
+  for (int a = 0; a < nproj; a++) t.atom_ptr[a + 1] += t.atom_ptr[a];
+  t.atom_ent.assign(total, 0);
+  {
+    std::vector<int> fill(t.atom_ptr.begin(), t.atom_ptr.end() - 1);
+    for (long i = 0; i < total; i++) t.atom_ent[fill[t.ent_atom[i]]++] = (int)i;
+  }
   t.scale.resize((size_t)nproj * L);
   for (int a = 0; a < nproj; a++)
     for (int l = 0; l < L; l++) t.scale[(size_t)a * L + l] = ctx.dV * coeff[(size_t)a * L + l];
@@ -300,6 +317,10 @@ int upload_proj_tables(const inqb_ctx& ctx, ProjTables& t) {
   INQB_TRY(upload(t.d_pt_ent, t.pt_ent));
   INQB_TRY(upload(t.d_ent_relpos, t.ent_relpos));
   INQB_TRY(upload(t.d_scale, t.scale));
+  INQB_TRY(upload(t.d_atom_ptr, t.atom_ptr));
+  INQB_TRY(upload(t.d_atom_ent, t.atom_ent));
+  INQB_TRY(upload(t.d_ent_pt, t.ent_pt));
+  INQB_TRY(upload(t.d_ent_xyz, t.ent_xyz));
   if (ctx.precision == INQB_FP64) {
     INQB_TRY(upload(t.d_ent_beta, t.ent_beta));
   } else {

@@ -232,6 +232,40 @@ class KSHamiltonian:
         call("inqb_dipole", self._h, rho.data_ptr(), dptr(out), self._stream())
         return out
 
+    # -- adjoint building blocks
+    def axpby_(self, a, x, b, y):
+        """y <- a x + b y (complex scalars, orbital blocks)."""
+        self._check(x), self._check(y)
+        a, b = complex(a), complex(b)
+        call("inqb_axpby", self._h, x.shape[1], a.real, a.imag, x.data_ptr(), x.stride(0), b.real, b.imag,
+             y.data_ptr(), y.stride(0), self._stream())
+        return y
+
+    def position_scale(self, psi, occ, direction=0, scale=1.0, out=None):
+        """out = scale * occ[m] * r_dir(p) * psi (the dipole's derivative for scale = dV)."""
+        psi = self._check(psi)
+        out = torch.empty_like(psi) if out is None else self._check(out)
+        occ_t = torch.as_tensor(occ, dtype=torch.float64, device=self.device).contiguous()
+        call("inqb_position_scale", self._h, psi.data_ptr(), psi.stride(0), out.data_ptr(), out.stride(0),
+             psi.shape[1], int(direction), occ_t.data_ptr(), float(scale), self._stream())
+        return out
+
+    def accum_potential_gradient_(self, gV, u, w, c=1.0):
+        """gV[p] += Re(c sum_m conj(u) w) -- <u| dH/dV(p) |w>."""
+        self._check(u), self._check(w)
+        c = complex(c)
+        call("inqb_accum_potential_gradient", self._h, u.data_ptr(), w.data_ptr(), u.shape[1], u.stride(0), c.real,
+             c.imag, gV.data_ptr(), self._stream())
+        return gV
+
+    def accum_vector_potential_gradient_(self, gA, u, w, c=1.0):
+        """gA[d] += Re(c <u| dH/dA_d |w>) at the current k + A (gA: 3 FP64 on the device)."""
+        self._check(u), self._check(w)
+        c = complex(c)
+        call("inqb_accum_vector_potential_gradient", self._h, u.data_ptr(), w.data_ptr(), u.shape[1], u.stride(0),
+             c.real, c.imag, gA.data_ptr(), self._stream())
+        return gA
+
     def timing_start(self, max_applies: int):
         """Record CUDA events around the three passes of the next max_applies H applies."""
         call("inqb_timing_start", self._h, int(max_applies))
