@@ -73,6 +73,13 @@ int inqb_set_local_potential(inqb_ctx* ctx, const double* V);
  * (src/hamiltonian/ks_hamiltonian.hpp:214-221, used as phi.kpoint() + A). */
 int inqb_set_vector_potential(inqb_ctx* ctx, const double kA_cov[3]);
 
+/* operations::transform::zero_outside_sphere (src/operations/transform.hpp:363-364,
+ * src/basis/fourier_space.hpp:87-93) applied to the kinetic term: with enable = 1
+ * the kinetic energy of Fourier points with sum_d (n_d/N_d)^2 > 1/4 is zeroed, so
+ * H = P K P + V + V_nl (still Hermitian).  Off by default, as in INQ; it keeps
+ * Taylor propagators stable when 1/2|G_max|^2 dt/2 exceeds 2 sqrt(2). */
+int inqb_set_fourier_sphere_mask(inqb_ctx* ctx, int enable);
+
 /* ---------------------------------------------------------------- projector setup
  * Setup helpers; they need no context and no GPU.
  * basis::spherical_grid (src/basis/spherical_grid.hpp:59-158): the grid points

@@ -85,6 +85,7 @@ struct Recip {
   double b[3][3];
   double kA[3];
   int nr[3];
+  int mask;
 };
 
 // acc[2d..2d+1] += sum_{G,m} conj(U) (G + kA)_d W   (U, W forward FFTs, natural order)
@@ -99,11 +100,21 @@ __global__ void k_velocity_dot(long N, int M, const cplx<T>* __restrict__ U, con
     const int k[3] = {(int)(p / nyz), (int)((p / r.nr[2]) % r.nr[1]), (int)(p % r.nr[2])};
     double n[3];
     for (int c = 0; c < 3; c++) n[c] = (k[c] >= (r.nr[c] + 1) / 2) ? k[c] - r.nr[c] : k[c];
+    // with the mask, the Laplacian term P(1/2 g^2 + kA.G)P drops its G outside the sphere
+    // while the 1/2|kA|^2 shift stays: the derivative there is kA alone
+    double gf = 1.0;
+    if (r.mask) {
+      const long long a0 = (long long)r.nr[1] * r.nr[2], a1 = (long long)r.nr[0] * r.nr[2],
+                      a2 = (long long)r.nr[0] * r.nr[1];
+      const long long tot = (long long)r.nr[0] * r.nr[1] * r.nr[2];
+      const long long i0 = (long long)n[0], i1 = (long long)n[1], i2 = (long long)n[2];
+      if (4 * (i0 * i0 * a0 * a0 + i1 * i1 * a1 * a1 + i2 * i2 * a2 * a2) > tot * tot) gf = 0.0;
+    }
     const cplx<T> a = U[p * ld + m], b = W[p * ld + m];
     const double re = (double)a.x * b.x + (double)a.y * b.y;
     const double im = (double)a.x * b.y - (double)a.y * b.x;
     for (int d = 0; d < 3; d++) {
-      const double v = n[0] * r.b[0][d] + n[1] * r.b[1][d] + n[2] * r.b[2][d] + r.kA[d];
+      const double v = gf * (n[0] * r.b[0][d] + n[1] * r.b[1][d] + n[2] * r.b[2][d]) + r.kA[d];
       s[2 * d] += v * re;
       s[2 * d + 1] += v * im;
     }
@@ -253,6 +264,7 @@ static int agrad_impl(const inqb_ctx& ctx, const void* U, const void* W, const v
     for (int j = 0; j < 3; j++) r.b[i][j] = ctx.cell.rlat[i][j];
   }
   ctx.cell.cov_to_cart(ctx.kA_cov, r.kA);
+  r.mask = ctx.fourier_mask;
   INQB_CUDA_TRY(cudaMemsetAsync(acc, 0, 12 * sizeof(double), st));
   k_velocity_dot<T><<<grid_for(ctx.N * M, 256), 256, 0, st>>>(ctx.N, M, (const cplx<T>*)U, (const cplx<T>*)W, M, r,
                                                              acc);

@@ -126,6 +126,7 @@ int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long l
   a.beta[0] = beta[0];
   a.beta[1] = beta[1];
   a.stream = stream;
+  a.fourier_mask = ctx->fourier_mask;
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) a.rlat[i][j] = ctx->cell.rlat[i][j];
   ctx->cell.cov_to_cart(ctx->kA_cov, a.kA_cart);
@@ -343,6 +344,12 @@ int inqb_set_vector_potential(inqb_ctx* ctx, const double kA_cov[3]) {
   INQB_GUARD(ctx);
   INQB_TRY(set_kA(ctx, kA_cov, nullptr));
   INQB_CUDA_TRY(cudaStreamSynchronize(nullptr));
+  return INQB_OK;
+}
+
+int inqb_set_fourier_sphere_mask(inqb_ctx* ctx, int enable) {
+  INQB_CHECK_CTX(ctx);
+  ctx->fourier_mask = enable ? 1 : 0;
   return INQB_OK;
 }
 

@@ -89,7 +89,19 @@ struct KinParams {
   T b[3][3];  // reciprocal vectors: G_cart = sum_d n_d b[d]
   T kA[3];    // cartesian k + A
   T scale;    // 1/N folded into the kinetic factor
+  int mask;   // zero the Laplacian term outside the Fourier sphere (|n/N|^2 > 1/4)
+  int nr[3];
+  T shift;    // 1/2 |k+A|^2 / N, moved to the epilogue when the mask is on
 };
+
+// INQ's fourier_space::outside_sphere (src/basis/fourier_space.hpp:87-93) in exact
+// integer arithmetic: sum_d (n_d / N_d)^2 > 1/4.
+__device__ __forceinline__ bool outside_sphere(const int nr[3], int n0, int n1, int n2) {
+  const long long a = (long long)nr[1] * nr[2], b = (long long)nr[0] * nr[2], c = (long long)nr[0] * nr[1];
+  const long long lhs = 4 * ((long long)n0 * n0 * a * a + (long long)n1 * n1 * b * b + (long long)n2 * n2 * c * c);
+  const long long tot = (long long)nr[0] * nr[1] * nr[2];
+  return lhs > tot * tot;
+}
 
 template <typename T>
 __device__ __forceinline__ T kinetic(const KinParams<T>& kp, int n0, int n1, int n2) {
@@ -104,6 +116,7 @@ __device__ __forceinline__ int sym_freq(int k, int n) { return (k >= (n + 1) / 2
 template <typename T>
 struct EpiParams {
   const T* V;               // [N] local potential
+  T vshift;                 // added to V (1/2 |k+A|^2 when the Fourier mask is on)
   const cplx<T>* base;      // optional [N][ld_base]
   long ld_base;
   cplx<T> alpha, beta;      // out = alpha * H in + beta * base
@@ -450,7 +463,9 @@ __global__ void __launch_bounds__(kThreads) k_line_x(cplx<T>* __restrict__ tmp, 
         for (int x = 0; x < NX; ++x) {
           const T kx = (T)sym_freq(x, NX);
           const T g0 = kx * kp.b[0][0] + gp[0], g1 = kx * kp.b[0][1] + gp[1], g2 = kx * kp.b[0][2] + gp[2];
-          v[x] = ((T)0.5 * kp.scale * (g0 * g0 + g1 * g1 + g2 * g2)) * v[x];
+          T k = (T)0.5 * kp.scale * (g0 * g0 + g1 * g1 + g2 * g2);
+          if (kp.mask) k = outside_sphere(kp.nr, sym_freq(x, NX), ky, kz) ? (T)0 : k - kp.shift;
+          v[x] = k * v[x];
         }
         DFT<NX, true, T>::run(v);
 #pragma unroll
@@ -463,7 +478,9 @@ __global__ void __launch_bounds__(kThreads) k_line_x(cplx<T>* __restrict__ tmp, 
         const int c = (it / G) / AX::N1;
         const int yz = yz0 + c;
         const int ky = yz / nz, kz = yz - ky * nz;
-        const T k = kinetic(kp, sym_freq(kx, NX), sym_freq(ky, ny), sym_freq(kz, nz));
+        const int n0 = sym_freq(kx, NX), n1 = sym_freq(ky, ny), n2 = sym_freq(kz, nz);
+        T k = kinetic(kp, n0, n1, n2);
+        if (kp.mask) k = outside_sphere(kp.nr, n0, n1, n2) ? (T)0 : k - kp.shift;
         return k * v;
       });
       __syncthreads();
@@ -605,7 +622,7 @@ __global__ void __launch_bounds__(PlaneGeom<T, NY, NZ>::THREADS)
         const int q = q0 + b * blockDim.x;
         if (q < NY * NZ) {
           const long p = pbase + q;
-          vp[b] = ep.V[p];
+          vp[b] = ep.V[p] + ep.vshift;
           load_group<T, G>(in + p * ld_in + m0, x[b], gcount, v);
           if (ep.base) load_group<T, G>(ep.base + p * ep.ld_base + m0, bb[b], gcount, v);
         }
@@ -707,6 +724,12 @@ static int launch_h_impl(const LaunchArgs& a) {
     kp.kA[d] = (T)a.kA_cart[d];
   }
   kp.scale = (T)(1.0 / ((double)NX * NY * NZ));
+  kp.mask = a.fourier_mask;
+  const double kA2 = a.kA_cart[0] * a.kA_cart[0] + a.kA_cart[1] * a.kA_cart[1] + a.kA_cart[2] * a.kA_cart[2];
+  kp.shift = (T)(0.5 * kA2 / ((double)NX * NY * NZ));
+  kp.nr[0] = NX;
+  kp.nr[1] = NY;
+  kp.nr[2] = NZ;
 
   const dim3 gplane(groups, NX);
   const dim3 gline((NY * NZ + K::CX - 1) / K::CX, groups);
@@ -722,6 +745,7 @@ static int launch_h_impl(const LaunchArgs& a) {
     if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
     EpiParams<T> ep;
     ep.V = (const T*)a.V;
+    ep.vshift = a.fourier_mask ? (T)(0.5 * kA2) : (T)0;
     ep.base = (const cplx<T>*)a.base;
     ep.ld_base = a.ld_base;
     ep.alpha = mk<T>((T)a.alpha[0], (T)a.alpha[1]);

@@ -122,6 +122,7 @@ struct inqb_ctx {
   double kA_cov[3] = {0, 0, 0};
   const inqb::Plan* plan = nullptr;
   bool proj_phases_valid = false;  // device phases match kA_cov
+  int fourier_mask = 0;            // zero_outside_sphere on the kinetic term
 
   std::vector<double> V_host;
   inqb::DevBuf d_V;       // [N] in context precision

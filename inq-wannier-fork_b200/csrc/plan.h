@@ -22,6 +22,7 @@ struct LaunchArgs {
   double alpha[2] = {1.0, 0.0};
   double beta[2] = {0.0, 0.0};
   void* stream = nullptr;
+  int fourier_mask = 0;             // zero the kinetic term outside the Fourier sphere
   void* events[4] = {nullptr, nullptr, nullptr, nullptr};  // optional cudaEvent_t around the passes
 };
 

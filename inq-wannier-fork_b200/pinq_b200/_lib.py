@@ -35,6 +35,7 @@ SIGNATURES = {
     "inqb_cart_to_cov": (ctypes.c_int, [_ctxp, _dp, _dp]),
     "inqb_set_local_potential": (ctypes.c_int, [_ctxp, _dp]),
     "inqb_set_vector_potential": (ctypes.c_int, [_ctxp, _dp]),
+    "inqb_set_fourier_sphere_mask": (ctypes.c_int, [_ctxp, ctypes.c_int]),
     "inqb_sphere_size": (ctypes.c_int, [_dp, _ip, _dp, ctypes.c_double, _ip]),
     "inqb_sphere_points": (ctypes.c_int, [_dp, _ip, _dp, ctypes.c_double, ctypes.c_int, _ip, _fp, _fp]),
     "inqb_gaussian_kb_beta": (ctypes.c_int, [_dp, ctypes.c_int, _fp, _fp, ctypes.c_double, _dp]),

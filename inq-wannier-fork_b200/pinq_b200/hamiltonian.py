@@ -129,6 +129,10 @@ class KSHamiltonian:
     def set_uniform_vector_potential(self, A_cart, kpoint_cart=(0.0, 0.0, 0.0)):
         self.set_vector_potential_cov(self.cart_to_cov(np.asarray(A_cart, float) + np.asarray(kpoint_cart, float)))
 
+    def set_fourier_sphere_mask(self, enable: bool = True):
+        """INQ's zero_outside_sphere on the kinetic term (off by default, as in INQ)."""
+        call("inqb_set_fourier_sphere_mask", self._h, int(bool(enable)))
+
     def set_projectors(self, kb):
         nproj = len(kb["counts"])
         counts = np.ascontiguousarray(kb["counts"], np.int32)

@@ -50,6 +50,7 @@ def lib():
         L.orc_set_potential.argtypes = [ctypes.c_void_p, _dp]
         L.orc_set_vector_potential_cov.argtypes = [ctypes.c_void_p, _dp]
         L.orc_cart_to_cov.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_set_fourier_mask.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_sphere.restype = ctypes.c_int
         L.orc_sphere.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, _ip, _fp, _fp]
         L.orc_gaussian_beta.argtypes = [ctypes.c_void_p, ctypes.c_int, _fp, _fp, ctypes.c_double, _dp]
@@ -117,6 +118,9 @@ class System:
     def set_vector_potential_cov(self, kA):
         kA = np.ascontiguousarray(kA, dtype=np.float64).reshape(3)
         lib().orc_set_vector_potential_cov(self._h, _d(kA))
+
+    def set_fourier_mask(self, enable=True):
+        lib().orc_set_fourier_mask(self._h, int(bool(enable)))
 
     def cart_to_cov(self, v):
         v = np.ascontiguousarray(v, dtype=np.float64).reshape(3)

@@ -337,6 +337,7 @@ struct System {
   Grid grid;
   std::vector<double> V;  // [N]
   v3 kA{{0, 0, 0}};        // covariant k + A
+  bool fourier_mask = false;  // zero_outside_sphere on the kinetic term (transform.hpp:363-364)
   // projector_all members (projector_all.hpp:410-419)
   int nproj = 0, L = 0, smax = 0;
   std::vector<int> counts;        // [nproj]
@@ -393,6 +394,11 @@ void apply_h(const System &s, int M, const cd *psi, cd *hpsi) {
         v3 G{{g.sym(ix, 0) * 2.0 * M_PI, g.sym(iy, 1) * 2.0 * M_PI, g.sym(iz, 2) * 2.0 * M_PI}};
         double g2 = g.cell.norm_cov(G);
         double lapl = -0.5 * (-g2 + dot(gradcoeff, G));
+        if (s.fourier_mask) {  // fourier_space::outside_sphere (fourier_space.hpp:87-93)
+          double xx = double(g.sym(ix, 0)) / g.nr[0], yy = double(g.sym(iy, 1)) / g.nr[1],
+                 zz = double(g.sym(iz, 2)) / g.nr[2];
+          if (xx * xx + yy * yy + zz * zz > 0.25) lapl = 0.0;
+        }
         long p = g.linear(ix, iy, iz);
         for (int m = 0; m < M; m++) fs[(size_t)p * M + m] *= lapl;
       }
@@ -469,6 +475,8 @@ void orc_set_vector_potential_cov(void *h, const double *kA) {
   auto *s = (System *)h;
   for (int d = 0; d < 3; d++) s->kA[d] = kA[d];
 }
+
+void orc_set_fourier_mask(void *h, int enable) { ((System *)h)->fourier_mask = enable != 0; }
 
 void orc_cart_to_cov(void *h, const double *cart, double *cov) {
   auto *s = (System *)h;

@@ -1,0 +1,61 @@
+// C++ host-adapter check (built and run by tests/test_host_adapter.py).
+// Harmonic oscillator of ks_hamiltonian.hpp:356-397 through inq::b200::ks_hamiltonian,
+// then the generic INQ-style Taylor exponential written against HamiltonianType
+// against the library's fused exponential, and one ETRS step.
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <vector>
+
+#include "../../inq-wannier-fork_b200/host/inq_b200.hpp"
+
+using cd = std::complex<double>;
+
+int main() {
+  namespace b2 = inq::b200;
+  const std::array<double, 9> lat = {10, 0, 0, 0, 10, 0, 0, 0, 10};
+  const std::array<int, 3> nr = {20, 20, 20};
+  const long N = 8000;
+  const int M = 6;
+  const double w = 2.0;
+  std::vector<double> V(N), r2(N);
+  for (int ix = 0; ix < 20; ix++)
+    for (int iy = 0; iy < 20; iy++)
+      for (int iz = 0; iz < 20; iz++) {
+        auto s = [](int i) { return (i >= 10 ? i - 20 : i) * 0.5; };
+        const long p = (ix * 20L + iy) * 20 + iz;
+        r2[p] = s(ix) * s(ix) + s(iy) * s(iy) + s(iz) * s(iz);
+        V[p] = 0.5 * w * w * r2[p];
+      }
+  std::vector<cd> psi(N * M);
+  for (long p = 0; p < N; p++)
+    for (int m = 0; m < M; m++) psi[p * M + m] = std::exp(-w * r2[p]);
+
+  b2::ks_hamiltonian ham(lat, nr, b2::precision::fp64);
+  ham.set_scalar_potential(V);
+  b2::device_orbitals phi(N, M, b2::precision::fp64);
+  phi.upload(psi);
+  auto hphi = ham(phi).download();
+  double diff = 0.0;
+  for (long i = 0; i < N * M; i++) diff += std::abs(hphi[i] - 1.5 * w * psi[i]);
+  std::printf("ho_mean_abs_diff %.12e\n", diff / (N * M));
+
+  // generic exponential (HamiltonianType + axpby) vs the fused Horner exponential
+  b2::device_orbitals a = phi, b = phi;
+  b2::exponential_generic(ham, cd(0.0, 0.025), a);
+  b2::exponential_in_place(ham, cd(0.0, 0.025), b);
+  auto va = a.download(), vb = b.download();
+  double dmax = 0.0, vmax = 0.0;
+  for (long i = 0; i < N * M; i++) {
+    dmax = std::max(dmax, std::abs(va[i] - vb[i]));
+    vmax = std::max(vmax, std::abs(vb[i]));
+  }
+  std::printf("exp_generic_vs_fused %.12e\n", dmax / vmax);
+
+  b2::etrs(ham, 0.05, {0.01, 0.0, 0.0}, {0.02, 0.0, 0.0}, b);
+  auto vc = b.download();
+  double nrm = 0.0;
+  for (auto& x : vc) nrm += std::norm(x);
+  std::printf("etrs_norm %.12e\n", nrm * ham.volume_element());
+  return 0;
+}

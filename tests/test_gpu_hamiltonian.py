@@ -163,3 +163,20 @@ def test_apply_h_host_buffers(pb, cfg0_small):
     dev = h(_dev(s["psi"])).cpu().numpy()
     host = h.apply_host(np.ascontiguousarray(s["psi"]))
     assert rel_max(host, dev) < 1e-14
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_apply_h_fourier_mask(pb, oracle_mod, cfg0_small, precision, tol):
+    """INQ's zero_outside_sphere on the Laplacian term (transform.hpp:363-364), k + A != 0."""
+    s = cfg0_small
+    o = oracle_mod.System(s["lattice"], s["nr"])
+    kA = o.cart_to_cov(np.array([0.03, 0.01, -0.02]))
+    o = make_oracle(oracle_mod, s, kA)
+    o.set_fourier_mask(True)
+    h = make_product(pb, s, precision, kA)
+    h.set_fourier_sphere_mask(True)
+    dt = torch.complex128 if precision == "fp64" else torch.complex64
+    out = h(_dev(s["psi"], dt)).cpu().numpy()
+    ref = o.apply_h(s["psi"])
+    err = rel_max(out, ref) if precision == "fp64" else rel_norm(out, ref)
+    assert err < tol, err

@@ -162,3 +162,22 @@ def test_etrs_reduces_to_two_taylor_half_steps(oracle_mod):
     o.set_vector_potential_cov(kA2)
     ref = o.exponential(0.025j, ref)
     assert np.abs(out - ref).max() == 0.0
+
+
+def test_fourier_sphere_mask(oracle_mod):
+    """transform.hpp:428-440: zero_outside_sphere keeps 0.5160349854 of a 14^3 box
+    (cubic 6.66 / 0.46320257); with the mask H's Laplacian acts on those points only."""
+    lat = np.eye(3) * 6.66
+    nr = _grid([6.66] * 3, 0.46320257)
+    assert nr == (14, 14, 14)
+    f = [np.where(np.arange(n) >= (n + 1) // 2, np.arange(n) - n, np.arange(n)) / n for n in nr]
+    inside = (f[0][:, None, None] ** 2 + f[1][None, :, None] ** 2 + f[2][None, None, :] ** 2) <= 0.25
+    assert inside.mean() == pytest.approx(0.5160349854, rel=1.2e-5)
+    o = oracle_mod.System(lat, nr)
+    o.set_fourier_mask(True)
+    rng = np.random.default_rng(4)
+    psi = rng.standard_normal((o.N, 2)) + 1j * rng.standard_normal((o.N, 2))
+    G = 2 * np.pi * np.stack(np.meshgrid(*[fi * n for fi, n in zip(f, nr)], indexing="ij"), -1) / 6.66
+    lap = 0.5 * (G ** 2).sum(-1) * inside
+    ref = np.fft.ifftn(lap[..., None] * np.fft.fftn(psi.reshape(*nr, 2), axes=(0, 1, 2)), axes=(0, 1, 2))
+    assert np.abs(o.apply_h(psi) - ref.reshape(-1, 2)).max() < 1e-12 * np.abs(ref).max()
