@@ -115,6 +115,21 @@ int inqb_apply_h_host(inqb_ctx* ctx, const void* psi_host, void* hpsi_host, int 
 int inqb_fft_forward(inqb_ctx* ctx, const void* in, void* out, int M, int ld, void* stream);
 int inqb_fft_backward(inqb_ctx* ctx, const void* in, void* out, int M, int ld, void* stream);
 
+/* ---------------------------------------------------------------- batched cells
+ * Many independent cells (each its own context: grid, potential, projectors)
+ * applied together as one CUDA graph with one concurrent branch per cell.  The
+ * reference runs cells one after another; this has no single reference
+ * counterpart (it batches ks_hamiltonian::operator(), ks_hamiltonian.hpp:132-152).
+ * The first call with a given set of pointers and sizes captures and instantiates
+ * the graph (it also runs each cell once, uncaptured, to set up workspace); later
+ * calls with the same arguments only launch it.  The contexts must outlive the
+ * batch and must not be used concurrently with it. */
+typedef struct inqb_batch inqb_batch;
+int inqb_batch_create(inqb_ctx* const* cells, int ncells, inqb_batch** out);
+int inqb_batch_destroy(inqb_batch* batch);
+int inqb_batch_apply_h(inqb_batch* batch, const void* const* psis, void* const* hpsis, const int* Ms,
+                       const int* lds, void* stream);
+
 /* ---------------------------------------------------------------- propagation
  * operations::exponential_in_place (src/operations/exponential.hpp:21-34):
  * psi <- sum_{k<=order} (f H)^k / k! psi, f = f_re + i f_im, in place. */

@@ -167,6 +167,68 @@ int exponential(inqb_ctx* ctx, void* psi, int M, long ld, double fre, double fim
 }  // namespace
 }  // namespace inqb
 
+// A set of independent cells whose H applications run as one CUDA graph: one
+// branch per cell (its three fused kernels), all branches concurrent.
+struct inqb_batch {
+  std::vector<inqb_ctx*> cells;
+  int device = 0;
+  std::vector<cudaStream_t> streams;  // capture streams: [0] origin, [1..n] one per cell
+  std::vector<cudaEvent_t> events;    // [0] fork, [1..n] joins
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  // arguments the instantiated graph was built with
+  std::vector<const void*> psis;
+  std::vector<void*> hpsis;
+  std::vector<int> Ms, lds;
+};
+
+namespace inqb {
+namespace {
+
+void batch_release_graph(inqb_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+int batch_capture(inqb_batch* b, const void* const* psis, void* const* hpsis, const int* Ms, const int* lds) {
+  const int n = (int)b->cells.size();
+  cudaStream_t s0 = b->streams[0];
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  INQB_CUDA_TRY(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+  int st = INQB_OK;
+  if (cudaEventRecord(b->events[0], s0) != cudaSuccess) st = fail(INQB_ERR_CUDA, "fork event");
+  for (int i = 0; i < n && st == INQB_OK; i++) {
+    cudaStream_t si = b->streams[i + 1];
+    if (cudaStreamWaitEvent(si, b->events[0], 0) != cudaSuccess) {
+      st = fail(INQB_ERR_CUDA, "fork wait");
+      break;
+    }
+    st = apply(b->cells[i], LaunchArgs::H, psis[i], lds[i], hpsis[i], lds[i], Ms[i], nullptr, 0, one, zero, si);
+    if (st == INQB_OK && cudaEventRecord(b->events[i + 1], si) != cudaSuccess) st = fail(INQB_ERR_CUDA, "join event");
+    if (st == INQB_OK && cudaStreamWaitEvent(s0, b->events[i + 1], 0) != cudaSuccess) st = fail(INQB_ERR_CUDA, "join");
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(s0, &g);
+  if (st != INQB_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (ec != cudaSuccess) return fail(INQB_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(ec));
+  batch_release_graph(b);
+  b->graph = g;
+  INQB_CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  b->psis.assign(psis, psis + n);
+  b->hpsis.assign(hpsis, hpsis + n);
+  b->Ms.assign(Ms, Ms + n);
+  b->lds.assign(lds, lds + n);
+  return INQB_OK;
+}
+
+}  // namespace
+}  // namespace inqb
+
 using namespace inqb;
 
 extern "C" {
@@ -499,6 +561,78 @@ int inqb_orthonormalize(inqb_ctx* ctx, void* psi, int M, int ld, void* stream) {
   INQB_TRY(info.ensure(sizeof(int)));
   return launch_orthonormalize(ctx->precision, psi, ld, M, ctx->N, ctx->dV, S.as<double2>(), X.as<double2>(),
                                info.as<int>(), stream);
+}
+
+int inqb_batch_create(inqb_ctx* const* cells, int ncells, inqb_batch** out) {
+  if (!cells || !out || ncells <= 0) return fail(INQB_ERR_INVALID, "bad batch arguments");
+  *out = nullptr;
+  for (int i = 0; i < ncells; i++) {
+    if (!cells[i]) return fail(INQB_ERR_INVALID, "null cell context");
+    if (cells[i]->device != cells[0]->device) return fail(INQB_ERR_INVALID, "cells on different devices");
+  }
+  DeviceGuard guard(cells[0]->device);
+  if (guard.status != INQB_OK) return guard.status;
+  auto* b = new inqb_batch();
+  b->cells.assign(cells, cells + ncells);
+  b->device = cells[0]->device;
+  for (int i = 0; i <= ncells; i++) {
+    cudaStream_t s;
+    cudaEvent_t e;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      for (auto x : b->streams) cudaStreamDestroy(x);
+      for (auto x : b->events) cudaEventDestroy(x);
+      delete b;
+      return fail(INQB_ERR_CUDA, "stream or event creation failed");
+    }
+    b->streams.push_back(s);
+    b->events.push_back(e);
+  }
+  *out = b;
+  return INQB_OK;
+}
+
+int inqb_batch_destroy(inqb_batch* b) {
+  if (!b) return INQB_OK;
+  DeviceGuard guard(b->device);
+  cudaDeviceSynchronize();
+  batch_release_graph(b);
+  for (auto x : b->streams) cudaStreamDestroy(x);
+  for (auto x : b->events) cudaEventDestroy(x);
+  delete b;
+  return INQB_OK;
+}
+
+int inqb_batch_apply_h(inqb_batch* b, const void* const* psis, void* const* hpsis, const int* Ms, const int* lds,
+                       void* stream) {
+  if (!b || !psis || !hpsis || !Ms || !lds) return fail(INQB_ERR_INVALID, "null batch argument");
+  const int n = (int)b->cells.size();
+  for (int i = 0; i < n; i++) {
+    INQB_TRY(check_block(b->cells[i], psis[i], Ms[i], lds[i]));
+    INQB_TRY(check_block(b->cells[i], hpsis[i], Ms[i], lds[i]));
+  }
+  DeviceGuard guard(b->device);
+  if (guard.status != INQB_OK) return guard.status;
+  bool same = b->exec != nullptr;
+  for (int i = 0; i < n && same; i++)
+    same = b->psis[i] == psis[i] && b->hpsis[i] == hpsis[i] && b->Ms[i] == Ms[i] && b->lds[i] == lds[i];
+  if (!same) {
+    // workspace, attributes and phases are set up outside the capture
+    for (int i = 0; i < n; i++) {
+      INQB_TRY(reserve(b->cells[i], Ms[i]));
+      if (!b->cells[i]->proj_phases_valid) {
+        INQB_TRY(update_phases(b->cells[i], nullptr));
+        b->cells[i]->proj_phases_valid = true;
+      }
+      const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+      INQB_TRY(apply(b->cells[i], LaunchArgs::H, psis[i], lds[i], hpsis[i], lds[i], Ms[i], nullptr, 0, one, zero,
+                     nullptr));
+    }
+    INQB_CUDA_TRY(cudaDeviceSynchronize());
+    INQB_TRY(batch_capture(b, psis, hpsis, Ms, lds));
+  }
+  INQB_CUDA_TRY(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+  return INQB_OK;
 }
 
 int inqb_axpby(inqb_ctx* ctx, int M, double a_re, double a_im, const void* x, int ldx, double b_re, double b_im,

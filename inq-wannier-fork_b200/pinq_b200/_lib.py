@@ -58,6 +58,11 @@ SIGNATURES = {
                                                      ctypes.c_double, _vp, _vp]),
     "inqb_accum_vector_potential_gradient": (ctypes.c_int, [_ctxp, _vp, _vp, ctypes.c_int, ctypes.c_int,
                                                             ctypes.c_double, ctypes.c_double, _vp, _vp]),
+    "inqb_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "inqb_batch_destroy": (ctypes.c_int, [_vp]),
+    "inqb_batch_apply_h": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), _ip,
+                                          _ip, _vp]),
     "inqb_timing_start": (ctypes.c_int, [_ctxp, ctypes.c_int]),
     "inqb_timing_stop": (ctypes.c_int, [_ctxp, _dp, _ip]),
 }
