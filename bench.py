@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--orbitals", type=int, default=128)
     ap.add_argument("--etrs-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample length")
+    ap.add_argument("--no-cells", dest="cells", action="store_false", help="skip the 16-cell batch measurement")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false", help="skip the adjoint measurement")
     return ap.parse_args()
 
 
@@ -205,6 +207,102 @@ def cpu_baseline(lattice, nr, pos, V, seconds, steps=None, warmup=0):
                       f"{n} applies ({total:.1f} s)"}, times
 
 
+def _timed_ms(fn, K, W):
+    import torch
+
+    for _ in range(W):
+        fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(K):
+        fn()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e)
+
+
+def bench_cells(args, local):
+    """cfg3: 16 uneven cells (grids 24..48^3, 8..64 orbitals, 2..16 atoms), mixed
+    precision; one CUDA graph (one branch per cell) against cell-by-cell launches."""
+    import torch
+
+    import pinq_b200 as pb
+    from pinq_b200 import systems
+
+    hams, xs, ys = [], [], []
+    for c in systems.cfg3_cells(seed=0):
+        h = pb.KSHamiltonian(c["lattice"], c["nr"], "mixed", device=local)
+        h.set_scalar_potential(systems.gaussian_potential(c["lattice"], c["nr"], c["positions"]))
+        h.set_gaussian_projectors(c["positions"])
+        h.reserve(c["M"])
+        x = torch.as_tensor(systems.random_orbitals(c["lattice"], c["nr"], c["M"], 25.0, c["seed"])).to(
+            "cuda", torch.complex64)
+        hams.append(h)
+        xs.append(x)
+        ys.append(torch.empty_like(x))
+    batch = pb.CellBatch(hams)
+    K = max(20, args.steps // 4)
+    ms_graph = _timed_ms(lambda: batch.apply(xs, ys), K, 3)
+
+    def seq():
+        for h, x, y in zip(hams, xs, ys):
+            h.apply(x, y)
+
+    ms_seq = _timed_ms(seq, K, 3)
+    norb = sum(x.shape[1] for x in xs)
+    return {"ncells": len(hams), "grids": [h.nr[0] for h in hams], "orbitals": norb, "steps": K,
+            "graph_orbital_applies_per_s": norb * K / (ms_graph * 1e-3),
+            "sequential_orbital_applies_per_s": norb * K / (ms_seq * 1e-3),
+            "graph_speedup": ms_seq / ms_graph, "precision": "mixed"}
+
+
+def bench_adjoint(args, local):
+    """cfg2: ETRS forward (200 steps, dt 0.05, 16 orbitals on the 32^3 / 8-atom cell,
+    checkpoints every 20) and its adjoint, FP64 and mixed; wall times of the
+    device-synchronised calls."""
+    import torch
+
+    import pinq_b200 as pb
+    from pinq_b200 import systems
+    from pinq_b200.adjoint import DipolePropagation
+
+    cfg = systems.config("cfg2")
+    out = {"config": "cfg2: a=10.26, 32^3, 8 atoms, 16 orbitals, dt=0.05, 200 steps, checkpoint every 20, "
+                     "Fourier sphere mask on", "steps": cfg["steps"]}
+    for precision in ("fp64", "mixed"):
+        h = pb.KSHamiltonian(cfg["lattice"], cfg["nr"], precision, device=local)
+        h.set_scalar_potential(cfg["V"])
+        h.set_gaussian_projectors(cfg["positions"])
+        h.set_fourier_sphere_mask(True)
+        dt = torch.complex128 if precision == "fp64" else torch.complex64
+        prop = DipolePropagation(h, torch.as_tensor(cfg["psi"]).to("cuda", dt), cfg["occ"], cfg["dt"],
+                                 cfg["checkpoint_every"])
+        prop.forward(cfg["amplitudes"], keep=True)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d = prop.forward(cfg["amplitudes"], keep=True)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        gA, gV = prop.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        out[precision] = {"dipole": d, "forward_s": t1 - t0, "backward_s": t2 - t1,
+                          "forward_steps_per_s": cfg["steps"] / (t1 - t0),
+                          "total_over_forward": (t2 - t0) / (t1 - t0),
+                          "grad_amplitudes_norm": float(gA.norm()), "grad_V_norm": float(gV.norm())}
+        out[precision]["_gA"] = gA.cpu().numpy()
+        out[precision]["_gV"] = gV.cpu().numpy()
+    g64, g32 = out["fp64"], out["mixed"]
+    out["mixed_vs_fp64"] = {
+        "dipole_rel": abs(g32["dipole"] - g64["dipole"]) / max(1e-300, abs(g64["dipole"])),
+        "grad_amplitudes_rel": float(np.linalg.norm(g32["_gA"] - g64["_gA"]) / np.linalg.norm(g64["_gA"])),
+        "grad_V_rel": float(np.linalg.norm(g32["_gV"] - g64["_gV"]) / np.linalg.norm(g64["_gV"]))}
+    for p in ("fp64", "mixed"):
+        del out[p]["_gA"], out[p]["_gV"]
+    return out
+
+
 def run_reference(args):
     world, rank, local = dist_setup(args.gpus)
     if rank != 0:
@@ -338,6 +436,9 @@ def run_ours(args):
     ms_e2e = max_over_ranks(dist, s2.elapsed_time(e2))
     wall_e2e = time.perf_counter() - t0
 
+    cells = bench_cells(args, local) if args.cells else None
+    adj = bench_adjoint(args, local) if args.adjoint else None
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -390,6 +491,10 @@ def run_ours(args):
                  "H_applies_per_step": 8, "dt": 0.05},
         "error": {"mixed_vs_fp64_gpu_rel_norm": err_fp64, "vs_oracle": err_oracle},
     }
+    if cells is not None:
+        line["cells"] = cells
+    if adj is not None:
+        line["adjoint"] = adj
     if world == 1:
         try:
             res, _ = cpu_baseline(lattice, nr, pos, V, seconds=args.cpu_seconds)
