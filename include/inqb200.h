@@ -153,6 +153,19 @@ int inqb_dipole(inqb_ctx* ctx, const double* rho, double out[3], void* stream);
 /* operations::orthogonalize (src/operations/orthogonalize.hpp:25-32): FP64
  * overlap S = dV psi^H psi, Cholesky S = U^H U, psi <- psi U^-1; synchronous. */
 int inqb_orthonormalize(inqb_ctx* ctx, void* psi, int M, int ld, void* stream);
+/* The same orthonormalisation without any device allocation (no counterpart in the
+ * reference).  inqb_orthonormalize allocates its M x M scratch on every call; this
+ * one uses a fixed array of 2 MiB compiled into the library, which every GPU that
+ * loads the library holds until the process exits.  It is for callers that may not
+ * call cudaMalloc: code running inside another framework's memory pool or allocator
+ * hooks, or a service whose device memory budget is fixed after start-up.
+ *   - M <= 256 orbitals; larger M returns INQB_ERR_UNSUPPORTED.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls on a device share the array: calls that overlap on the GPU (from
+ *     different streams or threads) race.  Each call clears what it accumulates.
+ *   - Synchronous, like inqb_orthonormalize; the context itself was created earlier. */
+int inqb_orthonormalize_noalloc(inqb_ctx* ctx, void* psi, int M, int ld, void* stream);
 
 /* ---------------------------------------------------------------- adjoint building blocks
  * The reverse-mode pieces of the ETRS step (the reference has no adjoint; these

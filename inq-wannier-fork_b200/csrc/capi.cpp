@@ -683,4 +683,11 @@ int inqb_accum_vector_potential_gradient(inqb_ctx* ctx, const void* u, const voi
                       stream);
 }
 
+int inqb_orthonormalize_noalloc(inqb_ctx* ctx, void* psi, int M, int ld, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  INQB_GUARD(ctx);
+  return orthonormalize_noalloc(ctx->precision, ctx->device, psi, ld, M, ctx->N, ctx->dV, stream);
+}
+
 }  // extern "C"

@@ -7,6 +7,8 @@
 // Input orbitals may be complex64 (mixed) or complex128; every sum is FP64.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "dft.cuh"
 #include "inqb_internal.h"
 #include "observables.h"
@@ -258,6 +260,44 @@ int launch_orthonormalize(int precision, void* psi, long ld, int M, long N, doub
   return precision == INQB_FP64
              ? orthonormalize_impl<double>(psi, ld, M, N, dV, S, X, info, (cudaStream_t)stream)
              : orthonormalize_impl<float>(psi, ld, M, N, dV, S, X, info, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------- orthonormalisation without allocation
+// The same kernels as launch_orthonormalize, with their scratch (overlap S, inverse
+// factor X, pivot status) taken from a fixed array in device memory rather than from
+// cudaMalloc, for callers that may not allocate device memory.
+namespace {
+constexpr size_t kNoAllocMat = (size_t)kOrthoNoAllocMaxStates * kOrthoNoAllocMaxStates;
+// S (M x M) | X (M x M) | status: 2 MiB plus a little, held by every GPU that loads
+// the library until the process exits.  All calls on a device share it.
+static __device__ __align__(256) double2 g_orth_scratch[2 * kNoAllocMat + 16];
+std::mutex g_orth_scratch_mutex;
+double2* g_orth_scratch_ptr[64] = {};
+}  // namespace
+
+int orthonormalize_noalloc(int precision, int device, void* psi, long ld, int M, long N, double dV, void* stream) {
+  if (M > kOrthoNoAllocMaxStates)
+    return fail(INQB_ERR_UNSUPPORTED, "allocation-free orthonormalisation takes at most " +
+                                          std::to_string(kOrthoNoAllocMaxStates) + " orbitals, got " +
+                                          std::to_string(M));
+  if (device < 0 || device >= 64) return fail(INQB_ERR_INVALID, "device index out of range");
+  double2* base = nullptr;
+  {
+    // once per device, with that device current: the device address of the array
+    std::lock_guard<std::mutex> lock(g_orth_scratch_mutex);
+    if (!g_orth_scratch_ptr[device]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_orth_scratch);
+      if (e != cudaSuccess)
+        return fail(INQB_ERR_CUDA, std::string("cudaGetSymbolAddress of the orthonormalisation scratch: ") +
+                                       cudaGetErrorString(e));
+      g_orth_scratch_ptr[device] = static_cast<double2*>(p);
+    }
+    base = g_orth_scratch_ptr[device];
+  }
+  // launch_orthonormalize zeroes S and the status before accumulating into them
+  return launch_orthonormalize(precision, psi, ld, M, N, dV, base, base + kNoAllocMat,
+                               reinterpret_cast<int*>(base + 2 * kNoAllocMat), stream);
 }
 
 }  // namespace inqb

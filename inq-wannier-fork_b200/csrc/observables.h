@@ -10,5 +10,8 @@ int launch_density(int precision, const void* psi, long ld, int M, long N, const
 int launch_dipole(const double* rho, long N, const double lat[3][3], const int nr[3], double* out_dev, void* stream);
 int launch_orthonormalize(int precision, void* psi, long ld, int M, long N, double dV, double2* S, double2* X,
                           int* info, void* stream);
+// Largest orbital count of the allocation-free orthonormalisation (fixed device scratch).
+constexpr int kOrthoNoAllocMaxStates = 256;
+int orthonormalize_noalloc(int precision, int device, void* psi, long ld, int M, long N, double dV, void* stream);
 
 }  // namespace inqb

@@ -50,6 +50,7 @@ SIGNATURES = {
     "inqb_density": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "inqb_dipole": (ctypes.c_int, [_ctxp, _vp, _dp, _vp]),
     "inqb_orthonormalize": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "inqb_orthonormalize_noalloc": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "inqb_axpby": (ctypes.c_int, [_ctxp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int,
                                   ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int, _vp]),
     "inqb_position_scale": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
