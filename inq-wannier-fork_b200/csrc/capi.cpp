@@ -1,6 +1,7 @@
 // extern "C" entry points of libinqb200 (declared in include/inqb200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -54,13 +55,15 @@ ProjView<T> proj_view(inqb_ctx* ctx) {
   const ProjTables& t = ctx->proj;
   v.nproj = t.nproj;
   v.L = t.L;
+  v.max_plane_atoms = t.max_plane_atoms;
   v.seg_ptr = t.d_seg_ptr.as<int>();
   v.seg_atom = t.d_seg_atom.as<int>();
   v.seg_ent = t.d_seg_ent.as<int>();
   v.ent_off = t.d_ent_off.as<int>();
   v.ent_atom = t.d_ent_atom.as<int>();
-  v.pt_ptr = t.d_pt_ptr.as<int>();
-  v.pt_ent = t.d_pt_ent.as<int>();
+  v.seg_local = t.d_seg_local.as<int>();
+  v.plane_ptr = t.d_plane_ptr.as<int>();
+  v.plane_atom = t.d_plane_atom.as<int>();
   v.ent_beta = t.d_ent_beta.as<T>();
   v.ent_phase = t.d_ent_phase.ptr;
   v.scale = t.d_scale.as<double>();
@@ -78,9 +81,9 @@ int check_block(const inqb_ctx* ctx, const void* a, int M, long ld) {
 }
 
 int reserve(inqb_ctx* ctx, int M) {
-  const int G = ctx->plan->G;
-  const size_t groups = (size_t)(M + G - 1) / G;
-  INQB_TRY(ctx->d_tmp.ensure(groups * G * (size_t)ctx->N * ctx->elem_bytes()));
+  const int G = ctx->plan->G, Gt = ctx->plan->G_tile;
+  const size_t padded = std::max((size_t)(M + G - 1) / G * G, (size_t)(M + Gt - 1) / Gt * Gt);
+  INQB_TRY(ctx->d_tmp.ensure(padded * (size_t)ctx->N * ctx->elem_bytes()));
   if (ctx->proj.nproj > 0) INQB_TRY(ctx->d_projacc.ensure(sizeof(double2) * (size_t)ctx->proj.nproj * ctx->proj.L * M));
   return INQB_OK;
 }

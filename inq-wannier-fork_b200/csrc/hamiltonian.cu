@@ -18,6 +18,7 @@
 // as the reference's scatter does (src/hamiltonian/projector_all.hpp:220-232).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <map>
 #include <tuple>
@@ -156,115 +157,11 @@ __device__ __forceinline__ void store_group(cplx<T>* __restrict__ dst, const cpl
   }
 }
 
-// ---------------------------------------------------------------- projection (pass 1)
-// Sum over the sphere entries of plane ix:  proj[a][l][m] += scale[a][l] *
-// sum_e beta_e[l] exp(+i (k+A).r_e) psi(r_e)[m]   (projector_all.hpp:104-165).
-template <typename T, int G, typename PG>
-__device__ __forceinline__ void project_plane(const cplx<T>* S, int ix, int m0, int gcount, int M,
-                                              const ProjView<T>& pj) {
-  using AZ = typename PG::AZ;
-  constexpr int NZ = AZ::N;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int s0 = pj.seg_ptr[ix], s1 = pj.seg_ptr[ix + 1];
-  const cplx<T>* phase = (const cplx<T>*)pj.ent_phase;
-  for (int s = s0 + warp; s < s1; s += nw) {
-    const int a = pj.seg_atom[s];
-    const int e0 = pj.seg_ent[s], e1 = pj.seg_ent[s + 1];
-    cplx<T> acc[LMAX][G];
-#pragma unroll
-    for (int l = 0; l < LMAX; ++l)
-#pragma unroll
-      for (int j = 0; j < G; ++j) acc[l][j] = mk<T>(0, 0);
-    for (int e = e0 + lane; e < e1; e += 32) {
-      const int off = pj.ent_off[e];
-      const int sl = (off / NZ) * PG::ZP + AZ::slot(off % NZ);
-      const cplx<T> ph = phase[e];
-      T b[LMAX];
-#pragma unroll
-      for (int l = 0; l < LMAX; ++l) b[l] = (l < pj.L) ? pj.ent_beta[(long)e * pj.L + l] : (T)0;
-#pragma unroll
-      for (int j = 0; j < G; ++j) {
-        cplx<T> x = ph * S[j * PG::PLANE + sl];
-#pragma unroll
-        for (int l = 0; l < LMAX; ++l) {
-          acc[l][j].x = fma(b[l], x.x, acc[l][j].x);
-          acc[l][j].y = fma(b[l], x.y, acc[l][j].y);
-        }
-      }
-    }
-#pragma unroll
-    for (int l = 0; l < LMAX; ++l)
-#pragma unroll
-      for (int j = 0; j < G; ++j)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          acc[l][j].x += __shfl_xor_sync(0xffffffffu, acc[l][j].x, o);
-          acc[l][j].y += __shfl_xor_sync(0xffffffffu, acc[l][j].y, o);
-        }
-#pragma unroll
-    for (int l = 0; l < LMAX; ++l)
-#pragma unroll
-      for (int j = 0; j < G; ++j) {
-        if (lane == ((l * G + j) & 31) && l < pj.L && j < gcount) {
-          const double sc = pj.scale[a * pj.L + l];
-          double2* dst = &pj.proj[((long)a * pj.L + l) * M + m0 + j];
-          atomicAdd(&dst->x, sc * (double)acc[l][j].x);
-          atomicAdd(&dst->y, sc * (double)acc[l][j].y);
-        }
-      }
-  }
-}
+}  // namespace inqb
 
-// Nonlocal scatter of plane ix into the real-space tile (pass 3):
-// S(r_e) += conj(exp(i (k+A).r_e)) sum_l beta_e[l] proj[a][l][m]
-// (projector_all.hpp:182-232).  One warp per atom segment; the atom's
-// projections are read once; shared-memory atomics merge overlapping spheres.
-template <typename T, int G, typename PG>
-__device__ __forceinline__ void nonlocal_plane(cplx<T>* S, int ix, int m0, int gcount, int M,
-                                               const ProjView<T>& pj) {
-  using AY = typename PG::AY;
-  using AZ = typename PG::AZ;
-  constexpr int NZ = AZ::N;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int s0 = pj.seg_ptr[ix], s1 = pj.seg_ptr[ix + 1];
-  const cplx<T>* phase = (const cplx<T>*)pj.ent_phase;
-  for (int s = s0 + warp; s < s1; s += nw) {
-    const int a = pj.seg_atom[s];
-    const int e0 = pj.seg_ent[s], e1 = pj.seg_ent[s + 1];
-    cplx<T> P[LMAX][G];
-#pragma unroll
-    for (int l = 0; l < LMAX; ++l)
-#pragma unroll
-      for (int j = 0; j < G; ++j) {
-        P[l][j] = mk<T>(0, 0);
-        if (l < pj.L && j < gcount) {
-          const double2 pr = pj.proj[((long)a * pj.L + l) * M + m0 + j];
-          P[l][j] = mk<T>((T)pr.x, (T)pr.y);
-        }
-      }
-    for (int e = e0 + lane; e < e1; e += 32) {
-      const int off = pj.ent_off[e];
-      const int iy = off / NZ, iz = off - iy * NZ;
-      const int sl = AY::slot_of_freq(iy) * PG::ZP + AZ::slot_of_freq(iz);
-      const cplx<T> ph = phase[e];
-      T b[LMAX];
-#pragma unroll
-      for (int l = 0; l < LMAX; ++l) b[l] = (l < pj.L) ? pj.ent_beta[(long)e * pj.L + l] : (T)0;
-#pragma unroll
-      for (int j = 0; j < G; ++j) {
-        cplx<T> t = mk<T>(0, 0);
-#pragma unroll
-        for (int l = 0; l < LMAX; ++l) {
-          t.x = fma(b[l], P[l][j].x, t.x);
-          t.y = fma(b[l], P[l][j].y, t.y);
-        }
-        const cplx<T> c = mul_conj(t, ph);
-        atomicAdd(&S[j * PG::PLANE + sl].x, c.x);
-        atomicAdd(&S[j * PG::PLANE + sl].y, c.y);
-      }
-    }
-  }
-}
+#include "tiles.cuh"
+
+namespace inqb {
 
 // ---------------------------------------------------------------- pass 1: plane forward
 // do_proj = 1: H apply (projection on); 0: plain forward FFT.
@@ -312,10 +209,6 @@ __global__ void __launch_bounds__(PlaneGeom<T, NY, NZ>::THREADS)
     }
   }
   __syncthreads();
-  if (do_proj && pj.nproj > 0) {
-    project_plane<T, G, PG>(S, ix, m0, gcount, M, pj);
-    __syncthreads();
-  }
   // z lines: (j, iy), contiguous
   step1<AZ, false>(S, G * NY * AZ::N2, twz, [](int it, int& base, int& es, int& j2) {
     j2 = it % AZ::N2;
@@ -606,10 +499,6 @@ __global__ void __launch_bounds__(PlaneGeom<T, NY, NZ>::THREADS)
     });
     __syncthreads();
   }
-  if (MODE_H && pj.nproj > 0) {
-    nonlocal_plane<T, G, PG>(S, ix, m0, gcount, M, pj);
-    __syncthreads();
-  }
 
   const long pbase = (long)ix * NYZ;
   constexpr int BE = 4;  // points per batch in the epilogue
@@ -692,8 +581,6 @@ static int launch_h_impl(const LaunchArgs& a) {
   if (dev < 64 && !attr_done[dev]) {
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_plane_fwd<T, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)PG::SMEM));
-    INQB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inv<T, NY, NZ, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)PG::SMEM));
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_plane_inv<T, NY, NZ, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)PG::SMEM));
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_line_x<T, NX, G, K::CX, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -734,14 +621,30 @@ static int launch_h_impl(const LaunchArgs& a) {
   const dim3 gplane(groups, NX);
   const dim3 gline((NY * NZ + K::CX - 1) / K::CX, groups);
   if (a.mode == LaunchArgs::H) {
+    using TG = TileGeom<T, NX, NY, NZ>;
+    constexpr int GT = TG::G;
+    static bool tile_attr_done[64] = {};
+    if (dev < 64 && !tile_attr_done[dev]) {
+      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_fwd<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)TG::smem_fwd(kAccAtomsMax)));
+      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)TG::SMEM_X));
+      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_inv<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)TG::SMEM_INV));
+      tile_attr_done[dev] = true;
+    }
+    const int tgroups = (a.M + GT - 1) / GT;
+    // 16-byte vectors of G orbitals: full groups, aligned pointers and leading dimensions
+    const int tvin = aligned16(a.in, a.ld_in, esz);
+    const int tvout = tvin && aligned16(a.out, a.ld_out, esz);
+    const int acc_cap = pj.nproj > 0 ? std::min(pj.max_plane_atoms, kAccAtomsMax) : 0;
     if (pj.nproj > 0)
       INQB_CUDA_TRY(cudaMemsetAsync(pj.proj, 0, sizeof(double2) * (size_t)pj.nproj * pj.L * a.M, st));
     if (a.events[0]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[0], st));
-    k_plane_fwd<T, NY, NZ><<<gplane, PG::THREADS, PG::SMEM, st>>>((const cplx<T>*)a.in, a.ld_in, a.M, tmp, NX, twy,
-                                                                 twz, pj, 1, vin);
+    k_tile_fwd<T, NX, NY, NZ><<<dim3(tgroups, NX), TG::THREADS, TG::smem_fwd(acc_cap), st>>>(
+        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pj, acc_cap, tvin);
     if (a.events[1]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[1], st));
-    k_line_x<T, NX, G, K::CX, 0><<<gline, K::LINE_THREADS, K::line_smem, st>>>(tmp, nullptr, nullptr, 0, a.M, NY, NZ,
-                                                                        twx, kp, 1);
+    k_tile_x<T, NX, NY, NZ><<<dim3(TG::Y2 * NZ, tgroups), TG::THREADS, TG::SMEM_X, st>>>(tmp, twx, kp);
     if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
     EpiParams<T> ep;
     ep.V = (const T*)a.V;
@@ -750,8 +653,8 @@ static int launch_h_impl(const LaunchArgs& a) {
     ep.ld_base = a.ld_base;
     ep.alpha = mk<T>((T)a.alpha[0], (T)a.alpha[1]);
     ep.beta = mk<T>((T)a.beta[0], (T)a.beta[1]);
-    k_plane_inv<T, NY, NZ, 1><<<gplane, PG::THREADS, PG::SMEM, st>>>(
-        tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, NX, twy, twz, pj, ep, vout);
+    k_tile_inv<T, NX, NY, NZ><<<dim3(tgroups, NX * TG::Y1), TG::THREADS, TG::SMEM_INV, st>>>(
+        tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, tvout);
     if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
   } else if (a.mode == LaunchArgs::FFT_FWD) {
     k_plane_fwd<T, NY, NZ><<<gplane, PG::THREADS, PG::SMEM, st>>>((const cplx<T>*)a.in, a.ld_in, a.M, tmp, NX, twy,
@@ -789,6 +692,7 @@ static Plan make_plan() {
   using K = Kernels<T, NX, NY, NZ>;
   Plan p;
   p.G = K::G;
+  p.G_tile = TileGeom<T, NX, NY, NZ>::G;
   p.launch = &launch_h_impl<T, NX, NY, NZ>;
   return p;
 }

@@ -74,8 +74,12 @@ struct DevBuf {
 struct ProjTables {
   int nproj = 0, L = 0;
   int nent = 0, nseg = 0;
-  // host copies
-  std::vector<int> seg_ptr, seg_atom, seg_ent, ent_off, ent_atom, pt_ptr, pt_ent;
+  int y1 = 1;               // row classes per x-plane (tiles per plane)
+  int max_plane_atoms = 0;  // most atoms whose spheres cut one x-plane
+  // host copies.  Tile (ix, y1) holds rows y = y1 + Y1 * r of plane ix; seg_ptr
+  // [NX * Y1 + 1] lists its atom segments (seg_atom, seg_ent range, seg_local =
+  // the atom's index among the atoms of plane ix, plane_ptr / plane_atom).
+  std::vector<int> seg_ptr, seg_atom, seg_ent, seg_local, plane_ptr, plane_atom, ent_off, ent_atom;
   std::vector<double> ent_beta;     // [nent][L]
   std::vector<float> ent_relpos;    // [nent][3] contravariant, float as the reference stores it
   std::vector<double> scale;        // [nproj][L] = dV * kb coefficient
@@ -83,7 +87,7 @@ struct ProjTables {
   std::vector<int> atom_ptr, atom_ent, ent_pt;  // [nproj+1], [nent], [nent] linear grid point
   std::vector<double> ent_xyz;      // [nent][3] cartesian relative position
   // device copies
-  DevBuf d_seg_ptr, d_seg_atom, d_seg_ent, d_ent_off, d_ent_atom, d_pt_ptr, d_pt_ent;
+  DevBuf d_seg_ptr, d_seg_atom, d_seg_ent, d_seg_local, d_plane_ptr, d_plane_atom, d_ent_off, d_ent_atom;
   DevBuf d_ent_beta;                // [nent][L] in the context precision
   DevBuf d_ent_relpos;              // [nent][3] float
   DevBuf d_ent_phase;               // [nent] complex, exp(+i (k+A).r), context precision
@@ -94,14 +98,15 @@ struct ProjTables {
 // Kernel view of the projector tables (T = float or double).
 template <typename T>
 struct ProjView {
-  int nproj, L;
-  const int* seg_ptr;
+  int nproj, L, max_plane_atoms;
+  const int* seg_ptr;     // [NX * Y1 + 1] segments of tile (ix, y1)
   const int* seg_atom;
-  const int* seg_ent;
-  const int* ent_off;
+  const int* seg_ent;     // [nseg + 1] entry ranges
+  const int* seg_local;   // plane-local atom index of a segment
+  const int* plane_ptr;   // [NX + 1] atoms of plane ix
+  const int* plane_atom;
+  const int* ent_off;     // tile-local (row * NZ + z)
   const int* ent_atom;
-  const int* pt_ptr;
-  const int* pt_ent;
   const T* ent_beta;
   const void* ent_phase;  // cplx<T>*
   const double* scale;

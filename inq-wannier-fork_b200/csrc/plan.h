@@ -11,7 +11,7 @@ struct LaunchArgs {
   void* out = nullptr;
   long ld_out = 0;
   int M = 0;
-  void* tmp = nullptr;              // Fourier workspace, [groups][N][G]
+  void* tmp = nullptr;              // Fourier workspace, [groups][N][G] rounded up for both tilings
   const void* tw = nullptr;         // twiddles x | y | z
   const void* proj_view = nullptr;  // ProjView<T>*
   const void* V = nullptr;          // [N] local potential (T)
@@ -27,7 +27,8 @@ struct LaunchArgs {
 };
 
 struct Plan {
-  int G = 1;  // orbitals per tile
+  int G = 1;       // orbitals per tile of the plain FFT kernels
+  int G_tile = 1;  // orbitals per tile of the H kernels
   int (*launch)(const LaunchArgs&) = nullptr;
 };
 

@@ -214,8 +214,13 @@ int build_proj_tables(const inqb_ctx& ctx, int nproj, int L, int smax, const int
   const int nx = ctx.nr[0], ny = ctx.nr[1], nz = ctx.nr[2];
   t.nproj = nproj;
   t.L = L;
-  // bucket entries by plane, keeping (atom, point) order inside a plane
-  std::vector<std::vector<std::pair<int, int>>> by_plane(nx);
+  // The H kernels tile plane ix into Y1 row classes: tile (ix, y1) holds the rows
+  // y = y1 + Y1 * r, r = 0..NY/Y1-1, where NY = Y2 * Y1 is the four-step split of
+  // the y axis.  Entries are bucketed by tile, keeping (atom, point) order inside.
+  int y2n = 0, y1n = 0;
+  if (split_of(ny, &y2n, &y1n) != INQB_OK) return fail(INQB_ERR_UNSUPPORTED, "unsupported y grid size");
+  const int ntile = nx * y1n;
+  std::vector<std::vector<std::pair<int, int>>> by_tile(ntile);
   long total = 0;
   for (int a = 0; a < nproj; a++) {
     if (counts[a] < 0 || counts[a] > smax) return fail(INQB_ERR_INVALID, "sphere count out of range");
@@ -223,59 +228,71 @@ int build_proj_tables(const inqb_ctx& ctx, int nproj, int L, int smax, const int
       const int* c = coords + ((long)a * smax + p) * 3;
       if (c[0] < 0 || c[0] >= nx || c[1] < 0 || c[1] >= ny || c[2] < 0 || c[2] >= nz)
         return fail(INQB_ERR_INVALID, "sphere point outside the grid");
-      by_plane[c[0]].push_back({a, p});
+      by_tile[c[0] * y1n + c[1] % y1n].push_back({a, p});
       total++;
     }
   }
   if (total > 0x7fffffff) return fail(INQB_ERR_UNSUPPORTED, "too many sphere points");
   t.nent = (int)total;
-  t.seg_ptr.assign(nx + 1, 0);
+  t.y1 = y1n;
+  t.seg_ptr.assign(ntile + 1, 0);
   t.seg_atom.clear();
   t.seg_ent.clear();
+  t.seg_local.clear();
+  t.plane_ptr.assign(nx + 1, 0);
+  t.plane_atom.clear();
   t.ent_off.resize(total);
   t.ent_atom.resize(total);
   t.ent_beta.resize(total * L);
   t.ent_relpos.resize(total * 3);
+  t.max_plane_atoms = 0;
+  std::vector<int> local_of(nproj, -1);
   int e = 0;
   for (int ix = 0; ix < nx; ix++) {
-    t.seg_ptr[ix] = (int)t.seg_atom.size();
-    int cur = -1;
-    for (auto [a, p] : by_plane[ix]) {
-      if (a != cur) {
-        t.seg_atom.push_back(a);
-        t.seg_ent.push_back(e);
-        cur = a;
+    // atoms of plane ix in increasing order: the plane-local accumulator index
+    t.plane_ptr[ix] = (int)t.plane_atom.size();
+    std::vector<char> in_plane(nproj, 0);
+    for (int y1 = 0; y1 < y1n; y1++)
+      for (auto [a, p] : by_tile[ix * y1n + y1]) in_plane[a] = 1;
+    for (int a = 0; a < nproj; a++)
+      if (in_plane[a]) {
+        local_of[a] = (int)t.plane_atom.size() - t.plane_ptr[ix];
+        t.plane_atom.push_back(a);
       }
-      const int* c = coords + ((long)a * smax + p) * 3;
-      t.ent_off[e] = c[1] * nz + c[2];
-      t.ent_atom[e] = a;
-      for (int l = 0; l < L; l++) t.ent_beta[(long)e * L + l] = beta[((long)a * L + l) * smax + p];
-      for (int d = 0; d < 3; d++) t.ent_relpos[(long)e * 3 + d] = relpos[((long)a * smax + p) * 3 + d];
-      e++;
+    t.max_plane_atoms = std::max(t.max_plane_atoms, (int)t.plane_atom.size() - t.plane_ptr[ix]);
+    for (int y1 = 0; y1 < y1n; y1++) {
+      const int tile = ix * y1n + y1;
+      t.seg_ptr[tile] = (int)t.seg_atom.size();
+      int cur = -1;
+      for (auto [a, p] : by_tile[tile]) {
+        if (a != cur) {
+          t.seg_atom.push_back(a);
+          t.seg_ent.push_back(e);
+          t.seg_local.push_back(local_of[a]);
+          cur = a;
+        }
+        const int* c = coords + ((long)a * smax + p) * 3;
+        t.ent_off[e] = (c[1] / y1n) * nz + c[2];  // tile-local row, z
+        t.ent_atom[e] = a;
+        for (int l = 0; l < L; l++) t.ent_beta[(long)e * L + l] = beta[((long)a * L + l) * smax + p];
+        for (int d = 0; d < 3; d++) t.ent_relpos[(long)e * 3 + d] = relpos[((long)a * smax + p) * 3 + d];
+        e++;
+      }
     }
   }
-  t.seg_ptr[nx] = (int)t.seg_atom.size();
+  t.seg_ptr[ntile] = (int)t.seg_atom.size();
+  t.plane_ptr[nx] = (int)t.plane_atom.size();
   t.seg_ent.push_back(e);
   t.nseg = (int)t.seg_atom.size();
-  // per-point lists for the owner-computes scatter
-  const long N = ctx.N;
-  t.pt_ptr.assign(N + 1, 0);
+  // grid point of every entry, in entry order
   std::vector<long> pt_of(total);
   {
     int ee = 0;
-    for (int ix = 0; ix < nx; ix++)
-      for (auto [a, p] : by_plane[ix]) {
+    for (int tile = 0; tile < ntile; tile++)
+      for (auto [a, p] : by_tile[tile]) {
         const int* c = coords + ((long)a * smax + p) * 3;
         pt_of[ee++] = ((long)c[0] * ny + c[1]) * nz + c[2];
       }
-  }
-  for (long i = 0; i < total; i++) t.pt_ptr[pt_of[i] + 1]++;
-  for (long p = 0; p < N; p++) t.pt_ptr[p + 1] += t.pt_ptr[p];
-  t.pt_ent.assign(total, 0);
-  {
-    std::vector<int> fill(t.pt_ptr.begin(), t.pt_ptr.end() - 1);
-    // order inside a point: by atom then sphere point, i.e. plane-bucket order
-    for (long i = 0; i < total; i++) t.pt_ent[fill[pt_of[i]]++] = (int)i;
   }
   // atom-major entry lists, grid points and cartesian relative positions
   t.ent_pt.resize(total);
@@ -313,8 +330,9 @@ int upload_proj_tables(const inqb_ctx& ctx, ProjTables& t) {
   INQB_TRY(upload(t.d_seg_ent, t.seg_ent));
   INQB_TRY(upload(t.d_ent_off, t.ent_off));
   INQB_TRY(upload(t.d_ent_atom, t.ent_atom));
-  INQB_TRY(upload(t.d_pt_ptr, t.pt_ptr));
-  INQB_TRY(upload(t.d_pt_ent, t.pt_ent));
+  INQB_TRY(upload(t.d_seg_local, t.seg_local));
+  INQB_TRY(upload(t.d_plane_ptr, t.plane_ptr));
+  INQB_TRY(upload(t.d_plane_atom, t.plane_atom));
   INQB_TRY(upload(t.d_ent_relpos, t.ent_relpos));
   INQB_TRY(upload(t.d_scale, t.scale));
   INQB_TRY(upload(t.d_atom_ptr, t.atom_ptr));

@@ -1,0 +1,470 @@
+// Six-step tiles of H|psi> (src/hamiltonian/ks_hamiltonian.hpp:132-152).
+//
+// The y axis is split NY = Y2 * Y1 (the four-step split of the size table):
+// y = y1 + Y1 * y2 and ky = ka + Y2 * kb.  Then
+//   X[ka + Y2 kb] = sum_y1 w_Y1^{y1 kb} [ w_NY^{y1 ka} sum_y2 w_Y2^{y2 ka} x[y1 + Y1 y2] ]
+// so a tile (x-plane ix, row class y1) of Y2 rows x NZ points finishes the z
+// transform and the inner y stage on its own, and the outer y stage lands in
+// the x-line pass.  Every tile moves whole 64-byte runs of G orbitals per grid
+// point (G = 8 complex64 or 4 complex128), so the orbital-fastest layout
+// [point][orbital] is read and written in full sectors.
+//
+//   pass A  k_tile_fwd  CTA (group, ix), loops over y1: psi rows -> KB projection
+//           (plane accumulators in shared memory, flushed once per plane) ->
+//           z FFT -> inner y stage -> tmp[g][ka][kz][ix][y1][G]
+//   pass B  k_tile_x    CTA (ka, kz, group): contiguous [ix][y1][G] block ->
+//           outer y stage -> x FFT -> 1/2 |G + k + A|^2 / N -> inverse x ->
+//           inverse outer y stage, in place
+//   pass C  k_tile_inv  CTA (group, ix, y1): inverse inner y stage -> inverse z
+//           -> nonlocal scatter -> alpha (K + V + V_nl) psi + beta base
+#pragma once
+
+#include "fft_tile.cuh"
+
+namespace inqb {
+
+// ---------------------------------------------------------------- cp.async
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
+
+// ---------------------------------------------------------------- geometry
+template <typename T, int NX, int NY, int NZ>
+struct TileGeom {
+  static constexpr int G = 64 / (int)sizeof(cplx<T>);  // orbitals per tile: one 64-byte run
+  static constexpr int PV = 16 / (int)sizeof(cplx<T>);  // complex values per 16-byte vector
+  static constexpr int VP = G / PV;                      // 16-byte vectors per point
+  using AX = Axis<Split<NX>::N1, Split<NX>::N2>;
+  using AY = Axis<Split<NY>::N1, Split<NY>::N2>;
+  using AZ = Axis<Split<NZ>::N1, Split<NZ>::N2>;
+  static constexpr int Y2 = AY::N1;  // rows per tile
+  static constexpr int Y1 = AY::N2;  // tiles per x-plane
+  static constexpr int ZS = AZ::SLOTS;  // padded z slots per row
+  static constexpr int TILE = Y2 * ZS * G;  // complex values of a tile in shared memory
+  static constexpr int PTS = Y2 * NZ;       // grid points of a tile
+  static constexpr int XS = (Y1 + 1) * G;   // x-slot stride of the x-line block (one point of padding)
+  static constexpr int XBLK = AX::SLOTS * XS;
+  static constexpr int BLK = NX * Y1 * G;   // complex values of one tmp block [ix][y1][G]
+  static constexpr int THREADS = 256;
+  static constexpr size_t smem_fwd(int acc_atoms) {
+    return sizeof(cplx<T>) * ((size_t)TILE + NY + NZ) + sizeof(double2) * (size_t)acc_atoms * LMAX * G;
+  }
+  static constexpr size_t SMEM_X = sizeof(cplx<T>) * ((size_t)XBLK + NX);
+  static constexpr size_t SMEM_INV = sizeof(cplx<T>) * ((size_t)TILE + (size_t)PTS * G + NY + NZ);
+};
+
+// Plane accumulators held in shared memory by pass A; atoms beyond this many per
+// plane accumulate straight into global memory.
+constexpr int kAccAtomsMax = 48;
+
+// ---------------------------------------------------------------- pass A
+template <typename T, int NX, int NY, int NZ>
+__global__ void __launch_bounds__(256)
+    k_tile_fwd(const cplx<T>* __restrict__ in, long ld, int M, cplx<T>* __restrict__ tmp,
+               const cplx<T>* __restrict__ tw_y, const cplx<T>* __restrict__ tw_z, ProjView<T> pj, int acc_cap,
+               int vec) {
+  using TG = TileGeom<T, NX, NY, NZ>;
+  using AZ = typename TG::AZ;
+  constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, ZS = TG::ZS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* twy = S + TG::TILE;
+  cplx<T>* twz = twy + NY;
+  double2* acc = reinterpret_cast<double2*>(twz + NZ);  // [acc_cap][LMAX][G]
+
+  const int grp = blockIdx.x, ix = blockIdx.y;
+  const int m0 = grp * G;
+  const int gcount = min(G, M - m0);
+  const bool v16 = vec && gcount == G;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const bool proj_on = pj.nproj > 0;
+  for (int i = threadIdx.x; i < NY; i += blockDim.x) twy[i] = tw_y[i];
+  for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = tw_z[i];
+  if (proj_on)
+    for (int i = threadIdx.x; i < acc_cap * LMAX * G; i += blockDim.x) acc[i] = make_double2(0.0, 0.0);
+
+  for (int y1 = 0; y1 < Y1; ++y1) {
+    // -- rows y1 + Y1 r of plane ix, G orbitals per point
+    if (v16) {
+      for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
+        const int v = q % VP, pt = q / VP;
+        const int z = pt % NZ, r = pt / NZ;
+        const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
+        cp_async16(S + (r * ZS + AZ::slot(z)) * G + v * PV, in + p * ld + m0 + v * PV);
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+    } else {
+      for (int q = threadIdx.x; q < TG::PTS * G; q += blockDim.x) {
+        const int j = q % G, pt = q / G;
+        const int z = pt % NZ, r = pt / NZ;
+        const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
+        S[(r * ZS + AZ::slot(z)) * G + j] = (j < gcount) ? in[p * ld + m0 + j] : mk<T>(0, 0);
+      }
+    }
+    __syncthreads();
+
+    // -- KB projection of the tile (projector_all.hpp:104-165): warp per atom
+    // segment, lanes = (orbital j, entry sub-lane)
+    if (proj_on) {
+      constexpr int ESUB = 32 / G;
+      const int j = lane % G, es = lane / G;
+      const cplx<T>* phase = (const cplx<T>*)pj.ent_phase;
+      const int tile = ix * Y1 + y1;
+      const int s0 = pj.seg_ptr[tile], s1 = pj.seg_ptr[tile + 1];
+      for (int s = s0 + warp; s < s1; s += nw) {
+        const int e0 = pj.seg_ent[s], e1 = pj.seg_ent[s + 1];
+        cplx<T> a[LMAX];
+#pragma unroll
+        for (int l = 0; l < LMAX; ++l) a[l] = mk<T>(0, 0);
+        for (int e = e0 + es; e < e1; e += ESUB) {
+          const int off = pj.ent_off[e];
+          const int r = off / NZ, z = off - r * NZ;
+          const cplx<T> x = phase[e] * S[(r * ZS + AZ::slot(z)) * G + j];
+#pragma unroll
+          for (int l = 0; l < LMAX; ++l) {
+            const T b = (l < pj.L) ? pj.ent_beta[(long)e * pj.L + l] : (T)0;
+            a[l].x = fma(b, x.x, a[l].x);
+            a[l].y = fma(b, x.y, a[l].y);
+          }
+        }
+#pragma unroll
+        for (int o = G; o < 32; o <<= 1)
+#pragma unroll
+          for (int l = 0; l < LMAX; ++l) {
+            a[l].x += __shfl_xor_sync(0xffffffffu, a[l].x, o);
+            a[l].y += __shfl_xor_sync(0xffffffffu, a[l].y, o);
+          }
+        if (es == 0 && j < gcount) {
+          const int sl = pj.seg_local[s];
+          if (sl < acc_cap) {
+            // one segment per atom in a tile, tiles separated by barriers: no race
+#pragma unroll
+            for (int l = 0; l < LMAX; ++l) {
+              double2& d = acc[(sl * LMAX + l) * G + j];
+              d.x += (double)a[l].x;
+              d.y += (double)a[l].y;
+            }
+          } else {
+            const int at = pj.seg_atom[s];
+#pragma unroll
+            for (int l = 0; l < LMAX; ++l) {
+              if (l >= pj.L) break;
+              const double sc = pj.scale[at * pj.L + l];
+              double2* dst = &pj.proj[((long)at * pj.L + l) * M + m0 + j];
+              atomicAdd(&dst->x, sc * (double)a[l].x);
+              atomicAdd(&dst->y, sc * (double)a[l].y);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+
+    // -- z lines: (r, j), element stride G
+    step1<AZ, false>(S, Y2 * G * AZ::N2, twz, [](int it, int& base, int& es, int& j2) {
+      const int j = it % G, rest = it / G;
+      j2 = rest % AZ::N2;
+      base = (rest / AZ::N2) * ZS * G + j;
+      es = G;
+    });
+    __syncthreads();
+    step2<AZ, false>(S, Y2 * G * AZ::N1, [](int it, int& base, int& es, int& k1) {
+      const int j = it % G, rest = it / G;
+      k1 = rest % AZ::N1;
+      base = (rest / AZ::N1) * ZS * G + j;
+      es = G;
+    });
+    __syncthreads();
+
+    // -- inner y stage: DFT_Y2 over the rows, twiddle w_NY^{y1 ka}
+    for (int it = threadIdx.x; it < NZ * G; it += blockDim.x) {
+      const int j = it % G, zi = it / G;
+      const int base = AZ::slot(zi) * G + j;
+      cplx<T> u[Y2];
+#pragma unroll
+      for (int r = 0; r < Y2; ++r) u[r] = S[base + r * ZS * G];
+      DFT<Y2, false, T>::run(u);
+#pragma unroll
+      for (int ka = 1; ka < Y2; ++ka) u[ka] = u[ka] * twy[ka * Y1 + y1];
+#pragma unroll
+      for (int ka = 0; ka < Y2; ++ka) S[base + ka * ZS * G] = u[ka];
+    }
+    __syncthreads();
+
+    // -- store (ka, kz) runs of G orbitals to tmp[g][ka][kz][ix][y1][G]
+    for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
+      const int v = q % VP, pt = q / VP;
+      const int kz = pt % NZ, ka = pt / NZ;
+      const float4 w = *reinterpret_cast<const float4*>(S + (ka * ZS + AZ::slot_of_freq(kz)) * G + v * PV);
+      cplx<T>* dst = tmp + (((long)(grp * Y2 + ka) * NZ + kz) * NX + ix) * (Y1 * G) + y1 * G + v * PV;
+      *reinterpret_cast<float4*>(dst) = w;
+    }
+    __syncthreads();
+  }
+
+  // -- flush the plane accumulators: proj[a][l][m] += dV ekb * sum
+  if (proj_on) {
+    const int a0 = pj.plane_ptr[ix];
+    const int na = min(pj.plane_ptr[ix + 1] - a0, acc_cap);
+    for (int i = threadIdx.x; i < na * LMAX * G; i += blockDim.x) {
+      const int j = i % G, l = (i / G) % LMAX, sl = i / (G * LMAX);
+      if (l >= pj.L || j >= gcount) continue;
+      const int at = pj.plane_atom[a0 + sl];
+      const double sc = pj.scale[at * pj.L + l];
+      const double2 v = acc[i];
+      double2* dst = &pj.proj[((long)at * pj.L + l) * M + m0 + j];
+      atomicAdd(&dst->x, sc * v.x);
+      atomicAdd(&dst->y, sc * v.y);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- pass B
+// One contiguous block tmp[g][ka][kz] = [ix][y1][G]; in shared memory the x
+// index goes to padded slots of stride XS and (y1, j) stays contiguous.
+template <typename T, int NX, int NY, int NZ>
+__global__ void __launch_bounds__(256)
+    k_tile_x(cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ tw_x, KinParams<T> kp) {
+  using TG = TileGeom<T, NX, NY, NZ>;
+  using AX = typename TG::AX;
+  constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, XS = TG::XS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* X = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* twx = X + TG::XBLK;
+
+  const int kz = blockIdx.x % NZ, ka = blockIdx.x / NZ, grp = blockIdx.y;
+  cplx<T>* blk = tmp + ((long)(grp * Y2 + ka) * NZ + kz) * TG::BLK;
+  for (int q = threadIdx.x; q < NX * Y1 * VP; q += blockDim.x) {
+    const int v = q % VP, r = q / VP;
+    const int y1 = r % Y1, ix = r / Y1;
+    cp_async16(X + AX::slot(ix) * XS + y1 * G + v * PV, blk + (long)q * PV);
+  }
+  cp_async_commit();
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) twx[i] = tw_x[i];
+  cp_async_wait<0>();
+  __syncthreads();
+
+  // outer y stage: DFT_Y1 over y1 -> kb, for each (ix, j)
+  for (int it = threadIdx.x; it < NX * G; it += blockDim.x) {
+    const int j = it % G, ix = it / G;
+    const int base = AX::slot(ix) * XS + j;
+    cplx<T> u[Y1];
+#pragma unroll
+    for (int y = 0; y < Y1; ++y) u[y] = X[base + y * G];
+    DFT<Y1, false, T>::run(u);
+#pragma unroll
+    for (int y = 0; y < Y1; ++y) X[base + y * G] = u[y];
+  }
+  __syncthreads();
+
+  auto map1 = [](int it, int& base, int& es, int& j2) {
+    const int j = it % G, rest = it / G;
+    j2 = rest % AX::N2;
+    base = (rest / AX::N2) * G + j;
+    es = XS;
+  };
+  auto map2 = [](int it, int& base, int& es, int& k1) {
+    const int j = it % G, rest = it / G;
+    k1 = rest % AX::N1;
+    base = (rest / AX::N1) * G + j;
+    es = XS;
+  };
+  const int n2 = sym_freq(kz, NZ);
+  step1<AX, false>(X, Y1 * G * AX::N2, twx, map1);
+  __syncthreads();
+  step2_fwd_op_inv<AX>(X, Y1 * G * AX::N1, twx, map2, [&](int it, int kx, cplx<T> v) {
+    const int kb = (it / G) / AX::N1;
+    const int n0 = sym_freq(kx, NX), n1 = sym_freq(ka + Y2 * kb, NY);
+    T k = kinetic(kp, n0, n1, n2);
+    if (kp.mask) k = outside_sphere(kp.nr, n0, n1, n2) ? (T)0 : k - kp.shift;
+    return k * v;
+  });
+  __syncthreads();
+  step1_inv_transposed<AX>(X, Y1 * G * AX::N2, map1);
+  __syncthreads();
+
+  // inverse outer y stage: kb -> y1
+  for (int it = threadIdx.x; it < NX * G; it += blockDim.x) {
+    const int j = it % G, ix = it / G;
+    const int base = AX::slot(ix) * XS + j;
+    cplx<T> u[Y1];
+#pragma unroll
+    for (int y = 0; y < Y1; ++y) u[y] = X[base + y * G];
+    DFT<Y1, true, T>::run(u);
+#pragma unroll
+    for (int y = 0; y < Y1; ++y) X[base + y * G] = u[y];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < NX * Y1 * VP; q += blockDim.x) {
+    const int v = q % VP, r = q / VP;
+    const int y1 = r % Y1, ix = r / Y1;
+    *reinterpret_cast<float4*>(blk + (long)q * PV) =
+        *reinterpret_cast<const float4*>(X + AX::slot(ix) * XS + y1 * G + v * PV);
+  }
+}
+
+// ---------------------------------------------------------------- pass C
+// The input orbitals of the tile (for V psi) are fetched into shared memory
+// with cp.async at the start, so that read overlaps the inverse transforms.
+template <typename T, int NX, int NY, int NZ>
+__global__ void __launch_bounds__(256)
+    k_tile_inv(const cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ in, long ld_in,
+               cplx<T>* __restrict__ out, long ld_out, int M, const cplx<T>* __restrict__ tw_y,
+               const cplx<T>* __restrict__ tw_z, ProjView<T> pj, EpiParams<T> ep, int vec) {
+  using TG = TileGeom<T, NX, NY, NZ>;
+  using AZ = typename TG::AZ;
+  constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, ZS = TG::ZS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* P = S + TG::TILE;  // [PTS][G] input orbitals of the tile
+  cplx<T>* twy = P + TG::PTS * G;
+  cplx<T>* twz = twy + NY;
+
+  const int grp = blockIdx.x, ix = blockIdx.y / Y1, y1 = blockIdx.y % Y1;
+  const int m0 = grp * G;
+  const int gcount = min(G, M - m0);
+  const bool v16 = vec && gcount == G;
+
+  // group 0: the (ka, kz) runs of this tile; group 1: the input orbitals
+  for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
+    const int v = q % VP, pt = q / VP;
+    const int kz = pt % NZ, ka = pt / NZ;
+    cp_async16(S + (ka * ZS + AZ::slot(kz)) * G + v * PV,
+               tmp + (((long)(grp * Y2 + ka) * NZ + kz) * NX + ix) * (Y1 * G) + y1 * G + v * PV);
+  }
+  cp_async_commit();
+  if (v16) {
+    for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
+      const int v = q % VP, pt = q / VP;
+      const int z = pt % NZ, r = pt / NZ;
+      const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
+      cp_async16(P + pt * G + v * PV, in + p * ld_in + m0 + v * PV);
+    }
+  }
+  cp_async_commit();
+  for (int i = threadIdx.x; i < NY; i += blockDim.x) twy[i] = tw_y[i];
+  for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = tw_z[i];
+  cp_async_wait<1>();
+  __syncthreads();
+
+  // inverse inner y stage: conj twiddle, inverse DFT_Y2 over ka -> rows
+  for (int it = threadIdx.x; it < NZ * G; it += blockDim.x) {
+    const int j = it % G, zi = it / G;
+    const int base = AZ::slot(zi) * G + j;
+    cplx<T> u[Y2];
+#pragma unroll
+    for (int ka = 0; ka < Y2; ++ka) u[ka] = S[base + ka * ZS * G];
+#pragma unroll
+    for (int ka = 1; ka < Y2; ++ka) u[ka] = mul_conj(u[ka], twy[ka * Y1 + y1]);
+    DFT<Y2, true, T>::run(u);
+#pragma unroll
+    for (int r = 0; r < Y2; ++r) S[base + r * ZS * G] = u[r];
+  }
+  __syncthreads();
+  // inverse z from natural order: element z ends in slot_of_freq(z)
+  step1<AZ, true>(S, Y2 * G * AZ::N2, twz, [](int it, int& base, int& es, int& j2) {
+    const int j = it % G, rest = it / G;
+    j2 = rest % AZ::N2;
+    base = (rest / AZ::N2) * ZS * G + j;
+    es = G;
+  });
+  __syncthreads();
+  step2<AZ, true>(S, Y2 * G * AZ::N1, [](int it, int& base, int& es, int& k1) {
+    const int j = it % G, rest = it / G;
+    k1 = rest % AZ::N1;
+    base = (rest / AZ::N1) * ZS * G + j;
+    es = G;
+  });
+  __syncthreads();
+
+  // nonlocal scatter (projector_all.hpp:182-232): warp per atom segment, lanes =
+  // (orbital j, entry sub-lane); shared-memory atomics merge overlapping spheres
+  if (pj.nproj > 0) {
+    constexpr int ESUB = 32 / G;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int j = lane % G, es = lane / G;
+    const cplx<T>* phase = (const cplx<T>*)pj.ent_phase;
+    const int tile = ix * Y1 + y1;
+    const int s0 = pj.seg_ptr[tile], s1 = pj.seg_ptr[tile + 1];
+    for (int s = s0 + warp; s < s1; s += nw) {
+      const int at = pj.seg_atom[s];
+      const int e0 = pj.seg_ent[s], e1 = pj.seg_ent[s + 1];
+      cplx<T> pr[LMAX];
+#pragma unroll
+      for (int l = 0; l < LMAX; ++l) {
+        pr[l] = mk<T>(0, 0);
+        if (l < pj.L && j < gcount) {
+          const double2 d = pj.proj[((long)at * pj.L + l) * M + m0 + j];
+          pr[l] = mk<T>((T)d.x, (T)d.y);
+        }
+      }
+      for (int e = e0 + es; e < e1; e += ESUB) {
+        const int off = pj.ent_off[e];
+        const int r = off / NZ, z = off - r * NZ;
+        cplx<T> t = mk<T>(0, 0);
+#pragma unroll
+        for (int l = 0; l < LMAX; ++l) {
+          const T b = (l < pj.L) ? pj.ent_beta[(long)e * pj.L + l] : (T)0;
+          t.x = fma(b, pr[l].x, t.x);
+          t.y = fma(b, pr[l].y, t.y);
+        }
+        const cplx<T> c = mul_conj(t, phase[e]);
+        cplx<T>* dst = S + (r * ZS + AZ::slot_of_freq(z)) * G + j;
+        atomicAdd(&dst->x, c.x);
+        atomicAdd(&dst->y, c.y);
+      }
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+
+  // epilogue: out = alpha (K psi + (V + vshift) psi + V_nl psi) + beta base
+  for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
+    const int v = q % VP, pt = q / VP;
+    const int z = pt % NZ, r = pt / NZ;
+    const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
+    const int sl = (r * ZS + AZ::slot_of_freq(z)) * G + v * PV;
+    const T vp = ep.V[p] + ep.vshift;
+    cplx<T> h[PV], x[PV], b[PV];
+#pragma unroll
+    for (int k = 0; k < PV; ++k) h[k] = S[sl + k];
+    const int jb = v * PV;
+    if (v16) {
+#pragma unroll
+      for (int k = 0; k < PV; ++k) x[k] = P[pt * G + jb + k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < PV; ++k) x[k] = (jb + k < gcount) ? in[p * ld_in + m0 + jb + k] : mk<T>(0, 0);
+    }
+    if (ep.base) {
+#pragma unroll
+      for (int k = 0; k < PV; ++k)
+        b[k] = (jb + k < gcount) ? ep.base[p * ep.ld_base + m0 + jb + k] : mk<T>(0, 0);
+    }
+#pragma unroll
+    for (int k = 0; k < PV; ++k) {
+      h[k].x = fma(vp, x[k].x, h[k].x);
+      h[k].y = fma(vp, x[k].y, h[k].y);
+      h[k] = ep.alpha * h[k];
+      if (ep.base) h[k] = h[k] + ep.beta * b[k];
+    }
+    if (v16) {
+      float4 w;
+      memcpy(&w, h, 16);
+      *reinterpret_cast<float4*>(out + p * ld_out + m0 + jb) = w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < PV; ++k)
+        if (jb + k < gcount) out[p * ld_out + m0 + jb + k] = h[k];
+    }
+  }
+}
+
+}  // namespace inqb
