@@ -448,12 +448,16 @@ def run_ours(args):
     b = 8  # bytes per complex64
     bT = 4
     L = 4
+    rec = 32  # bytes of one sphere-entry record (phase, L radial values, offset, segment)
     alg = {  # algorithmic bytes per launch
-        "plane_fwd": 2 * N * M * b + nent * (L * bT + b + 4),
-        "line_x": 2 * N * M * b,
-        "plane_inv": 3 * N * M * b + N * bT + 4 * (N + 1) + nent * (4 + 4 + L * bT + b),
+        # orbitals in, Fourier tiles out, the entry records once
+        "tile_fwd": 2 * N * M * b + nent * rec,
+        # Fourier tiles in and out
+        "tile_x": 2 * N * M * b,
+        # Fourier tiles and orbitals in, H psi out, V, the records and the per-point index once
+        "tile_inv": 3 * N * M * b + N * bT + nent * rec + 4 * N,
     }
-    per_launch_ms = {k: pass_ms[i] / max(1, napplies) for i, k in enumerate(["plane_fwd", "line_x", "plane_inv"])}
+    per_launch_ms = {k: pass_ms[i] / max(1, napplies) for i, k in enumerate(["tile_fwd", "tile_x", "tile_inv"])}
     kernels = {}
     traffic = profiled_traffic()
     for k in alg:

@@ -193,8 +193,9 @@ int inqb_accum_vector_potential_gradient(inqb_ctx* ctx, const void* u, const voi
  * on the stream the kernels run on; the counterpart of INQ's scoped timers
  * (CALI_CXX_MARK_SCOPE, src/utils/profiling.hpp:12, external_libs/kalimotxo/cali.h).
  * inqb_timing_stop waits for the recorded events and returns the summed
- * milliseconds of the three passes (plane forward + projection, x lines +
- * kinetic, plane inverse + potential/nonlocal epilogue). */
+ * milliseconds of the three passes (z and inner y transforms + projection,
+ * outer y and x transforms + kinetic, inverse transforms + potential/nonlocal
+ * epilogue). */
 int inqb_timing_start(inqb_ctx* ctx, int max_applies);
 int inqb_timing_stop(inqb_ctx* ctx, double ms_per_pass[3], int* napplies);
 

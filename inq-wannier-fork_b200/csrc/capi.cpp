@@ -56,6 +56,12 @@ ProjView<T> proj_view(inqb_ctx* ctx) {
   v.nproj = t.nproj;
   v.L = t.L;
   v.max_plane_atoms = t.max_plane_atoms;
+  v.max_tile_ent = t.max_tile_ent;
+  v.max_tile_seg = t.max_tile_seg;
+  v.pt_stride = t.pt_stride;
+  v.ent_rec = t.d_ent_rec.as<EntRec<T>>();
+  v.ent_rec_pt = t.d_ent_rec_pt.as<EntRec<T>>();
+  v.pt_ptr = t.d_pt_ptr.as<int>();
   v.seg_ptr = t.d_seg_ptr.as<int>();
   v.seg_atom = t.d_seg_atom.as<int>();
   v.seg_ent = t.d_seg_ent.as<int>();
@@ -91,7 +97,8 @@ int reserve(inqb_ctx* ctx, int M) {
 int update_phases(inqb_ctx* ctx, void* stream) {
   if (ctx->proj.nproj == 0 || ctx->proj.nent == 0) return INQB_OK;
   return launch_phases(ctx->precision, ctx->proj.nent, ctx->proj.d_ent_relpos.as<float>(), ctx->kA_cov,
-                       ctx->proj.d_ent_phase.ptr, stream);
+                       ctx->proj.d_ent_phase.ptr, ctx->proj.d_ent_rec.ptr, ctx->proj.d_ent_rec_pt.ptr,
+                       ctx->proj.d_pt_pos.as<int>(), stream);
 }
 
 int set_kA(inqb_ctx* ctx, const double kA[3], void* stream) {

@@ -544,13 +544,18 @@ __global__ void __launch_bounds__(PlaneGeom<T, NY, NZ>::THREADS)
 // ---------------------------------------------------------------- phases
 template <typename T>
 __global__ void k_phases(int nent, const float* __restrict__ relpos, double k0, double k1, double k2,
-                         cplx<T>* __restrict__ phase) {
+                         cplx<T>* __restrict__ phase, EntRec<T>* __restrict__ rec, EntRec<T>* __restrict__ rec_pt,
+                         const int* __restrict__ pt_pos) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nent) return;
   const double th = k0 * (double)relpos[3 * e] + k1 * (double)relpos[3 * e + 1] + k2 * (double)relpos[3 * e + 2];
   double s, c;
   sincos(th, &s, &c);
   phase[e] = mk<T>((T)c, (T)s);
+  rec[e].ph[0] = (T)c;
+  rec[e].ph[1] = (T)s;
+  rec_pt[pt_pos[e]].ph[0] = (T)c;
+  rec_pt[pt_pos[e]].ph[1] = (T)s;
 }
 
 // ---------------------------------------------------------------- plan instantiation
@@ -626,11 +631,11 @@ static int launch_h_impl(const LaunchArgs& a) {
     static bool tile_attr_done[64] = {};
     if (dev < 64 && !tile_attr_done[dev]) {
       INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_fwd<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)TG::smem_fwd(kAccAtomsMax)));
+                                         (int)TG::smem_fwd(kAccAtomsMax, kRecCapMax)));
       INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)TG::SMEM_X));
       INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_inv<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)TG::SMEM_INV));
+                                         (int)TG::smem_inv(kRecCapMax, kAccAtomsMax)));
       tile_attr_done[dev] = true;
     }
     const int tgroups = (a.M + GT - 1) / GT;
@@ -638,11 +643,15 @@ static int launch_h_impl(const LaunchArgs& a) {
     const int tvin = aligned16(a.in, a.ld_in, esz);
     const int tvout = tvin && aligned16(a.out, a.ld_out, esz);
     const int acc_cap = pj.nproj > 0 ? std::min(pj.max_plane_atoms, kAccAtomsMax) : 0;
+    const int rec_cap = pj.nproj > 0 ? std::min(pj.max_tile_ent, kRecCapMax) : 0;
+    const int seg_cap = pj.nproj > 0 ? std::min(pj.max_tile_seg, kAccAtomsMax) : 0;
+    if (pj.nproj > 0 && pj.pt_stride != TG::PSTRIDE)
+      return fail(INQB_ERR_INVALID, "projector tables were built for another tiling of this grid");
     if (pj.nproj > 0)
       INQB_CUDA_TRY(cudaMemsetAsync(pj.proj, 0, sizeof(double2) * (size_t)pj.nproj * pj.L * a.M, st));
     if (a.events[0]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[0], st));
-    k_tile_fwd<T, NX, NY, NZ><<<dim3(tgroups, NX), TG::THREADS, TG::smem_fwd(acc_cap), st>>>(
-        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pj, acc_cap, tvin);
+    k_tile_fwd<T, NX, NY, NZ><<<dim3(tgroups, NX * TG::YSPLIT), TG::THREADS, TG::smem_fwd(acc_cap, rec_cap), st>>>(
+        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pj, acc_cap, rec_cap, tvin);
     if (a.events[1]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[1], st));
     k_tile_x<T, NX, NY, NZ><<<dim3(TG::Y2 * NZ, tgroups), TG::THREADS, TG::SMEM_X, st>>>(tmp, twx, kp);
     if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
@@ -653,8 +662,9 @@ static int launch_h_impl(const LaunchArgs& a) {
     ep.ld_base = a.ld_base;
     ep.alpha = mk<T>((T)a.alpha[0], (T)a.alpha[1]);
     ep.beta = mk<T>((T)a.beta[0], (T)a.beta[1]);
-    k_tile_inv<T, NX, NY, NZ><<<dim3(tgroups, NX * TG::Y1), TG::THREADS, TG::SMEM_INV, st>>>(
-        tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, tvout);
+    k_tile_inv<T, NX, NY, NZ><<<dim3(tgroups, NX * TG::Y1), TG::THREADS, TG::smem_inv(rec_cap, seg_cap), st>>>(
+        tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap, seg_cap,
+        tvout);
     if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
   } else if (a.mode == LaunchArgs::FFT_FWD) {
     k_plane_fwd<T, NY, NZ><<<gplane, PG::THREADS, PG::SMEM, st>>>((const cplx<T>*)a.in, a.ld_in, a.M, tmp, NX, twy,
@@ -673,17 +683,19 @@ static int launch_h_impl(const LaunchArgs& a) {
 }
 
 template <typename T>
-static int launch_phases_impl(int nent, const float* relpos, const double kA[3], void* phase, void* stream) {
+static int launch_phases_impl(int nent, const float* relpos, const double kA[3], void* phase, void* rec,
+                              void* rec_pt, const int* pt_pos, void* stream) {
   if (nent == 0) return INQB_OK;
-  k_phases<T><<<(nent + 255) / 256, 256, 0, (cudaStream_t)stream>>>(nent, relpos, kA[0], kA[1], kA[2],
-                                                                   (cplx<T>*)phase);
+  k_phases<T><<<(nent + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+      nent, relpos, kA[0], kA[1], kA[2], (cplx<T>*)phase, (EntRec<T>*)rec, (EntRec<T>*)rec_pt, pt_pos);
   INQB_CUDA_TRY(cudaGetLastError());
   return INQB_OK;
 }
 
-int launch_phases(int precision, int nent, const float* relpos, const double kA[3], void* phase, void* stream) {
-  return precision == INQB_FP64 ? launch_phases_impl<double>(nent, relpos, kA, phase, stream)
-                                : launch_phases_impl<float>(nent, relpos, kA, phase, stream);
+int launch_phases(int precision, int nent, const float* relpos, const double kA[3], void* phase, void* rec,
+                  void* rec_pt, const int* pt_pos, void* stream) {
+  return precision == INQB_FP64 ? launch_phases_impl<double>(nent, relpos, kA, phase, rec, rec_pt, pt_pos, stream)
+                                : launch_phases_impl<float>(nent, relpos, kA, phase, rec, rec_pt, pt_pos, stream);
 }
 
 // ---------------------------------------------------------------- registry

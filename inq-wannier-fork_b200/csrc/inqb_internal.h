@@ -69,6 +69,17 @@ struct DevBuf {
   P* as() const { return reinterpret_cast<P*>(ptr); }
 };
 
+// One sphere entry as the H tiles read it: exp(+i (k+A).r), the KB radial values
+// (zero past L) and the tile-local offset (row * NZ + z), padded to whole
+// 16-byte vectors so a tile's run of entries is copied with cp.async.
+template <typename T>
+struct alignas(16) EntRec {
+  T ph[2];
+  T beta[4];
+  int off;
+  int tseg;  // segment index within the tile (its atom's slot in the tile's projections)
+};
+
 // Projector tables in the layout the fused H kernels read (built on the host
 // from projector_all-style per-atom sphere tables, then uploaded).
 struct ProjTables {
@@ -76,6 +87,10 @@ struct ProjTables {
   int nent = 0, nseg = 0;
   int y1 = 1;               // row classes per x-plane (tiles per plane)
   int max_plane_atoms = 0;  // most atoms whose spheres cut one x-plane
+  int max_tile_ent = 0;     // most sphere entries in one tile
+  int max_tile_seg = 0;     // most atom segments in one tile
+  int tile_pts = 0;         // grid points of a tile (NY / Y1 rows x NZ)
+  int pt_stride = 0;        // tile stride of pt_ptr: tile_pts + 1 rounded up to 4
   // host copies.  Tile (ix, y1) holds rows y = y1 + Y1 * r of plane ix; seg_ptr
   // [NX * Y1 + 1] lists its atom segments (seg_atom, seg_ent range, seg_local =
   // the atom's index among the atoms of plane ix, plane_ptr / plane_atom).
@@ -91,6 +106,12 @@ struct ProjTables {
   DevBuf d_ent_beta;                // [nent][L] in the context precision
   DevBuf d_ent_relpos;              // [nent][3] float
   DevBuf d_ent_phase;               // [nent] complex, exp(+i (k+A).r), context precision
+  DevBuf d_ent_rec;                 // [nent] EntRec<T>, phases filled with d_ent_phase
+  // the same records in point order inside each tile (for the owner-computes
+  // nonlocal scatter): rec_pt[pt_pos[e]] is entry e; pt_ptr[tile * pt_stride + q]
+  // is the first record of tile-local point q relative to the tile's first entry
+  std::vector<int> pt_pos, pt_ptr;
+  DevBuf d_ent_rec_pt, d_pt_pos, d_pt_ptr;
   DevBuf d_scale;                   // [nproj][L] double
   DevBuf d_atom_ptr, d_atom_ent, d_ent_pt, d_ent_xyz;
 };
@@ -98,7 +119,7 @@ struct ProjTables {
 // Kernel view of the projector tables (T = float or double).
 template <typename T>
 struct ProjView {
-  int nproj, L, max_plane_atoms;
+  int nproj, L, max_plane_atoms, max_tile_ent, max_tile_seg, pt_stride;
   const int* seg_ptr;     // [NX * Y1 + 1] segments of tile (ix, y1)
   const int* seg_atom;
   const int* seg_ent;     // [nseg + 1] entry ranges
@@ -109,6 +130,9 @@ struct ProjView {
   const int* ent_atom;
   const T* ent_beta;
   const void* ent_phase;  // cplx<T>*
+  const EntRec<T>* ent_rec;     // segment (atom) order
+  const EntRec<T>* ent_rec_pt;  // point order inside each tile
+  const int* pt_ptr;            // [tiles][pt_stride]
   const double* scale;
   double2* proj;          // [nproj][L][M] accumulators (FP64 in both precisions)
 };

@@ -284,6 +284,25 @@ int build_proj_tables(const inqb_ctx& ctx, int nproj, int L, int smax, const int
   t.plane_ptr[nx] = (int)t.plane_atom.size();
   t.seg_ent.push_back(e);
   t.nseg = (int)t.seg_atom.size();
+  t.max_tile_ent = 0;
+  t.max_tile_seg = 0;
+  for (int tile = 0; tile < ntile; tile++) {
+    t.max_tile_ent = std::max(t.max_tile_ent, (int)by_tile[tile].size());
+    t.max_tile_seg = std::max(t.max_tile_seg, t.seg_ptr[tile + 1] - t.seg_ptr[tile]);
+  }
+  // point order inside each tile: stable sort of the tile's entries by offset
+  t.tile_pts = y2n * nz;
+  t.pt_stride = (t.tile_pts + 1 + 3) / 4 * 4;
+  t.pt_pos.assign(total, 0);
+  t.pt_ptr.assign((size_t)ntile * t.pt_stride, 0);
+  for (int tile = 0; tile < ntile; tile++) {
+    const int e0 = t.seg_ent[t.seg_ptr[tile]], e1 = t.seg_ent[t.seg_ptr[tile + 1]];
+    int* tp = &t.pt_ptr[(size_t)tile * t.pt_stride];
+    for (int e = e0; e < e1; e++) tp[t.ent_off[e] + 1]++;
+    for (int q = 0; q < t.tile_pts; q++) tp[q + 1] += tp[q];
+    std::vector<int> fill(tp, tp + t.tile_pts);
+    for (int e = e0; e < e1; e++) t.pt_pos[e] = e0 + fill[t.ent_off[e]]++;
+  }
   // grid point of every entry, in entry order
   std::vector<long> pt_of(total);
   {
@@ -324,6 +343,23 @@ static int upload(DevBuf& b, const std::vector<T>& v) {
   return INQB_OK;
 }
 
+// Entry records with zero phases (the phase kernel fills them for each k + A).
+// point_order: record e goes to pt_pos[e] instead of e.
+template <typename T>
+static std::vector<EntRec<T>> ent_records(const ProjTables& t, bool point_order = false) {
+  std::vector<EntRec<T>> rec((size_t)t.nent);
+  for (int tile = 0; tile + 1 < (int)t.seg_ptr.size(); tile++)
+    for (int s = t.seg_ptr[tile]; s < t.seg_ptr[tile + 1]; s++)
+      for (int e = t.seg_ent[s]; e < t.seg_ent[s + 1]; e++) {
+        EntRec<T>& r = rec[point_order ? t.pt_pos[e] : e];
+        r.ph[0] = r.ph[1] = (T)0;
+        for (int l = 0; l < 4; l++) r.beta[l] = (l < t.L) ? (T)t.ent_beta[(size_t)e * t.L + l] : (T)0;
+        r.off = t.ent_off[e];
+        r.tseg = s - t.seg_ptr[tile];
+      }
+  return rec;
+}
+
 int upload_proj_tables(const inqb_ctx& ctx, ProjTables& t) {
   INQB_TRY(upload(t.d_seg_ptr, t.seg_ptr));
   INQB_TRY(upload(t.d_seg_atom, t.seg_atom));
@@ -346,6 +382,15 @@ int upload_proj_tables(const inqb_ctx& ctx, ProjTables& t) {
     INQB_TRY(upload(t.d_ent_beta, bf));
   }
   INQB_TRY(t.d_ent_phase.ensure(std::max<size_t>((size_t)t.nent * ctx.elem_bytes(), 16)));
+  if (ctx.precision == INQB_FP64) {
+    INQB_TRY(upload(t.d_ent_rec, ent_records<double>(t)));
+    INQB_TRY(upload(t.d_ent_rec_pt, ent_records<double>(t, true)));
+  } else {
+    INQB_TRY(upload(t.d_ent_rec, ent_records<float>(t)));
+    INQB_TRY(upload(t.d_ent_rec_pt, ent_records<float>(t, true)));
+  }
+  INQB_TRY(upload(t.d_pt_pos, t.pt_pos));
+  INQB_TRY(upload(t.d_pt_ptr, t.pt_ptr));
   return INQB_OK;
 }
 

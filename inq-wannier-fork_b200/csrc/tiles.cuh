@@ -9,8 +9,9 @@
 // point (G = 8 complex64 or 4 complex128), so the orbital-fastest layout
 // [point][orbital] is read and written in full sectors.
 //
-//   pass A  k_tile_fwd  CTA (group, ix), loops over y1: psi rows -> KB projection
-//           (plane accumulators in shared memory, flushed once per plane) ->
+//   pass A  k_tile_fwd  CTA (group, ix, half of the y1 classes), loops over y1: psi
+//           rows -> KB projection (plane accumulators in shared memory, flushed
+//           once per CTA) ->
 //           z FFT -> inner y stage -> tmp[g][ka][kz][ix][y1][G]
 //   pass B  k_tile_x    CTA (ka, kz, group): contiguous [ix][y1][G] block ->
 //           outer y stage -> x FFT -> 1/2 |G + k + A|^2 / N -> inverse x ->
@@ -52,23 +53,63 @@ struct TileGeom {
   static constexpr int XBLK = AX::SLOTS * XS;
   static constexpr int BLK = NX * Y1 * G;   // complex values of one tmp block [ix][y1][G]
   static constexpr int THREADS = 256;
-  static constexpr size_t smem_fwd(int acc_atoms) {
-    return sizeof(cplx<T>) * ((size_t)TILE + NY + NZ) + sizeof(double2) * (size_t)acc_atoms * LMAX * G;
+  static constexpr size_t smem_fwd(int acc_atoms, int rec_cap) {
+    return sizeof(cplx<T>) * ((size_t)TILE + NY + NZ) + sizeof(double2) * (size_t)acc_atoms * LMAX * G +
+           sizeof(EntRec<T>) * (size_t)rec_cap;
   }
   static constexpr size_t SMEM_X = sizeof(cplx<T>) * ((size_t)XBLK + NX);
-  static constexpr size_t SMEM_INV = sizeof(cplx<T>) * ((size_t)TILE + (size_t)PTS * G + NY + NZ);
+  static constexpr int PSTRIDE = (PTS + 1 + 3) / 4 * 4;  // ints of a tile's point index
+  // pass C prefetches the input orbitals of its tile into shared memory in FP64
+  // (two CTAs per SM either way, so the copy overlaps the transforms for free);
+  // in FP32 the smaller footprint buys a third CTA per SM instead.
+  static constexpr bool PREFETCH = sizeof(T) == 8;
+  static constexpr size_t smem_inv(int rec_cap, int seg_cap) {
+    return sizeof(cplx<T>) * ((size_t)TILE + (PREFETCH ? (size_t)PTS * G : 0) + NY + NZ) +
+           sizeof(EntRec<T>) * (size_t)rec_cap + sizeof(int) * (size_t)PSTRIDE +
+           sizeof(cplx<T>) * (size_t)seg_cap * LMAX * G;
+  }
+  // pass A: each CTA takes Y1 / YSPLIT row classes of one plane
+  static constexpr int YSPLIT = (Y1 % 2 == 0) ? 2 : 1;
 };
+
+// Entry records staged in shared memory per tile; a tile with more entries
+// reads its records from global memory.
+constexpr int kRecCapMax = 1024;
+
+// Start the cp.async copy of tile `tile`'s entry records (from `recs`) into R
+// (cap records).  Returns the records to index with (e - roff): R when staged,
+// else global memory.
+template <typename T>
+__device__ __forceinline__ const EntRec<T>* stage_entries(const ProjView<T>& pj, const EntRec<T>* recs, int tile,
+                                                          int cap, EntRec<T>* R, int& roff) {
+  const int e0 = pj.seg_ent[pj.seg_ptr[tile]], e1 = pj.seg_ent[pj.seg_ptr[tile + 1]];
+  if (e1 - e0 > cap) {
+    roff = 0;
+    return recs;
+  }
+  constexpr int V = (int)(sizeof(EntRec<T>) / 16);
+  const float4* src = reinterpret_cast<const float4*>(recs + e0);
+  float4* dst = reinterpret_cast<float4*>(R);
+  for (int q = threadIdx.x; q < (e1 - e0) * V; q += blockDim.x) cp_async16(dst + q, src + q);
+  roff = e0;
+  return R;
+}
 
 // Plane accumulators held in shared memory by pass A; atoms beyond this many per
 // plane accumulate straight into global memory.
 constexpr int kAccAtomsMax = 48;
+
+template <typename T>
+__device__ __forceinline__ int roff_base(const ProjView<T>& pj, int s0, bool on) {
+  return on ? pj.seg_ent[s0] : 0;
+}
 
 // ---------------------------------------------------------------- pass A
 template <typename T, int NX, int NY, int NZ>
 __global__ void __launch_bounds__(256)
     k_tile_fwd(const cplx<T>* __restrict__ in, long ld, int M, cplx<T>* __restrict__ tmp,
                const cplx<T>* __restrict__ tw_y, const cplx<T>* __restrict__ tw_z, ProjView<T> pj, int acc_cap,
-               int vec) {
+               int rec_cap, int vec) {
   using TG = TileGeom<T, NX, NY, NZ>;
   using AZ = typename TG::AZ;
   constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, ZS = TG::ZS;
@@ -77,8 +118,10 @@ __global__ void __launch_bounds__(256)
   cplx<T>* twy = S + TG::TILE;
   cplx<T>* twz = twy + NY;
   double2* acc = reinterpret_cast<double2*>(twz + NZ);  // [acc_cap][LMAX][G]
+  EntRec<T>* R = reinterpret_cast<EntRec<T>*>(acc + acc_cap * LMAX * G);  // [rec_cap]
 
-  const int grp = blockIdx.x, ix = blockIdx.y;
+  constexpr int YS = TG::YSPLIT, YPER = Y1 / YS;
+  const int grp = blockIdx.x, ix = blockIdx.y / YS, yh = blockIdx.y % YS;
   const int m0 = grp * G;
   const int gcount = min(G, M - m0);
   const bool v16 = vec && gcount == G;
@@ -89,7 +132,7 @@ __global__ void __launch_bounds__(256)
   if (proj_on)
     for (int i = threadIdx.x; i < acc_cap * LMAX * G; i += blockDim.x) acc[i] = make_double2(0.0, 0.0);
 
-  for (int y1 = 0; y1 < Y1; ++y1) {
+  for (int y1 = yh * YPER; y1 < (yh + 1) * YPER; ++y1) {
     // -- rows y1 + Y1 r of plane ix, G orbitals per point
     if (v16) {
       for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
@@ -98,8 +141,6 @@ __global__ void __launch_bounds__(256)
         const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
         cp_async16(S + (r * ZS + AZ::slot(z)) * G + v * PV, in + p * ld + m0 + v * PV);
       }
-      cp_async_commit();
-      cp_async_wait<0>();
     } else {
       for (int q = threadIdx.x; q < TG::PTS * G; q += blockDim.x) {
         const int j = q % G, pt = q / G;
@@ -108,6 +149,10 @@ __global__ void __launch_bounds__(256)
         S[(r * ZS + AZ::slot(z)) * G + j] = (j < gcount) ? in[p * ld + m0 + j] : mk<T>(0, 0);
       }
     }
+    int roff = 0;
+    const EntRec<T>* rec = proj_on ? stage_entries(pj, pj.ent_rec, ix * Y1 + y1, rec_cap, R, roff) : pj.ent_rec;
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
 
     // -- KB projection of the tile (projector_all.hpp:104-165): warp per atom
@@ -115,7 +160,6 @@ __global__ void __launch_bounds__(256)
     if (proj_on) {
       constexpr int ESUB = 32 / G;
       const int j = lane % G, es = lane / G;
-      const cplx<T>* phase = (const cplx<T>*)pj.ent_phase;
       const int tile = ix * Y1 + y1;
       const int s0 = pj.seg_ptr[tile], s1 = pj.seg_ptr[tile + 1];
       for (int s = s0 + warp; s < s1; s += nw) {
@@ -124,12 +168,13 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int l = 0; l < LMAX; ++l) a[l] = mk<T>(0, 0);
         for (int e = e0 + es; e < e1; e += ESUB) {
-          const int off = pj.ent_off[e];
+          const EntRec<T>& re = rec[e - roff];
+          const int off = re.off;
           const int r = off / NZ, z = off - r * NZ;
-          const cplx<T> x = phase[e] * S[(r * ZS + AZ::slot(z)) * G + j];
+          const cplx<T> x = mk<T>(re.ph[0], re.ph[1]) * S[(r * ZS + AZ::slot(z)) * G + j];
 #pragma unroll
           for (int l = 0; l < LMAX; ++l) {
-            const T b = (l < pj.L) ? pj.ent_beta[(long)e * pj.L + l] : (T)0;
+            const T b = re.beta[l];
             a[l].x = fma(b, x.x, a[l].x);
             a[l].y = fma(b, x.y, a[l].y);
           }
@@ -317,15 +362,19 @@ template <typename T, int NX, int NY, int NZ>
 __global__ void __launch_bounds__(256)
     k_tile_inv(const cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ in, long ld_in,
                cplx<T>* __restrict__ out, long ld_out, int M, const cplx<T>* __restrict__ tw_y,
-               const cplx<T>* __restrict__ tw_z, ProjView<T> pj, EpiParams<T> ep, int vec) {
+               const cplx<T>* __restrict__ tw_z, ProjView<T> pj, EpiParams<T> ep, int rec_cap, int seg_cap,
+               int vec) {
   using TG = TileGeom<T, NX, NY, NZ>;
   using AZ = typename TG::AZ;
   constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, ZS = TG::ZS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* S = reinterpret_cast<cplx<T>*>(smem_raw);
-  cplx<T>* P = S + TG::TILE;  // [PTS][G] input orbitals of the tile
-  cplx<T>* twy = P + TG::PTS * G;
+  cplx<T>* P = S + TG::TILE;  // [PTS][G] input orbitals of the tile (PREFETCH)
+  cplx<T>* twy = P + (TG::PREFETCH ? TG::PTS * G : 0);
   cplx<T>* twz = twy + NY;
+  EntRec<T>* R = reinterpret_cast<EntRec<T>*>(twz + NZ);  // [rec_cap] records in point order
+  int* TP = reinterpret_cast<int*>(R + rec_cap);           // [PSTRIDE] point index of the tile
+  cplx<T>* PT = reinterpret_cast<cplx<T>*>(TP + TG::PSTRIDE);  // [seg_cap][LMAX][G] projections
 
   const int grp = blockIdx.x, ix = blockIdx.y / Y1, y1 = blockIdx.y % Y1;
   const int m0 = grp * G;
@@ -339,8 +388,22 @@ __global__ void __launch_bounds__(256)
     cp_async16(S + (ka * ZS + AZ::slot(kz)) * G + v * PV,
                tmp + (((long)(grp * Y2 + ka) * NZ + kz) * NX + ix) * (Y1 * G) + y1 * G + v * PV);
   }
+  const bool proj_on = pj.nproj > 0;
+  const int tile = ix * Y1 + y1;
+  int roff = 0, s0 = 0, nseg = 0;
+  const EntRec<T>* rec = pj.ent_rec_pt;
+  if (proj_on) {
+    rec = stage_entries(pj, pj.ent_rec_pt, tile, rec_cap, R, roff);
+    const int* tp = pj.pt_ptr + (long)tile * TG::PSTRIDE;
+    for (int q = threadIdx.x; q < TG::PSTRIDE / 4; q += blockDim.x)
+      cp_async16(reinterpret_cast<int4*>(TP) + q, reinterpret_cast<const int4*>(tp) + q);
+    s0 = pj.seg_ptr[tile];
+    nseg = pj.seg_ptr[tile + 1] - s0;
+  }
+  // the point index counts from the tile's first record
+  const int rbase = (rec == R) ? 0 : roff_base(pj, s0, proj_on);
   cp_async_commit();
-  if (v16) {
+  if (TG::PREFETCH && v16) {
     for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
       const int v = q % VP, pt = q / VP;
       const int z = pt % NZ, r = pt / NZ;
@@ -351,6 +414,19 @@ __global__ void __launch_bounds__(256)
   cp_async_commit();
   for (int i = threadIdx.x; i < NY; i += blockDim.x) twy[i] = tw_y[i];
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = tw_z[i];
+  // the tile's atom projections, in the tile precision
+  const bool pt_staged = nseg <= seg_cap;
+  if (proj_on && pt_staged) {
+    for (int i = threadIdx.x; i < nseg * LMAX * G; i += blockDim.x) {
+      const int j = i % G, l = (i / G) % LMAX, ts = i / (G * LMAX);
+      cplx<T> v = mk<T>(0, 0);
+      if (l < pj.L && j < gcount) {
+        const double2 d = pj.proj[((long)pj.seg_atom[s0 + ts] * pj.L + l) * M + m0 + j];
+        v = mk<T>((T)d.x, (T)d.y);
+      }
+      PT[i] = v;
+    }
+  }
   cp_async_wait<1>();
   __syncthreads();
 
@@ -384,85 +460,94 @@ __global__ void __launch_bounds__(256)
   });
   __syncthreads();
 
-  // nonlocal scatter (projector_all.hpp:182-232): warp per atom segment, lanes =
-  // (orbital j, entry sub-lane); shared-memory atomics merge overlapping spheres
-  if (pj.nproj > 0) {
-    constexpr int ESUB = 32 / G;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int j = lane % G, es = lane / G;
-    const cplx<T>* phase = (const cplx<T>*)pj.ent_phase;
-    const int tile = ix * Y1 + y1;
-    const int s0 = pj.seg_ptr[tile], s1 = pj.seg_ptr[tile + 1];
-    for (int s = s0 + warp; s < s1; s += nw) {
-      const int at = pj.seg_atom[s];
-      const int e0 = pj.seg_ent[s], e1 = pj.seg_ent[s + 1];
-      cplx<T> pr[LMAX];
-#pragma unroll
-      for (int l = 0; l < LMAX; ++l) {
-        pr[l] = mk<T>(0, 0);
-        if (l < pj.L && j < gcount) {
-          const double2 d = pj.proj[((long)at * pj.L + l) * M + m0 + j];
-          pr[l] = mk<T>((T)d.x, (T)d.y);
-        }
-      }
-      for (int e = e0 + es; e < e1; e += ESUB) {
-        const int off = pj.ent_off[e];
-        const int r = off / NZ, z = off - r * NZ;
-        cplx<T> t = mk<T>(0, 0);
-#pragma unroll
-        for (int l = 0; l < LMAX; ++l) {
-          const T b = (l < pj.L) ? pj.ent_beta[(long)e * pj.L + l] : (T)0;
-          t.x = fma(b, pr[l].x, t.x);
-          t.y = fma(b, pr[l].y, t.y);
-        }
-        const cplx<T> c = mul_conj(t, phase[e]);
-        cplx<T>* dst = S + (r * ZS + AZ::slot_of_freq(z)) * G + j;
-        atomicAdd(&dst->x, c.x);
-        atomicAdd(&dst->y, c.y);
-      }
-    }
-  }
+  // epilogue: out = alpha (K psi + (V + vshift) psi + V_nl psi) + beta base, with
+  // V_nl psi(r) = sum over the entries at r of conj(exp(i (k+A).r_e)) sum_l
+  // beta_e[l] proj[a_e][l] (projector_all.hpp:182-232), summed by the point's owner.
+  // BE pieces of PV orbitals per thread, their loads issued together.
+  constexpr int BE = 4;
   cp_async_wait<0>();
   __syncthreads();
-
-  // epilogue: out = alpha (K psi + (V + vshift) psi + V_nl psi) + beta base
-  for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
-    const int v = q % VP, pt = q / VP;
-    const int z = pt % NZ, r = pt / NZ;
-    const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
-    const int sl = (r * ZS + AZ::slot_of_freq(z)) * G + v * PV;
-    const T vp = ep.V[p] + ep.vshift;
-    cplx<T> h[PV], x[PV], b[PV];
+  for (int q0 = threadIdx.x; q0 < TG::PTS * VP; q0 += BE * blockDim.x) {
+    cplx<T> x[BE][PV];
+    T vp[BE];
 #pragma unroll
-    for (int k = 0; k < PV; ++k) h[k] = S[sl + k];
-    const int jb = v * PV;
-    if (v16) {
+    for (int b = 0; b < BE; ++b) {
+      const int q = q0 + b * blockDim.x;
+      if (q >= TG::PTS * VP) continue;
+      const int v = q % VP, pt = q / VP;
+      const int z = pt % NZ, r = pt / NZ;
+      const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
+      const int jb = v * PV;
+      vp[b] = ep.V[p] + ep.vshift;
+      if (TG::PREFETCH && v16) {
 #pragma unroll
-      for (int k = 0; k < PV; ++k) x[k] = P[pt * G + jb + k];
-    } else {
+        for (int k = 0; k < PV; ++k) x[b][k] = P[pt * G + jb + k];
+      } else if (v16) {
+        const float4 w = *reinterpret_cast<const float4*>(in + p * ld_in + m0 + jb);
+        memcpy(x[b], &w, 16);
+      } else {
 #pragma unroll
-      for (int k = 0; k < PV; ++k) x[k] = (jb + k < gcount) ? in[p * ld_in + m0 + jb + k] : mk<T>(0, 0);
+        for (int k = 0; k < PV; ++k) x[b][k] = (jb + k < gcount) ? in[p * ld_in + m0 + jb + k] : mk<T>(0, 0);
+      }
     }
-    if (ep.base) {
 #pragma unroll
-      for (int k = 0; k < PV; ++k)
-        b[k] = (jb + k < gcount) ? ep.base[p * ep.ld_base + m0 + jb + k] : mk<T>(0, 0);
-    }
+    for (int b = 0; b < BE; ++b) {
+      const int q = q0 + b * blockDim.x;
+      if (q >= TG::PTS * VP) continue;
+      const int v = q % VP, pt = q / VP;
+      const int z = pt % NZ, r = pt / NZ;
+      const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
+      const int jb = v * PV;
+      const int sl = (r * ZS + AZ::slot_of_freq(z)) * G + jb;
+      cplx<T> h[PV];
 #pragma unroll
-    for (int k = 0; k < PV; ++k) {
-      h[k].x = fma(vp, x[k].x, h[k].x);
-      h[k].y = fma(vp, x[k].y, h[k].y);
-      h[k] = ep.alpha * h[k];
-      if (ep.base) h[k] = h[k] + ep.beta * b[k];
-    }
-    if (v16) {
-      float4 w;
-      memcpy(&w, h, 16);
-      *reinterpret_cast<float4*>(out + p * ld_out + m0 + jb) = w;
-    } else {
+      for (int k = 0; k < PV; ++k) h[k] = S[sl + k];
+      if (proj_on) {
+        const int k0 = TP[pt], k1 = TP[pt + 1];
+        for (int kk = k0; kk < k1; ++kk) {
+          const EntRec<T>& re = rec[kk + rbase];
+          const cplx<T> ph = mk<T>(re.ph[0], re.ph[1]);
 #pragma unroll
-      for (int k = 0; k < PV; ++k)
-        if (jb + k < gcount) out[p * ld_out + m0 + jb + k] = h[k];
+          for (int k = 0; k < PV; ++k) {
+            cplx<T> t = mk<T>(0, 0);
+#pragma unroll
+            for (int l = 0; l < LMAX; ++l) {
+              cplx<T> pv;
+              if (pt_staged) {
+                pv = PT[(re.tseg * LMAX + l) * G + jb + k];
+              } else {
+                pv = mk<T>(0, 0);
+                if (l < pj.L && jb + k < gcount) {
+                  const double2 d = pj.proj[((long)pj.seg_atom[s0 + re.tseg] * pj.L + l) * M + m0 + jb + k];
+                  pv = mk<T>((T)d.x, (T)d.y);
+                }
+              }
+              t.x = fma(re.beta[l], pv.x, t.x);
+              t.y = fma(re.beta[l], pv.y, t.y);
+            }
+            h[k] = h[k] + mul_conj(t, ph);
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < PV; ++k) {
+        h[k].x = fma(vp[b], x[b][k].x, h[k].x);
+        h[k].y = fma(vp[b], x[b][k].y, h[k].y);
+        h[k] = ep.alpha * h[k];
+        if (ep.base) {
+          const cplx<T> bb = (jb + k < gcount) ? ep.base[p * ep.ld_base + m0 + jb + k] : mk<T>(0, 0);
+          h[k] = h[k] + ep.beta * bb;
+        }
+      }
+      if (v16) {
+        float4 w;
+        memcpy(&w, h, 16);
+        *reinterpret_cast<float4*>(out + p * ld_out + m0 + jb) = w;
+      } else {
+#pragma unroll
+        for (int k = 0; k < PV; ++k)
+          if (jb + k < gcount) out[p * ld_out + m0 + jb + k] = h[k];
+      }
     }
   }
 }

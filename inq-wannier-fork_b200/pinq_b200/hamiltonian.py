@@ -275,7 +275,7 @@ class KSHamiltonian:
         call("inqb_timing_start", self._h, int(max_applies))
 
     def timing_stop(self):
-        """(summed ms of [plane_fwd, line_x, plane_inv], number of timed applies)."""
+        """(summed ms of [tile_fwd, tile_x, tile_inv], number of timed applies)."""
         ms = np.zeros(3)
         n = ctypes.c_int(0)
         call("inqb_timing_stop", self._h, dptr(ms), ctypes.byref(n))
