@@ -5,6 +5,7 @@
 //   V gradient   gV[p] += Re(c sum_m conj(u) w)      (<u| dH/dV(p) |w>, H's local term)
 //   A gradient   gA[d] += Re(c <u| dH/dA_d |w>)      kinetic (G + k + A)_d in Fourier space
 //                plus the nonlocal position commutator i S [conj(p_u) r_w - conj(r_u) p_w]
+//                from per-chunk moments (deterministic: no atomics on the moments)
 //                (the structure of projector_all::position_commutator,
 //                src/hamiltonian/projector_all.hpp:319-403).
 // All sums are FP64 whatever the orbital precision.
@@ -137,61 +138,98 @@ __global__ void k_velocity_dot(long N, int M, const cplx<T>* __restrict__ U, con
   }
 }
 
-// Nonlocal part of <u| dH/dA_d |w> per atom: one thread per orbital walks the
-// atom's sphere entries; acc[6 + 2d..] += sum_l S_l i [conj(p_u) r_w,d - conj(r_u,d) p_w].
+// Nonlocal part of <u| dH/dA_d |w>, step 1: moments of one chunk of an atom's
+// sphere entries,
+//   p_u[l] = sum_e beta_e[l] exp(i(k+A).r_e) u(r_e),  r_u[l][d] = the same with x_e[d],
+// and likewise for w; 16 FP64 values (4 complex for u, 4 for w) per (l, orbital).
+// Block: 32 orbitals x LMAX projectors x 2 entry lanes.  part[chunk][l][q][M].
 template <typename T>
-__global__ void k_nl_dA(int nproj, int L, int M, const cplx<T>* __restrict__ u, const cplx<T>* __restrict__ w,
-                        long ld, const int* __restrict__ atom_ptr, const int* __restrict__ atom_ent,
-                        const int* __restrict__ ent_pt, const double* __restrict__ ent_xyz,
-                        const T* __restrict__ ent_beta, const cplx<T>* __restrict__ phase,
-                        const double* __restrict__ scale, double* __restrict__ acc) {
-  constexpr int LM = 4;
-  const int a = blockIdx.x;
-  const int m = blockIdx.y * blockDim.x + threadIdx.x;
-  double out[6] = {0, 0, 0, 0, 0, 0};
-  if (m < M) {
-    double pu[LM][2] = {}, pw[LM][2] = {}, ru[LM][3][2] = {}, rw[LM][3][2] = {};
-    for (int i = atom_ptr[a]; i < atom_ptr[a + 1]; i++) {
+__global__ void __launch_bounds__(256)
+    k_nl_moments(int L, int M, const cplx<T>* __restrict__ u, const cplx<T>* __restrict__ w, long ld,
+                 const int* __restrict__ chunk_atom, const int* __restrict__ chunk_beg,
+                 const int* __restrict__ atom_ptr, const int* __restrict__ atom_ent, const int* __restrict__ ent_pt,
+                 const double* __restrict__ ent_xyz, const EntRec<T>* __restrict__ rec, double* __restrict__ part) {
+  constexpr int LM = 4, Q = 16;
+  __shared__ double red[LM][32][Q + 1];
+  const int c = blockIdx.x;
+  const int m = blockIdx.y * 32 + (threadIdx.x & 31);
+  const int l = (threadIdx.x >> 5) & (LM - 1), es = threadIdx.x >> 7;
+  const int a = chunk_atom[c];
+  const int i0 = chunk_beg[c], i1 = min(i0 + kNlChunk, atom_ptr[a + 1]);
+  double s[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) s[q] = 0.0;
+  if (m < M && l < L) {
+    for (int i = i0 + es; i < i1; i += 2) {
       const int e = atom_ent[i];
       const long pt = ent_pt[e];
-      const cplx<T> ph = phase[e];
+      const EntRec<T> r = rec[e];
       const cplx<T> uu = u[pt * ld + m], ww = w[pt * ld + m];
-      // phase * value in FP64
-      const double ur = (double)ph.x * uu.x - (double)ph.y * uu.y, ui = (double)ph.x * uu.y + (double)ph.y * uu.x;
-      const double wr = (double)ph.x * ww.x - (double)ph.y * ww.y, wi = (double)ph.x * ww.y + (double)ph.y * ww.x;
-      const double x[3] = {ent_xyz[3 * e], ent_xyz[3 * e + 1], ent_xyz[3 * e + 2]};
-      for (int l = 0; l < L && l < LM; l++) {
-        const double b = (double)ent_beta[(long)e * L + l];
-        pu[l][0] += b * ur;
-        pu[l][1] += b * ui;
-        pw[l][0] += b * wr;
-        pw[l][1] += b * wi;
-        for (int d = 0; d < 3; d++) {
-          ru[l][d][0] += b * x[d] * ur;
-          ru[l][d][1] += b * x[d] * ui;
-          rw[l][d][0] += b * x[d] * wr;
-          rw[l][d][1] += b * x[d] * wi;
-        }
-      }
-    }
-    for (int l = 0; l < L && l < LM; l++) {
-      const double S = scale[a * L + l];
-      for (int d = 0; d < 3; d++) {
-        // z1 = conj(pu) rw, z2 = conj(ru) pw, result += S i (z1 - z2)
-        const double z1r = pu[l][0] * rw[l][d][0] + pu[l][1] * rw[l][d][1];
-        const double z1i = pu[l][0] * rw[l][d][1] - pu[l][1] * rw[l][d][0];
-        const double z2r = ru[l][d][0] * pw[l][0] + ru[l][d][1] * pw[l][1];
-        const double z2i = ru[l][d][0] * pw[l][1] - ru[l][d][1] * pw[l][0];
-        out[2 * d] += -S * (z1i - z2i);
-        out[2 * d + 1] += S * (z1r - z2r);
-      }
+      const double b = (double)r.beta[l];
+      const double pr = (double)r.ph[0], pi = (double)r.ph[1];
+      // b exp(i (k+A).r) u and the same for w, in FP64
+      const double ur = b * (pr * uu.x - pi * uu.y), ui = b * (pr * uu.y + pi * uu.x);
+      const double wr = b * (pr * ww.x - pi * ww.y), wi = b * (pr * ww.y + pi * ww.x);
+      const double x0 = ent_xyz[3 * e], x1 = ent_xyz[3 * e + 1], x2 = ent_xyz[3 * e + 2];
+      s[0] += ur; s[1] += ui;
+      s[2] += x0 * ur; s[3] += x0 * ui; s[4] += x1 * ur; s[5] += x1 * ui; s[6] += x2 * ur; s[7] += x2 * ui;
+      s[8] += wr; s[9] += wi;
+      s[10] += x0 * wr; s[11] += x0 * wi; s[12] += x1 * wr; s[13] += x1 * wi; s[14] += x2 * wr; s[15] += x2 * wi;
     }
   }
-  for (int q = 0; q < 6; q++) {
-    double v = out[q];
+  if (es == 1) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&acc[6 + q], v);
+    for (int q = 0; q < Q; ++q) red[l][threadIdx.x & 31][q] = s[q];
+  }
+  __syncthreads();
+  if (es == 0 && m < M && l < L) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) part[(((long)c * L + l) * Q + q) * M + m] = s[q] + red[l][threadIdx.x & 31][q];
+  }
+}
+
+// Step 2: per atom, sum its chunks and add S_l i [conj(p_u) r_w,d - conj(r_u,d) p_w]
+// over l and orbitals into acc[6 + 2d .. 6 + 2d + 1].
+__global__ void __launch_bounds__(128)
+    k_nl_combine(int L, int M, const int* __restrict__ atom_chunk_ptr, const double* __restrict__ part,
+                 const double* __restrict__ scale, double* __restrict__ acc) {
+  constexpr int Q = 16;
+  const int a = blockIdx.x;
+  const int c0 = atom_chunk_ptr[a], c1 = atom_chunk_ptr[a + 1];
+  double out[6] = {0, 0, 0, 0, 0, 0};
+  for (int idx = threadIdx.x; idx < L * M; idx += blockDim.x) {
+    const int l = idx / M, m = idx - l * M;
+    double v[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) v[q] = 0.0;
+    for (int c = c0; c < c1; ++c)
+#pragma unroll
+      for (int q = 0; q < Q; ++q) v[q] += part[(((long)c * L + l) * Q + q) * M + m];
+    const double S = scale[a * L + l];
+    const double pur = v[0], pui = v[1], pwr = v[8], pwi = v[9];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double rur = v[2 + 2 * d], rui = v[3 + 2 * d], rwr = v[10 + 2 * d], rwi = v[11 + 2 * d];
+      // z1 = conj(p_u) r_w, z2 = conj(r_u) p_w, result += S i (z1 - z2)
+      const double z1r = pur * rwr + pui * rwi, z1i = pur * rwi - pui * rwr;
+      const double z2r = rur * pwr + rui * pwi, z2i = rur * pwi - rui * pwr;
+      out[2 * d] += -S * (z1i - z2i);
+      out[2 * d + 1] += S * (z1r - z2r);
+    }
+  }
+  __shared__ double red[6][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = 0; q < 6; q++) {
+    double x = out[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) red[q][warp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double x = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) x += red[threadIdx.x][k];
+    atomicAdd(&acc[6 + threadIdx.x], x);
   }
 }
 
@@ -270,12 +308,17 @@ static int agrad_impl(const inqb_ctx& ctx, const void* U, const void* W, const v
                                                              acc);
   INQB_CUDA_TRY(cudaGetLastError());
   const ProjTables& t = ctx.proj;
-  if (t.nproj > 0) {
-    dim3 grid(t.nproj, (M + 31) / 32);
-    k_nl_dA<T><<<grid, 32, 0, st>>>(t.nproj, t.L, M, (const cplx<T>*)u, (const cplx<T>*)w, ld,
-                                    t.d_atom_ptr.as<int>(), t.d_atom_ent.as<int>(), t.d_ent_pt.as<int>(),
-                                    t.d_ent_xyz.as<double>(), t.d_ent_beta.as<T>(),
-                                    (const cplx<T>*)t.d_ent_phase.ptr, t.d_scale.as<double>(), acc);
+  const int nchunks = (int)t.chunk_atom.size();
+  if (t.nproj > 0 && nchunks > 0) {
+    if (ctx.d_nlpart.bytes < (size_t)nchunks * t.L * 16 * M * sizeof(double))
+      return fail(INQB_ERR_INVALID, "nonlocal moment workspace not reserved");
+    double* part = ctx.d_nlpart.as<double>();
+    k_nl_moments<T><<<dim3(nchunks, (M + 31) / 32), 256, 0, st>>>(
+        t.L, M, (const cplx<T>*)u, (const cplx<T>*)w, ld, t.d_chunk_atom.as<int>(), t.d_chunk_beg.as<int>(),
+        t.d_atom_ptr.as<int>(), t.d_atom_ent.as<int>(), t.d_ent_pt.as<int>(), t.d_ent_xyz.as<double>(),
+        t.d_ent_rec.as<EntRec<T>>(), part);
+    INQB_CUDA_TRY(cudaGetLastError());
+    k_nl_combine<<<t.nproj, 128, 0, st>>>(t.L, M, t.d_atom_chunk_ptr.as<int>(), part, t.d_scale.as<double>(), acc);
     INQB_CUDA_TRY(cudaGetLastError());
   }
   k_finish_dA<<<1, 32, 0, st>>>(acc, 1.0 / (double)ctx.N, cre, cim, gA);

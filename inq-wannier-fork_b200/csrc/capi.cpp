@@ -686,6 +686,8 @@ int inqb_accum_vector_potential_gradient(inqb_ctx* ctx, const void* u, const voi
   INQB_TRY(ctx->d_adjU.ensure(bytes));
   INQB_TRY(ctx->d_adjW.ensure(bytes));
   INQB_TRY(ctx->d_red.ensure(256));
+  INQB_TRY(ctx->d_nlpart.ensure(std::max<size_t>(
+      (size_t)ctx->proj.chunk_atom.size() * ctx->proj.L * 16 * M * sizeof(double), 16)));
   const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
   INQB_TRY(apply(ctx, LaunchArgs::FFT_FWD, u, ld, ctx->d_adjU.ptr, M, M, nullptr, 0, one, zero, stream));
   INQB_TRY(apply(ctx, LaunchArgs::FFT_FWD, w, ld, ctx->d_adjW.ptr, M, M, nullptr, 0, one, zero, stream));

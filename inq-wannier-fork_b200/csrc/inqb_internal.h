@@ -101,6 +101,9 @@ struct ProjTables {
   // atom-major view used by the derivative kernels of the adjoint
   std::vector<int> atom_ptr, atom_ent, ent_pt;  // [nproj+1], [nent], [nent] linear grid point
   std::vector<double> ent_xyz;      // [nent][3] cartesian relative position
+  // chunks of at most kNlChunk consecutive entries of one atom (atom-major order),
+  // the unit of work of the nonlocal moment kernel of the adjoint
+  std::vector<int> chunk_atom, chunk_beg, atom_chunk_ptr;
   // device copies
   DevBuf d_seg_ptr, d_seg_atom, d_seg_ent, d_seg_local, d_plane_ptr, d_plane_atom, d_ent_off, d_ent_atom;
   DevBuf d_ent_beta;                // [nent][L] in the context precision
@@ -114,6 +117,7 @@ struct ProjTables {
   DevBuf d_ent_rec_pt, d_pt_pos, d_pt_ptr;
   DevBuf d_scale;                   // [nproj][L] double
   DevBuf d_atom_ptr, d_atom_ent, d_ent_pt, d_ent_xyz;
+  DevBuf d_chunk_atom, d_chunk_beg, d_atom_chunk_ptr;
 };
 
 // Kernel view of the projector tables (T = float or double).
@@ -136,6 +140,8 @@ struct ProjView {
   const double* scale;
   double2* proj;          // [nproj][L][M] accumulators (FP64 in both precisions)
 };
+
+constexpr int kNlChunk = 128;  // sphere entries per chunk of the adjoint's nonlocal moments
 
 struct Plan;  // kernel launch plan for one (precision, grid) pair
 
@@ -165,6 +171,7 @@ struct inqb_ctx {
   inqb::DevBuf d_work2;
   inqb::DevBuf d_red;     // small reduction buffers
   inqb::DevBuf d_adjU, d_adjW;  // Fourier transforms for the dH/dA inner products
+  inqb::DevBuf d_nlpart;        // per-chunk nonlocal moments of the dH/dA inner products
   size_t elem_bytes() const { return precision == INQB_FP64 ? 16 : 8; }
 
   // optional per-pass CUDA-event timing of H applications

@@ -330,6 +330,17 @@ int build_proj_tables(const inqb_ctx& ctx, int nproj, int L, int smax, const int
     std::vector<int> fill(t.atom_ptr.begin(), t.atom_ptr.end() - 1);
     for (long i = 0; i < total; i++) t.atom_ent[fill[t.ent_atom[i]]++] = (int)i;
   }
+  t.chunk_atom.clear();
+  t.chunk_beg.clear();
+  t.atom_chunk_ptr.assign(nproj + 1, 0);
+  for (int a = 0; a < nproj; a++) {
+    t.atom_chunk_ptr[a] = (int)t.chunk_atom.size();
+    for (int i = t.atom_ptr[a]; i < t.atom_ptr[a + 1]; i += kNlChunk) {
+      t.chunk_atom.push_back(a);
+      t.chunk_beg.push_back(i);
+    }
+  }
+  t.atom_chunk_ptr[nproj] = (int)t.chunk_atom.size();
   t.scale.resize((size_t)nproj * L);
   for (int a = 0; a < nproj; a++)
     for (int l = 0; l < L; l++) t.scale[(size_t)a * L + l] = ctx.dV * coeff[(size_t)a * L + l];
@@ -375,6 +386,9 @@ int upload_proj_tables(const inqb_ctx& ctx, ProjTables& t) {
   INQB_TRY(upload(t.d_atom_ent, t.atom_ent));
   INQB_TRY(upload(t.d_ent_pt, t.ent_pt));
   INQB_TRY(upload(t.d_ent_xyz, t.ent_xyz));
+  INQB_TRY(upload(t.d_chunk_atom, t.chunk_atom));
+  INQB_TRY(upload(t.d_chunk_beg, t.chunk_beg));
+  INQB_TRY(upload(t.d_atom_chunk_ptr, t.atom_chunk_ptr));
   if (ctx.precision == INQB_FP64) {
     INQB_TRY(upload(t.d_ent_beta, t.ent_beta));
   } else {
