@@ -188,6 +188,22 @@ int inqb_accum_potential_gradient(inqb_ctx* ctx, const void* u, const void* w, i
 int inqb_accum_vector_potential_gradient(inqb_ctx* ctx, const void* u, const void* w, int M, int ld, double c_re,
                                          double c_im, double* gA, void* stream);
 
+/* One ETRS step (the reference's real_time::etrs step with a density-independent
+ * H, src/real_time/etrs.hpp:22-82) that also keeps what its adjoint needs:
+ * psi <- T(kA_tdt) T(kA_t) psi, T = sum_{k<=4} (i dt/2 H)^k / k!, and powers =
+ * 8 contiguous [N][M] blocks (leading dimension M): H^k psi_t at kA_t, k = 0..3,
+ * then H^k phi at kA_tdt, phi the half-stepped orbitals.  Unlike inqb_etrs_step it
+ * sums the series term by term (no Horner), like the reference's exponential. */
+int inqb_etrs_step_powers(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                          const double kA_tdt_cov[3], void* powers, void* stream);
+/* Reverse of that step for a real objective (the reference has no adjoint):
+ * lambda <- U^dagger lambda, gV[p] += 2 Re sum_i conj(Xi_i) Phi_i and
+ * gA_t[d], gA_tdt[d] += 2 Re sum_i <Xi_i| dH/dA_d |Phi_i> for the two half steps,
+ * where Phi_i are the stored powers and Xi_i = sum_j conj(c_{i+j+1}) H^j lambda. */
+int inqb_etrs_adjoint_step(inqb_ctx* ctx, void* lambda, int M, int ld, double dt, const double kA_t_cov[3],
+                           const double kA_tdt_cov[3], const void* powers, double* gV, double* gA_t,
+                           double* gA_tdt, void* stream);
+
 /* ---------------------------------------------------------------- profiling
  * Per-pass CUDA-event timing of the next max_applies H applications, recorded
  * on the stream the kernels run on; the counterpart of INQ's scoped timers

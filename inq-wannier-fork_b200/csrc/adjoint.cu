@@ -30,6 +30,30 @@ __global__ void k_axpby(long N, int M, cplx<T> a, const cplx<T>* __restrict__ x,
   }
 }
 
+// y = sum_{k < K} a_k x_k over orbital blocks (K <= kMaxTerms); y may be one of the x_k.
+constexpr int kMaxTerms = 5;
+template <typename T>
+struct LinTerms {
+  const cplx<T>* x[kMaxTerms];
+  long ld[kMaxTerms];
+  cplx<T> a[kMaxTerms];
+  int K;
+};
+
+template <typename T>
+__global__ void k_lincomb(long N, int M, LinTerms<T> t, cplx<T>* __restrict__ y, long ldy) {
+  const long total = N * M;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const long p = i / M;
+    const int m = (int)(i - p * M);
+    cplx<T> acc = mk<T>(0, 0);
+#pragma unroll
+    for (int k = 0; k < kMaxTerms; ++k)
+      if (k < t.K) fma_acc(acc, t.a[k], t.x[k][p * t.ld[k] + m]);
+    y[p * ldy + m] = acc;
+  }
+}
+
 struct Lat {
   double lat[3][3];
   int nr[3];
@@ -260,6 +284,28 @@ int launch_axpby(int precision, long N, int M, const double a[2], const void* x,
                  long ldy, void* stream) {
   return precision == INQB_FP64 ? axpby_impl<double>(N, M, a, x, ldx, b, y, ldy, (cudaStream_t)stream)
                                 : axpby_impl<float>(N, M, a, x, ldx, b, y, ldy, (cudaStream_t)stream);
+}
+
+template <typename T>
+static int lincomb_impl(long N, int M, int K, const double (*a)[2], const void* const* x, const long* ldx, void* y,
+                        long ldy, cudaStream_t st) {
+  LinTerms<T> t{};
+  t.K = K;
+  for (int k = 0; k < K; k++) {
+    t.x[k] = (const cplx<T>*)x[k];
+    t.ld[k] = ldx[k];
+    t.a[k] = mk<T>((T)a[k][0], (T)a[k][1]);
+  }
+  k_lincomb<T><<<grid_for(N * M, 256), 256, 0, st>>>(N, M, t, (cplx<T>*)y, ldy);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_lincomb(int precision, long N, int M, int K, const double (*a)[2], const void* const* x, const long* ldx,
+                   void* y, long ldy, void* stream) {
+  if (K < 1 || K > kMaxTerms) return fail(INQB_ERR_INVALID, "linear combination of 1 to 5 blocks");
+  return precision == INQB_FP64 ? lincomb_impl<double>(N, M, K, a, x, ldx, y, ldy, (cudaStream_t)stream)
+                                : lincomb_impl<float>(N, M, K, a, x, ldx, y, ldy, (cudaStream_t)stream);
 }
 
 int launch_position_scale(int precision, const inqb_ctx& ctx, const void* psi, long ld, void* out, long ldo, int M,

@@ -7,6 +7,9 @@ namespace inqb {
 
 int launch_axpby(int precision, long N, int M, const double a[2], const void* x, long ldx, const double b[2], void* y,
                  long ldy, void* stream);
+// y = sum_k a_k x_k, 1 <= K <= 5 blocks; y may alias an x_k with the same leading dimension
+int launch_lincomb(int precision, long N, int M, int K, const double (*a)[2], const void* const* x, const long* ldx,
+                   void* y, long ldy, void* stream);
 int launch_position_scale(int precision, const inqb_ctx& ctx, const void* psi, long ld, void* out, long ldo, int M,
                           int dir, const double* occ, double s, void* stream);
 int launch_vgrad(int precision, long N, int M, const void* u, const void* w, long ld, double cre, double cim,

@@ -695,6 +695,144 @@ int inqb_accum_vector_potential_gradient(inqb_ctx* ctx, const void* u, const voi
                       stream);
 }
 
+// ---------------------------------------------------------------- native ETRS adjoint step
+namespace inqb {
+namespace {
+
+// c_k = (i dt/2)^k / k!, k = 0..4: the Taylor coefficients of one ETRS half step
+void taylor_coeffs(double dt, double c[5][2]) {
+  double re = 1.0, im = 0.0;
+  c[0][0] = 1.0;
+  c[0][1] = 0.0;
+  for (int k = 1; k <= 4; k++) {
+    const double f = 0.5 * dt / k;  // (i f) * (re + i im)
+    const double nre = -f * im, nim = f * re;
+    re = nre;
+    im = nim;
+    c[k][0] = re;
+    c[k][1] = im;
+  }
+}
+
+// One half step psi -> sum_k c_k H^k psi at the current k + A, keeping
+// P[0..3] = H^k psi (P[0] a copy of the input); `out` receives the result.
+int half_step_powers(inqb_ctx* ctx, const void* in, long ld_in, void* const P[4], void* out, long ld_out, int M,
+                     const double c[5][2], void* stream) {
+  const long Mi = M;
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  void* H4 = ctx->d_adjL.ptr;
+  {
+    const double a[1][2] = {{1.0, 0.0}};
+    const void* x[1] = {in};
+    const long ldx[1] = {ld_in};
+    INQB_TRY(launch_lincomb(ctx->precision, ctx->N, M, 1, a, x, ldx, P[0], Mi, stream));
+  }
+  for (int k = 1; k < 4; k++)
+    INQB_TRY(apply(ctx, LaunchArgs::H, P[k - 1], Mi, P[k], Mi, M, nullptr, 0, one, zero, stream));
+  INQB_TRY(apply(ctx, LaunchArgs::H, P[3], Mi, H4, Mi, M, nullptr, 0, one, zero, stream));
+  const void* x[5] = {P[0], P[1], P[2], P[3], H4};
+  const long ldx[5] = {Mi, Mi, Mi, Mi, Mi};
+  return launch_lincomb(ctx->precision, ctx->N, M, 5, c, x, ldx, out, ld_out, stream);
+}
+
+// Reverse of one half step at the current k + A: with Lambda_j = H^j lam,
+//   Xi_i = sum_j conj(c_{i+j+1}) Lambda_j,   gV += 2 Re conj(Xi_i) Phi_i,
+//   gA += 2 Re <Xi_i| dH/dA |Phi_i>,          lam <- sum_k conj(c_k) Lambda_k.
+int half_back(inqb_ctx* ctx, void* lam, long ld, int M, const double c[5][2], const void* const Phi[4], double* gV,
+              double* gA, void* stream) {
+  const long Mi = M;
+  const size_t blk = (size_t)ctx->N * M * ctx->elem_bytes();
+  char* w = static_cast<char*>(ctx->d_adjL.ptr);
+  void* Lam[5] = {lam, w + blk, w + 2 * blk, w + 3 * blk, w + 4 * blk};
+  void* Xi = w + 5 * blk;
+  const long ldL[5] = {ld, Mi, Mi, Mi, Mi};
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  for (int j = 1; j <= 4; j++)
+    INQB_TRY(apply(ctx, LaunchArgs::H, Lam[j - 1], ldL[j - 1], Lam[j], Mi, M, nullptr, 0, one, zero, stream));
+  double cc[5][2];
+  for (int k = 0; k < 5; k++) {
+    cc[k][0] = c[k][0];
+    cc[k][1] = -c[k][1];
+  }
+  for (int i = 0; i < 4; i++) {
+    const int K = 4 - i;
+    double a[4][2];
+    const void* x[4];
+    long ldx[4];
+    for (int j = 0; j < K; j++) {
+      a[j][0] = cc[i + j + 1][0];
+      a[j][1] = cc[i + j + 1][1];
+      x[j] = Lam[j];
+      ldx[j] = ldL[j];
+    }
+    INQB_TRY(launch_lincomb(ctx->precision, ctx->N, M, K, a, x, ldx, Xi, Mi, stream));
+    INQB_TRY(launch_vgrad(ctx->precision, ctx->N, M, Xi, Phi[i], Mi, 2.0, 0.0, gV, stream));
+    INQB_TRY(apply(ctx, LaunchArgs::FFT_FWD, Xi, Mi, ctx->d_adjU.ptr, Mi, M, nullptr, 0, one, zero, stream));
+    INQB_TRY(apply(ctx, LaunchArgs::FFT_FWD, Phi[i], Mi, ctx->d_adjW.ptr, Mi, M, nullptr, 0, one, zero, stream));
+    INQB_TRY(launch_agrad(*ctx, ctx->d_adjU.ptr, ctx->d_adjW.ptr, Xi, Phi[i], Mi, M, ctx->d_red.as<double>(), 2.0,
+                          0.0, gA, stream));
+  }
+  const void* x[5] = {Lam[0], Lam[1], Lam[2], Lam[3], Lam[4]};
+  return launch_lincomb(ctx->precision, ctx->N, M, 5, cc, x, ldL, lam, ld, stream);
+}
+
+int adjoint_workspace(inqb_ctx* ctx, int M) {
+  const size_t blk = (size_t)ctx->N * M * ctx->elem_bytes();
+  INQB_TRY(ctx->d_adjL.ensure(6 * blk));
+  INQB_TRY(ctx->d_adjU.ensure(blk));
+  INQB_TRY(ctx->d_adjW.ensure(blk));
+  INQB_TRY(ctx->d_red.ensure(256));
+  INQB_TRY(ctx->d_nlpart.ensure(std::max<size_t>(
+      (size_t)ctx->proj.chunk_atom.size() * ctx->proj.L * 16 * M * sizeof(double), 16)));
+  return reserve(ctx, M);
+}
+
+}  // namespace
+}  // namespace inqb
+
+int inqb_etrs_step_powers(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                          const double kA_tdt_cov[3], void* powers, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  INQB_TRY(check_block(ctx, powers, M, M));
+  if (!kA_t_cov || !kA_tdt_cov || !std::isfinite(dt)) return fail(INQB_ERR_INVALID, "bad step arguments");
+  INQB_GUARD(ctx);
+  INQB_TRY(adjoint_workspace(ctx, M));
+  double c[5][2];
+  taylor_coeffs(dt, c);
+  const size_t blk = (size_t)ctx->N * M * ctx->elem_bytes();
+  char* P = static_cast<char*>(powers);
+  void* P1[4] = {P, P + blk, P + 2 * blk, P + 3 * blk};
+  void* P2[4] = {P + 4 * blk, P + 5 * blk, P + 6 * blk, P + 7 * blk};
+  INQB_TRY(set_kA(ctx, kA_t_cov, stream));
+  // phi = the first half step, written straight into P2[0]
+  INQB_TRY(half_step_powers(ctx, psi, ld, P1, P2[0], M, M, c, stream));
+  INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
+  return half_step_powers(ctx, P2[0], M, P2, psi, ld, M, c, stream);
+}
+
+int inqb_etrs_adjoint_step(inqb_ctx* ctx, void* lambda, int M, int ld, double dt, const double kA_t_cov[3],
+                           const double kA_tdt_cov[3], const void* powers, double* gV, double* gA_t,
+                           double* gA_tdt, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, lambda, M, ld));
+  INQB_TRY(check_block(ctx, powers, M, M));
+  if (!kA_t_cov || !kA_tdt_cov || !std::isfinite(dt)) return fail(INQB_ERR_INVALID, "bad step arguments");
+  if (!gV || !gA_t || !gA_tdt) return fail(INQB_ERR_INVALID, "null gradient");
+  INQB_GUARD(ctx);
+  INQB_TRY(adjoint_workspace(ctx, M));
+  double c[5][2];
+  taylor_coeffs(dt, c);
+  const size_t blk = (size_t)ctx->N * M * ctx->elem_bytes();
+  const char* P = static_cast<const char*>(powers);
+  const void* P1[4] = {P, P + blk, P + 2 * blk, P + 3 * blk};
+  const void* P2[4] = {P + 4 * blk, P + 5 * blk, P + 6 * blk, P + 7 * blk};
+  INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
+  INQB_TRY(half_back(ctx, lambda, ld, M, c, P2, gV, gA_tdt, stream));
+  INQB_TRY(set_kA(ctx, kA_t_cov, stream));
+  return half_back(ctx, lambda, ld, M, c, P1, gV, gA_t, stream);
+}
+
 int inqb_orthonormalize_noalloc(inqb_ctx* ctx, void* psi, int M, int ld, void* stream) {
   INQB_CHECK_CTX(ctx);
   INQB_TRY(check_block(ctx, psi, M, ld));

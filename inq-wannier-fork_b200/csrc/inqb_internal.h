@@ -172,6 +172,7 @@ struct inqb_ctx {
   inqb::DevBuf d_red;     // small reduction buffers
   inqb::DevBuf d_adjU, d_adjW;  // Fourier transforms for the dH/dA inner products
   inqb::DevBuf d_nlpart;        // per-chunk nonlocal moments of the dH/dA inner products
+  inqb::DevBuf d_adjL;          // adjoint step: H^j lambda (4 blocks), Xi, spare
   size_t elem_bytes() const { return precision == INQB_FP64 ? 16 : 8; }
 
   // optional per-pass CUDA-event timing of H applications

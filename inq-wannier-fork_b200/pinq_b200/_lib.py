@@ -51,6 +51,10 @@ SIGNATURES = {
     "inqb_dipole": (ctypes.c_int, [_ctxp, _vp, _dp, _vp]),
     "inqb_orthonormalize": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "inqb_orthonormalize_noalloc": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "inqb_etrs_step_powers": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
+                                             _vp, _vp]),
+    "inqb_etrs_adjoint_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
+                                              _vp, _vp, _vp, _vp, _vp]),
     "inqb_axpby": (ctypes.c_int, [_ctxp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int,
                                   ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int, _vp]),
     "inqb_position_scale": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,

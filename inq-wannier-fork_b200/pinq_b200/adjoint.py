@@ -19,21 +19,14 @@ Xi_i = sum_j conj(c_{i+j+1}) H^j lam.  dH/dV(p) is pointwise; dH/dA_x is the
 kinetic (G + A)_x plus the nonlocal position commutator.  The forward orbitals are
 checkpointed every `every` steps and recomputed segment by segment.
 
-Everything runs in libinqb200's kernels; torch holds device memory and supplies
-the autograd interface.
+The steps run in libinqb200 (inqb_etrs_step, inqb_etrs_step_powers,
+inqb_etrs_adjoint_step); torch holds device memory and supplies the autograd
+interface.
 """
 from __future__ import annotations
 
 import numpy as np
 import torch
-
-
-def _coeffs(dt: float, order: int = 4):
-    f = 0.5j * dt
-    c = [1.0 + 0j]
-    for k in range(1, order + 1):
-        c.append(c[-1] * f / k)
-    return c
 
 
 class DipolePropagation:
@@ -47,7 +40,6 @@ class DipolePropagation:
         self.dt = float(dt)
         self.every = int(every)
         self.direction = int(direction)
-        self.c = _coeffs(self.dt)
 
     # -- helpers
     def _kA(self, a: float):
@@ -58,9 +50,6 @@ class DipolePropagation:
     @staticmethod
     def _amp(amps, n):
         return float(amps[min(n, len(amps) - 1)])
-
-    def _set_A(self, a):
-        self.h.set_vector_potential_cov(self._kA(a))
 
     # -- forward
     def forward(self, amplitudes, keep=True) -> float:
@@ -79,34 +68,13 @@ class DipolePropagation:
             self.psi_final = psi
         return d
 
-    def _powers(self, a, phi):
-        """[H^0 phi .. H^4 phi] at amplitude a."""
-        self._set_A(a)
-        out = [phi]
-        for _ in range(4):
-            out.append(self.h.apply(out[-1]))
-        return out
-
-    def _combine(self, coefs, blocks):
-        """sum_k coefs[k] blocks[k] with the library's axpby."""
-        acc = torch.zeros_like(blocks[0])
-        for c, b in zip(coefs, blocks):
-            if c != 0:
-                self.h.axpby_(c, b, 1.0, acc)
-        return acc
-
-    def _half_back(self, a, lam, Phi, gV, gA_row):
-        L = self._powers(a, lam)  # Lambda_j = H^j lam, k + A set to a
-        cc = [np.conj(x) for x in self.c]
-        for i in range(4):
-            xi = self._combine([cc[i + j + 1] for j in range(4 - i)], L[: 4 - i])
-            self.h.accum_potential_gradient_(gV, xi, Phi[i], 2.0)
-            self.h.accum_vector_potential_gradient_(gA_row, xi, Phi[i], 2.0)
-        return self._combine(cc, L)
-
     # -- backward
     def backward(self):
-        """(d d/d amplitudes [len(amps)], d d/d V [N]) as FP64 device tensors."""
+        """(d d/d amplitudes [len(amps)], d d/d V [N]) as FP64 device tensors.
+
+        Each checkpoint segment is recomputed with inqb_etrs_step_powers, which keeps
+        the Taylor powers of every step, then walked backwards with
+        inqb_etrs_adjoint_step; both run entirely in the library."""
         h = self.h
         amps = self.amps
         nsteps = len(amps)
@@ -114,22 +82,19 @@ class DipolePropagation:
         gV = torch.zeros(h.N, dtype=torch.float64, device=dev)
         gA = torch.zeros((nsteps, 3), dtype=torch.float64, device=dev)
         lam = h.position_scale(self.psi_final, self.occ, self.direction, h.volume_element)
+        seg = min(self.every, nsteps)
+        store = torch.empty((seg, 8, h.N, self.M), dtype=self.psi0.dtype, device=dev)
         for s0 in reversed(range(0, nsteps, self.every)):
             s1 = min(s0 + self.every, nsteps)
             psi = self.checkpoints[s0].clone()
-            store = []
             for n in range(s0, s1):
-                P1 = self._powers(self._amp(amps, n), psi)
-                phi = self._combine(self.c, P1)
-                P2 = self._powers(self._amp(amps, n + 1), phi)
-                psi = self._combine(self.c, P2)
-                store.append((P1[:4], P2[:4]))
+                h.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)),
+                                    store[n - s0])
             for n in reversed(range(s0, s1)):
-                P1, P2 = store[n - s0]
                 n2 = min(n + 1, nsteps - 1)
-                lam = self._half_back(self._amp(amps, n + 1), lam, P2, gV, gA[n2])
-                lam = self._half_back(self._amp(amps, n), lam, P1, gV, gA[n])
-            del store
+                h.etrs_adjoint_step_(lam, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)),
+                                     store[n - s0], gV, gA[n], gA[n2])
+        del store
         return gA[:, self.direction].clone(), gV
 
 

@@ -222,6 +222,36 @@ class KSHamiltonian:
              self._stream())
         return psi
 
+    def etrs_step_powers_(self, psi, dt, kA_t_cov, kA_tdt_cov, powers):
+        """One ETRS step in place that also writes the 8 Taylor-power blocks the
+        adjoint step reads into `powers` ([8, N, M], contiguous)."""
+        psi = self._check(psi)
+        self._check_powers(powers, psi.shape[1])
+        a = np.ascontiguousarray(kA_t_cov, np.float64).reshape(3)
+        b = np.ascontiguousarray(kA_tdt_cov, np.float64).reshape(3)
+        call("inqb_etrs_step_powers", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), float(dt), dptr(a),
+             dptr(b), powers.data_ptr(), self._stream())
+        return psi
+
+    def etrs_adjoint_step_(self, lam, dt, kA_t_cov, kA_tdt_cov, powers, gV, gA_t, gA_tdt):
+        """Reverse of one ETRS step: lam <- U^dagger lam and the V / A gradients
+        accumulated into gV [N] and gA_t, gA_tdt [3] (FP64 CUDA tensors)."""
+        lam = self._check(lam)
+        self._check_powers(powers, lam.shape[1])
+        for g, n in ((gV, self.N), (gA_t, 3), (gA_tdt, 3)):
+            if g.dtype != torch.float64 or g.device.type != "cuda" or g.numel() < n or not g.is_contiguous():
+                raise TypeError("gradients must be contiguous FP64 CUDA tensors")
+        a = np.ascontiguousarray(kA_t_cov, np.float64).reshape(3)
+        b = np.ascontiguousarray(kA_tdt_cov, np.float64).reshape(3)
+        call("inqb_etrs_adjoint_step", self._h, lam.data_ptr(), lam.shape[1], lam.stride(0), float(dt), dptr(a),
+             dptr(b), powers.data_ptr(), gV.data_ptr(), gA_t.data_ptr(), gA_tdt.data_ptr(), self._stream())
+        return lam
+
+    def _check_powers(self, powers, M):
+        if (not torch.is_tensor(powers) or powers.device.type != "cuda" or powers.dtype != self.dtype
+                or tuple(powers.shape) != (8, self.N, M) or not powers.is_contiguous()):
+            raise ValueError(f"powers must be a contiguous [8, {self.N}, {M}] {self.dtype} CUDA tensor")
+
     def density(self, psi, occ) -> torch.Tensor:
         psi = self._check(psi)
         occ_t = torch.as_tensor(occ, dtype=torch.float64, device=self.device).contiguous()

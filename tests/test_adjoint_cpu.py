@@ -61,6 +61,45 @@ class DenseHam:
         psi.copy_(self._T(float(kA2[0]), dt, self._T(float(kA1[0]), dt, psi)))
         return psi
 
+    @staticmethod
+    def _c(dt):
+        c = [1.0 + 0j]
+        for k in range(1, 5):
+            c.append(c[-1] * 0.5j * dt / k)
+        return c
+
+    def _half(self, a, dt, x, P):
+        # the library's half step with powers: P[k] = H^k x, result sum_k c_k H^k x
+        self.a = a
+        c = self._c(dt)
+        P[0].copy_(x)
+        for k in range(1, 4):
+            P[k].copy_(self.H() @ P[k - 1])
+        h4 = self.H() @ P[3]
+        return sum(c[k] * P[k] for k in range(4)) + c[4] * h4
+
+    def etrs_step_powers_(self, psi, dt, kA1, kA2, powers):
+        phi = self._half(float(kA1[0]), dt, psi, powers[0:4])
+        psi.copy_(self._half(float(kA2[0]), dt, phi, powers[4:8]))
+        return psi
+
+    def _back(self, a, dt, lam, Phi, gV, gA):
+        self.a = a
+        cc = [np.conj(x) for x in self._c(dt)]
+        L = [lam.clone()]
+        for _ in range(4):
+            L.append(self.H() @ L[-1])
+        for i in range(4):
+            xi = sum(cc[i + j + 1] * L[j] for j in range(4 - i))
+            gV += (2.0 * (xi.conj() * Phi[i]).sum(1)).real
+            gA[0] += (2.0 * (xi.conj() * (self.D @ Phi[i])).sum()).real
+        return sum(cc[k] * L[k] for k in range(5))
+
+    def etrs_adjoint_step_(self, lam, dt, kA1, kA2, powers, gV, gA_t, gA_tdt):
+        lam.copy_(self._back(float(kA2[0]), dt, lam, powers[4:8], gV, gA_tdt))
+        lam.copy_(self._back(float(kA1[0]), dt, lam, powers[0:4], gV, gA_t))
+        return lam
+
     def density(self, psi, occ):
         return ((psi.abs() ** 2) * torch.as_tensor(occ)[None, :]).sum(1)
 
