@@ -366,8 +366,13 @@ def run_ours(args):
         ref = o.apply_h(sub)
         mixed = y32[:, :4].cpu().numpy().astype(np.complex128)
         fp64 = y64[:, :4].cpu().numpy()
+        eps_ref = o.band_energies(sub, ref)
+        eps32 = h32.band_energies(x32[:, :4], y32[:, :4])
+        eps64 = h64.band_energies(x64[:, :4], y64[:, :4])
         err_oracle = {"mixed_rel_norm": float(np.linalg.norm(mixed - ref) / np.linalg.norm(ref)),
                       "fp64_rel_max": float(np.abs(fp64 - ref).max() / np.abs(ref).max()),
+                      "band_energies_mixed_rel_max": float(np.abs(eps32 - eps_ref).max() / np.abs(eps_ref).max()),
+                      "band_energies_fp64_rel_max": float(np.abs(eps64 - eps_ref).max() / np.abs(eps_ref).max()),
                       "orbitals_checked": 4}
 
     def timed(fn, K, W):

@@ -7,6 +7,7 @@
 // Input orbitals may be complex64 (mixed) or complex128; every sum is FP64.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "dft.cuh"
@@ -209,6 +210,47 @@ int launch_density(int precision, const void* psi, long ld, int M, long N, const
                    void* stream) {
   return precision == INQB_FP64 ? density_impl<double>(psi, ld, M, N, occ, rho, (cudaStream_t)stream)
                                 : density_impl<float>(psi, ld, M, N, occ, rho, (cudaStream_t)stream);
+}
+
+// acc[3 m .. 3 m + 2] += (Re, Im) sum_p conj(hpsi) psi and sum_p |psi|^2 over this
+// block's points (overlap_diagonal.hpp:118-127); threads run along the orbitals.
+template <typename T>
+__global__ void k_band_sums(const cplx<T>* __restrict__ psi, const cplx<T>* __restrict__ hpsi, long ld, int M,
+                            long N, long pts_per_block, double* __restrict__ acc) {
+  const long p0 = (long)blockIdx.x * pts_per_block, p1 = min(N, p0 + pts_per_block);
+  for (int m = blockIdx.y * blockDim.x + threadIdx.x; m < M; m += gridDim.y * blockDim.x) {
+    double vr = 0.0, vi = 0.0, nn = 0.0;
+    for (long p = p0; p < p1; p++) {
+      const cplx<T> a = hpsi[p * ld + m], b = psi[p * ld + m];
+      const double ax = a.x, ay = a.y, bx = b.x, by = b.y;
+      vr += ax * bx + ay * by;
+      vi += ax * by - ay * bx;
+      nn += bx * bx + by * by;
+    }
+    atomicAdd(&acc[3 * m], vr);
+    atomicAdd(&acc[3 * m + 1], vi);
+    atomicAdd(&acc[3 * m + 2], nn);
+  }
+}
+
+template <typename T>
+static int band_sums_impl(const void* psi, const void* hpsi, long ld, int M, long N, double* acc, cudaStream_t st) {
+  INQB_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * 3 * (size_t)M, st));
+  const int threads = 128;
+  const int ym = (M + threads - 1) / threads;
+  // about 4 blocks per SM over the points
+  const long nblk = std::max<long>(1, std::min<long>(N, 148L * 4 / ym + 1));
+  const long per = (N + nblk - 1) / nblk;
+  k_band_sums<T><<<dim3((unsigned)((N + per - 1) / per), ym), threads, 0, st>>>(
+      (const cplx<T>*)psi, (const cplx<T>*)hpsi, ld, M, N, per, acc);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_band_sums(int precision, const void* psi, const void* hpsi, long ld, int M, long N, double* acc,
+                     void* stream) {
+  return precision == INQB_FP64 ? band_sums_impl<double>(psi, hpsi, ld, M, N, acc, (cudaStream_t)stream)
+                                : band_sums_impl<float>(psi, hpsi, ld, M, N, acc, (cudaStream_t)stream);
 }
 
 int launch_dipole(const double* rho, long N, const double lat[3][3], const int nr[3], double* out_dev,

@@ -7,6 +7,9 @@ namespace inqb {
 
 int launch_density(int precision, const void* psi, long ld, int M, long N, const double* occ, double* rho,
                    void* stream);
+// acc[3 m + {0,1,2}] = (Re, Im) sum_p conj(hpsi) psi, sum_p |psi|^2 (FP64)
+int launch_band_sums(int precision, const void* psi, const void* hpsi, long ld, int M, long N, double* acc,
+                     void* stream);
 int launch_dipole(const double* rho, long N, const double lat[3][3], const int nr[3], double* out_dev, void* stream);
 int launch_orthonormalize(int precision, void* psi, long ld, int M, long N, double dV, double2* S, double2* X,
                           int* info, void* stream);

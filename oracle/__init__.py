@@ -63,6 +63,9 @@ def lib():
         L.orc_etrs_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
         L.orc_density.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]
         L.orc_dipole.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_band_energies.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]
+        L.orc_crank_nicolson_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp,
+                                              ctypes.c_int, ctypes.c_double, _ip, _dp]
         L.orc_rvectors.argtypes = [ctypes.c_void_p, _dp]
         L.orc_orthonormalize.restype = ctypes.c_int
         L.orc_orthonormalize.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
@@ -202,6 +205,17 @@ class System:
         lib().orc_etrs_step(self._h, out.shape[1], float(dt), _d(a), _d(b), _d(out.view(np.float64)))
         return out
 
+    def crank_nicolson_step(self, psi, dt, kA_t, kA_tdt, max_sweeps=300, tol=1e-10):
+        """(new orbitals, sweeps run, last residual)"""
+        out = self._psi(psi).copy()
+        a = np.ascontiguousarray(kA_t, np.float64).reshape(3)
+        b = np.ascontiguousarray(kA_tdt, np.float64).reshape(3)
+        k = ctypes.c_int(0)
+        r = ctypes.c_double(0.0)
+        lib().orc_crank_nicolson_step(self._h, out.shape[1], float(dt), _d(a), _d(b), _d(out.view(np.float64)),
+                                      int(max_sweeps), float(tol), ctypes.byref(k), ctypes.byref(r))
+        return out, k.value, r.value
+
     def density(self, psi, occ):
         psi = self._psi(psi)
         occ = np.ascontiguousarray(occ, np.float64).reshape(psi.shape[1])
@@ -214,6 +228,13 @@ class System:
         out = np.zeros(3)
         lib().orc_dipole(self._h, _d(rho), _d(out))
         return out
+
+    def band_energies(self, psi, hpsi):
+        psi = self._psi(psi)
+        hpsi = self._psi(hpsi)
+        eps = np.zeros(psi.shape[1])
+        lib().orc_band_energies(self._h, psi.shape[1], _d(psi.view(np.float64)), _d(hpsi.view(np.float64)), _d(eps))
+        return eps
 
     def rvectors(self):
         out = np.zeros((self.N, 3))

@@ -553,6 +553,76 @@ void orc_etrs_step(void *h, int M, double dt, const double *kA_t, const double *
   exponential_in_place(*s, M, cd(0.0, dt / 2.0), (cd *)psi, 4);
 }
 
+// crank_nicolson_op (crank_nicolson.hpp:22-38): out = phi + factor H phi
+static void cn_op(const System &s, int M, cd factor, const cd *phi, cd *out) {
+  apply_h(s, M, phi, out);
+  const long n = s.grid.npoints * (long)M;
+  for (long i = 0; i < n; i++) out[i] = phi[i] + factor * out[i];
+}
+
+// solvers::steepest_descent without preconditioner (steepest_descent.hpp:22-80):
+// num_steps = 5 updates phi += lambda r, lambda the root cc / qq of the quadratic
+// built from mm = (<hsd|hsd>, <r|hsd>, <r|r>) (overlap_diagonal, dV included).
+// Returns max_m |<r|r>| of the last step.
+static double steepest_descent(const System &s, int M, cd factor, const cd *rhs, cd *phi) {
+  const long N = s.grid.npoints, n = N * (long)M;
+  const double dV = s.grid.volume_element();
+  std::vector<cd> r(n), hsd(n);
+  std::vector<double> normres(M);
+  for (int istep = 0; istep < 5; istep++) {
+    cn_op(s, M, factor, phi, r.data());
+    for (long i = 0; i < n; i++) r[i] -= rhs[i];
+    cn_op(s, M, factor, r.data(), hsd.data());
+    for (int m = 0; m < M; m++) {
+      cd m0 = 0.0, m1 = 0.0, m2 = 0.0;
+      for (long p = 0; p < N; p++) {
+        const cd a = r[p * M + m], b = hsd[p * M + m];
+        m0 += std::conj(b) * b;
+        m1 += std::conj(a) * b;
+        m2 += std::conj(a) * a;
+      }
+      const cd ca = dV * m0;
+      const double cb = 4.0 * (dV * m1).real();
+      const cd cc = dV * m2;
+      normres[m] = std::abs(cc);
+      const cd sqarg = cb * cb - 4.0 * ca * cc;
+      const double signb = ((std::conj(cd(cb)) * sqarg).real() >= 0) ? 1.0 : -1.0;
+      const cd qq = -0.5 * (cb + signb * std::sqrt(sqarg));
+      const cd lam = cc / qq;
+      for (long p = 0; p < N; p++) phi[p * M + m] += lam * r[p * M + m];
+    }
+  }
+  double mx = 0.0;
+  for (double v : normres) mx = std::max(mx, v);
+  return mx;
+}
+
+// Crank-Nicolson step for a density-independent Hamiltonian (crank_nicolson.hpp:41-114):
+// rhs = psi - i dt/2 H(t) psi; then sweeps of steepest_descent on
+// (1 + i dt/2 H(t+dt)) phi = rhs from phi = psi until the returned residual is below
+// tol or max_sweeps ran.  (The reference ends its outer loop on the density change
+// under Broyden mixing, which for a density-independent H only sets how many sweeps
+// run; here the solver residual sets it.)
+void orc_crank_nicolson_step(void *h, int M, double dt, const double *kA_t, const double *kA_tdt, double *psi_,
+                             int max_sweeps, double tol, int *sweeps, double *residual) {
+  auto *s = (System *)h;
+  cd *psi = (cd *)psi_;
+  const long n = s->grid.npoints * (long)M;
+  std::vector<cd> rhs(n);
+  orc_set_vector_potential_cov(h, kA_t);
+  cn_op(*s, M, cd(0.0, -0.5 * dt), psi, rhs.data());
+  orc_set_vector_potential_cov(h, kA_tdt);
+  double res = 0.0;
+  int k = 0;
+  while (k < max_sweeps) {
+    res = steepest_descent(*s, M, cd(0.0, 0.5 * dt), rhs.data(), psi);
+    k++;
+    if (res < tol) break;
+  }
+  *sweeps = k;
+  *residual = res;
+}
+
 // density::calculate_add (density.hpp:23-33)
 void orc_density(void *h, int M, const double *psi, const double *occ, double *rho) {
   auto *s = (System *)h;
@@ -562,6 +632,25 @@ void orc_density(void *h, int M, const double *psi, const double *occ, double *r
     double acc = 0.0;
     for (int m = 0; m < M; m++) acc += occ[m] * std::norm(ps[p * M + m]);
     rho[p] = acc;
+  }
+}
+
+// Band energies: operations::overlap_diagonal_normalized(H psi, psi, real_part)
+// (overlap_diagonal.hpp:118-170, called by energy.hpp:74-76):
+// eps[m] = Re( sum_p conj(Hpsi[p][m]) psi[p][m] / sum_p |psi[p][m]|^2 ).
+void orc_band_energies(void *h, int M, const double *psi, const double *hpsi, double *eps) {
+  auto *s = (System *)h;
+  const cd *ps = (const cd *)psi, *hs = (const cd *)hpsi;
+  const long N = s->grid.npoints;
+#pragma omp parallel for
+  for (int m = 0; m < M; m++) {
+    cd value = 0.0;
+    double norm = 0.0;
+    for (long p = 0; p < N; p++) {
+      value += std::conj(hs[p * M + m]) * ps[p * M + m];
+      norm += std::norm(ps[p * M + m]);
+    }
+    eps[m] = (value / norm).real();
   }
 }
 

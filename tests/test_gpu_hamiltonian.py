@@ -180,3 +180,16 @@ def test_apply_h_fourier_mask(pb, oracle_mod, cfg0_small, precision, tol):
     ref = o.apply_h(s["psi"])
     err = rel_max(out, ref) if precision == "fp64" else rel_norm(out, ref)
     assert err < tol, err
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 1e-6)])
+def test_band_energies_match_oracle(pb, oracle_mod, cfg0_small, precision, tol):
+    """inqb_band_energies (overlap_diagonal_normalized(H psi, psi, real_part)) against
+    the oracle's H psi and band energies, relative to the largest |eps|."""
+    s = cfg0_small
+    o = make_oracle(oracle_mod, s)
+    ref = o.band_energies(s["psi"], o.apply_h(s["psi"]))
+    h = make_product(pb, s, precision)
+    dt = torch.complex128 if precision == "fp64" else torch.complex64
+    eps = h.band_energies(_dev(s["psi"], dt))
+    assert np.abs(eps - ref).max() <= tol * np.abs(ref).max(), (eps, ref)

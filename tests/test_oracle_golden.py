@@ -181,3 +181,23 @@ def test_fourier_sphere_mask(oracle_mod):
     lap = 0.5 * (G ** 2).sum(-1) * inside
     ref = np.fft.ifftn(lap[..., None] * np.fft.fftn(psi.reshape(*nr, 2), axes=(0, 1, 2)), axes=(0, 1, 2))
     assert np.abs(o.apply_h(psi) - ref.reshape(-1, 2)).max() < 1e-12 * np.abs(ref).max()
+
+
+def test_band_energies_normalized_overlap(oracle_mod):
+    """overlap_diagonal_normalized on the complex field_set of its unit test
+    (operations/overlap_diagonal.hpp:280-343): 800 points, 12 vectors,
+    aa = 20 (i+1) sqrt(j+1) e^{i(-pi/4 + pi i/7)}, bb = -0.05/(i+1) sqrt(j+1)
+    e^{i(pi/4 + pi i/7)}.  Band energies take the real part with phi1 = H psi = aa
+    and phi2 = psi = bb.  In closed form conj(aa) bb = -i (j+1), so the ratio is
+    -i K with K = 800 / (0.0025 sum_i 1/(i+1)^2) for every vector: real part 0;
+    with aa rotated by e^{i pi/3} the real part is -K sqrt(3)/2."""
+    i = np.arange(800)[:, None]
+    j = np.arange(12)[None, :]
+    aa = 20.0 * (i + 1) * np.sqrt(j + 1) * np.exp(1j * (-np.pi / 4 + np.pi / 7 * i))
+    bb = -0.05 / (i + 1) * np.sqrt(j + 1) * np.exp(1j * (np.pi / 4 + np.pi / 7 * i))
+    K = 800.0 / (0.0025 * (1.0 / (np.arange(800) + 1.0) ** 2).sum())
+    o = oracle_mod.System(np.diag([8.0, 10.0, 10.0]), (8, 10, 10))
+    eps = o.band_energies(bb, aa)
+    assert np.abs(eps).max() < 1e-13 * K
+    eps = o.band_energies(bb, aa * np.exp(1j * np.pi / 3))
+    assert np.allclose(eps, -K * np.sqrt(3.0) / 2.0, rtol=1e-13, atol=0)
