@@ -150,6 +150,13 @@ int inqb_density(inqb_ctx* ctx, const void* psi, int M, int ld, const double* oc
  * out = dV sum_p r_p rho[p] with symmetric-range r; rho on device, out on
  * host; synchronous. */
 int inqb_dipole(inqb_ctx* ctx, const double* rho, double out[3], void* stream);
+/* Band energies eps[m] = Re(<Hpsi_m|psi_m>) / <psi_m|psi_m> as
+ * operations::overlap_diagonal_normalized(H psi, psi, real_part) computes them
+ * for hamiltonian::energy (src/operations/overlap_diagonal.hpp:118-170,
+ * src/hamiltonian/energy.hpp:74-76); FP64 sums in both precisions.  eps is host
+ * memory [M]; synchronous. */
+int inqb_band_energies(inqb_ctx* ctx, const void* psi, const void* hpsi, int M, int ld, double* eps,
+                       void* stream);
 /* operations::orthogonalize (src/operations/orthogonalize.hpp:25-32): FP64
  * overlap S = dV psi^H psi, Cholesky S = U^H U, psi <- psi U^-1; synchronous. */
 int inqb_orthonormalize(inqb_ctx* ctx, void* psi, int M, int ld, void* stream);
@@ -188,6 +195,18 @@ int inqb_accum_potential_gradient(inqb_ctx* ctx, const void* u, const void* w, i
 int inqb_accum_vector_potential_gradient(inqb_ctx* ctx, const void* u, const void* w, int M, int ld, double c_re,
                                          double c_im, double* gA, void* stream);
 
+/* real_time::crank_nicolson for a density-independent H
+ * (src/real_time/crank_nicolson.hpp:22-114): rhs = (1 - i dt/2 H(kA_t)) psi, then
+ * sweeps of solvers::steepest_descent (five steps each, no preconditioner,
+ * src/solvers/steepest_descent.hpp:22-80) on (1 + i dt/2 H(kA_tdt)) psi' = rhs,
+ * starting from psi, until the largest residual dV <r|r> of a sweep is below tol
+ * or max_sweeps ran (the reference caps its loop at 300).  The reference ends the
+ * loop on the density change under Broyden mixing, which for a density-independent
+ * H only sets the number of sweeps.  Solver sums and step lengths are FP64.
+ * Synchronous (one read-back per sweep); sweeps and residual may be NULL. */
+int inqb_crank_nicolson_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                             const double kA_tdt_cov[3], int max_sweeps, double tol, int* sweeps, double* residual,
+                             void* stream);
 /* One ETRS step (the reference's real_time::etrs step with a density-independent
  * H, src/real_time/etrs.hpp:22-82) that also keeps what its adjoint needs:
  * psi <- T(kA_tdt) T(kA_t) psi, T = sum_{k<=4} (i dt/2 H)^k / k!, and powers =

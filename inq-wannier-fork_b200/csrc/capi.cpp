@@ -10,6 +10,7 @@
 #include "inqb_internal.h"
 #include "adjoint.h"
 #include "observables.h"
+#include "propagators.h"
 #include "plan.h"
 
 namespace inqb {
@@ -539,6 +540,64 @@ int inqb_etrs_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const dou
   return INQB_OK;
 }
 
+int inqb_crank_nicolson_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                             const double kA_tdt_cov[3], int max_sweeps, double tol, int* sweeps, double* residual,
+                             void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!kA_t_cov || !kA_tdt_cov || !std::isfinite(dt) || max_sweeps < 1 || !(tol >= 0.0))
+    return fail(INQB_ERR_INVALID, "bad step arguments");
+  INQB_GUARD(ctx);
+  INQB_TRY(reserve(ctx, M));
+  const size_t blk = (size_t)ctx->N * M * ctx->elem_bytes();
+  INQB_TRY(ctx->d_cn.ensure(3 * blk));
+  INQB_TRY(ctx->d_cnred.ensure(sizeof(double) * 5 * (size_t)M));
+  char* w = static_cast<char*>(ctx->d_cn.ptr);
+  void* rhs = w;
+  void* r = w + blk;
+  void* hsd = w + 2 * blk;
+  double* acc = ctx->d_cnred.as<double>();
+  double* normres = acc + 4 * (size_t)M;
+  const long Mi = M;
+  cudaStream_t st = (cudaStream_t)stream;
+  // rhs = (1 - i dt/2 H(t)) psi  (op_rhs, crank_nicolson.hpp:49-55)
+  INQB_TRY(set_kA(ctx, kA_t_cov, stream));
+  const double one[2] = {1.0, 0.0};
+  const double fr[2] = {0.0, -0.5 * dt}, fl[2] = {0.0, 0.5 * dt};
+  INQB_TRY(apply(ctx, LaunchArgs::H, psi, ld, rhs, Mi, M, psi, ld, fr, one, stream));
+  INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
+  std::vector<double> hres(M);
+  double res = 0.0;
+  int k = 0;
+  while (k < max_sweeps) {
+    // steepest_descent (steepest_descent.hpp:22-80): five steps, no preconditioner
+    for (int step = 0; step < 5; step++) {
+      // r = (1 + i dt/2 H) phi - rhs
+      INQB_TRY(apply(ctx, LaunchArgs::H, psi, ld, r, Mi, M, psi, ld, fl, one, stream));
+      {
+        const double a[2][2] = {{1.0, 0.0}, {-1.0, 0.0}};
+        const void* x[2] = {r, rhs};
+        const long ldx[2] = {Mi, Mi};
+        INQB_TRY(launch_lincomb(ctx->precision, ctx->N, M, 2, a, x, ldx, r, Mi, stream));
+      }
+      // hsd = (1 + i dt/2 H) r
+      INQB_TRY(apply(ctx, LaunchArgs::H, r, Mi, hsd, Mi, M, r, Mi, fl, one, stream));
+      INQB_TRY(launch_sd_sums(ctx->precision, r, hsd, Mi, M, ctx->N, acc, stream));
+      INQB_TRY(launch_sd_update(ctx->precision, psi, ld, r, Mi, M, ctx->N, acc, ctx->dV, normres, stream));
+    }
+    k++;
+    INQB_CUDA_TRY(cudaMemcpyAsync(hres.data(), normres, sizeof(double) * M, cudaMemcpyDeviceToHost, st));
+    INQB_CUDA_TRY(cudaStreamSynchronize(st));
+    res = 0.0;
+    for (double v : hres) res = std::max(res, v);
+    if (!std::isfinite(res)) return fail(INQB_ERR_NONFINITE, "Crank-Nicolson residual is not finite");
+    if (res < tol) break;
+  }
+  if (sweeps) *sweeps = k;
+  if (residual) *residual = res;
+  return INQB_OK;
+}
+
 int inqb_density(inqb_ctx* ctx, const void* psi, int M, int ld, const double* occ, double* rho, void* stream) {
   INQB_CHECK_CTX(ctx);
   INQB_TRY(check_block(ctx, psi, M, ld));
@@ -558,6 +617,23 @@ int inqb_dipole(inqb_ctx* ctx, const double* rho, double out[3], void* stream) {
   INQB_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
   INQB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
   for (int k = 0; k < 3; k++) out[k] = ctx->dV * h[k];
+  return INQB_OK;
+}
+
+int inqb_band_energies(inqb_ctx* ctx, const void* psi, const void* hpsi, int M, int ld, double* eps,
+                       void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  INQB_TRY(check_block(ctx, hpsi, M, ld));
+  if (!eps) return fail(INQB_ERR_INVALID, "null output");
+  INQB_GUARD(ctx);
+  INQB_TRY(ctx->d_band.ensure(sizeof(double) * 3 * (size_t)M));
+  double* d = ctx->d_band.as<double>();
+  INQB_TRY(launch_band_sums(ctx->precision, psi, hpsi, ld, M, ctx->N, d, stream));
+  std::vector<double> h(3 * (size_t)M);
+  INQB_CUDA_TRY(cudaMemcpyAsync(h.data(), d, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  INQB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  for (int m = 0; m < M; m++) eps[m] = h[3 * m] / h[3 * m + 2];
   return INQB_OK;
 }
 

@@ -170,9 +170,12 @@ struct inqb_ctx {
   inqb::DevBuf d_work;    // one orbital block for propagators
   inqb::DevBuf d_work2;
   inqb::DevBuf d_red;     // small reduction buffers
+  inqb::DevBuf d_band;    // band-energy sums, 3 doubles per orbital
   inqb::DevBuf d_adjU, d_adjW;  // Fourier transforms for the dH/dA inner products
   inqb::DevBuf d_nlpart;        // per-chunk nonlocal moments of the dH/dA inner products
   inqb::DevBuf d_adjL;          // adjoint step: H^j lambda (4 blocks), Xi, spare
+  inqb::DevBuf d_cn;            // Crank-Nicolson: rhs, residual, (1 + i dt/2 H) residual
+  inqb::DevBuf d_cnred;         // Crank-Nicolson: 4 sums and the residual norm per orbital
   size_t elem_bytes() const { return precision == INQB_FP64 ? 16 : 8; }
 
   // optional per-pass CUDA-event timing of H applications

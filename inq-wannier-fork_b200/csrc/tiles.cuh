@@ -74,7 +74,7 @@ struct TileGeom {
 
 // Entry records staged in shared memory per tile; a tile with more entries
 // reads its records from global memory.
-constexpr int kRecCapMax = 1024;
+constexpr int kRecCapMax = 0;
 
 // Start the cp.async copy of tile `tile`'s entry records (from `recs`) into R
 // (cap records).  Returns the records to index with (e - roff): R when staged,

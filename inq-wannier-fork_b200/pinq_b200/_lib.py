@@ -50,7 +50,10 @@ SIGNATURES = {
     "inqb_density": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "inqb_dipole": (ctypes.c_int, [_ctxp, _vp, _dp, _vp]),
     "inqb_orthonormalize": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "inqb_band_energies": (ctypes.c_int, [_ctxp, _vp, _vp, ctypes.c_int, ctypes.c_int, _dp, _vp]),
     "inqb_orthonormalize_noalloc": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "inqb_crank_nicolson_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
+                                                ctypes.c_int, ctypes.c_double, _ip, _dp, _vp]),
     "inqb_etrs_step_powers": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
                                              _vp, _vp]),
     "inqb_etrs_adjoint_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,

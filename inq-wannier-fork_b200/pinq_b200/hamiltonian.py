@@ -222,6 +222,17 @@ class KSHamiltonian:
              self._stream())
         return psi
 
+    def crank_nicolson_step_(self, psi, dt, kA_t_cov, kA_tdt_cov, max_sweeps=300, tol=1e-10):
+        """One Crank-Nicolson step in place; returns (sweeps run, last residual)."""
+        psi = self._check(psi)
+        a = np.ascontiguousarray(kA_t_cov, np.float64).reshape(3)
+        b = np.ascontiguousarray(kA_tdt_cov, np.float64).reshape(3)
+        k = ctypes.c_int(0)
+        r = ctypes.c_double(0.0)
+        call("inqb_crank_nicolson_step", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), float(dt), dptr(a),
+             dptr(b), int(max_sweeps), float(tol), ctypes.byref(k), ctypes.byref(r), self._stream())
+        return k.value, r.value
+
     def etrs_step_powers_(self, psi, dt, kA_t_cov, kA_tdt_cov, powers):
         """One ETRS step in place that also writes the 8 Taylor-power blocks the
         adjoint step reads into `powers` ([8, N, M], contiguous)."""
@@ -310,6 +321,20 @@ class KSHamiltonian:
         n = ctypes.c_int(0)
         call("inqb_timing_stop", self._h, dptr(ms), ctypes.byref(n))
         return ms, n.value
+
+    def band_energies(self, psi, hpsi=None) -> np.ndarray:
+        """eps[m] = Re<H psi_m|psi_m> / <psi_m|psi_m> (FP64 sums); H psi is applied
+        here when not given."""
+        psi = self._check(psi)
+        if hpsi is None:
+            hpsi = self.apply(psi)
+        hpsi = self._check(hpsi)
+        if hpsi.shape != psi.shape or hpsi.stride(0) != psi.stride(0):
+            raise ValueError("psi and hpsi must have the same shape and leading dimension")
+        eps = np.zeros(psi.shape[1])
+        call("inqb_band_energies", self._h, psi.data_ptr(), hpsi.data_ptr(), psi.shape[1], psi.stride(0), dptr(eps),
+             self._stream())
+        return eps
 
     def orthonormalize_(self, psi):
         psi = self._check(psi)

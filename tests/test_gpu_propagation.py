@@ -100,3 +100,37 @@ def test_orthonormalize_rejects_dependent_set(pb):
     with pytest.raises(pb.InqbError) as e:
         h.orthonormalize_(_dev(psi))
     assert e.value.status == 6
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 2e-5)])
+def test_crank_nicolson_matches_oracle(pb, oracle_mod, sysd, precision, tol):
+    """One Crank-Nicolson step (crank_nicolson.hpp:41-114, steepest_descent.hpp:22-80)
+    with a vector potential changing over the step and a fixed three sweeps
+    (tol = 0): the same fifteen solver steps on the GPU and in the oracle."""
+    o = make_oracle(oracle_mod, sysd)
+    h = make_product(pb, sysd, precision)
+    k1 = o.cart_to_cov(np.array([0.01, 0.0, 0.0]))
+    k2 = o.cart_to_cov(np.array([0.02, 0.0, 0.0]))
+    ref, kref, rref = o.crank_nicolson_step(sysd["psi"], 0.05, k1, k2, max_sweeps=3, tol=0.0)
+    dt = torch.complex128 if precision == "fp64" else torch.complex64
+    x = _dev(sysd["psi"], dt)
+    k, r = h.crank_nicolson_step_(x, 0.05, k1, k2, max_sweeps=3, tol=0.0)
+    assert k == kref == 3
+    err = rel_max(x.cpu().numpy(), ref) if precision == "fp64" else rel_norm(x.cpu().numpy(), ref)
+    assert err <= tol, err
+    assert abs(r - rref) <= 1e-3 * rref + 1e-12
+
+
+def test_crank_nicolson_converges_and_keeps_norms(pb, oracle_mod, sysd):
+    """Solved to a small residual the step is the Cayley transform of H: unitary, so
+    the orbital norms are kept; and it agrees with ETRS run with -dt (the reference's
+    CN propagates with exp(-i dt H), its ETRS with exp(+i dt H)) to O(dt^3)."""
+    h = make_product(pb, sysd, "fp64")
+    x = _dev(sysd["psi"])
+    n0 = x.norm(dim=0)
+    k, r = h.crank_nicolson_step_(x, 0.01, np.zeros(3), np.zeros(3), max_sweeps=300, tol=1e-22)
+    assert r < 1e-22 and k < 300
+    assert float(((x.norm(dim=0) - n0).abs() / n0).max()) < 1e-10
+    o = make_oracle(oracle_mod, sysd)
+    e = o.etrs_step(sysd["psi"], -0.01, np.zeros(3), np.zeros(3))
+    assert rel_norm(x.cpu().numpy(), e) < 1e-3
