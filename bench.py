@@ -427,6 +427,20 @@ def run_ours(args):
     ms_etrs32 = timed(lambda: etrs(h32, xe32), args.etrs_steps, W)
     ms_etrs64 = timed(lambda: etrs(h64, xe64), args.etrs_steps, W)
 
+    # -- Crank-Nicolson steps (steepest-descent sweeps to a residual of 1e-10), 2 steps each
+    cn = {}
+    for name, h, x in (("mixed", h32, x32), ("fp64", h64, x64)):
+        xc = x[:, :32].clone()
+        h.crank_nicolson_step_(xc, 0.05, cov[0], cov[1], 300, 1e-10)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sweeps = [h.crank_nicolson_step_(xc, 0.05, cov[n], cov[n + 1], 300, 1e-10)[0] for n in range(2)]
+        torch.cuda.synchronize()
+        cn[f"{name}_steps_per_s"] = 2 / (time.perf_counter() - t0)
+        cn[f"{name}_sweeps_per_step"] = sweeps
+    cn.update({"orbitals": 32, "dt": 0.05, "tol": 1e-10, "H_applies_per_sweep": 10,
+               "timing": "wall clock around device-synchronised calls (one read-back per sweep)"})
+
     # -- e2e through the host-buffer C-ABI call (pinned host memory, copies in the timed region)
     xh = x32.cpu().pin_memory()
     yh = torch.empty_like(xh).pin_memory()
@@ -502,6 +516,7 @@ def run_ours(args):
         "etrs": {"mixed_steps_per_s": world * args.etrs_steps / (ms_etrs32 * 1e-3),
                  "fp64_steps_per_s": world * args.etrs_steps / (ms_etrs64 * 1e-3),
                  "H_applies_per_step": 8, "dt": 0.05},
+        "crank_nicolson": cn,
         "error": {"mixed_vs_fp64_gpu_rel_norm": err_fp64, "vs_oracle": err_oracle},
     }
     if cells is not None:
