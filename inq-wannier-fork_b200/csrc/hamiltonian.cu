@@ -662,8 +662,11 @@ static int launch_h_impl(const LaunchArgs& a) {
     ep.ld_base = a.ld_base;
     ep.alpha = mk<T>((T)a.alpha[0], (T)a.alpha[1]);
     ep.beta = mk<T>((T)a.beta[0], (T)a.beta[1]);
-    k_tile_inv<T, NX, NY, NZ><<<dim3(tgroups, NX * TG::Y1), TG::THREADS, TG::smem_inv(rec_cap, seg_cap), st>>>(
-        tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap, seg_cap,
+    // pass C stages the records in shared memory only in FP64 (where the orbital
+    // prefetch already limits it to two CTAs per SM); FP32 keeps the smem for CTAs
+    const int rec_cap_inv = TG::PREFETCH ? rec_cap : 0;
+    k_tile_inv<T, NX, NY, NZ><<<dim3(tgroups, NX * TG::Y1), TG::THREADS, TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
+        tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv, seg_cap,
         tvout);
     if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
   } else if (a.mode == LaunchArgs::FFT_FWD) {

@@ -57,7 +57,7 @@ struct TileGeom {
     return sizeof(cplx<T>) * ((size_t)TILE + NY + NZ) + sizeof(double2) * (size_t)acc_atoms * LMAX * G +
            sizeof(EntRec<T>) * (size_t)rec_cap;
   }
-  static constexpr size_t SMEM_X = sizeof(cplx<T>) * ((size_t)XBLK + NX);
+  static constexpr size_t SMEM_X = sizeof(cplx<T>) * ((size_t)XBLK + NX) + sizeof(T) * 2 * Y1;
   static constexpr int PSTRIDE = (PTS + 1 + 3) / 4 * 4;  // ints of a tile's point index
   // pass C prefetches the input orbitals of its tile into shared memory in FP64
   // (two CTAs per SM either way, so the copy overlaps the transforms for free);
@@ -74,7 +74,7 @@ struct TileGeom {
 
 // Entry records staged in shared memory per tile; a tile with more entries
 // reads its records from global memory.
-constexpr int kRecCapMax = 0;
+constexpr int kRecCapMax = 1024;
 
 // Start the cp.async copy of tile `tile`'s entry records (from `recs`) into R
 // (cap records).  Returns the records to index with (e - roff): R when staged,
@@ -283,6 +283,8 @@ __global__ void __launch_bounds__(256)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* X = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* twx = X + TG::XBLK;
+  T* kinB = reinterpret_cast<T*>(twx + NX);  // [Y1] linear and [Y1] constant term per kb
+  T* kinC = kinB + Y1;
 
   const int kz = blockIdx.x % NZ, ka = blockIdx.x / NZ, grp = blockIdx.y;
   cplx<T>* blk = tmp + ((long)(grp * Y2 + ka) * NZ + kz) * TG::BLK;
@@ -293,8 +295,25 @@ __global__ void __launch_bounds__(256)
   }
   cp_async_commit();
   for (int i = threadIdx.x; i < NX; i += blockDim.x) twx[i] = tw_x[i];
+  // Along an x line 1/2 |G + k + A|^2 / N = kA2 n0^2 + kinB n0 + kinC with
+  // q = n1 b1 + n2 b2 + k + A:  kA2 = |b0|^2 / 2N, kinB = b0.q / N, kinC = |q|^2 / 2N
+  if (threadIdx.x < Y1) {
+    const int kb = threadIdx.x;
+    const T n1 = (T)sym_freq(ka + Y2 * kb, NY), n2 = (T)sym_freq(kz, NZ);
+    T q[3], bq = 0, qq = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      q[d] = n1 * kp.b[1][d] + n2 * kp.b[2][d] + kp.kA[d];
+      bq += kp.b[0][d] * q[d];
+      qq += q[d] * q[d];
+    }
+    kinB[kb] = kp.scale * bq;
+    kinC[kb] = (T)0.5 * kp.scale * qq;
+  }
   cp_async_wait<0>();
   __syncthreads();
+  const T kinA = (T)0.5 * kp.scale *
+                 (kp.b[0][0] * kp.b[0][0] + kp.b[0][1] * kp.b[0][1] + kp.b[0][2] * kp.b[0][2]);
 
   // outer y stage: DFT_Y1 over y1 -> kb, for each (ix, j)
   for (int it = threadIdx.x; it < NX * G; it += blockDim.x) {
@@ -326,9 +345,10 @@ __global__ void __launch_bounds__(256)
   __syncthreads();
   step2_fwd_op_inv<AX>(X, Y1 * G * AX::N1, twx, map2, [&](int it, int kx, cplx<T> v) {
     const int kb = (it / G) / AX::N1;
-    const int n0 = sym_freq(kx, NX), n1 = sym_freq(ka + Y2 * kb, NY);
-    T k = kinetic(kp, n0, n1, n2);
-    if (kp.mask) k = outside_sphere(kp.nr, n0, n1, n2) ? (T)0 : k - kp.shift;
+    const int n0 = sym_freq(kx, NX);
+    const T f0 = (T)n0;
+    T k = fma(fma(kinA, f0, kinB[kb]), f0, kinC[kb]);
+    if (kp.mask) k = outside_sphere(kp.nr, n0, sym_freq(ka + Y2 * kb, NY), n2) ? (T)0 : k - kp.shift;
     return k * v;
   });
   __syncthreads();
@@ -393,7 +413,7 @@ __global__ void __launch_bounds__(256)
   int roff = 0, s0 = 0, nseg = 0;
   const EntRec<T>* rec = pj.ent_rec_pt;
   if (proj_on) {
-    rec = stage_entries(pj, pj.ent_rec_pt, tile, rec_cap, R, roff);
+    rec = stage_entries(pj, pj.ent_rec_pt, tile, TG::PREFETCH ? rec_cap : 0, R, roff);
     const int* tp = pj.pt_ptr + (long)tile * TG::PSTRIDE;
     for (int q = threadIdx.x; q < TG::PSTRIDE / 4; q += blockDim.x)
       cp_async16(reinterpret_cast<int4*>(TP) + q, reinterpret_cast<const int4*>(tp) + q);
