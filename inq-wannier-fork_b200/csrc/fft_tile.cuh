@@ -28,10 +28,12 @@ struct Axis {
   static constexpr int PAD = PAD_ >= 0 ? PAD_ : ((N2 % 2 == 0 && N2 > 1) ? 1 : 0);
   static constexpr int ROW = N2 + PAD;
   static constexpr int SLOTS = N1 * ROW;  // slots used by one padded line
+  // slot of row j1, column j2 of the N1 x N2 four-step view
+  __host__ __device__ static constexpr int at(int j1, int j2) { return j1 * ROW + j2; }
   // slot of natural element n
-  __host__ __device__ static constexpr int slot(int n) { return (n / N2) * ROW + n % N2; }
+  __host__ __device__ static constexpr int slot(int n) { return at(n / N2, n % N2); }
   // slot holding frequency k after a forward (or inverse-from-natural) transform
-  __host__ __device__ static constexpr int slot_of_freq(int k) { return (k % N1) * ROW + k / N1; }
+  __host__ __device__ static constexpr int slot_of_freq(int k) { return at(k % N1, k / N1); }
 };
 
 // Twiddle table layout in shared memory: tw[k1 * N2 + j2] = exp(-2 pi i j2 k1 / N).
@@ -49,14 +51,14 @@ __device__ __forceinline__ void step1(cplx<T>* S, int nitems, const cplx<T>* tw,
     map(it, base, es, j2);
     cplx<T> v[A::N1];
 #pragma unroll
-    for (int j1 = 0; j1 < A::N1; ++j1) v[j1] = S[base + (j1 * A::ROW + j2) * es];
+    for (int j1 = 0; j1 < A::N1; ++j1) v[j1] = S[base + A::at(j1, j2) * es];
     DFT<A::N1, INV, T>::run(v);
     if (A::N2 > 1) {
 #pragma unroll
       for (int k1 = 1; k1 < A::N1; ++k1) v[k1] = twiddle<A, INV>(v[k1], tw, k1, j2);
     }
 #pragma unroll
-    for (int k1 = 0; k1 < A::N1; ++k1) S[base + (k1 * A::ROW + j2) * es] = v[k1];
+    for (int k1 = 0; k1 < A::N1; ++k1) S[base + A::at(k1, j2) * es] = v[k1];
   }
 }
 
@@ -69,10 +71,10 @@ __device__ __forceinline__ void step2(cplx<T>* S, int nitems, Map map) {
     map(it, base, es, k1);
     cplx<T> v[A::N2];
 #pragma unroll
-    for (int j2 = 0; j2 < A::N2; ++j2) v[j2] = S[base + (k1 * A::ROW + j2) * es];
+    for (int j2 = 0; j2 < A::N2; ++j2) v[j2] = S[base + A::at(k1, j2) * es];
     DFT<A::N2, INV, T>::run(v);
 #pragma unroll
-    for (int k2 = 0; k2 < A::N2; ++k2) S[base + (k1 * A::ROW + k2) * es] = v[k2];
+    for (int k2 = 0; k2 < A::N2; ++k2) S[base + A::at(k1, k2) * es] = v[k2];
   }
 }
 
@@ -87,7 +89,7 @@ __device__ __forceinline__ void step2_inv_transposed(cplx<T>* S, int nitems, con
     map(it, base, es, k1);
     cplx<T> v[A::N2];
 #pragma unroll
-    for (int k2 = 0; k2 < A::N2; ++k2) v[k2] = pre(it, k1 + A::N1 * k2, S[base + (k1 * A::ROW + k2) * es]);
+    for (int k2 = 0; k2 < A::N2; ++k2) v[k2] = pre(it, k1 + A::N1 * k2, S[base + A::at(k1, k2) * es]);
     DFT<A::N2, true, T>::run(v);
     if (A::N2 > 1) {
 #pragma unroll
@@ -95,7 +97,7 @@ __device__ __forceinline__ void step2_inv_transposed(cplx<T>* S, int nitems, con
         if (k1 > 0) v[j2] = twiddle<A, true>(v[j2], tw, k1, j2);
     }
 #pragma unroll
-    for (int j2 = 0; j2 < A::N2; ++j2) S[base + (k1 * A::ROW + j2) * es] = v[j2];
+    for (int j2 = 0; j2 < A::N2; ++j2) S[base + A::at(k1, j2) * es] = v[j2];
   }
 }
 
@@ -108,7 +110,7 @@ __device__ __forceinline__ void step2_fwd_op_inv(cplx<T>* S, int nitems, const c
     map(it, base, es, k1);
     cplx<T> v[A::N2];
 #pragma unroll
-    for (int j2 = 0; j2 < A::N2; ++j2) v[j2] = S[base + (k1 * A::ROW + j2) * es];
+    for (int j2 = 0; j2 < A::N2; ++j2) v[j2] = S[base + A::at(k1, j2) * es];
     DFT<A::N2, false, T>::run(v);
 #pragma unroll
     for (int k2 = 0; k2 < A::N2; ++k2) v[k2] = op(it, k1 + A::N1 * k2, v[k2]);
@@ -119,7 +121,7 @@ __device__ __forceinline__ void step2_fwd_op_inv(cplx<T>* S, int nitems, const c
         if (k1 > 0) v[j2] = twiddle<A, true>(v[j2], tw, k1, j2);
     }
 #pragma unroll
-    for (int j2 = 0; j2 < A::N2; ++j2) S[base + (k1 * A::ROW + j2) * es] = v[j2];
+    for (int j2 = 0; j2 < A::N2; ++j2) S[base + A::at(k1, j2) * es] = v[j2];
   }
 }
 
@@ -131,10 +133,10 @@ __device__ __forceinline__ void step1_inv_transposed(cplx<T>* S, int nitems, Map
     map(it, base, es, j2);
     cplx<T> v[A::N1];
 #pragma unroll
-    for (int k1 = 0; k1 < A::N1; ++k1) v[k1] = S[base + (k1 * A::ROW + j2) * es];
+    for (int k1 = 0; k1 < A::N1; ++k1) v[k1] = S[base + A::at(k1, j2) * es];
     DFT<A::N1, true, T>::run(v);
 #pragma unroll
-    for (int j1 = 0; j1 < A::N1; ++j1) S[base + (j1 * A::ROW + j2) * es] = v[j1];
+    for (int j1 = 0; j1 < A::N1; ++j1) S[base + A::at(j1, j2) * es] = v[j1];
   }
 }
 
