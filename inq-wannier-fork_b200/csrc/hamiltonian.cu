@@ -663,7 +663,8 @@ static int launch_h_impl(const LaunchArgs& a) {
     ep.alpha = mk<T>((T)a.alpha[0], (T)a.alpha[1]);
     ep.beta = mk<T>((T)a.beta[0], (T)a.beta[1]);
     // pass C stages the records in shared memory only in FP64 (where the orbital
-    // prefetch already limits it to two CTAs per SM); FP32 keeps the smem for CTAs
+    // prefetch already limits it to two CTAs per SM); in FP32 the smem is worth more
+    // as a fourth CTA per SM, and the epilogue prefetches records into registers
     const int rec_cap_inv = TG::PREFETCH ? rec_cap : 0;
     k_tile_inv<T, NX, NY, NZ><<<dim3(tgroups, NX * TG::Y1), TG::THREADS, TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
         tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv, seg_cap,

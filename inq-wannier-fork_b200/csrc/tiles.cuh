@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(256)
 // The input orbitals of the tile (for V psi) are fetched into shared memory
 // with cp.async at the start, so that read overlaps the inverse transforms.
 template <typename T, int NX, int NY, int NZ>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::PREFETCH ? 1 : 4)
     k_tile_inv(const cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ in, long ld_in,
                cplx<T>* __restrict__ out, long ld_out, int M, const cplx<T>* __restrict__ tw_y,
                const cplx<T>* __restrict__ tw_z, ProjView<T> pj, EpiParams<T> ep, int rec_cap, int seg_cap,
@@ -401,19 +401,21 @@ __global__ void __launch_bounds__(256)
   const int gcount = min(G, M - m0);
   const bool v16 = vec && gcount == G;
 
-  // group 0: the (ka, kz) runs of this tile; group 1: the input orbitals
+  // group 0: the (ka, kz) runs of this tile, needed first; group 1: what only the
+  // epilogue reads (entry records, point index, and in FP64 the input orbitals)
   for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
     const int v = q % VP, pt = q / VP;
     const int kz = pt % NZ, ka = pt / NZ;
     cp_async16(S + (ka * ZS + AZ::slot(kz)) * G + v * PV,
                tmp + (((long)(grp * Y2 + ka) * NZ + kz) * NX + ix) * (Y1 * G) + y1 * G + v * PV);
   }
+  cp_async_commit();
   const bool proj_on = pj.nproj > 0;
   const int tile = ix * Y1 + y1;
   int roff = 0, s0 = 0, nseg = 0;
   const EntRec<T>* rec = pj.ent_rec_pt;
   if (proj_on) {
-    rec = stage_entries(pj, pj.ent_rec_pt, tile, TG::PREFETCH ? rec_cap : 0, R, roff);
+    rec = stage_entries(pj, pj.ent_rec_pt, tile, rec_cap, R, roff);
     const int* tp = pj.pt_ptr + (long)tile * TG::PSTRIDE;
     for (int q = threadIdx.x; q < TG::PSTRIDE / 4; q += blockDim.x)
       cp_async16(reinterpret_cast<int4*>(TP) + q, reinterpret_cast<const int4*>(tp) + q);
@@ -422,7 +424,6 @@ __global__ void __launch_bounds__(256)
   }
   // the point index counts from the tile's first record
   const int rbase = (rec == R) ? 0 : roff_base(pj, s0, proj_on);
-  cp_async_commit();
   if (TG::PREFETCH && v16) {
     for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
       const int v = q % VP, pt = q / VP;
@@ -484,20 +485,33 @@ __global__ void __launch_bounds__(256)
   // V_nl psi(r) = sum over the entries at r of conj(exp(i (k+A).r_e)) sum_l
   // beta_e[l] proj[a_e][l] (projector_all.hpp:182-232), summed by the point's owner.
   // BE pieces of PV orbitals per thread, their loads issued together.
-  constexpr int BE = 4;
+  // pieces per thread whose loads are issued together: FP32 keeps four CTAs per SM
+  // within 64 registers a thread, FP64 (two CTAs per SM) takes more in flight
+  constexpr int BE = TG::PREFETCH ? 4 : 2;
   cp_async_wait<0>();
   __syncthreads();
   for (int q0 = threadIdx.x; q0 < TG::PTS * VP; q0 += BE * blockDim.x) {
     cplx<T> x[BE][PV];
     T vp[BE];
+    // the first entry record of each point, fetched with the orbitals
+    EntRec<T> r0[BE];
+    int k0[BE], k1[BE];
 #pragma unroll
     for (int b = 0; b < BE; ++b) {
       const int q = q0 + b * blockDim.x;
+      k0[b] = k1[b] = 0;
       if (q >= TG::PTS * VP) continue;
       const int v = q % VP, pt = q / VP;
       const int z = pt % NZ, r = pt / NZ;
       const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
       const int jb = v * PV;
+      if (proj_on) {
+        k0[b] = TP[pt];
+        k1[b] = TP[pt + 1];
+        // FP32 reads records from global memory: start the first one now; FP64 has
+        // them in shared memory already
+        if (!TG::PREFETCH && k1[b] > k0[b]) r0[b] = rec[k0[b] + rbase];
+      }
       vp[b] = ep.V[p] + ep.vshift;
       if (TG::PREFETCH && v16) {
 #pragma unroll
@@ -523,9 +537,8 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int k = 0; k < PV; ++k) h[k] = S[sl + k];
       if (proj_on) {
-        const int k0 = TP[pt], k1 = TP[pt + 1];
-        for (int kk = k0; kk < k1; ++kk) {
-          const EntRec<T>& re = rec[kk + rbase];
+        for (int kk = k0[b]; kk < k1[b]; ++kk) {
+          const EntRec<T> re = (!TG::PREFETCH && kk == k0[b]) ? r0[b] : rec[kk + rbase];
           const cplx<T> ph = mk<T>(re.ph[0], re.ph[1]);
 #pragma unroll
           for (int k = 0; k < PV; ++k) {
