@@ -166,13 +166,14 @@ __global__ void k_velocity_dot(long N, int M, const cplx<T>* __restrict__ U, con
 // sphere entries,
 //   p_u[l] = sum_e beta_e[l] exp(i(k+A).r_e) u(r_e),  r_u[l][d] = the same with x_e[d],
 // and likewise for w; 16 FP64 values (4 complex for u, 4 for w) per (l, orbital).
-// Block: 32 orbitals x LMAX projectors x 2 entry lanes.  part[chunk][l][q][M].
+// Each entry is one atom-major record (phase, beta, position, grid point), so the
+// only dependent load is the orbital gather.  Block: 32 orbitals x LMAX projectors
+// x 2 entry lanes.  part[chunk][l][q][M].
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_nl_moments(int L, int M, const cplx<T>* __restrict__ u, const cplx<T>* __restrict__ w, long ld,
                  const int* __restrict__ chunk_atom, const int* __restrict__ chunk_beg,
-                 const int* __restrict__ atom_ptr, const int* __restrict__ atom_ent, const int* __restrict__ ent_pt,
-                 const double* __restrict__ ent_xyz, const EntRec<T>* __restrict__ rec, double* __restrict__ part) {
+                 const int* __restrict__ atom_ptr, const AdjRec<T>* __restrict__ adj, double* __restrict__ part) {
   constexpr int LM = 4, Q = 16;
   __shared__ double red[LM][32][Q + 1];
   const int c = blockIdx.x;
@@ -184,17 +185,16 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int q = 0; q < Q; ++q) s[q] = 0.0;
   if (m < M && l < L) {
+#pragma unroll 2
     for (int i = i0 + es; i < i1; i += 2) {
-      const int e = atom_ent[i];
-      const long pt = ent_pt[e];
-      const EntRec<T> r = rec[e];
-      const cplx<T> uu = u[pt * ld + m], ww = w[pt * ld + m];
+      const AdjRec<T> r = adj[i];
+      const cplx<T> uu = u[(long)r.pt * ld + m], ww = w[(long)r.pt * ld + m];
       const double b = (double)r.beta[l];
       const double pr = (double)r.ph[0], pi = (double)r.ph[1];
       // b exp(i (k+A).r) u and the same for w, in FP64
       const double ur = b * (pr * uu.x - pi * uu.y), ui = b * (pr * uu.y + pi * uu.x);
       const double wr = b * (pr * ww.x - pi * ww.y), wi = b * (pr * ww.y + pi * ww.x);
-      const double x0 = ent_xyz[3 * e], x1 = ent_xyz[3 * e + 1], x2 = ent_xyz[3 * e + 2];
+      const double x0 = r.xyz[0], x1 = r.xyz[1], x2 = r.xyz[2];
       s[0] += ur; s[1] += ui;
       s[2] += x0 * ur; s[3] += x0 * ui; s[4] += x1 * ur; s[5] += x1 * ui; s[6] += x2 * ur; s[7] += x2 * ui;
       s[8] += wr; s[9] += wi;
@@ -212,48 +212,46 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Step 2: per atom, sum its chunks and add S_l i [conj(p_u) r_w,d - conj(r_u,d) p_w]
-// over l and orbitals into acc[6 + 2d .. 6 + 2d + 1].
-__global__ void __launch_bounds__(128)
+// Step 2: block (atom a, projector l, 32 orbitals); thread (q, m) sums moment q of
+// orbital m over the atom's chunks, then the orbital's threads add
+// S_l i [conj(p_u) r_w,d - conj(r_u,d) p_w] into acc[6 + 2d .. 6 + 2d + 1].
+__global__ void __launch_bounds__(512)
     k_nl_combine(int L, int M, const int* __restrict__ atom_chunk_ptr, const double* __restrict__ part,
                  const double* __restrict__ scale, double* __restrict__ acc) {
   constexpr int Q = 16;
-  const int a = blockIdx.x;
+  __shared__ double mom[Q][33];
+  const int a = blockIdx.x, l = blockIdx.y;
+  const int mi = threadIdx.x & 31, q = threadIdx.x >> 5;
+  const int m = blockIdx.z * 32 + mi;
   const int c0 = atom_chunk_ptr[a], c1 = atom_chunk_ptr[a + 1];
+  double v = 0.0;
+  if (m < M)
+    for (int c = c0; c < c1; ++c) v += part[(((long)c * L + l) * Q + q) * M + m];
+  mom[q][mi] = v;
+  __syncthreads();
   double out[6] = {0, 0, 0, 0, 0, 0};
-  for (int idx = threadIdx.x; idx < L * M; idx += blockDim.x) {
-    const int l = idx / M, m = idx - l * M;
-    double v[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) v[q] = 0.0;
-    for (int c = c0; c < c1; ++c)
-#pragma unroll
-      for (int q = 0; q < Q; ++q) v[q] += part[(((long)c * L + l) * Q + q) * M + m];
+  if (q == 0 && m < M) {
     const double S = scale[a * L + l];
-    const double pur = v[0], pui = v[1], pwr = v[8], pwi = v[9];
+    const double pur = mom[0][mi], pui = mom[1][mi], pwr = mom[8][mi], pwi = mom[9][mi];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double rur = v[2 + 2 * d], rui = v[3 + 2 * d], rwr = v[10 + 2 * d], rwi = v[11 + 2 * d];
+      const double rur = mom[2 + 2 * d][mi], rui = mom[3 + 2 * d][mi];
+      const double rwr = mom[10 + 2 * d][mi], rwi = mom[11 + 2 * d][mi];
       // z1 = conj(p_u) r_w, z2 = conj(r_u) p_w, result += S i (z1 - z2)
       const double z1r = pur * rwr + pui * rwi, z1i = pur * rwi - pui * rwr;
       const double z2r = rur * pwr + rui * pwi, z2i = rur * pwi - rui * pwr;
-      out[2 * d] += -S * (z1i - z2i);
-      out[2 * d + 1] += S * (z1r - z2r);
+      out[2 * d] = -S * (z1i - z2i);
+      out[2 * d + 1] = S * (z1r - z2r);
     }
   }
-  __shared__ double red[6][4];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int q = 0; q < 6; q++) {
-    double x = out[q];
+  if (q == 0) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    if (lane == 0) red[q][warp] = x;
-  }
-  __syncthreads();
-  if (threadIdx.x < 6) {
-    double x = 0.0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); k++) x += red[threadIdx.x][k];
-    atomicAdd(&acc[6 + threadIdx.x], x);
+    for (int k = 0; k < 6; k++) {
+      double x = out[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if (mi == 0) atomicAdd(&acc[6 + k], x);
+    }
   }
 }
 
@@ -361,10 +359,10 @@ static int agrad_impl(const inqb_ctx& ctx, const void* U, const void* W, const v
     double* part = ctx.d_nlpart.as<double>();
     k_nl_moments<T><<<dim3(nchunks, (M + 31) / 32), 256, 0, st>>>(
         t.L, M, (const cplx<T>*)u, (const cplx<T>*)w, ld, t.d_chunk_atom.as<int>(), t.d_chunk_beg.as<int>(),
-        t.d_atom_ptr.as<int>(), t.d_atom_ent.as<int>(), t.d_ent_pt.as<int>(), t.d_ent_xyz.as<double>(),
-        t.d_ent_rec.as<EntRec<T>>(), part);
+        t.d_atom_ptr.as<int>(), t.d_adj_rec.as<AdjRec<T>>(), part);
     INQB_CUDA_TRY(cudaGetLastError());
-    k_nl_combine<<<t.nproj, 128, 0, st>>>(t.L, M, t.d_atom_chunk_ptr.as<int>(), part, t.d_scale.as<double>(), acc);
+    k_nl_combine<<<dim3(t.nproj, t.L, (M + 31) / 32), 512, 0, st>>>(t.L, M, t.d_atom_chunk_ptr.as<int>(), part,
+                                                                   t.d_scale.as<double>(), acc);
     INQB_CUDA_TRY(cudaGetLastError());
   }
   k_finish_dA<<<1, 32, 0, st>>>(acc, 1.0 / (double)ctx.N, cre, cim, gA);

@@ -99,7 +99,8 @@ int update_phases(inqb_ctx* ctx, void* stream) {
   if (ctx->proj.nproj == 0 || ctx->proj.nent == 0) return INQB_OK;
   return launch_phases(ctx->precision, ctx->proj.nent, ctx->proj.d_ent_relpos.as<float>(), ctx->kA_cov,
                        ctx->proj.d_ent_phase.ptr, ctx->proj.d_ent_rec.ptr, ctx->proj.d_ent_rec_pt.ptr,
-                       ctx->proj.d_pt_pos.as<int>(), stream);
+                       ctx->proj.d_pt_pos.as<int>(), ctx->proj.d_adj_rec.ptr, ctx->proj.d_atom_pos.as<int>(),
+                       stream);
 }
 
 int set_kA(inqb_ctx* ctx, const double kA[3], void* stream) {

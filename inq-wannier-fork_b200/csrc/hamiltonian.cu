@@ -545,7 +545,8 @@ __global__ void __launch_bounds__(PlaneGeom<T, NY, NZ>::THREADS)
 template <typename T>
 __global__ void k_phases(int nent, const float* __restrict__ relpos, double k0, double k1, double k2,
                          cplx<T>* __restrict__ phase, EntRec<T>* __restrict__ rec, EntRec<T>* __restrict__ rec_pt,
-                         const int* __restrict__ pt_pos) {
+                         const int* __restrict__ pt_pos, AdjRec<T>* __restrict__ adj,
+                         const int* __restrict__ atom_pos) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nent) return;
   const double th = k0 * (double)relpos[3 * e] + k1 * (double)relpos[3 * e + 1] + k2 * (double)relpos[3 * e + 2];
@@ -556,6 +557,8 @@ __global__ void k_phases(int nent, const float* __restrict__ relpos, double k0, 
   rec[e].ph[1] = (T)s;
   rec_pt[pt_pos[e]].ph[0] = (T)c;
   rec_pt[pt_pos[e]].ph[1] = (T)s;
+  adj[atom_pos[e]].ph[0] = (T)c;
+  adj[atom_pos[e]].ph[1] = (T)s;
 }
 
 // ---------------------------------------------------------------- plan instantiation
@@ -688,18 +691,20 @@ static int launch_h_impl(const LaunchArgs& a) {
 
 template <typename T>
 static int launch_phases_impl(int nent, const float* relpos, const double kA[3], void* phase, void* rec,
-                              void* rec_pt, const int* pt_pos, void* stream) {
+                              void* rec_pt, const int* pt_pos, void* adj, const int* atom_pos, void* stream) {
   if (nent == 0) return INQB_OK;
   k_phases<T><<<(nent + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
-      nent, relpos, kA[0], kA[1], kA[2], (cplx<T>*)phase, (EntRec<T>*)rec, (EntRec<T>*)rec_pt, pt_pos);
+      nent, relpos, kA[0], kA[1], kA[2], (cplx<T>*)phase, (EntRec<T>*)rec, (EntRec<T>*)rec_pt, pt_pos,
+      (AdjRec<T>*)adj, atom_pos);
   INQB_CUDA_TRY(cudaGetLastError());
   return INQB_OK;
 }
 
 int launch_phases(int precision, int nent, const float* relpos, const double kA[3], void* phase, void* rec,
-                  void* rec_pt, const int* pt_pos, void* stream) {
-  return precision == INQB_FP64 ? launch_phases_impl<double>(nent, relpos, kA, phase, rec, rec_pt, pt_pos, stream)
-                                : launch_phases_impl<float>(nent, relpos, kA, phase, rec, rec_pt, pt_pos, stream);
+                  void* rec_pt, const int* pt_pos, void* adj, const int* atom_pos, void* stream) {
+  return precision == INQB_FP64
+             ? launch_phases_impl<double>(nent, relpos, kA, phase, rec, rec_pt, pt_pos, adj, atom_pos, stream)
+             : launch_phases_impl<float>(nent, relpos, kA, phase, rec, rec_pt, pt_pos, adj, atom_pos, stream);
 }
 
 // ---------------------------------------------------------------- registry

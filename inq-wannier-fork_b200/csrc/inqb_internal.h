@@ -80,6 +80,16 @@ struct alignas(16) EntRec {
   int tseg;  // segment index within the tile (its atom's slot in the tile's projections)
 };
 
+// One sphere entry in atom-major order for the adjoint's nonlocal moments: phase,
+// radial values, cartesian position relative to the atom and linear grid point.
+template <typename T>
+struct alignas(16) AdjRec {
+  T ph[2];
+  T beta[4];
+  double xyz[3];
+  int pt;
+};
+
 // Projector tables in the layout the fused H kernels read (built on the host
 // from projector_all-style per-atom sphere tables, then uploaded).
 struct ProjTables {
@@ -104,6 +114,8 @@ struct ProjTables {
   // chunks of at most kNlChunk consecutive entries of one atom (atom-major order),
   // the unit of work of the nonlocal moment kernel of the adjoint
   std::vector<int> chunk_atom, chunk_beg, atom_chunk_ptr;
+  std::vector<int> atom_pos;        // [nent] position of entry e in atom-major order
+  DevBuf d_adj_rec, d_atom_pos;     // [nent] AdjRec<T> in atom-major order
   // device copies
   DevBuf d_seg_ptr, d_seg_atom, d_seg_ent, d_seg_local, d_plane_ptr, d_plane_atom, d_ent_off, d_ent_atom;
   DevBuf d_ent_beta;                // [nent][L] in the context precision

@@ -34,6 +34,6 @@ struct Plan {
 
 const Plan* find_plan(int nx, int ny, int nz, int precision);
 int launch_phases(int precision, int nent, const float* relpos, const double kA[3], void* phase, void* rec,
-                  void* rec_pt, const int* pt_pos, void* stream);
+                  void* rec_pt, const int* pt_pos, void* adj, const int* atom_pos, void* stream);
 
 }  // namespace inqb

@@ -330,6 +330,8 @@ int build_proj_tables(const inqb_ctx& ctx, int nproj, int L, int smax, const int
     std::vector<int> fill(t.atom_ptr.begin(), t.atom_ptr.end() - 1);
     for (long i = 0; i < total; i++) t.atom_ent[fill[t.ent_atom[i]]++] = (int)i;
   }
+  t.atom_pos.assign(total, 0);
+  for (long i = 0; i < total; i++) t.atom_pos[t.atom_ent[i]] = (int)i;
   t.chunk_atom.clear();
   t.chunk_beg.clear();
   t.atom_chunk_ptr.assign(nproj + 1, 0);
@@ -371,6 +373,21 @@ static std::vector<EntRec<T>> ent_records(const ProjTables& t, bool point_order 
   return rec;
 }
 
+// Atom-major adjoint records with zero phases (the phase kernel fills them).
+template <typename T>
+static std::vector<AdjRec<T>> adj_records(const ProjTables& t) {
+  std::vector<AdjRec<T>> rec((size_t)t.nent);
+  for (int i = 0; i < t.nent; i++) {
+    const int e = t.atom_ent[i];
+    AdjRec<T>& r = rec[i];
+    r.ph[0] = r.ph[1] = (T)0;
+    for (int l = 0; l < 4; l++) r.beta[l] = (l < t.L) ? (T)t.ent_beta[(size_t)e * t.L + l] : (T)0;
+    for (int d = 0; d < 3; d++) r.xyz[d] = t.ent_xyz[3 * (size_t)e + d];
+    r.pt = t.ent_pt[e];
+  }
+  return rec;
+}
+
 int upload_proj_tables(const inqb_ctx& ctx, ProjTables& t) {
   INQB_TRY(upload(t.d_seg_ptr, t.seg_ptr));
   INQB_TRY(upload(t.d_seg_atom, t.seg_atom));
@@ -404,6 +421,12 @@ int upload_proj_tables(const inqb_ctx& ctx, ProjTables& t) {
     INQB_TRY(upload(t.d_ent_rec_pt, ent_records<float>(t, true)));
   }
   INQB_TRY(upload(t.d_pt_pos, t.pt_pos));
+  INQB_TRY(upload(t.d_atom_pos, t.atom_pos));
+  if (ctx.precision == INQB_FP64) {
+    INQB_TRY(upload(t.d_adj_rec, adj_records<double>(t)));
+  } else {
+    INQB_TRY(upload(t.d_adj_rec, adj_records<float>(t)));
+  }
   INQB_TRY(upload(t.d_pt_ptr, t.pt_ptr));
   return INQB_OK;
 }
