@@ -273,37 +273,48 @@ def bench_adjoint(args, local):
 
     cfg = systems.config("cfg2")
     out = {"config": "cfg2: a=10.26, 32^3, 8 atoms, 16 orbitals, dt=0.05, 200 steps, checkpoint every 20, "
-                     "Fourier sphere mask on", "steps": cfg["steps"]}
+                     "Fourier sphere mask on", "steps": cfg["steps"],
+           "ratio": "(forward keeping what the backward needs + backward) / plain forward",
+           "timing": "wall clock around device-synchronised calls"}
     for precision in ("fp64", "mixed"):
         h = pb.KSHamiltonian(cfg["lattice"], cfg["nr"], precision, device=local)
         h.set_scalar_potential(cfg["V"])
         h.set_gaussian_projectors(cfg["positions"])
         h.set_fourier_sphere_mask(True)
         dt = torch.complex128 if precision == "fp64" else torch.complex64
-        prop = DipolePropagation(h, torch.as_tensor(cfg["psi"]).to("cuda", dt), cfg["occ"], cfg["dt"],
-                                 cfg["checkpoint_every"])
-        prop.forward(cfg["amplitudes"], keep=True)  # warm-up
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        d = prop.forward(cfg["amplitudes"], keep=True)
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        gA, gV = prop.backward()
-        torch.cuda.synchronize()
-        t2 = time.perf_counter()
-        out[precision] = {"dipole": d, "forward_s": t1 - t0, "backward_s": t2 - t1,
-                          "forward_steps_per_s": cfg["steps"] / (t1 - t0),
-                          "total_over_forward": (t2 - t0) / (t1 - t0),
-                          "grad_amplitudes_norm": float(gA.norm()), "grad_V_norm": float(gV.norm())}
-        out[precision]["_gA"] = gA.cpu().numpy()
-        out[precision]["_gV"] = gV.cpu().numpy()
-    g64, g32 = out["fp64"], out["mixed"]
-    out["mixed_vs_fp64"] = {
-        "dipole_rel": abs(g32["dipole"] - g64["dipole"]) / max(1e-300, abs(g64["dipole"])),
-        "grad_amplitudes_rel": float(np.linalg.norm(g32["_gA"] - g64["_gA"]) / np.linalg.norm(g64["_gA"])),
-        "grad_V_rel": float(np.linalg.norm(g32["_gV"] - g64["_gV"]) / np.linalg.norm(g64["_gV"]))}
+        psi0 = torch.as_tensor(cfg["psi"]).to("cuda", dt)
+        res = {}
+        for mode, store in (("checkpointed", False), ("stored_powers", True)):
+            prop = DipolePropagation(h, psi0, cfg["occ"], cfg["dt"], cfg["checkpoint_every"], store_powers=store)
+            prop.forward(cfg["amplitudes"], keep=True)  # warm-up
+            prop.backward()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            prop.forward(cfg["amplitudes"], keep=False)  # the plain forward run
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            d = prop.forward(cfg["amplitudes"], keep=True)
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            gA, gV = prop.backward()
+            torch.cuda.synchronize()
+            t3 = time.perf_counter()
+            res[mode] = {"forward_s": t1 - t0, "forward_keep_s": t2 - t1, "backward_s": t3 - t2,
+                         "total_over_forward": (t3 - t1) / (t1 - t0), "dipole": d,
+                         "grad_amplitudes_norm": float(gA.norm()), "grad_V_norm": float(gV.norm()),
+                         "_gA": gA.cpu().numpy(), "_gV": gV.cpu().numpy()}
+            del prop
+        out[precision] = {"forward_steps_per_s": cfg["steps"] / res["checkpointed"]["forward_s"], "modes": res}
+    out["mixed_vs_fp64"] = {}
+    for mode in ("checkpointed", "stored_powers"):
+        g64, g32 = out["fp64"]["modes"][mode], out["mixed"]["modes"][mode]
+        out["mixed_vs_fp64"][mode] = {
+            "dipole_rel": abs(g32["dipole"] - g64["dipole"]) / max(1e-300, abs(g64["dipole"])),
+            "grad_amplitudes_rel": float(np.linalg.norm(g32["_gA"] - g64["_gA"]) / np.linalg.norm(g64["_gA"])),
+            "grad_V_rel": float(np.linalg.norm(g32["_gV"] - g64["_gV"]) / np.linalg.norm(g64["_gV"]))}
     for p in ("fp64", "mixed"):
-        del out[p]["_gA"], out[p]["_gV"]
+        for mode in ("checkpointed", "stored_powers"):
+            del out[p]["modes"][mode]["_gA"], out[p]["modes"][mode]["_gV"]
     return out
 
 

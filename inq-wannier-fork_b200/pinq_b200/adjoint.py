@@ -32,7 +32,11 @@ import torch
 class DipolePropagation:
     """ETRS propagation of one orbital block with checkpoints, forward and adjoint."""
 
-    def __init__(self, ham, psi0: torch.Tensor, occ, dt: float, every: int = 20, direction: int = 0):
+    def __init__(self, ham, psi0: torch.Tensor, occ, dt: float, every: int = 20, direction: int = 0,
+                 store_powers: bool = False):
+        """every: checkpoint interval of the recomputing backward.  store_powers:
+        keep the Taylor powers of every step during the forward pass instead (8
+        orbital blocks per step; no recompute in the backward)."""
         self.h = ham
         self.psi0 = psi0
         self.M = psi0.shape[1]
@@ -40,6 +44,8 @@ class DipolePropagation:
         self.dt = float(dt)
         self.every = int(every)
         self.direction = int(direction)
+        self.store_powers = bool(store_powers)
+        self.powers = None
 
     # -- helpers
     def _kA(self, a: float):
@@ -56,10 +62,18 @@ class DipolePropagation:
         amps = np.asarray(amplitudes, float)
         psi = self.psi0.clone()
         cps = {}
-        for n in range(len(amps)):
-            if keep and n % self.every == 0:
-                cps[n] = psi.clone()
-            self.h.etrs_step_(psi, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)))
+        self.powers = None
+        if keep and self.store_powers:
+            powers = torch.empty((len(amps), 8, self.h.N, self.M), dtype=psi.dtype, device=psi.device)
+            for n in range(len(amps)):
+                self.h.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)),
+                                         self._kA(self._amp(amps, n + 1)), powers[n])
+            self.powers = powers
+        else:
+            for n in range(len(amps)):
+                if keep and n % self.every == 0:
+                    cps[n] = psi.clone()
+                self.h.etrs_step_(psi, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)))
         rho = self.h.density(psi, self.occ)
         d = float(self.h.dipole(rho)[self.direction])
         if keep:
@@ -82,6 +96,12 @@ class DipolePropagation:
         gV = torch.zeros(h.N, dtype=torch.float64, device=dev)
         gA = torch.zeros((nsteps, 3), dtype=torch.float64, device=dev)
         lam = h.position_scale(self.psi_final, self.occ, self.direction, h.volume_element)
+        if self.powers is not None:
+            for n in reversed(range(nsteps)):
+                n2 = min(n + 1, nsteps - 1)
+                h.etrs_adjoint_step_(lam, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)),
+                                     self.powers[n], gV, gA[n], gA[n2])
+            return gA[:, self.direction].clone(), gV
         seg = min(self.every, nsteps)
         store = torch.empty((seg, 8, h.N, self.M), dtype=self.psi0.dtype, device=dev)
         for s0 in reversed(range(0, nsteps, self.every)):

@@ -124,3 +124,22 @@ def test_dH_dA_matches_oracle_difference(pb, oracle_mod, precision, tol, mask):
         ref[d] = ((vals[0] - vals[1]) / (2 * eps)).real
     assert np.abs(gA - ref).max() <= tol * np.abs(ref).max(), (gA, ref)
     del rng
+
+
+def test_stored_powers_mode_matches_checkpointed(pb, cfg2):
+    """Keeping every step's Taylor powers in the forward pass (no recompute) gives
+    the checkpointed backward's gradients: the same kernels on the same powers."""
+    from pinq_b200.adjoint import DipolePropagation
+
+    h = make_product(pb, cfg2, "fp64")
+    h.set_fourier_sphere_mask(True)
+    psi0 = torch.as_tensor(cfg2["psi"]).to("cuda", torch.complex128)
+    amps = cfg2["amps"][:30]
+    out = []
+    for store in (False, True):
+        prop = DipolePropagation(h, psi0, cfg2["occ"], 0.05, 10, store_powers=store)
+        prop.forward(amps, keep=True)
+        gA, gV = prop.backward()
+        out.append((gA.cpu().numpy(), gV.cpu().numpy()))
+    assert np.abs(out[0][0] - out[1][0]).max() <= 1e-10 * np.abs(out[0][0]).max()
+    assert np.abs(out[0][1] - out[1][1]).max() <= 1e-10 * np.abs(out[0][1]).max()
