@@ -1,0 +1,76 @@
+"""Orbital sharding over two processes on the CPU (gloo): every orbital lands on
+exactly one rank, the all-reduced density equals the density of all orbitals,
+and timings reduce by their maximum.  The density kernel is stood in for by
+numpy here; the GPU path calls the library's inqb_density through the same
+pinq_b200.parallel.sharded_density."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.multiprocessing as mp
+
+from pinq_b200.parallel import orbital_range
+
+
+class _NumpyDensity:
+    def density(self, psi, occ):
+        rho = (np.abs(psi) ** 2 * np.asarray(occ)[None, :]).sum(1)
+        return torch.tensor(rho, dtype=torch.float64)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, M, out_dir):
+    import datetime
+
+    import torch.distributed as dist
+
+    from pinq_b200.parallel import max_over_ranks, sharded_density
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        rng = np.random.default_rng(0)  # every rank builds the same full set
+        psi = rng.standard_normal((500, M)) + 1j * rng.standard_normal((500, M))
+        occ = rng.uniform(0.5, 2.0, M)
+        first, count = orbital_range(M, world, rank)
+        rho = sharded_density(_NumpyDensity(), psi[:, first:first + count], occ[first:first + count])
+        t = max_over_ranks(1.0 + rank)
+        np.save(os.path.join(out_dir, f"rho{rank}.npy"), rho.numpy())
+        np.save(os.path.join(out_dir, f"t{rank}.npy"), np.array([t]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_orbital_range_partitions():
+    for M in (0, 1, 7, 16, 128, 131):
+        for world in (1, 2, 3, 8):
+            seen = []
+            for r in range(world):
+                f, c = orbital_range(M, world, r)
+                assert c >= 0
+                seen.extend(range(f, f + c))
+            assert seen == list(range(M))
+    with pytest.raises(ValueError):
+        orbital_range(4, 2, 2)
+
+
+@pytest.mark.parametrize("M", [7, 16])
+def test_sharded_density_two_ranks(tmp_path, M):
+    world = 2
+    mp.start_processes(_rank_main, args=(world, _free_port(), M, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    rng = np.random.default_rng(0)
+    psi = rng.standard_normal((500, M)) + 1j * rng.standard_normal((500, M))
+    occ = rng.uniform(0.5, 2.0, M)
+    ref = (np.abs(psi) ** 2 * occ[None, :]).sum(1)
+    for r in range(world):
+        assert np.allclose(np.load(tmp_path / f"rho{r}.npy"), ref, rtol=1e-14, atol=0)
+        assert float(np.load(tmp_path / f"t{r}.npy")[0]) == 2.0
