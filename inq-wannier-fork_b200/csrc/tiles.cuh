@@ -375,10 +375,133 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---------------------------------------------------------------- pass B of the plain FFTs
+// DIR = 0 (to_fourier): block tmp[g][ka][kz] -> outer y stage -> forward x ->
+//   out[kx][ky][kz][m] in natural frequency order (transform.hpp:115-188, sign -1).
+// DIR = 1 (to_real, first half): in[kx][ky][kz][m] -> inverse x -> inverse outer
+//   y stage -> block tmp[g][ka][kz]; pass C finishes with the inner y and z stages
+//   and the 1/N (transform.hpp:250-332).
+template <typename T, int NX, int NY, int NZ, int DIR>
+__global__ void __launch_bounds__(256)
+    k_tile_x_fft(cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ in, cplx<T>* __restrict__ out, long ld,
+                 int M, const cplx<T>* __restrict__ tw_x, int vec) {
+  using TG = TileGeom<T, NX, NY, NZ>;
+  using AX = typename TG::AX;
+  constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, XS = TG::XS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* X = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* twx = X + TG::XBLK;
+
+  const int kz = blockIdx.x % NZ, ka = blockIdx.x / NZ, grp = blockIdx.y;
+  const int m0 = grp * G;
+  const int gcount = min(G, M - m0);
+  const bool v16 = vec && gcount == G;
+  cplx<T>* blk = tmp + ((long)(grp * Y2 + ka) * NZ + kz) * TG::BLK;
+  // point of frequency (kx, ka + Y2 kb, kz) in the orbital layout
+  auto point = [&](int kx, int kb) { return ((long)kx * NY + ka + Y2 * kb) * NZ + kz; };
+  auto map1 = [](int it, int& base, int& es, int& j2) {
+    const int j = it % G, rest = it / G;
+    j2 = rest % AX::N2;
+    base = (rest / AX::N2) * G + j;
+    es = XS;
+  };
+  auto map2 = [](int it, int& base, int& es, int& k1) {
+    const int j = it % G, rest = it / G;
+    k1 = rest % AX::N1;
+    base = (rest / AX::N1) * G + j;
+    es = XS;
+  };
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) twx[i] = tw_x[i];
+
+  if (DIR == 0) {
+    for (int q = threadIdx.x; q < NX * Y1 * VP; q += blockDim.x) {
+      const int v = q % VP, r = q / VP;
+      const int y1 = r % Y1, ix = r / Y1;
+      cp_async16(X + AX::slot(ix) * XS + y1 * G + v * PV, blk + (long)q * PV);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    // outer y stage: y1 -> kb
+    for (int it = threadIdx.x; it < NX * G; it += blockDim.x) {
+      const int j = it % G, ix = it / G;
+      const int base = AX::slot(ix) * XS + j;
+      cplx<T> u[Y1];
+#pragma unroll
+      for (int y = 0; y < Y1; ++y) u[y] = X[base + y * G];
+      DFT<Y1, false, T>::run(u);
+#pragma unroll
+      for (int y = 0; y < Y1; ++y) X[base + y * G] = u[y];
+    }
+    __syncthreads();
+    step1<AX, false>(X, Y1 * G * AX::N2, twx, map1);
+    __syncthreads();
+    step2<AX, false>(X, Y1 * G * AX::N1, map2);
+    __syncthreads();
+    // kx sits in slot_of_freq(kx)
+    if (v16) {
+      for (int q = threadIdx.x; q < NX * Y1 * VP; q += blockDim.x) {
+        const int v = q % VP, r = q / VP;
+        const int kb = r % Y1, kx = r / Y1;
+        *reinterpret_cast<float4*>(out + point(kx, kb) * ld + m0 + v * PV) =
+            *reinterpret_cast<const float4*>(X + AX::slot_of_freq(kx) * XS + kb * G + v * PV);
+      }
+    } else {
+      for (int q = threadIdx.x; q < NX * Y1 * G; q += blockDim.x) {
+        const int j = q % G, r = q / G;
+        const int kb = r % Y1, kx = r / Y1;
+        if (j < gcount) out[point(kx, kb) * ld + m0 + j] = X[AX::slot_of_freq(kx) * XS + kb * G + j];
+      }
+    }
+  } else {
+    // natural kx into slot(kx); the inverse from natural order leaves ix in slot_of_freq(ix)
+    if (v16) {
+      for (int q = threadIdx.x; q < NX * Y1 * VP; q += blockDim.x) {
+        const int v = q % VP, r = q / VP;
+        const int kb = r % Y1, kx = r / Y1;
+        cp_async16(X + AX::slot(kx) * XS + kb * G + v * PV, in + point(kx, kb) * ld + m0 + v * PV);
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+    } else {
+      for (int q = threadIdx.x; q < NX * Y1 * G; q += blockDim.x) {
+        const int j = q % G, r = q / G;
+        const int kb = r % Y1, kx = r / Y1;
+        X[AX::slot(kx) * XS + kb * G + j] = (j < gcount) ? in[point(kx, kb) * ld + m0 + j] : mk<T>(0, 0);
+      }
+    }
+    __syncthreads();
+    step1<AX, true>(X, Y1 * G * AX::N2, twx, map1);
+    __syncthreads();
+    step2<AX, true>(X, Y1 * G * AX::N1, map2);
+    __syncthreads();
+    // inverse outer y stage: kb -> y1
+    for (int it = threadIdx.x; it < NX * G; it += blockDim.x) {
+      const int j = it % G, ix = it / G;
+      const int base = AX::slot_of_freq(ix) * XS + j;
+      cplx<T> u[Y1];
+#pragma unroll
+      for (int y = 0; y < Y1; ++y) u[y] = X[base + y * G];
+      DFT<Y1, true, T>::run(u);
+#pragma unroll
+      for (int y = 0; y < Y1; ++y) X[base + y * G] = u[y];
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < NX * Y1 * VP; q += blockDim.x) {
+      const int v = q % VP, r = q / VP;
+      const int y1 = r % Y1, ix = r / Y1;
+      *reinterpret_cast<float4*>(blk + (long)q * PV) =
+          *reinterpret_cast<const float4*>(X + AX::slot_of_freq(ix) * XS + y1 * G + v * PV);
+    }
+  }
+}
+
 // ---------------------------------------------------------------- pass C
 // The input orbitals of the tile (for V psi) are fetched into shared memory
 // with cp.async at the start, so that read overlaps the inverse transforms.
-template <typename T, int NX, int NY, int NZ>
+// MODE_H = 1: the H epilogue; 0: out = alpha * (inverse transform), the second
+// half of to_real (alpha = 1/N), reading neither orbitals, V nor projectors.
+template <typename T, int NX, int NY, int NZ, int MODE_H = 1>
 __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::PREFETCH ? 1 : 4)
     k_tile_inv(const cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ in, long ld_in,
                cplx<T>* __restrict__ out, long ld_out, int M, const cplx<T>* __restrict__ tw_y,
@@ -410,7 +533,7 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::PREFETCH ? 1 : 4
                tmp + (((long)(grp * Y2 + ka) * NZ + kz) * NX + ix) * (Y1 * G) + y1 * G + v * PV);
   }
   cp_async_commit();
-  const bool proj_on = pj.nproj > 0;
+  const bool proj_on = MODE_H && pj.nproj > 0;
   const int tile = ix * Y1 + y1;
   int roff = 0, s0 = 0, nseg = 0;
   const EntRec<T>* rec = pj.ent_rec_pt;
@@ -424,7 +547,7 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::PREFETCH ? 1 : 4
   }
   // the point index counts from the tile's first record
   const int rbase = (rec == R) ? 0 : roff_base(pj, s0, proj_on);
-  if (TG::PREFETCH && v16) {
+  if (MODE_H && TG::PREFETCH && v16) {
     for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
       const int v = q % VP, pt = q / VP;
       const int z = pt % NZ, r = pt / NZ;
@@ -490,6 +613,28 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::PREFETCH ? 1 : 4
   constexpr int BE = TG::PREFETCH ? 4 : 2;
   cp_async_wait<0>();
   __syncthreads();
+  if (!MODE_H) {
+    for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
+      const int v = q % VP, pt = q / VP;
+      const int z = pt % NZ, r = pt / NZ;
+      const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
+      const int jb = v * PV;
+      const int sl = (r * ZS + AZ::slot_of_freq(z)) * G + jb;
+      cplx<T> h[PV];
+#pragma unroll
+      for (int k = 0; k < PV; ++k) h[k] = ep.alpha * S[sl + k];
+      if (v16) {
+        float4 w;
+        memcpy(&w, h, 16);
+        *reinterpret_cast<float4*>(out + p * ld_out + m0 + jb) = w;
+      } else {
+#pragma unroll
+        for (int k = 0; k < PV; ++k)
+          if (jb + k < gcount) out[p * ld_out + m0 + jb + k] = h[k];
+      }
+    }
+    return;
+  }
   for (int q0 = threadIdx.x; q0 < TG::PTS * VP; q0 += BE * blockDim.x) {
     cplx<T> x[BE][PV];
     T vp[BE];
