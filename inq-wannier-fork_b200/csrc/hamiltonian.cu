@@ -105,7 +105,7 @@ static int launch_h_impl(const LaunchArgs& a) {
   INQB_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 64 && !attr_done[dev]) {
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_fwd<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)TG::smem_fwd(kAccAtomsMax, kRecCapMax)));
+                                       (int)std::min(TG::smem_fwd(kAccAtomsMax, kRecCapMax), TG::SMEM_MAX)));
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)TG::SMEM_X));
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x_fft<T, NX, NY, NZ, 0>,
@@ -113,7 +113,7 @@ static int launch_h_impl(const LaunchArgs& a) {
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x_fft<T, NX, NY, NZ, 1>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TG::SMEM_X));
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_inv<T, NX, NY, NZ, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)TG::smem_inv(kRecCapMax, kAccAtomsMax)));
+                                       (int)std::min(TG::smem_inv(kRecCapMax, kAccAtomsMax), TG::SMEM_MAX)));
     INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_inv<T, NX, NY, NZ, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)TG::smem_inv(0, 0)));
     attr_done[dev] = true;
@@ -147,8 +147,11 @@ static int launch_h_impl(const LaunchArgs& a) {
 
   if (a.mode == LaunchArgs::H) {
     const int acc_cap = pj.nproj > 0 ? std::min(pj.max_plane_atoms, kAccAtomsMax) : 0;
-    const int rec_cap = pj.nproj > 0 ? std::min(pj.max_tile_ent, kRecCapMax) : 0;
     const int seg_cap = pj.nproj > 0 ? std::min(pj.max_tile_seg, kAccAtomsMax) : 0;
+    // stage a tile's records only when all of them fit beside the tile (the kernel
+    // reads them from global memory otherwise)
+    int rec_cap = pj.nproj > 0 ? std::min(pj.max_tile_ent, kRecCapMax) : 0;
+    if (TG::smem_fwd(acc_cap, rec_cap) > TG::SMEM_MAX) rec_cap = 0;
     if (pj.nproj > 0 && pj.pt_stride != TG::PSTRIDE)
       return fail(INQB_ERR_INVALID, "projector tables were built for another tiling of this grid");
     if (pj.nproj > 0)
@@ -169,7 +172,10 @@ static int launch_h_impl(const LaunchArgs& a) {
     // pass C stages the records in shared memory only in FP64 (where the orbital
     // prefetch already limits it to two CTAs per SM); in FP32 the smem is worth more
     // as a fourth CTA per SM, and the epilogue prefetches records into registers
-    const int rec_cap_inv = TG::PREFETCH ? rec_cap : 0;
+    int rec_cap_inv = TG::PREFETCH ? rec_cap : 0;
+    if (TG::smem_inv(rec_cap_inv, seg_cap) > TG::SMEM_MAX) rec_cap_inv = 0;
+    if (TG::smem_inv(rec_cap_inv, seg_cap) > TG::SMEM_MAX)
+      return fail(INQB_ERR_UNSUPPORTED, "tile of this grid does not fit in shared memory");
     k_tile_inv<T, NX, NY, NZ, 1><<<ginv, TG::THREADS, TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
         tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv, seg_cap,
         vin && vout);
@@ -232,6 +238,7 @@ static const std::map<std::tuple<int, int, int, int>, Plan>& registry() {
   static const std::map<std::tuple<int, int, int, int>, Plan> reg = {
       INQB_CUBIC(16) INQB_CUBIC(20) INQB_CUBIC(24) INQB_CUBIC(32) INQB_CUBIC(40) INQB_CUBIC(48)
       INQB_CUBIC(64)
+      INQB_CUBIC(144)
       INQB_GRID(18, 24, 20)
   };
   return reg;

@@ -53,6 +53,7 @@ struct TileGeom {
   static constexpr int XBLK = AX::SLOTS * XS;
   static constexpr int BLK = NX * Y1 * G;   // complex values of one tmp block [ix][y1][G]
   static constexpr int THREADS = 256;
+  static constexpr size_t SMEM_MAX = 227 * 1024;  // dynamic shared memory a CTA may have
   static constexpr size_t smem_fwd(int acc_atoms, int rec_cap) {
     return sizeof(cplx<T>) * ((size_t)TILE + NY + NZ) + sizeof(double2) * (size_t)acc_atoms * LMAX * G +
            sizeof(EntRec<T>) * (size_t)rec_cap;
@@ -62,7 +63,10 @@ struct TileGeom {
   // pass C prefetches the input orbitals of its tile into shared memory in FP64
   // (two CTAs per SM either way, so the copy overlaps the transforms for free);
   // in FP32 the smaller footprint buys a third CTA per SM instead.
-  static constexpr bool PREFETCH = sizeof(T) == 8;
+  static constexpr size_t TILE_BYTES = sizeof(cplx<T>) * (size_t)TILE;
+  static constexpr bool PREFETCH = sizeof(T) == 8 && 2 * TILE_BYTES <= 150 * 1024;
+  // pass C in FP32 keeps four CTAs per SM (64 registers a thread) where they fit
+  static constexpr int INV_MIN_CTAS = (!PREFETCH && TILE_BYTES <= 40 * 1024) ? 4 : 1;
   static constexpr size_t smem_inv(int rec_cap, int seg_cap) {
     return sizeof(cplx<T>) * ((size_t)TILE + (PREFETCH ? (size_t)PTS * G : 0) + NY + NZ) +
            sizeof(EntRec<T>) * (size_t)rec_cap + sizeof(int) * (size_t)PSTRIDE +
@@ -502,7 +506,7 @@ __global__ void __launch_bounds__(256)
 // MODE_H = 1: the H epilogue; 0: out = alpha * (inverse transform), the second
 // half of to_real (alpha = 1/N), reading neither orbitals, V nor projectors.
 template <typename T, int NX, int NY, int NZ, int MODE_H = 1>
-__global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::PREFETCH ? 1 : 4)
+__global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
     k_tile_inv(const cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ in, long ld_in,
                cplx<T>* __restrict__ out, long ld_out, int M, const cplx<T>* __restrict__ tw_y,
                const cplx<T>* __restrict__ tw_z, ProjView<T> pj, EpiParams<T> ep, int rec_cap, int seg_cap,
@@ -610,7 +614,7 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::PREFETCH ? 1 : 4
   // BE pieces of PV orbitals per thread, their loads issued together.
   // pieces per thread whose loads are issued together: FP32 keeps four CTAs per SM
   // within 64 registers a thread, FP64 (two CTAs per SM) takes more in flight
-  constexpr int BE = TG::PREFETCH ? 4 : 2;
+  constexpr int BE = (TG::INV_MIN_CTAS == 4) ? 2 : 4;
   cp_async_wait<0>();
   __syncthreads();
   if (!MODE_H) {

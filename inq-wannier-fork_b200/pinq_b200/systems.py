@@ -7,6 +7,7 @@ here from fixed seeds.  Pure numpy (input preparation, not the hot path).
   cfg1  cubic a=20.52, 64 atoms (2x2x2 diamond), 64^3, 128 orbitals
   cfg2  cfg0 cell, 16 orbitals, ETRS dt=0.05, 200 steps, A_x ~ N(0, 0.01^2)
   cfg3  16 cubic cells, grids from {24,32,40,48}^3, 8..64 orbitals, 2..16 atoms
+  cfg4  cubic a=30, 240 atoms on a jittered shell of radius 6.7, 144^3, ecut 30 Ha
 """
 from __future__ import annotations
 
@@ -90,6 +91,21 @@ def random_orbitals(lattice, nr, M, ecut=25.0, seed=0, dtype=np.complex128) -> n
 
 def cubic(a: float) -> np.ndarray:
     return np.eye(3) * a
+
+
+def shell_positions(n_atoms: int = 240, radius: float = 6.7, jitter: float = 0.05, center=(15.0, 15.0, 15.0),
+                    seed: int = 0) -> np.ndarray:
+    """Atoms on a jittered closed shell (the 240-atom fullerene-like cage of the
+    large-cell configuration): n points of a golden-angle (Fibonacci) spiral on the
+    sphere, each moved by N(0, jitter^2) per coordinate.  The spiral stands in for a
+    fullerene's exact geometry, which the configuration does not give."""
+    rng = np.random.default_rng(seed)
+    k = np.arange(n_atoms) + 0.5
+    z = 1.0 - 2.0 * k / n_atoms
+    r = np.sqrt(1.0 - z * z)
+    phi = k * np.pi * (3.0 - np.sqrt(5.0))
+    unit = np.stack([r * np.cos(phi), r * np.sin(phi), z], 1)
+    return np.asarray(center, float)[None, :] + radius * unit + rng.normal(0.0, jitter, (n_atoms, 3))
 
 
 def config(name: str, M: int | None = None, seed: int = 0) -> dict:
