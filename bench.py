@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample length")
     ap.add_argument("--no-cells", dest="cells", action="store_false", help="skip the 16-cell batch measurement")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false", help="skip the adjoint measurement")
+    ap.add_argument("--cfg4", action="store_true", help="also run the large-cell (144^3, 480 orbitals) section")
     return ap.parse_args()
 
 
@@ -318,6 +319,77 @@ def bench_adjoint(args, local):
     return out
 
 
+def bench_cfg4(args, local):
+    """Large cell (opt-in, --cfg4): cubic a=30, 144^3, 240 atoms on a jittered shell
+    (radius 6.7), 960 projectors, 480 orbitals (11.5 GB in complex64, 23 GB in
+    complex128), inputs made on the device.  H|psi> and ETRS steps/s in both
+    precisions, peak device memory, and the adjoint gradient (50 steps, checkpoints
+    every 10) of 16 of the orbitals in both precisions."""
+    import torch
+
+    import pinq_b200 as pb
+    from pinq_b200 import systems
+    from pinq_b200.adjoint import DipolePropagation
+
+    lattice = systems.cubic(30.0)
+    nr = (144, 144, 144)
+    pos = systems.shell_positions(240, 6.7, 0.05, (15.0, 15.0, 15.0), seed=0)
+    V = systems.gaussian_potential_device(lattice, nr, pos, device=f"cuda:{local}")
+    M = 480
+    out = {"config": "cfg4: cubic a=30, 144^3, 240 atoms on a jittered shell r=6.7 (Fibonacci sphere), "
+                     "960 projectors, ecut 30 Ha, 480 orbitals", "timing": "CUDA events"}
+    ys = {}
+    for precision in ("fp64", "mixed"):
+        torch.cuda.empty_cache()
+        torch.cuda.reset_peak_memory_stats()
+        h = pb.KSHamiltonian(lattice, nr, precision, device=local)
+        h.set_scalar_potential(V)
+        kb = h.set_gaussian_projectors(pos, 3.0, 1.0, 1.5, -0.7)
+        x = systems.random_orbitals_device(h, M, 30.0, seed=3)
+        y = torch.empty_like(x)
+        for _ in range(2):
+            h.apply(x, y)
+        ms = _timed_ms(lambda: h.apply(x, y), 5, 1) / 5
+        ys[precision] = y[:, :32].to(torch.complex128).cpu()
+        cov = [h.cart_to_cov(np.array([a, 0.0, 0.0])) for a in (0.0, 0.01, -0.01)]
+        ms_etrs = _timed_ms(lambda: h.etrs_step_(x, 0.05, cov[1], cov[2]), 2, 1) / 2
+        free, total = torch.cuda.mem_get_info()
+        out[precision] = {"apply_ms": ms, "orbital_applies_per_s": M / (ms * 1e-3),
+                          "etrs_steps_per_s": 1.0 / (ms_etrs * 1e-3), "sphere_points": int(kb["counts"].sum()),
+                          "device_memory_in_use_gb": (total - free) / 1e9,
+                          "torch_peak_gb": torch.cuda.max_memory_allocated() / 1e9}
+        del x, y, h
+    out["mixed_vs_fp64_apply_rel_norm_32_orbitals"] = float((ys["mixed"] - ys["fp64"]).norm() / ys["fp64"].norm())
+    # adjoint on 16 orbitals: 50 steps, checkpoints every 10
+    amps = np.random.default_rng(9).normal(0.0, 0.01, 50)
+    grads = {}
+    for precision in ("fp64", "mixed"):
+        torch.cuda.empty_cache()
+        h = pb.KSHamiltonian(lattice, nr, precision, device=local)
+        h.set_scalar_potential(V)
+        h.set_gaussian_projectors(pos, 3.0, 1.0, 1.5, -0.7)
+        h.set_fourier_sphere_mask(True)
+        psi0 = systems.random_orbitals_device(h, 16, 30.0, seed=4)
+        prop = DipolePropagation(h, psi0, np.full(16, 2.0), 0.05, 10)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d = prop.forward(amps, keep=True)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        gA, gV = prop.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        grads[precision] = (d, gA.cpu().numpy(), gV.cpu().numpy())
+        out[precision]["adjoint_16_orbitals"] = {"forward_s": t1 - t0, "backward_s": t2 - t1,
+                                                 "total_over_forward": (t2 - t0) / (t1 - t0)}
+        del prop, psi0, h
+    (d64, a64, v64), (d32, a32, v32) = grads["fp64"], grads["mixed"]
+    out["adjoint_mixed_vs_fp64"] = {"dipole_rel": abs(d32 - d64) / abs(d64),
+                                    "grad_amplitudes_rel": float(np.linalg.norm(a32 - a64) / np.linalg.norm(a64)),
+                                    "grad_V_rel": float(np.linalg.norm(v32 - v64) / np.linalg.norm(v64))}
+    return out
+
+
 def run_reference(args):
     world, rank, local = dist_setup(args.gpus)
     if rank != 0:
@@ -472,6 +544,7 @@ def run_ours(args):
 
     cells = bench_cells(args, local) if args.cells else None
     adj = bench_adjoint(args, local) if args.adjoint else None
+    big = bench_cfg4(args, local) if args.cfg4 else None
 
     if rank != 0:
         if dist is not None:
@@ -534,6 +607,8 @@ def run_ours(args):
         line["cells"] = cells
     if adj is not None:
         line["adjoint"] = adj
+    if big is not None:
+        line["cfg4"] = big
     if world == 1:
         try:
             res, _ = cpu_baseline(lattice, nr, pos, V, seconds=args.cpu_seconds)

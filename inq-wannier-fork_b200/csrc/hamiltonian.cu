@@ -150,7 +150,7 @@ static int launch_h_impl(const LaunchArgs& a) {
     const int seg_cap = pj.nproj > 0 ? std::min(pj.max_tile_seg, kAccAtomsMax) : 0;
     // stage a tile's records only when all of them fit beside the tile (the kernel
     // reads them from global memory otherwise)
-    int rec_cap = pj.nproj > 0 ? std::min(pj.max_tile_ent, kRecCapMax) : 0;
+    int rec_cap = (pj.nproj > 0 && pj.max_tile_ent <= kRecCapMax) ? pj.max_tile_ent : 0;
     if (TG::smem_fwd(acc_cap, rec_cap) > TG::SMEM_MAX) rec_cap = 0;
     if (pj.nproj > 0 && pj.pt_stride != TG::PSTRIDE)
       return fail(INQB_ERR_INVALID, "projector tables were built for another tiling of this grid");

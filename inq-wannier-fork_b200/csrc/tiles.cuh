@@ -6,8 +6,9 @@
 // so a tile (x-plane ix, row class y1) of Y2 rows x NZ points finishes the z
 // transform and the inner y stage on its own, and the outer y stage lands in
 // the x-line pass.  Every tile moves whole 64-byte runs of G orbitals per grid
-// point (G = 8 complex64 or 4 complex128), so the orbital-fastest layout
-// [point][orbital] is read and written in full sectors.
+// point (G = 8 complex64 or 4 complex128; 32-byte runs for the long rows of
+// 144^3), so the orbital-fastest layout [point][orbital] is read and written in
+// full sectors.
 //
 //   pass A  k_tile_fwd  CTA (group, ix, half of the y1 classes), loops over y1: psi
 //           rows -> KB projection (plane accumulators in shared memory, flushed
@@ -38,15 +39,19 @@ __device__ __forceinline__ void cp_async_wait() {
 // ---------------------------------------------------------------- geometry
 template <typename T, int NX, int NY, int NZ>
 struct TileGeom {
-  static constexpr int G = 64 / (int)sizeof(cplx<T>);  // orbitals per tile: one 64-byte run
-  static constexpr int PV = 16 / (int)sizeof(cplx<T>);  // complex values per 16-byte vector
-  static constexpr int VP = G / PV;                      // 16-byte vectors per point
   using AX = Axis<Split<NX>::N1, Split<NX>::N2>;
   using AY = Axis<Split<NY>::N1, Split<NY>::N2>;
   using AZ = Axis<Split<NZ>::N1, Split<NZ>::N2>;
   static constexpr int Y2 = AY::N1;  // rows per tile
   static constexpr int Y1 = AY::N2;  // tiles per x-plane
   static constexpr int ZS = AZ::SLOTS;  // padded z slots per row
+  // orbitals per tile: one 64-byte run per grid point, or in FP32 one 32-byte sector
+  // where a 64-byte tile would pass 80 KB (long rows: 144^3), which buys a second CTA
+  // per SM (measured: FP32 144^3 apply 75 -> 65 ms; FP64 is faster with 64 bytes)
+  static constexpr int RUN = (sizeof(T) == 4 && Y2 * ZS * 64 > 80 * 1024) ? 32 : 64;
+  static constexpr int G = RUN / (int)sizeof(cplx<T>);
+  static constexpr int PV = 16 / (int)sizeof(cplx<T>);  // complex values per 16-byte vector
+  static constexpr int VP = G / PV;                      // 16-byte vectors per point
   static constexpr int TILE = Y2 * ZS * G;  // complex values of a tile in shared memory
   static constexpr int PTS = Y2 * NZ;       // grid points of a tile
   static constexpr int XS = (Y1 + 1) * G;   // x-slot stride of the x-line block (one point of padding)

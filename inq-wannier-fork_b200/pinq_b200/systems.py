@@ -61,6 +61,48 @@ def gaussian_potential(lattice, nr, positions, amplitude=-4.0, sigma=0.8) -> np.
     return V
 
 
+def gaussian_potential_device(lattice, nr, positions, device="cuda", amplitude=-4.0, sigma=0.8):
+    """gaussian_potential evaluated with torch on the device (FP64), for grids whose
+    host evaluation would be slow; returns a numpy array [N]."""
+    import torch
+
+    lat = torch.tensor(np.asarray(lattice, float).reshape(3, 3), dtype=torch.float64, device=device)
+    f = [torch.tensor(sym(n) / n, dtype=torch.float64, device=device) for n in nr]
+    c = torch.stack(torch.meshgrid(*f, indexing="ij"), -1).reshape(-1, 3)
+    r = c @ lat
+    V = torch.zeros(r.shape[0], dtype=torch.float64, device=device)
+    pos = torch.tensor(np.asarray(positions, float).reshape(-1, 3), dtype=torch.float64, device=device)
+    cut2 = (8 * sigma) ** 2
+    for i in (-1, 0, 1):
+        for j in (-1, 0, 1):
+            for k in (-1, 0, 1):
+                shift = i * lat[0] + j * lat[1] + k * lat[2]
+                for p in pos:
+                    d2 = ((r - (p + shift)) ** 2).sum(1)
+                    V += torch.where(d2 < cut2, amplitude * torch.exp(-d2 / (2 * sigma * sigma)),
+                                     torch.zeros_like(d2))
+    return V.cpu().numpy()
+
+
+def random_orbitals_device(ham, M, ecut=25.0, seed=0):
+    """random_orbitals built on the device with the library: complex N(0,1)
+    plane-wave coefficients for 1/2|G|^2 <= ecut, the library's inverse FFT, then
+    its FP64 orthonormalisation.  A torch tensor [N, M] in the context precision."""
+    import torch
+
+    nx, ny, nz = ham.nr
+    recip = 2 * np.pi * np.linalg.inv(np.asarray(ham.lattice, float).reshape(3, 3)).T
+    n = np.stack(np.meshgrid(sym(nx), sym(ny), sym(nz), indexing="ij"), -1).reshape(-1, 3)
+    mask = 0.5 * ((n @ recip) ** 2).sum(1) <= ecut
+    g = torch.Generator(device=ham.device).manual_seed(int(seed))
+    coef = torch.randn((ham.N, M, 2), generator=g, device=ham.device, dtype=torch.float32)
+    box = torch.view_as_complex(coef).to(ham.dtype) / np.sqrt(2.0)
+    box *= torch.as_tensor(mask, device=ham.device)[:, None]
+    psi = ham.to_real(box)
+    del box, coef
+    return ham.orthonormalize_(psi)
+
+
 def orthonormalize(psi: np.ndarray, dV: float) -> np.ndarray:
     """psi U^-1 with dV psi^H psi = U^H U."""
     import scipy.linalg as sla
