@@ -255,11 +255,19 @@ def bench_cells(args, local):
             h.apply(x, y)
 
     ms_seq = _timed_ms(seq, K, 3)
+    # the same graph with every cell's launch schedule picked by the autotuner
+    t0 = time.perf_counter()
+    scheds = batch.autotune([x.shape[1] for x in xs])
+    tune_s = time.perf_counter() - t0
+    ms_tuned = _timed_ms(lambda: batch.apply(xs, ys), K, 3)
     norb = sum(x.shape[1] for x in xs)
     return {"ncells": len(hams), "grids": [h.nr[0] for h in hams], "orbitals": norb, "steps": K,
             "graph_orbital_applies_per_s": norb * K / (ms_graph * 1e-3),
             "sequential_orbital_applies_per_s": norb * K / (ms_seq * 1e-3),
-            "graph_speedup": ms_seq / ms_graph, "precision": "mixed"}
+            "graph_speedup": ms_seq / ms_graph,
+            "graph_autotuned_orbital_applies_per_s": norb * K / (ms_tuned * 1e-3),
+            "autotune_speedup_over_default_graph": ms_graph / ms_tuned, "autotune_s": tune_s,
+            "schedules": [list(sc) for sc in scheds], "precision": "mixed"}
 
 
 def bench_adjoint(args, local):

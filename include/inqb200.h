@@ -223,6 +223,20 @@ int inqb_etrs_adjoint_step(inqb_ctx* ctx, void* lambda, int M, int ld, double dt
                            const double kA_tdt_cov[3], const void* powers, double* gV, double* gA_t,
                            double* gA_tdt, void* stream);
 
+/* ---------------------------------------------------------------- launch schedules
+ * (no counterpart in the reference; its kernels have fixed launch shapes).  A
+ * schedule is {ysplit, threads of pass 1, of pass 2, of pass 3}: ysplit CTAs share
+ * one x-plane in the first pass (a divisor of the tiles per plane), and each pass
+ * runs 64..256 threads per CTA (multiples of 32).  Schedules are kept per orbital
+ * count M; counts without one use the compiled default. */
+/* Time the candidates (every ysplit with 128 and 256 threads for the first pass,
+ * 128 and 256 threads for the others) on zeroed M-orbital blocks with CUDA events
+ * and keep the fastest for M; schedule (may be NULL) receives it.  Allocates two
+ * scratch blocks for the duration of the call; synchronous. */
+int inqb_autotune(inqb_ctx* ctx, int M, void* stream, int schedule[4]);
+/* Set (or with schedule NULL, clear) the schedule used for M orbitals. */
+int inqb_set_schedule(inqb_ctx* ctx, int M, const int schedule[4]);
+
 /* ---------------------------------------------------------------- profiling
  * Per-pass CUDA-event timing of the next max_applies H applications, recorded
  * on the stream the kernels run on; the counterpart of INQ's scoped timers

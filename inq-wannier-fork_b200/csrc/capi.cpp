@@ -142,6 +142,11 @@ int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long l
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) a.rlat[i][j] = ctx->cell.rlat[i][j];
   ctx->cell.cov_to_cart(ctx->kA_cov, a.kA_cart);
+  const auto sched = ctx->schedules.find(M);
+  if (sched != ctx->schedules.end()) {
+    a.ysplit = sched->second[0];
+    for (int k = 0; k < 3; k++) a.threads[k] = sched->second[1 + k];
+  }
   if (ctx->timing_on && mode == LaunchArgs::H && ctx->timing_count < ctx->timing_capacity) {
     for (int i = 0; i < 4; i++) a.events[i] = ctx->timing_events[4 * ctx->timing_count + i];
     ctx->timing_count++;
@@ -156,6 +161,30 @@ int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long l
     a.proj_view = &v32;
   }
   return ctx->plan->launch(a);
+}
+
+// One H application with the four pass events recorded (used by the autotuner).
+int apply_events(inqb_ctx* ctx, const void* in, void* out, int M, const double alpha[2], const double beta[2],
+                 void* stream, cudaEvent_t ev[4]) {
+  INQB_TRY(reserve(ctx, M));
+  if (!ctx->proj_phases_valid) {
+    INQB_TRY(update_phases(ctx, stream));
+    ctx->proj_phases_valid = true;
+  }
+  const bool on = ctx->timing_on;
+  const int cap = ctx->timing_capacity, count = ctx->timing_count;
+  std::vector<cudaEvent_t> saved;
+  saved.swap(ctx->timing_events);
+  ctx->timing_events.assign(ev, ev + 4);
+  ctx->timing_on = true;
+  ctx->timing_capacity = 1;
+  ctx->timing_count = 0;
+  const int st = apply(ctx, LaunchArgs::H, in, M, out, M, M, nullptr, 0, alpha, beta, stream);
+  ctx->timing_events.swap(saved);
+  ctx->timing_on = on;
+  ctx->timing_capacity = cap;
+  ctx->timing_count = count;
+  return st;
 }
 
 // psi <- sum_{k <= order} (f H)^k / k! psi by Horner's rule:
@@ -908,6 +937,95 @@ int inqb_etrs_adjoint_step(inqb_ctx* ctx, void* lambda, int M, int ld, double dt
   INQB_TRY(half_back(ctx, lambda, ld, M, c, P2, gV, gA_tdt, stream));
   INQB_TRY(set_kA(ctx, kA_t_cov, stream));
   return half_back(ctx, lambda, ld, M, c, P1, gV, gA_t, stream);
+}
+
+int inqb_set_schedule(inqb_ctx* ctx, int M, const int schedule[4]) {
+  INQB_CHECK_CTX(ctx);
+  if (M <= 0) return fail(INQB_ERR_INVALID, "M must be positive");
+  if (!schedule) {
+    ctx->schedules.erase(M);
+    return INQB_OK;
+  }
+  if (schedule[0] < 1 || ctx->plan->y1 % schedule[0] != 0)
+    return fail(INQB_ERR_INVALID, "schedule: ysplit must divide " + std::to_string(ctx->plan->y1));
+  for (int k = 1; k < 4; k++)
+    if (schedule[k] < 64 || schedule[k] > 256 || schedule[k] % 32 != 0)
+      return fail(INQB_ERR_INVALID, "schedule: threads per CTA must be a multiple of 32 in [64, 256]");
+  ctx->schedules[M] = {schedule[0], schedule[1], schedule[2], schedule[3]};
+  return INQB_OK;
+}
+
+int inqb_autotune(inqb_ctx* ctx, int M, void* stream, int schedule[4]) {
+  INQB_CHECK_CTX(ctx);
+  if (M <= 0) return fail(INQB_ERR_INVALID, "M must be positive");
+  INQB_GUARD(ctx);
+  INQB_TRY(reserve(ctx, M));
+  // the timings do not depend on the values: zeroed blocks
+  DevBuf in, out;
+  const size_t bytes = (size_t)ctx->N * M * ctx->elem_bytes();
+  INQB_TRY(in.ensure(bytes));
+  INQB_TRY(out.ensure(bytes));
+  cudaStream_t st = (cudaStream_t)stream;
+  INQB_CUDA_TRY(cudaMemsetAsync(in.ptr, 0, bytes, st));
+  cudaEvent_t ev[4];
+  for (auto& e : ev) INQB_CUDA_TRY(cudaEventCreate(&e));
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  const bool saved_timing = ctx->timing_on;
+  ctx->timing_on = false;
+  std::array<int, 4> best = {ctx->plan->ysplit, 256, 256, 256};
+  // pass times (ms) of one schedule: the best of three applications after a warm-up
+  auto pass_ms = [&](const std::array<int, 4>& s, float out_ms[3]) -> int {
+    ctx->schedules[M] = s;
+    for (int k = 0; k < 3; k++) out_ms[k] = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+      INQB_TRY(apply_events(ctx, in.ptr, out.ptr, M, one, zero, stream, ev));
+      INQB_CUDA_TRY(cudaEventSynchronize(ev[3]));
+      if (rep == 0) continue;
+      for (int k = 0; k < 3; k++) {
+        float t = 0.f;
+        INQB_CUDA_TRY(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+        out_ms[k] = std::min(out_ms[k], t);
+      }
+    }
+    return INQB_OK;
+  };
+  int status = INQB_OK;
+  float t[3], best_t[3] = {1e30f, 1e30f, 1e30f};
+  // pass A: every divisor of Y1 times every thread count; passes B and C: thread counts
+  for (int ys = 1; ys <= ctx->plan->y1 && status == INQB_OK; ys++) {
+    if (ctx->plan->y1 % ys != 0) continue;
+    for (int thr : kScheduleThreads) {
+      std::array<int, 4> s = best;
+      s[0] = ys;
+      s[1] = thr;
+      if ((status = pass_ms(s, t)) != INQB_OK) break;
+      if (t[0] < best_t[0]) {
+        best_t[0] = t[0];
+        best[0] = ys;
+        best[1] = thr;
+      }
+    }
+  }
+  for (int k = 1; k < 3 && status == INQB_OK; k++)
+    for (int thr : kScheduleThreads) {
+      std::array<int, 4> s = best;
+      s[1 + k] = thr;
+      if ((status = pass_ms(s, t)) != INQB_OK) break;
+      if (t[k] < best_t[k]) {
+        best_t[k] = t[k];
+        best[1 + k] = thr;
+      }
+    }
+  for (auto& e : ev) cudaEventDestroy(e);
+  ctx->timing_on = saved_timing;
+  if (status != INQB_OK) {
+    ctx->schedules.erase(M);
+    return status;
+  }
+  ctx->schedules[M] = best;
+  if (schedule)
+    for (int k = 0; k < 4; k++) schedule[k] = best[k];
+  return INQB_OK;
 }
 
 int inqb_orthonormalize_noalloc(inqb_ctx* ctx, void* psi, int M, int ld, void* stream) {

@@ -129,7 +129,15 @@ static int launch_h_impl(const LaunchArgs& a) {
   // 16-byte vectors of G orbitals: full groups, aligned pointers and leading dimensions
   const int vin = aligned16(a.in, a.ld_in, esz);
   const int vout = aligned16(a.out, a.ld_out, esz);
-  const dim3 gfwd(tgroups, NX * TG::YSPLIT), gx(TG::Y2 * NZ, tgroups), ginv(tgroups, NX * TG::Y1);
+  int ysplit = a.ysplit > 0 ? a.ysplit : TG::YSPLIT;
+  if (TG::Y1 % ysplit != 0) return fail(INQB_ERR_INVALID, "schedule: ysplit must divide the tiles per plane");
+  int thr[3];
+  for (int k = 0; k < 3; k++) {
+    thr[k] = a.threads[k] > 0 ? a.threads[k] : TG::THREADS;
+    if (thr[k] % 32 != 0 || thr[k] < 64 || thr[k] > TG::THREADS)
+      return fail(INQB_ERR_INVALID, "schedule: threads per CTA must be a multiple of 32 in [64, 256]");
+  }
+  const dim3 gfwd(tgroups, NX * ysplit), gx(TG::Y2 * NZ, tgroups), ginv(tgroups, NX * TG::Y1);
 
   ProjView<T> pj = *reinterpret_cast<const ProjView<T>*>(a.proj_view);
   KinParams<T> kp;
@@ -157,10 +165,10 @@ static int launch_h_impl(const LaunchArgs& a) {
     if (pj.nproj > 0)
       INQB_CUDA_TRY(cudaMemsetAsync(pj.proj, 0, sizeof(double2) * (size_t)pj.nproj * pj.L * a.M, st));
     if (a.events[0]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[0], st));
-    k_tile_fwd<T, NX, NY, NZ><<<gfwd, TG::THREADS, TG::smem_fwd(acc_cap, rec_cap), st>>>(
-        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pj, acc_cap, rec_cap, vin);
+    k_tile_fwd<T, NX, NY, NZ><<<gfwd, thr[0], TG::smem_fwd(acc_cap, rec_cap), st>>>(
+        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pj, acc_cap, rec_cap, ysplit, vin);
     if (a.events[1]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[1], st));
-    k_tile_x<T, NX, NY, NZ><<<gx, TG::THREADS, TG::SMEM_X, st>>>(tmp, twx, kp);
+    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp);
     if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
     EpiParams<T> ep;
     ep.V = (const T*)a.V;
@@ -176,25 +184,25 @@ static int launch_h_impl(const LaunchArgs& a) {
     if (TG::smem_inv(rec_cap_inv, seg_cap) > TG::SMEM_MAX) rec_cap_inv = 0;
     if (TG::smem_inv(rec_cap_inv, seg_cap) > TG::SMEM_MAX)
       return fail(INQB_ERR_UNSUPPORTED, "tile of this grid does not fit in shared memory");
-    k_tile_inv<T, NX, NY, NZ, 1><<<ginv, TG::THREADS, TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
+    k_tile_inv<T, NX, NY, NZ, 1><<<ginv, thr[2], TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
         tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv, seg_cap,
         vin && vout);
     if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
   } else if (a.mode == LaunchArgs::FFT_FWD) {
     ProjView<T> none = pj;
     none.nproj = 0;
-    k_tile_fwd<T, NX, NY, NZ><<<gfwd, TG::THREADS, TG::smem_fwd(0, 0), st>>>(
-        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, none, 0, 0, vin);
-    k_tile_x_fft<T, NX, NY, NZ, 0><<<gx, TG::THREADS, TG::SMEM_X, st>>>(tmp, nullptr, (cplx<T>*)a.out, a.ld_out,
+    k_tile_fwd<T, NX, NY, NZ><<<gfwd, thr[0], TG::smem_fwd(0, 0), st>>>(
+        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, none, 0, 0, ysplit, vin);
+    k_tile_x_fft<T, NX, NY, NZ, 0><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, nullptr, (cplx<T>*)a.out, a.ld_out,
                                                                        a.M, twx, vout);
   } else {
-    k_tile_x_fft<T, NX, NY, NZ, 1><<<gx, TG::THREADS, TG::SMEM_X, st>>>(tmp, (const cplx<T>*)a.in, nullptr, a.ld_in,
+    k_tile_x_fft<T, NX, NY, NZ, 1><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, (const cplx<T>*)a.in, nullptr, a.ld_in,
                                                                        a.M, twx, vin);
     EpiParams<T> ep{};
     ep.alpha = mk<T>(kp.scale, (T)0);
     ProjView<T> none = pj;
     none.nproj = 0;
-    k_tile_inv<T, NX, NY, NZ, 0><<<ginv, TG::THREADS, TG::smem_inv(0, 0), st>>>(
+    k_tile_inv<T, NX, NY, NZ, 0><<<ginv, thr[2], TG::smem_inv(0, 0), st>>>(
         tmp, nullptr, 0, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, none, ep, 0, 0, vout);
   }
   INQB_CUDA_TRY(cudaGetLastError());
@@ -225,6 +233,8 @@ static Plan make_plan() {
   Plan p;
   p.G = TileGeom<T, NX, NY, NZ>::G;
   p.G_tile = TileGeom<T, NX, NY, NZ>::G;
+  p.y1 = TileGeom<T, NX, NY, NZ>::Y1;
+  p.ysplit = TileGeom<T, NX, NY, NZ>::YSPLIT;
   p.launch = &launch_h_impl<T, NX, NY, NZ>;
   return p;
 }

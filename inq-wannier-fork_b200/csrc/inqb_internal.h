@@ -4,7 +4,9 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -189,6 +191,10 @@ struct inqb_ctx {
   inqb::DevBuf d_cn;            // Crank-Nicolson: rhs, residual, (1 + i dt/2 H) residual
   inqb::DevBuf d_cnred;         // Crank-Nicolson: 4 sums and the residual norm per orbital
   size_t elem_bytes() const { return precision == INQB_FP64 ? 16 : 8; }
+
+  // launch schedules per orbital count (ysplit, threads of the three passes), set
+  // by inqb_autotune or inqb_set_schedule; absent counts use the compiled default
+  std::map<int, std::array<int, 4>> schedules;
 
   // optional per-pass CUDA-event timing of H applications
   std::vector<cudaEvent_t> timing_events;  // 4 per recorded application

@@ -24,11 +24,20 @@ struct LaunchArgs {
   void* stream = nullptr;
   int fourier_mask = 0;             // zero the kinetic term outside the Fourier sphere
   void* events[4] = {nullptr, nullptr, nullptr, nullptr};  // optional cudaEvent_t around the passes
+  // launch schedule (0 = the compiled default): CTAs sharing one x-plane in the first
+  // pass (a divisor of the y split's Y1), and threads per CTA of the three passes
+  int ysplit = 0;
+  int threads[3] = {0, 0, 0};
 };
+
+// Candidate values the autotuner tries.
+constexpr int kScheduleThreads[2] = {128, 256};
 
 struct Plan {
   int G = 1;       // orbitals per tile of the plain FFT kernels
   int G_tile = 1;  // orbitals per tile of the H kernels
+  int y1 = 1;      // tiles per x-plane (the divisors of y1 are the first pass's splits)
+  int ysplit = 1;  // default split
   int (*launch)(const LaunchArgs&) = nullptr;
 };
 

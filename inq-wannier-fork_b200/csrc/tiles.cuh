@@ -77,7 +77,7 @@ struct TileGeom {
            sizeof(EntRec<T>) * (size_t)rec_cap + sizeof(int) * (size_t)PSTRIDE +
            sizeof(cplx<T>) * (size_t)seg_cap * LMAX * G;
   }
-  // pass A: each CTA takes Y1 / YSPLIT row classes of one plane
+  // pass A default: two CTAs per x-plane where Y1 is even
   static constexpr int YSPLIT = (Y1 % 2 == 0) ? 2 : 1;
 };
 
@@ -118,7 +118,7 @@ template <typename T, int NX, int NY, int NZ>
 __global__ void __launch_bounds__(256)
     k_tile_fwd(const cplx<T>* __restrict__ in, long ld, int M, cplx<T>* __restrict__ tmp,
                const cplx<T>* __restrict__ tw_y, const cplx<T>* __restrict__ tw_z, ProjView<T> pj, int acc_cap,
-               int rec_cap, int vec) {
+               int rec_cap, int ysplit, int vec) {
   using TG = TileGeom<T, NX, NY, NZ>;
   using AZ = typename TG::AZ;
   constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, ZS = TG::ZS;
@@ -129,7 +129,8 @@ __global__ void __launch_bounds__(256)
   double2* acc = reinterpret_cast<double2*>(twz + NZ);  // [acc_cap][LMAX][G]
   EntRec<T>* R = reinterpret_cast<EntRec<T>*>(acc + acc_cap * LMAX * G);  // [rec_cap]
 
-  constexpr int YS = TG::YSPLIT, YPER = Y1 / YS;
+  // ysplit CTAs share plane ix, each taking Y1 / ysplit row classes
+  const int YS = ysplit, YPER = Y1 / ysplit;
   const int grp = blockIdx.x, ix = blockIdx.y / YS, yh = blockIdx.y % YS;
   const int m0 = grp * G;
   const int gcount = min(G, M - m0);

@@ -19,6 +19,17 @@ class CellBatch:
         call("inqb_batch_create", arr, len(self.hams), ctypes.byref(out))
         self._b = out
 
+    def autotune(self, Ms):
+        """Pick each cell's launch schedule for its orbital count (inqb_autotune) and
+        start a fresh batch, so the next apply captures the graph with them."""
+        scheds = [h.autotune(int(M)) for h, M in zip(self.hams, Ms)]
+        self.close()
+        arr = (ctypes.c_void_p * len(self.hams))(*[h._h.value for h in self.hams])
+        out = ctypes.c_void_p()
+        call("inqb_batch_create", arr, len(self.hams), ctypes.byref(out))
+        self._b = out
+        return scheds
+
     def close(self):
         if getattr(self, "_b", None) is not None and self._b.value:
             lib().inqb_batch_destroy(self._b)

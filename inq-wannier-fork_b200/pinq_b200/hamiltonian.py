@@ -148,6 +148,18 @@ class KSHamiltonian:
         self.set_projectors(kb)
         return kb
 
+    def autotune(self, M: int) -> tuple:
+        """Time the launch schedules for M orbitals and keep the fastest; returns
+        (ysplit, threads of the three passes)."""
+        sched = (ctypes.c_int * 4)()
+        call("inqb_autotune", self._h, int(M), self._stream(), sched)
+        return tuple(sched)
+
+    def set_schedule(self, M: int, schedule=None):
+        """Use schedule (ysplit, t1, t2, t3) for M orbitals; None restores the default."""
+        arr = None if schedule is None else (ctypes.c_int * 4)(*[int(v) for v in schedule])
+        call("inqb_set_schedule", self._h, int(M), arr)
+
     def reserve(self, M: int):
         call("inqb_ctx_reserve", self._h, int(M))
 

@@ -54,3 +54,28 @@ def test_batch_fp64_matches_oracle(pb, oracle_mod):
         sub = np.ascontiguousarray(c["psi"][:, :4])
         ref = o.apply_h(sub)
         assert rel_max(outs[k].cpu().numpy()[:, :4], ref) < 1e-10
+
+
+def test_every_schedule_gives_the_same_h(pb, oracle_mod):
+    """H|psi> under every launch schedule the autotuner may pick (each ysplit with
+    128 and 256 threads per pass) matches the oracle; the autotuner keeps one of them."""
+    from helpers import make_oracle, make_product, rel_norm, small_system
+
+    s = small_system(pb, n=32, M=8, seed=21)
+    o = make_oracle(oracle_mod, s)
+    ref = o.apply_h(s["psi"])
+    h = make_product(pb, s, "mixed")
+    x = torch.as_tensor(s["psi"]).to("cuda", torch.complex64)
+    y1 = 4  # tiles per x-plane of the 32^3 grid (32 = 8 x 4)
+    for ys in (1, 2, 4):
+        for t in (128, 256):
+            h.set_schedule(8, (ys, t, 256 if t == 128 else 128, t))
+            out = h.apply(x).cpu().numpy().astype(np.complex128)
+            assert rel_norm(out, ref) < 1e-6, (ys, t)
+    sched = h.autotune(8)
+    assert y1 % sched[0] == 0 and all(v in (128, 256) for v in sched[1:])
+    out = h.apply(x).cpu().numpy().astype(np.complex128)
+    assert rel_norm(out, ref) < 1e-6
+    with pytest.raises(Exception):
+        h.set_schedule(8, (3, 256, 256, 256))
+    h.set_schedule(8, None)
