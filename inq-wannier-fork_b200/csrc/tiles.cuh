@@ -298,12 +298,6 @@ __global__ void __launch_bounds__(256)
 
   const int kz = blockIdx.x % NZ, ka = blockIdx.x / NZ, grp = blockIdx.y;
   cplx<T>* blk = tmp + ((long)(grp * Y2 + ka) * NZ + kz) * TG::BLK;
-  for (int q = threadIdx.x; q < NX * Y1 * VP; q += blockDim.x) {
-    const int v = q % VP, r = q / VP;
-    const int y1 = r % Y1, ix = r / Y1;
-    cp_async16(X + AX::slot(ix) * XS + y1 * G + v * PV, blk + (long)q * PV);
-  }
-  cp_async_commit();
   for (int i = threadIdx.x; i < NX; i += blockDim.x) twx[i] = tw_x[i];
   // Along an x line 1/2 |G + k + A|^2 / N = kA2 n0^2 + kinB n0 + kinC with
   // q = n1 b1 + n2 b2 + k + A:  kA2 = |b0|^2 / 2N, kinB = b0.q / N, kinC = |q|^2 / 2N
@@ -320,21 +314,32 @@ __global__ void __launch_bounds__(256)
     kinB[kb] = kp.scale * bq;
     kinC[kb] = (T)0.5 * kp.scale * qq;
   }
-  cp_async_wait<0>();
-  __syncthreads();
   const T kinA = (T)0.5 * kp.scale *
                  (kp.b[0][0] * kp.b[0][0] + kp.b[0][1] * kp.b[0][1] + kp.b[0][2] * kp.b[0][2]);
 
-  // outer y stage: DFT_Y1 over y1 -> kb, for each (ix, j)
-  for (int it = threadIdx.x; it < NX * G; it += blockDim.x) {
-    const int j = it % G, ix = it / G;
-    const int base = AX::slot(ix) * XS + j;
-    cplx<T> u[Y1];
+  // outer y stage straight from HBM: a thread loads the Y1 values of its (ix, j)
+  // column (lanes along j read whole 64-byte runs), DFT_Y1 over y1 -> kb, and
+  // writes the column to shared memory once; two columns per thread in flight
+  for (int it0 = threadIdx.x; it0 < NX * G; it0 += 2 * blockDim.x) {
+    cplx<T> u[2][Y1];
 #pragma unroll
-    for (int y = 0; y < Y1; ++y) u[y] = X[base + y * G];
-    DFT<Y1, false, T>::run(u);
+    for (int c = 0; c < 2; ++c) {
+      const int it = it0 + c * blockDim.x;
+      if (it >= NX * G) continue;
+      const int j = it % G, ix = it / G;
 #pragma unroll
-    for (int y = 0; y < Y1; ++y) X[base + y * G] = u[y];
+      for (int y = 0; y < Y1; ++y) u[c][y] = blk[(ix * Y1 + y) * G + j];
+    }
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int it = it0 + c * blockDim.x;
+      if (it >= NX * G) continue;
+      const int j = it % G, ix = it / G;
+      DFT<Y1, false, T>::run(u[c]);
+      const int base = AX::slot(ix) * XS + j;
+#pragma unroll
+      for (int y = 0; y < Y1; ++y) X[base + y * G] = u[c][y];
+    }
   }
   __syncthreads();
 
@@ -365,7 +370,7 @@ __global__ void __launch_bounds__(256)
   step1_inv_transposed<AX>(X, Y1 * G * AX::N2, map1);
   __syncthreads();
 
-  // inverse outer y stage: kb -> y1
+  // inverse outer y stage kb -> y1, written straight back to HBM
   for (int it = threadIdx.x; it < NX * G; it += blockDim.x) {
     const int j = it % G, ix = it / G;
     const int base = AX::slot(ix) * XS + j;
@@ -374,14 +379,7 @@ __global__ void __launch_bounds__(256)
     for (int y = 0; y < Y1; ++y) u[y] = X[base + y * G];
     DFT<Y1, true, T>::run(u);
 #pragma unroll
-    for (int y = 0; y < Y1; ++y) X[base + y * G] = u[y];
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < NX * Y1 * VP; q += blockDim.x) {
-    const int v = q % VP, r = q / VP;
-    const int y1 = r % Y1, ix = r / Y1;
-    *reinterpret_cast<float4*>(blk + (long)q * PV) =
-        *reinterpret_cast<const float4*>(X + AX::slot(ix) * XS + y1 * G + v * PV);
+    for (int y = 0; y < Y1; ++y) blk[(ix * Y1 + y) * G + j] = u[y];
   }
 }
 
