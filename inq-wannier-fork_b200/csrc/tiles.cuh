@@ -238,28 +238,20 @@ __global__ void __launch_bounds__(256)
     });
     __syncthreads();
 
-    // -- inner y stage: DFT_Y2 over the rows, twiddle w_NY^{y1 ka}
+    // -- inner y stage: DFT_Y2 over the rows, twiddle w_NY^{y1 ka}, written straight
+    // to tmp[g][ka][kz][ix][y1][G] (lanes along j write whole 64-byte runs)
     for (int it = threadIdx.x; it < NZ * G; it += blockDim.x) {
-      const int j = it % G, zi = it / G;
-      const int base = AZ::slot(zi) * G + j;
+      const int j = it % G, kz = it / G;
+      const int base = AZ::slot_of_freq(kz) * G + j;
       cplx<T> u[Y2];
 #pragma unroll
       for (int r = 0; r < Y2; ++r) u[r] = S[base + r * ZS * G];
       DFT<Y2, false, T>::run(u);
 #pragma unroll
       for (int ka = 1; ka < Y2; ++ka) u[ka] = u[ka] * twy[ka * Y1 + y1];
+      cplx<T>* dst = tmp + (((long)grp * Y2 * NZ + kz) * NX + ix) * (Y1 * G) + y1 * G + j;
 #pragma unroll
-      for (int ka = 0; ka < Y2; ++ka) S[base + ka * ZS * G] = u[ka];
-    }
-    __syncthreads();
-
-    // -- store (ka, kz) runs of G orbitals to tmp[g][ka][kz][ix][y1][G]
-    for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
-      const int v = q % VP, pt = q / VP;
-      const int kz = pt % NZ, ka = pt / NZ;
-      const float4 w = *reinterpret_cast<const float4*>(S + (ka * ZS + AZ::slot_of_freq(kz)) * G + v * PV);
-      cplx<T>* dst = tmp + (((long)(grp * Y2 + ka) * NZ + kz) * NX + ix) * (Y1 * G) + y1 * G + v * PV;
-      *reinterpret_cast<float4*>(dst) = w;
+      for (int ka = 0; ka < Y2; ++ka) dst[(long)ka * NZ * TG::BLK] = u[ka];
     }
     __syncthreads();
   }
@@ -533,7 +525,8 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
   const bool v16 = vec && gcount == G;
 
   // group 0: the (ka, kz) runs of this tile, needed first; group 1: what only the
-  // epilogue reads (entry records, point index, and in FP64 the input orbitals)
+  // epilogue reads (entry records, point index, and in FP64 the input orbitals).
+  // (Reading the runs into registers for the y stage measured slower than staging.)
   for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
     const int v = q % VP, pt = q / VP;
     const int kz = pt % NZ, ka = pt / NZ;
