@@ -213,35 +213,45 @@ int launch_density(int precision, const void* psi, long ld, int M, long N, const
 }
 
 // acc[3 m .. 3 m + 2] += (Re, Im) sum_p conj(hpsi) psi and sum_p |psi|^2 over this
-// block's points (overlap_diagonal.hpp:118-127); threads run along the orbitals.
+// block's points (overlap_diagonal.hpp:118-127).  Block: 32 orbitals (lanes) x 8
+// point lanes, reduced in shared memory before one FP64 atomic per orbital and sum.
 template <typename T>
-__global__ void k_band_sums(const cplx<T>* __restrict__ psi, const cplx<T>* __restrict__ hpsi, long ld, int M,
-                            long N, long pts_per_block, double* __restrict__ acc) {
+__global__ void __launch_bounds__(256)
+    k_band_sums(const cplx<T>* __restrict__ psi, const cplx<T>* __restrict__ hpsi, long ld, int M, long N,
+                long pts_per_block, double* __restrict__ acc) {
+  __shared__ double red[8][32][3];
+  const int tm = threadIdx.x & 31, tp = threadIdx.x >> 5;
+  const int m = blockIdx.y * 32 + tm;
   const long p0 = (long)blockIdx.x * pts_per_block, p1 = min(N, p0 + pts_per_block);
-  for (int m = blockIdx.y * blockDim.x + threadIdx.x; m < M; m += gridDim.y * blockDim.x) {
-    double vr = 0.0, vi = 0.0, nn = 0.0;
-    for (long p = p0; p < p1; p++) {
+  double vr = 0.0, vi = 0.0, nn = 0.0;
+  if (m < M) {
+    for (long p = p0 + tp; p < p1; p += 8) {
       const cplx<T> a = hpsi[p * ld + m], b = psi[p * ld + m];
       const double ax = a.x, ay = a.y, bx = b.x, by = b.y;
       vr += ax * bx + ay * by;
       vi += ax * by - ay * bx;
       nn += bx * bx + by * by;
     }
-    atomicAdd(&acc[3 * m], vr);
-    atomicAdd(&acc[3 * m + 1], vi);
-    atomicAdd(&acc[3 * m + 2], nn);
+  }
+  red[tp][tm][0] = vr;
+  red[tp][tm][1] = vi;
+  red[tp][tm][2] = nn;
+  __syncthreads();
+  if (tp < 3 && m < M) {
+    double v = 0.0;
+    for (int k = 0; k < 8; k++) v += red[k][tm][tp];
+    atomicAdd(&acc[3 * m + tp], v);
   }
 }
 
 template <typename T>
 static int band_sums_impl(const void* psi, const void* hpsi, long ld, int M, long N, double* acc, cudaStream_t st) {
   INQB_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * 3 * (size_t)M, st));
-  const int threads = 128;
-  const int ym = (M + threads - 1) / threads;
-  // about 4 blocks per SM over the points
-  const long nblk = std::max<long>(1, std::min<long>(N, 148L * 4 / ym + 1));
+  const int ym = (M + 31) / 32;
+  // about 8 blocks per SM over the points
+  const long nblk = std::max<long>(1, std::min<long>(N / 64 + 1, 148L * 8 / ym + 1));
   const long per = (N + nblk - 1) / nblk;
-  k_band_sums<T><<<dim3((unsigned)((N + per - 1) / per), ym), threads, 0, st>>>(
+  k_band_sums<T><<<dim3((unsigned)((N + per - 1) / per), ym), 256, 0, st>>>(
       (const cplx<T>*)psi, (const cplx<T>*)hpsi, ld, M, N, per, acc);
   INQB_CUDA_TRY(cudaGetLastError());
   return INQB_OK;

@@ -16,13 +16,19 @@
 
 namespace inqb {
 
+// Block: 32 orbitals (lanes) x 8 point lanes; the point lanes' partial sums meet in
+// shared memory, then one FP64 atomic per orbital and sum.
 template <typename T>
-__global__ void k_sd_sums(const cplx<T>* __restrict__ r, const cplx<T>* __restrict__ hsd, long ld, int M, long N,
-                          long pts_per_block, double* __restrict__ acc) {
+__global__ void __launch_bounds__(256)
+    k_sd_sums(const cplx<T>* __restrict__ r, const cplx<T>* __restrict__ hsd, long ld, int M, long N,
+              long pts_per_block, double* __restrict__ acc) {
+  __shared__ double red[8][32][5];
+  const int tm = threadIdx.x & 31, tp = threadIdx.x >> 5;
+  const int m = blockIdx.y * 32 + tm;
   const long p0 = (long)blockIdx.x * pts_per_block, p1 = min(N, p0 + pts_per_block);
-  for (int m = blockIdx.y * blockDim.x + threadIdx.x; m < M; m += gridDim.y * blockDim.x) {
-    double hh = 0.0, rhr = 0.0, rhi = 0.0, rr = 0.0;
-    for (long p = p0; p < p1; p++) {
+  double hh = 0.0, rhr = 0.0, rhi = 0.0, rr = 0.0;
+  if (m < M) {
+    for (long p = p0 + tp; p < p1; p += 8) {
       const cplx<T> a = r[p * ld + m], b = hsd[p * ld + m];
       const double ax = a.x, ay = a.y, bx = b.x, by = b.y;
       hh += bx * bx + by * by;
@@ -30,10 +36,16 @@ __global__ void k_sd_sums(const cplx<T>* __restrict__ r, const cplx<T>* __restri
       rhi += ax * by - ay * bx;
       rr += ax * ax + ay * ay;
     }
-    atomicAdd(&acc[4 * m], hh);
-    atomicAdd(&acc[4 * m + 1], rhr);
-    atomicAdd(&acc[4 * m + 2], rhi);
-    atomicAdd(&acc[4 * m + 3], rr);
+  }
+  red[tp][tm][0] = hh;
+  red[tp][tm][1] = rhr;
+  red[tp][tm][2] = rhi;
+  red[tp][tm][3] = rr;
+  __syncthreads();
+  if (tp < 4 && m < M) {
+    double v = 0.0;
+    for (int k = 0; k < 8; k++) v += red[k][tm][tp];
+    atomicAdd(&acc[4 * m + tp], v);
   }
 }
 
@@ -83,11 +95,10 @@ __global__ void k_sd_update(cplx<T>* __restrict__ phi, long ldp, const cplx<T>* 
 template <typename T>
 static int sd_sums_impl(const void* r, const void* hsd, long ld, int M, long N, double* acc, cudaStream_t st) {
   INQB_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * 4 * (size_t)M, st));
-  const int threads = 128;
-  const int ym = (M + threads - 1) / threads;
-  const long nblk = std::max<long>(1, std::min<long>(N, 148L * 4 / ym + 1));
+  const int ym = (M + 31) / 32;
+  const long nblk = std::max<long>(1, std::min<long>(N / 64 + 1, 148L * 8 / ym + 1));
   const long per = (N + nblk - 1) / nblk;
-  k_sd_sums<T><<<dim3((unsigned)((N + per - 1) / per), ym), threads, 0, st>>>(
+  k_sd_sums<T><<<dim3((unsigned)((N + per - 1) / per), ym), 256, 0, st>>>(
       (const cplx<T>*)r, (const cplx<T>*)hsd, ld, M, N, per, acc);
   INQB_CUDA_TRY(cudaGetLastError());
   return INQB_OK;
