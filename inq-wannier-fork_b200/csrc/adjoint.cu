@@ -224,10 +224,21 @@ __global__ void __launch_bounds__(512)
   const int mi = threadIdx.x & 31, q = threadIdx.x >> 5;
   const int m = blockIdx.z * 32 + mi;
   const int c0 = atom_chunk_ptr[a], c1 = atom_chunk_ptr[a + 1];
-  double v = 0.0;
-  if (m < M)
-    for (int c = c0; c < c1; ++c) v += part[(((long)c * L + l) * Q + q) * M + m];
-  mom[q][mi] = v;
+  // four independent partial sums keep four loads in flight (fixed order: deterministic)
+  double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+  if (m < M) {
+    const long stride = (long)L * Q * M;
+    const double* pp = part + (((long)c0 * L + l) * Q + q) * M + m;
+    int c = c0;
+    for (; c + 3 < c1; c += 4, pp += 4 * stride) {
+      v0 += pp[0];
+      v1 += pp[stride];
+      v2 += pp[2 * stride];
+      v3 += pp[3 * stride];
+    }
+    for (; c < c1; ++c, pp += stride) v0 += pp[0];
+  }
+  mom[q][mi] = (v0 + v1) + (v2 + v3);
   __syncthreads();
   double out[6] = {0, 0, 0, 0, 0, 0};
   if (q == 0 && m < M) {
@@ -348,8 +359,10 @@ static int agrad_impl(const inqb_ctx& ctx, const void* U, const void* W, const v
   ctx.cell.cov_to_cart(ctx.kA_cov, r.kA);
   r.mask = ctx.fourier_mask;
   INQB_CUDA_TRY(cudaMemsetAsync(acc, 0, 12 * sizeof(double), st));
-  k_velocity_dot<T><<<grid_for(ctx.N * M, 256), 256, 0, st>>>(ctx.N, M, (const cplx<T>*)U, (const cplx<T>*)W, M, r,
-                                                             acc);
+  // two CTAs per SM striding over the data: each CTA ends in 6 atomics on the same
+  // 6 accumulators, so their count, not the data, would otherwise set the time
+  k_velocity_dot<T><<<(int)std::min<long>((ctx.N * M + 255) / 256, 148L * 2), 256, 0, st>>>(
+      ctx.N, M, (const cplx<T>*)U, (const cplx<T>*)W, M, r, acc);
   INQB_CUDA_TRY(cudaGetLastError());
   const ProjTables& t = ctx.proj;
   const int nchunks = (int)t.chunk_atom.size();

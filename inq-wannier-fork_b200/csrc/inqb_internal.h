@@ -155,7 +155,7 @@ struct ProjView {
   double2* proj;          // [nproj][L][M] accumulators (FP64 in both precisions)
 };
 
-constexpr int kNlChunk = 128;  // sphere entries per chunk of the adjoint's nonlocal moments
+constexpr int kNlChunk = 64;  // sphere entries per chunk of the adjoint's nonlocal moments
 
 struct Plan;  // kernel launch plan for one (precision, grid) pair
 
