@@ -20,6 +20,8 @@
 #ifndef INQB200_H
 #define INQB200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -207,12 +209,16 @@ int inqb_accum_vector_potential_gradient(inqb_ctx* ctx, const void* u, const voi
 int inqb_crank_nicolson_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
                              const double kA_tdt_cov[3], int max_sweeps, double tol, int* sweeps, double* residual,
                              void* stream);
+/* Bytes of the powers buffer of one step of inqb_etrs_step_powers for M orbitals. */
+int inqb_etrs_powers_size(inqb_ctx* ctx, int M, size_t* bytes);
 /* One ETRS step (the reference's real_time::etrs step with a density-independent
  * H, src/real_time/etrs.hpp:22-82) that also keeps what its adjoint needs:
- * psi <- T(kA_tdt) T(kA_t) psi, T = sum_{k<=4} (i dt/2 H)^k / k!, and powers =
- * 8 contiguous [N][M] blocks (leading dimension M): H^k psi_t at kA_t, k = 0..3,
- * then H^k phi at kA_tdt, phi the half-stepped orbitals.  Unlike inqb_etrs_step it
- * sums the series term by term (no Horner), like the reference's exponential. */
+ * psi <- T(kA_tdt) T(kA_t) psi, T = sum_{k<=4} (i dt/2 H)^k / k!.  powers (16-byte
+ * aligned, inqb_etrs_powers_size bytes) receives 8 [N][M] blocks, H^k psi_t at kA_t
+ * (k = 0..3) then H^k phi at kA_tdt (phi the half-stepped orbitals), followed by
+ * their forward 3-D coefficients as the H kernels hold them (an opaque layout the
+ * adjoint step reads).  Unlike inqb_etrs_step it sums the series term by term (no
+ * Horner), like the reference's exponential. */
 int inqb_etrs_step_powers(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
                           const double kA_tdt_cov[3], void* powers, void* stream);
 /* Reverse of that step for a real objective (the reference has no adjoint):

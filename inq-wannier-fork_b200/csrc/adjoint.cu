@@ -14,6 +14,7 @@
 #include "adjoint.h"
 #include "dft.cuh"
 #include "inqb_internal.h"
+#include "plan.h"
 
 namespace inqb {
 
@@ -136,6 +137,66 @@ __global__ void k_velocity_dot(long N, int M, const cplx<T>* __restrict__ U, con
       if (4 * (i0 * i0 * a0 * a0 + i1 * i1 * a1 * a1 + i2 * i2 * a2 * a2) > tot * tot) gf = 0.0;
     }
     const cplx<T> a = U[p * ld + m], b = W[p * ld + m];
+    const double re = (double)a.x * b.x + (double)a.y * b.y;
+    const double im = (double)a.x * b.y - (double)a.y * b.x;
+    for (int d = 0; d < 3; d++) {
+      const double v = gf * (n[0] * r.b[0][d] + n[1] * r.b[1][d] + n[2] * r.b[2][d]) + r.kA[d];
+      s[2 * d] += v * re;
+      s[2 * d + 1] += v * im;
+    }
+  }
+  __shared__ double red[6][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = 0; q < 6; q++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
+    if (lane == 0) red[q][warp] = s[q];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    for (int q = 0; q < 6; q++) {
+      double v = lane < (int)(blockDim.x >> 5) ? red[q][lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) atomicAdd(&acc[q], v);
+    }
+  }
+}
+
+// The same reduction on coefficients in the tile layout [g][ka][kz][kx][kb][G] that
+// the H passes emit (ky = ka + Y2 kb); padded orbitals (m >= M) are skipped.
+struct TileFourier {
+  int G, Y1, Y2;
+};
+
+template <typename T>
+__global__ void k_velocity_dot_tiles(long nelem, int M, const cplx<T>* __restrict__ U, const cplx<T>* __restrict__ W,
+                                     TileFourier tf, Recip r, double* __restrict__ acc) {
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += (long)gridDim.x * blockDim.x) {
+    long t = e / tf.G;
+    const int j = (int)(e - t * tf.G);
+    const int kb = (int)(t % tf.Y1);
+    t /= tf.Y1;
+    const int kx = (int)(t % r.nr[0]);
+    t /= r.nr[0];
+    const int kz = (int)(t % r.nr[2]);
+    t /= r.nr[2];
+    const int ka = (int)(t % tf.Y2);
+    const long g = t / tf.Y2;
+    if (g * tf.G + j >= M) continue;
+    const int k[3] = {kx, ka + tf.Y2 * kb, kz};
+    double n[3];
+    for (int c = 0; c < 3; c++) n[c] = (k[c] >= (r.nr[c] + 1) / 2) ? k[c] - r.nr[c] : k[c];
+    double gf = 1.0;
+    if (r.mask) {
+      const long long a0 = (long long)r.nr[1] * r.nr[2], a1 = (long long)r.nr[0] * r.nr[2],
+                      a2 = (long long)r.nr[0] * r.nr[1];
+      const long long tot = (long long)r.nr[0] * r.nr[1] * r.nr[2];
+      const long long i0 = (long long)n[0], i1 = (long long)n[1], i2 = (long long)n[2];
+      if (4 * (i0 * i0 * a0 * a0 + i1 * i1 * a1 * a1 + i2 * i2 * a2 * a2) > tot * tot) gf = 0.0;
+    }
+    const cplx<T> a = U[e], b = W[e];
     const double re = (double)a.x * b.x + (double)a.y * b.y;
     const double im = (double)a.x * b.y - (double)a.y * b.x;
     for (int d = 0; d < 3; d++) {
@@ -350,7 +411,7 @@ int launch_vgrad(int precision, long N, int M, const void* u, const void* w, lon
 
 template <typename T>
 static int agrad_impl(const inqb_ctx& ctx, const void* U, const void* W, const void* u, const void* w, long ld, int M,
-                      double* acc, double cre, double cim, double* gA, cudaStream_t st) {
+                      double* acc, double cre, double cim, double* gA, cudaStream_t st, bool tiles) {
   Recip r;
   for (int i = 0; i < 3; i++) {
     r.nr[i] = ctx.nr[i];
@@ -361,8 +422,15 @@ static int agrad_impl(const inqb_ctx& ctx, const void* U, const void* W, const v
   INQB_CUDA_TRY(cudaMemsetAsync(acc, 0, 12 * sizeof(double), st));
   // two CTAs per SM striding over the data: each CTA ends in 6 atomics on the same
   // 6 accumulators, so their count, not the data, would otherwise set the time
-  k_velocity_dot<T><<<(int)std::min<long>((ctx.N * M + 255) / 256, 148L * 2), 256, 0, st>>>(
-      ctx.N, M, (const cplx<T>*)U, (const cplx<T>*)W, M, r, acc);
+  if (tiles) {
+    const int G = ctx.plan->G_tile;
+    const long nelem = (long)((M + G - 1) / G) * G * ctx.N;
+    k_velocity_dot_tiles<T><<<(int)std::min<long>((nelem + 255) / 256, 148L * 2), 256, 0, st>>>(
+        nelem, M, (const cplx<T>*)U, (const cplx<T>*)W, TileFourier{G, ctx.plan->y1, ctx.plan->y2}, r, acc);
+  } else {
+    k_velocity_dot<T><<<(int)std::min<long>((ctx.N * M + 255) / 256, 148L * 2), 256, 0, st>>>(
+        ctx.N, M, (const cplx<T>*)U, (const cplx<T>*)W, M, r, acc);
+  }
   INQB_CUDA_TRY(cudaGetLastError());
   const ProjTables& t = ctx.proj;
   const int nchunks = (int)t.chunk_atom.size();
@@ -384,10 +452,10 @@ static int agrad_impl(const inqb_ctx& ctx, const void* U, const void* W, const v
 }
 
 int launch_agrad(const inqb_ctx& ctx, const void* U, const void* W, const void* u, const void* w, long ld, int M,
-                 double* acc, double cre, double cim, double* gA, void* stream) {
+                 double* acc, double cre, double cim, double* gA, void* stream, bool tiles) {
   return ctx.precision == INQB_FP64
-             ? agrad_impl<double>(ctx, U, W, u, w, ld, M, acc, cre, cim, gA, (cudaStream_t)stream)
-             : agrad_impl<float>(ctx, U, W, u, w, ld, M, acc, cre, cim, gA, (cudaStream_t)stream);
+             ? agrad_impl<double>(ctx, U, W, u, w, ld, M, acc, cre, cim, gA, (cudaStream_t)stream, tiles)
+             : agrad_impl<float>(ctx, U, W, u, w, ld, M, acc, cre, cim, gA, (cudaStream_t)stream, tiles);
 }
 
 }  // namespace inqb

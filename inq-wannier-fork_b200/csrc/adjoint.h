@@ -14,7 +14,9 @@ int launch_position_scale(int precision, const inqb_ctx& ctx, const void* psi, l
                           int dir, const double* occ, double s, void* stream);
 int launch_vgrad(int precision, long N, int M, const void* u, const void* w, long ld, double cre, double cim,
                  double* gV, void* stream);
+// gA += Re(c <u| dH/dA |w>) from the forward coefficients U, W of u, w: natural order
+// [N][M] (tiles = false) or the tile layout the H passes emit (tiles = true)
 int launch_agrad(const inqb_ctx& ctx, const void* U, const void* W, const void* u, const void* w, long ld, int M,
-                 double* acc, double cre, double cim, double* gA, void* stream);
+                 double* acc, double cre, double cim, double* gA, void* stream, bool tiles = false);
 
 }  // namespace inqb

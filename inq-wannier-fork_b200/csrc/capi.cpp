@@ -115,7 +115,7 @@ int set_kA(inqb_ctx* ctx, const double kA[3], void* stream) {
 
 // One H application: out = alpha * H in + beta * base.
 int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long ld_out, int M, const void* base,
-          long ld_base, const double alpha[2], const double beta[2], void* stream) {
+          long ld_base, const double alpha[2], const double beta[2], void* stream, void* fourier_out = nullptr) {
   INQB_TRY(reserve(ctx, M));
   if (!ctx->proj_phases_valid) {
     INQB_TRY(update_phases(ctx, stream));
@@ -138,6 +138,7 @@ int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long l
   a.beta[0] = beta[0];
   a.beta[1] = beta[1];
   a.stream = stream;
+  a.fourier_out = fourier_out;
   a.fourier_mask = ctx->fourier_mask;
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) a.rlat[i][j] = ctx->cell.rlat[i][j];
@@ -820,10 +821,18 @@ void taylor_coeffs(double dt, double c[5][2]) {
   }
 }
 
+// Elements of one block of forward coefficients in the tile layout (orbital groups
+// padded to the tile's G).
+size_t fourier_elems(const inqb_ctx* ctx, int M) {
+  const size_t G = (size_t)ctx->plan->G_tile;
+  return (M + G - 1) / G * G * (size_t)ctx->N;
+}
+
 // One half step psi -> sum_k c_k H^k psi at the current k + A, keeping
-// P[0..3] = H^k psi (P[0] a copy of the input); `out` receives the result.
-int half_step_powers(inqb_ctx* ctx, const void* in, long ld_in, void* const P[4], void* out, long ld_out, int M,
-                     const double c[5][2], void* stream) {
+// P[0..3] = H^k psi (P[0] a copy of the input) and F[0..3] = their forward
+// coefficients (tile layout, written by the H applications); `out` receives the result.
+int half_step_powers(inqb_ctx* ctx, const void* in, long ld_in, void* const P[4], void* const F[4], void* out,
+                     long ld_out, int M, const double c[5][2], void* stream) {
   const long Mi = M;
   const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
   void* H4 = ctx->d_adjL.ptr;
@@ -834,8 +843,8 @@ int half_step_powers(inqb_ctx* ctx, const void* in, long ld_in, void* const P[4]
     INQB_TRY(launch_lincomb(ctx->precision, ctx->N, M, 1, a, x, ldx, P[0], Mi, stream));
   }
   for (int k = 1; k < 4; k++)
-    INQB_TRY(apply(ctx, LaunchArgs::H, P[k - 1], Mi, P[k], Mi, M, nullptr, 0, one, zero, stream));
-  INQB_TRY(apply(ctx, LaunchArgs::H, P[3], Mi, H4, Mi, M, nullptr, 0, one, zero, stream));
+    INQB_TRY(apply(ctx, LaunchArgs::H, P[k - 1], Mi, P[k], Mi, M, nullptr, 0, one, zero, stream, F[k - 1]));
+  INQB_TRY(apply(ctx, LaunchArgs::H, P[3], Mi, H4, Mi, M, nullptr, 0, one, zero, stream, F[3]));
   const void* x[5] = {P[0], P[1], P[2], P[3], H4};
   const long ldx[5] = {Mi, Mi, Mi, Mi, Mi};
   return launch_lincomb(ctx->precision, ctx->N, M, 5, c, x, ldx, out, ld_out, stream);
@@ -844,17 +853,26 @@ int half_step_powers(inqb_ctx* ctx, const void* in, long ld_in, void* const P[4]
 // Reverse of one half step at the current k + A: with Lambda_j = H^j lam,
 //   Xi_i = sum_j conj(c_{i+j+1}) Lambda_j,   gV += 2 Re conj(Xi_i) Phi_i,
 //   gA += 2 Re <Xi_i| dH/dA |Phi_i>,          lam <- sum_k conj(c_k) Lambda_k.
-int half_back(inqb_ctx* ctx, void* lam, long ld, int M, const double c[5][2], const void* const Phi[4], double* gV,
-              double* gA, void* stream) {
+// The kinetic part of dH/dA reads forward coefficients: those of Phi_i were kept by
+// the forward step (FPhi), those of Xi_i are the same combination of the Lambda_j's,
+// which the H applications below emit.
+int half_back(inqb_ctx* ctx, void* lam, long ld, int M, const double c[5][2], const void* const Phi[4],
+              const void* const FPhi[4], double* gV, double* gA, void* stream) {
   const long Mi = M;
   const size_t blk = (size_t)ctx->N * M * ctx->elem_bytes();
+  const size_t nF = fourier_elems(ctx, M);
+  const size_t fblk = nF * ctx->elem_bytes();
   char* w = static_cast<char*>(ctx->d_adjL.ptr);
   void* Lam[5] = {lam, w + blk, w + 2 * blk, w + 3 * blk, w + 4 * blk};
   void* Xi = w + 5 * blk;
+  char* wf = w + 6 * blk;
+  void* FL[4] = {wf, wf + fblk, wf + 2 * fblk, wf + 3 * fblk};
+  void* FXi = wf + 4 * fblk;
   const long ldL[5] = {ld, Mi, Mi, Mi, Mi};
   const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
   for (int j = 1; j <= 4; j++)
-    INQB_TRY(apply(ctx, LaunchArgs::H, Lam[j - 1], ldL[j - 1], Lam[j], Mi, M, nullptr, 0, one, zero, stream));
+    INQB_TRY(apply(ctx, LaunchArgs::H, Lam[j - 1], ldL[j - 1], Lam[j], Mi, M, nullptr, 0, one, zero, stream,
+                   FL[j - 1]));
   double cc[5][2];
   for (int k = 0; k < 5; k++) {
     cc[k][0] = c[k][0];
@@ -864,29 +882,35 @@ int half_back(inqb_ctx* ctx, void* lam, long ld, int M, const double c[5][2], co
     const int K = 4 - i;
     double a[4][2];
     const void* x[4];
-    long ldx[4];
+    const void* xf[4];
+    long ldx[4], ldf[4];
     for (int j = 0; j < K; j++) {
       a[j][0] = cc[i + j + 1][0];
       a[j][1] = cc[i + j + 1][1];
       x[j] = Lam[j];
       ldx[j] = ldL[j];
+      xf[j] = FL[j];
+      ldf[j] = 1;
     }
     INQB_TRY(launch_lincomb(ctx->precision, ctx->N, M, K, a, x, ldx, Xi, Mi, stream));
+    INQB_TRY(launch_lincomb(ctx->precision, (long)nF, 1, K, a, xf, ldf, FXi, 1, stream));
     INQB_TRY(launch_vgrad(ctx->precision, ctx->N, M, Xi, Phi[i], Mi, 2.0, 0.0, gV, stream));
-    INQB_TRY(apply(ctx, LaunchArgs::FFT_FWD, Xi, Mi, ctx->d_adjU.ptr, Mi, M, nullptr, 0, one, zero, stream));
-    INQB_TRY(apply(ctx, LaunchArgs::FFT_FWD, Phi[i], Mi, ctx->d_adjW.ptr, Mi, M, nullptr, 0, one, zero, stream));
-    INQB_TRY(launch_agrad(*ctx, ctx->d_adjU.ptr, ctx->d_adjW.ptr, Xi, Phi[i], Mi, M, ctx->d_red.as<double>(), 2.0,
-                          0.0, gA, stream));
+    INQB_TRY(launch_agrad(*ctx, FXi, FPhi[i], Xi, Phi[i], Mi, M, ctx->d_red.as<double>(), 2.0, 0.0, gA, stream,
+                          true));
   }
   const void* x[5] = {Lam[0], Lam[1], Lam[2], Lam[3], Lam[4]};
   return launch_lincomb(ctx->precision, ctx->N, M, 5, cc, x, ldL, lam, ld, stream);
 }
 
+// Bytes of one step's powers: 8 orbital blocks [N][M] then 8 coefficient blocks.
+size_t powers_bytes(const inqb_ctx* ctx, int M) {
+  return 8 * ((size_t)ctx->N * M + fourier_elems(ctx, M)) * ctx->elem_bytes();
+}
+
 int adjoint_workspace(inqb_ctx* ctx, int M) {
   const size_t blk = (size_t)ctx->N * M * ctx->elem_bytes();
-  INQB_TRY(ctx->d_adjL.ensure(6 * blk));
-  INQB_TRY(ctx->d_adjU.ensure(blk));
-  INQB_TRY(ctx->d_adjW.ensure(blk));
+  const size_t fblk = fourier_elems(ctx, M) * ctx->elem_bytes();
+  INQB_TRY(ctx->d_adjL.ensure(6 * blk + 5 * fblk));
   INQB_TRY(ctx->d_red.ensure(256));
   INQB_TRY(ctx->d_nlpart.ensure(std::max<size_t>(
       (size_t)ctx->proj.chunk_atom.size() * ctx->proj.L * 16 * M * sizeof(double), 16)));
@@ -896,25 +920,36 @@ int adjoint_workspace(inqb_ctx* ctx, int M) {
 }  // namespace
 }  // namespace inqb
 
+int inqb_etrs_powers_size(inqb_ctx* ctx, int M, size_t* bytes) {
+  INQB_CHECK_CTX(ctx);
+  if (M <= 0 || !bytes) return fail(INQB_ERR_INVALID, "M must be positive and bytes not null");
+  *bytes = powers_bytes(ctx, M);
+  return INQB_OK;
+}
+
 int inqb_etrs_step_powers(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
                           const double kA_tdt_cov[3], void* powers, void* stream) {
   INQB_CHECK_CTX(ctx);
   INQB_TRY(check_block(ctx, psi, M, ld));
-  INQB_TRY(check_block(ctx, powers, M, M));
+  if (!powers || (uintptr_t)powers % 16 != 0) return fail(INQB_ERR_INVALID, "powers must be 16-byte aligned");
   if (!kA_t_cov || !kA_tdt_cov || !std::isfinite(dt)) return fail(INQB_ERR_INVALID, "bad step arguments");
   INQB_GUARD(ctx);
   INQB_TRY(adjoint_workspace(ctx, M));
   double c[5][2];
   taylor_coeffs(dt, c);
   const size_t blk = (size_t)ctx->N * M * ctx->elem_bytes();
+  const size_t fblk = fourier_elems(ctx, M) * ctx->elem_bytes();
   char* P = static_cast<char*>(powers);
+  char* F = P + 8 * blk;
   void* P1[4] = {P, P + blk, P + 2 * blk, P + 3 * blk};
   void* P2[4] = {P + 4 * blk, P + 5 * blk, P + 6 * blk, P + 7 * blk};
+  void* F1[4] = {F, F + fblk, F + 2 * fblk, F + 3 * fblk};
+  void* F2[4] = {F + 4 * fblk, F + 5 * fblk, F + 6 * fblk, F + 7 * fblk};
   INQB_TRY(set_kA(ctx, kA_t_cov, stream));
   // phi = the first half step, written straight into P2[0]
-  INQB_TRY(half_step_powers(ctx, psi, ld, P1, P2[0], M, M, c, stream));
+  INQB_TRY(half_step_powers(ctx, psi, ld, P1, F1, P2[0], M, M, c, stream));
   INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
-  return half_step_powers(ctx, P2[0], M, P2, psi, ld, M, c, stream);
+  return half_step_powers(ctx, P2[0], M, P2, F2, psi, ld, M, c, stream);
 }
 
 int inqb_etrs_adjoint_step(inqb_ctx* ctx, void* lambda, int M, int ld, double dt, const double kA_t_cov[3],
@@ -922,7 +957,7 @@ int inqb_etrs_adjoint_step(inqb_ctx* ctx, void* lambda, int M, int ld, double dt
                            double* gA_tdt, void* stream) {
   INQB_CHECK_CTX(ctx);
   INQB_TRY(check_block(ctx, lambda, M, ld));
-  INQB_TRY(check_block(ctx, powers, M, M));
+  if (!powers || (uintptr_t)powers % 16 != 0) return fail(INQB_ERR_INVALID, "powers must be 16-byte aligned");
   if (!kA_t_cov || !kA_tdt_cov || !std::isfinite(dt)) return fail(INQB_ERR_INVALID, "bad step arguments");
   if (!gV || !gA_t || !gA_tdt) return fail(INQB_ERR_INVALID, "null gradient");
   INQB_GUARD(ctx);
@@ -930,13 +965,17 @@ int inqb_etrs_adjoint_step(inqb_ctx* ctx, void* lambda, int M, int ld, double dt
   double c[5][2];
   taylor_coeffs(dt, c);
   const size_t blk = (size_t)ctx->N * M * ctx->elem_bytes();
+  const size_t fblk = fourier_elems(ctx, M) * ctx->elem_bytes();
   const char* P = static_cast<const char*>(powers);
+  const char* F = P + 8 * blk;
   const void* P1[4] = {P, P + blk, P + 2 * blk, P + 3 * blk};
   const void* P2[4] = {P + 4 * blk, P + 5 * blk, P + 6 * blk, P + 7 * blk};
+  const void* F1[4] = {F, F + fblk, F + 2 * fblk, F + 3 * fblk};
+  const void* F2[4] = {F + 4 * fblk, F + 5 * fblk, F + 6 * fblk, F + 7 * fblk};
   INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
-  INQB_TRY(half_back(ctx, lambda, ld, M, c, P2, gV, gA_tdt, stream));
+  INQB_TRY(half_back(ctx, lambda, ld, M, c, P2, F2, gV, gA_tdt, stream));
   INQB_TRY(set_kA(ctx, kA_t_cov, stream));
-  return half_back(ctx, lambda, ld, M, c, P1, gV, gA_t, stream);
+  return half_back(ctx, lambda, ld, M, c, P1, F1, gV, gA_t, stream);
 }
 
 int inqb_set_schedule(inqb_ctx* ctx, int M, const int schedule[4]) {

@@ -168,7 +168,7 @@ static int launch_h_impl(const LaunchArgs& a) {
     k_tile_fwd<T, NX, NY, NZ><<<gfwd, thr[0], TG::smem_fwd(acc_cap, rec_cap), st>>>(
         (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pj, acc_cap, rec_cap, ysplit, vin);
     if (a.events[1]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[1], st));
-    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp);
+    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out);
     if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
     EpiParams<T> ep;
     ep.V = (const T*)a.V;
@@ -234,6 +234,7 @@ static Plan make_plan() {
   p.G = TileGeom<T, NX, NY, NZ>::G;
   p.G_tile = TileGeom<T, NX, NY, NZ>::G;
   p.y1 = TileGeom<T, NX, NY, NZ>::Y1;
+  p.y2 = TileGeom<T, NX, NY, NZ>::Y2;
   p.ysplit = TileGeom<T, NX, NY, NZ>::YSPLIT;
   p.launch = &launch_h_impl<T, NX, NY, NZ>;
   return p;

@@ -28,6 +28,9 @@ struct LaunchArgs {
   // pass (a divisor of the y split's Y1), and threads per CTA of the three passes
   int ysplit = 0;
   int threads[3] = {0, 0, 0};
+  // optional, H mode: forward 3-D coefficients of `in` (before the kinetic factor) in
+  // the tile layout [g][ka][kz][kx][kb][G] (groups padded to G orbitals)
+  void* fourier_out = nullptr;
 };
 
 // Candidate values the autotuner tries.
@@ -37,6 +40,7 @@ struct Plan {
   int G = 1;       // orbitals per tile of the plain FFT kernels
   int G_tile = 1;  // orbitals per tile of the H kernels
   int y1 = 1;      // tiles per x-plane (the divisors of y1 are the first pass's splits)
+  int y2 = 1;      // rows per tile (the y split is NY = y2 * y1)
   int ysplit = 1;  // default split
   int (*launch)(const LaunchArgs&) = nullptr;
 };

@@ -278,7 +278,8 @@ __global__ void __launch_bounds__(256)
 // index goes to padded slots of stride XS and (y1, j) stays contiguous.
 template <typename T, int NX, int NY, int NZ>
 __global__ void __launch_bounds__(256)
-    k_tile_x(cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ tw_x, KinParams<T> kp) {
+    k_tile_x(cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ tw_x, KinParams<T> kp,
+             cplx<T>* __restrict__ fout) {
   using TG = TileGeom<T, NX, NY, NZ>;
   using AX = typename TG::AX;
   constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, XS = TG::XS;
@@ -350,8 +351,12 @@ __global__ void __launch_bounds__(256)
   const int n2 = sym_freq(kz, NZ);
   step1<AX, false>(X, Y1 * G * AX::N2, twx, map1);
   __syncthreads();
+  // fout (optional): the forward coefficients of this block, before the kinetic
+  // factor, as [kx][kb][G] (the adjoint's velocity terms read them)
+  cplx<T>* fblk = fout ? fout + ((long)(grp * Y2 + ka) * NZ + kz) * TG::BLK : nullptr;
   step2_fwd_op_inv<AX>(X, Y1 * G * AX::N1, twx, map2, [&](int it, int kx, cplx<T> v) {
     const int kb = (it / G) / AX::N1;
+    if (fblk) fblk[(kx * Y1 + kb) * G + it % G] = v;
     const int n0 = sym_freq(kx, NX);
     const T f0 = (T)n0;
     T k = fma(fma(kinA, f0, kinB[kb]), f0, kinC[kb]);

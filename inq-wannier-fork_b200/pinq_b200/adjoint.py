@@ -36,7 +36,8 @@ class DipolePropagation:
                  store_powers: bool = False):
         """every: checkpoint interval of the recomputing backward.  store_powers:
         keep the Taylor powers of every step during the forward pass instead (8
-        orbital blocks per step; no recompute in the backward)."""
+        orbital blocks and their Fourier coefficients per step; no recompute in the
+        backward)."""
         self.h = ham
         self.psi0 = psi0
         self.M = psi0.shape[1]
@@ -64,7 +65,7 @@ class DipolePropagation:
         cps = {}
         self.powers = None
         if keep and self.store_powers:
-            powers = torch.empty((len(amps), 8, self.h.N, self.M), dtype=psi.dtype, device=psi.device)
+            powers = self.h.powers_buffer(len(amps), self.M)
             for n in range(len(amps)):
                 self.h.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)),
                                          self._kA(self._amp(amps, n + 1)), powers[n])
@@ -103,7 +104,7 @@ class DipolePropagation:
                                      self.powers[n], gV, gA[n], gA[n2])
             return gA[:, self.direction].clone(), gV
         seg = min(self.every, nsteps)
-        store = torch.empty((seg, 8, h.N, self.M), dtype=self.psi0.dtype, device=dev)
+        store = h.powers_buffer(seg, self.M)
         for s0 in reversed(range(0, nsteps, self.every)):
             s1 = min(s0 + self.every, nsteps)
             psi = self.checkpoints[s0].clone()

@@ -246,8 +246,9 @@ class KSHamiltonian:
         return k.value, r.value
 
     def etrs_step_powers_(self, psi, dt, kA_t_cov, kA_tdt_cov, powers):
-        """One ETRS step in place that also writes the 8 Taylor-power blocks the
-        adjoint step reads into `powers` ([8, N, M], contiguous)."""
+        """One ETRS step in place that also writes what the adjoint step reads (the
+        Taylor powers and their forward coefficients) into `powers`, one row of
+        powers_buffer(nsteps, M)."""
         psi = self._check(psi)
         self._check_powers(powers, psi.shape[1])
         a = np.ascontiguousarray(kA_t_cov, np.float64).reshape(3)
@@ -270,10 +271,22 @@ class KSHamiltonian:
              dptr(b), powers.data_ptr(), gV.data_ptr(), gA_t.data_ptr(), gA_tdt.data_ptr(), self._stream())
         return lam
 
+    def powers_buffer(self, nsteps: int, M: int) -> torch.Tensor:
+        """Storage for nsteps steps of etrs_step_powers_ ([nsteps, per-step elements];
+        pass row n to the step and to its adjoint)."""
+        nbytes = ctypes.c_size_t(0)
+        call("inqb_etrs_powers_size", self._h, int(M), ctypes.byref(nbytes))
+        esz = 16 if self.dtype == torch.complex128 else 8
+        return torch.empty((int(nsteps), nbytes.value // esz), dtype=self.dtype, device=self.device)
+
     def _check_powers(self, powers, M):
+        nbytes = ctypes.c_size_t(0)
+        call("inqb_etrs_powers_size", self._h, int(M), ctypes.byref(nbytes))
+        esz = 16 if self.dtype == torch.complex128 else 8
         if (not torch.is_tensor(powers) or powers.device.type != "cuda" or powers.dtype != self.dtype
-                or tuple(powers.shape) != (8, self.N, M) or not powers.is_contiguous()):
-            raise ValueError(f"powers must be a contiguous [8, {self.N}, {M}] {self.dtype} CUDA tensor")
+                or powers.numel() * esz != nbytes.value or not powers.is_contiguous()
+                or powers.data_ptr() % 16 != 0):
+            raise ValueError("powers must be one row of powers_buffer(nsteps, M)")
 
     def density(self, psi, occ) -> torch.Tensor:
         psi = self._check(psi)

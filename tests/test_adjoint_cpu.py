@@ -61,6 +61,9 @@ class DenseHam:
         psi.copy_(self._T(float(kA2[0]), dt, self._T(float(kA1[0]), dt, psi)))
         return psi
 
+    def powers_buffer(self, nsteps, M):
+        return torch.empty((nsteps, 8, self.N, M), dtype=torch.complex128)
+
     @staticmethod
     def _c(dt):
         c = [1.0 + 0j]
