@@ -169,6 +169,19 @@ struct TileFourier {
   int G, Y1, Y2;
 };
 
+// Eight orbital blocks of a backward half step, Lambda_0..3 and Phi_0..3 (or their
+// forward coefficients), and the weights of Xi_i = sum_j w[i][j] Lambda_j.
+template <typename T>
+struct EightBlocks {
+  const cplx<T>* L[4];
+  const cplx<T>* P[4];
+  long ldL[4];
+  long ldP;
+};
+struct PairWeights {
+  double w[4][4][2];  // w[i][j] = conj(c_{i+j+1}) for i + j <= 3
+};
+
 template <typename T>
 __global__ void k_velocity_dot_tiles(long nelem, int M, const cplx<T>* __restrict__ U, const cplx<T>* __restrict__ W,
                                      TileFourier tf, Recip r, double* __restrict__ acc) {
@@ -273,6 +286,54 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// The moments of the four pairs (Lambda_j, Phi_j), pair j = blockIdx.z, into
+// part[chunk][pair][l][q][M] (the same sums as k_nl_moments).
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_nl_moments_pairs(int L, int M, EightBlocks<T> b, const int* __restrict__ chunk_atom,
+                       const int* __restrict__ chunk_beg, const int* __restrict__ atom_ptr,
+                       const AdjRec<T>* __restrict__ adj, double* __restrict__ part) {
+  constexpr int LM = 4, Q = 16;
+  __shared__ double red[LM][32][Q + 1];
+  const int c = blockIdx.x, pr = blockIdx.z;
+  const int m = blockIdx.y * 32 + (threadIdx.x & 31);
+  const int l = (threadIdx.x >> 5) & (LM - 1), es = threadIdx.x >> 7;
+  const int a = chunk_atom[c];
+  const int i0 = chunk_beg[c], i1 = min(i0 + kNlChunk, atom_ptr[a + 1]);
+  const cplx<T>* u = b.L[pr];
+  const cplx<T>* w = b.P[pr];
+  const long ldu = b.ldL[pr], ldw = b.ldP;
+  double s[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) s[q] = 0.0;
+  if (m < M && l < L) {
+#pragma unroll 2
+    for (int i = i0 + es; i < i1; i += 2) {
+      const AdjRec<T> r = adj[i];
+      const cplx<T> uu = u[(long)r.pt * ldu + m], ww = w[(long)r.pt * ldw + m];
+      const double bb = (double)r.beta[l];
+      const double phr = (double)r.ph[0], phi = (double)r.ph[1];
+      const double ur = bb * (phr * uu.x - phi * uu.y), ui = bb * (phr * uu.y + phi * uu.x);
+      const double wr = bb * (phr * ww.x - phi * ww.y), wi = bb * (phr * ww.y + phi * ww.x);
+      const double x0 = r.xyz[0], x1 = r.xyz[1], x2 = r.xyz[2];
+      s[0] += ur; s[1] += ui;
+      s[2] += x0 * ur; s[3] += x0 * ui; s[4] += x1 * ur; s[5] += x1 * ui; s[6] += x2 * ur; s[7] += x2 * ui;
+      s[8] += wr; s[9] += wi;
+      s[10] += x0 * wr; s[11] += x0 * wi; s[12] += x1 * wr; s[13] += x1 * wi; s[14] += x2 * wr; s[15] += x2 * wi;
+    }
+  }
+  if (es == 1) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) red[l][threadIdx.x & 31][q] = s[q];
+  }
+  __syncthreads();
+  if (es == 0 && m < M && l < L) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+      part[((((long)c * 4 + pr) * L + l) * Q + q) * M + m] = s[q] + red[l][threadIdx.x & 31][q];
+  }
+}
+
 // Step 2: block (atom a, projector l, 32 orbitals); thread (q, m) sums moment q of
 // orbital m over the atom's chunks, then the orbital's threads add
 // S_l i [conj(p_u) r_w,d - conj(r_u,d) p_w] into acc[6 + 2d .. 6 + 2d + 1].
@@ -327,6 +388,187 @@ __global__ void __launch_bounds__(512)
   }
 }
 
+// ---------------------------------------------------------------- the gradient of one half step
+// With Xi_i = sum_j w[i][j] Lambda_j (w[i][j] = conj(c_{i+j+1}), zero for i + j > 3),
+// the half step's gradient terms are sums over i of bilinear forms in (Xi_i, Phi_i);
+// these kernels read the eight blocks Lambda_0..3, Phi_0..3 once and weight them.
+
+
+// gV[p] += 2 Re sum_m sum_i conj(Xi_i) Phi_i, one warp per grid point.
+template <typename T>
+__global__ void k_vgrad8(long N, int M, EightBlocks<T> b, PairWeights pw, double* __restrict__ gV) {
+  const int lane = threadIdx.x & 31;
+  const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+  for (long p = warp; p < N; p += nwarps) {
+    double re = 0.0;
+    for (int m = lane; m < M; m += 32) {
+      double lr[4], li[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const cplx<T> v = b.L[j][p * b.ldL[j] + m];
+        lr[j] = v.x;
+        li[j] = v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        double xr = 0.0, xi = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4 - i; ++j) {
+          xr += pw.w[i][j][0] * lr[j] - pw.w[i][j][1] * li[j];
+          xi += pw.w[i][j][0] * li[j] + pw.w[i][j][1] * lr[j];
+        }
+        const cplx<T> f = b.P[i][p * b.ldP + m];
+        re += xr * (double)f.x + xi * (double)f.y;  // Re conj(Xi) Phi
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) re += __shfl_xor_sync(0xffffffffu, re, o);
+    if (lane == 0) gV[p] += 2.0 * re;
+  }
+}
+
+// acc[2d..2d+1] += sum_{G,m} sum_i conj(Xi_i(G)) (G + kA)_d Phi_i(G) on the tile-layout
+// coefficients (b.L / b.P point at coefficient blocks, ld unused).
+template <typename T>
+__global__ void k_velocity_dot8(long nelem, int M, EightBlocks<T> b, PairWeights pw, TileFourier tf, Recip r,
+                                double* __restrict__ acc) {
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += (long)gridDim.x * blockDim.x) {
+    long t = e / tf.G;
+    const int j0 = (int)(e - t * tf.G);
+    const int kb = (int)(t % tf.Y1);
+    t /= tf.Y1;
+    const int kx = (int)(t % r.nr[0]);
+    t /= r.nr[0];
+    const int kz = (int)(t % r.nr[2]);
+    t /= r.nr[2];
+    const int ka = (int)(t % tf.Y2);
+    const long g = t / tf.Y2;
+    if (g * tf.G + j0 >= M) continue;
+    const int k[3] = {kx, ka + tf.Y2 * kb, kz};
+    double n[3];
+    for (int c = 0; c < 3; c++) n[c] = (k[c] >= (r.nr[c] + 1) / 2) ? k[c] - r.nr[c] : k[c];
+    double gf = 1.0;
+    if (r.mask) {
+      const long long a0 = (long long)r.nr[1] * r.nr[2], a1 = (long long)r.nr[0] * r.nr[2],
+                      a2 = (long long)r.nr[0] * r.nr[1];
+      const long long tot = (long long)r.nr[0] * r.nr[1] * r.nr[2];
+      const long long i0 = (long long)n[0], i1 = (long long)n[1], i2 = (long long)n[2];
+      if (4 * (i0 * i0 * a0 * a0 + i1 * i1 * a1 * a1 + i2 * i2 * a2 * a2) > tot * tot) gf = 0.0;
+    }
+    double lr[4], li[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const cplx<T> v = b.L[j][e];
+      lr[j] = v.x;
+      li[j] = v.y;
+    }
+    double re = 0.0, im = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      double xr = 0.0, xi = 0.0;
+#pragma unroll
+      for (int j = 0; j < 4 - i; ++j) {
+        xr += pw.w[i][j][0] * lr[j] - pw.w[i][j][1] * li[j];
+        xi += pw.w[i][j][0] * li[j] + pw.w[i][j][1] * lr[j];
+      }
+      const cplx<T> f = b.P[i][e];
+      re += xr * (double)f.x + xi * (double)f.y;
+      im += xr * (double)f.y - xi * (double)f.x;
+    }
+    for (int d = 0; d < 3; d++) {
+      const double v = gf * (n[0] * r.b[0][d] + n[1] * r.b[1][d] + n[2] * r.b[2][d]) + r.kA[d];
+      s[2 * d] += v * re;
+      s[2 * d + 1] += v * im;
+    }
+  }
+  __shared__ double red[6][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = 0; q < 6; q++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
+    if (lane == 0) red[q][warp] = s[q];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    for (int q = 0; q < 6; q++) {
+      double v = lane < (int)(blockDim.x >> 5) ? red[q][lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) atomicAdd(&acc[q], v);
+    }
+  }
+}
+
+// Nonlocal term over the pairs: block (atom, l, 32 orbitals), thread (q, m) sums
+// moment q of each pair (Lambda_j, Phi_j) over the atom's chunks
+// (part[chunk][pair][l][q][M], q < 8 of Lambda_j, q >= 8 of Phi_j); then per orbital
+// sum_i S_l i [conj(p_Xi_i) r_Phi_i - conj(r_Xi_i) p_Phi_i] with p_Xi_i = sum_j w p_Lambda_j.
+__global__ void __launch_bounds__(512)
+    k_nl_combine8(int L, int M, const int* __restrict__ atom_chunk_ptr, const double* __restrict__ part,
+                  const double* __restrict__ scale, PairWeights wb, double* __restrict__ acc) {
+  constexpr int Q = 16;
+  __shared__ double mom[4][Q][33];
+  const int a = blockIdx.x, l = blockIdx.y;
+  const int mi = threadIdx.x & 31, q = threadIdx.x >> 5;
+  const int m = blockIdx.z * 32 + mi;
+  const int c0 = atom_chunk_ptr[a], c1 = atom_chunk_ptr[a + 1];
+#pragma unroll
+  for (int pr = 0; pr < 4; ++pr) {
+    double v0 = 0.0, v1 = 0.0;
+    if (m < M) {
+      const long stride = 4L * L * Q * M;
+      const double* pp = part + (((long)c0 * 4 + pr) * L + l) * Q * M + (long)q * M + m;
+      int c = c0;
+      for (; c + 1 < c1; c += 2, pp += 2 * stride) {
+        v0 += pp[0];
+        v1 += pp[stride];
+      }
+      if (c < c1) v0 += pp[0];
+    }
+    mom[pr][q][mi] = v0 + v1;
+  }
+  __syncthreads();
+  if (q != 0) return;  // warp 0 goes on whole (lanes past M add zeros)
+  const double S = scale[a * L + l];
+  double out[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (m >= M) break;
+    // moments of Xi_i (u side, q 0..7) from those of the Lambda_j
+    double xu[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < 4 - i; ++j) {
+      const double wr = wb.w[i][j][0], wi = wb.w[i][j][1];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const double vr = mom[j][2 * k][mi], vi = mom[j][2 * k + 1][mi];
+        xu[2 * k] += wr * vr - wi * vi;
+        xu[2 * k + 1] += wr * vi + wi * vr;
+      }
+    }
+    const double pur = xu[0], pui = xu[1], pwr = mom[i][8][mi], pwi = mom[i][9][mi];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double rur = xu[2 + 2 * d], rui = xu[3 + 2 * d];
+      const double rwr = mom[i][10 + 2 * d][mi], rwi = mom[i][11 + 2 * d][mi];
+      const double z1r = pur * rwr + pui * rwi, z1i = pur * rwi - pui * rwr;
+      const double z2r = rur * pwr + rui * pwi, z2i = rur * pwi - rui * pwr;
+      out[2 * d] += -S * (z1i - z2i);
+      out[2 * d + 1] += S * (z1r - z2r);
+    }
+  }
+  // the q == 0 threads of this block are one full warp (threads 0..31)
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    double x = out[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (mi == 0) atomicAdd(&acc[6 + k], x);
+  }
+}
+
 // gA[d] += Re(c (kin[d] / N + nl[d]))
 __global__ void k_finish_dA(const double* __restrict__ acc, double invN, double cre, double cim,
                             double* __restrict__ gA) {
@@ -339,6 +581,71 @@ __global__ void k_finish_dA(const double* __restrict__ acc, double invN, double 
 }
 
 // ---------------------------------------------------------------- launchers
+template <typename T>
+static int half_grad_impl(const inqb_ctx& ctx, const void* const Lam[4], const long ldL[4], const void* const Phi[4],
+                          long ldP, const void* const FL[4], const void* const FP[4], const double w[4][4][2], int M,
+                          double* gV, double* gA, cudaStream_t st) {
+  PairWeights pw;
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++)
+      for (int c = 0; c < 2; c++) pw.w[i][j][c] = (i + j <= 3) ? w[i][j][c] : 0.0;
+  EightBlocks<T> b, fb;
+  for (int j = 0; j < 4; j++) {
+    b.L[j] = (const cplx<T>*)Lam[j];
+    b.ldL[j] = ldL[j];
+    b.P[j] = (const cplx<T>*)Phi[j];
+    fb.L[j] = (const cplx<T>*)FL[j];
+    fb.ldL[j] = 1;
+    fb.P[j] = (const cplx<T>*)FP[j];
+  }
+  b.ldP = ldP;
+  fb.ldP = 1;
+  // V gradient
+  const int vblocks = (int)std::min<long>((ctx.N * 32 + 255) / 256, 148L * 16);
+  k_vgrad8<T><<<vblocks, 256, 0, st>>>(ctx.N, M, b, pw, gV);
+  INQB_CUDA_TRY(cudaGetLastError());
+  // A gradient: kinetic velocity on the coefficients, nonlocal from the pair moments
+  double* acc = ctx.d_red.as<double>();
+  INQB_CUDA_TRY(cudaMemsetAsync(acc, 0, 12 * sizeof(double), st));
+  Recip r;
+  for (int i = 0; i < 3; i++) {
+    r.nr[i] = ctx.nr[i];
+    for (int j = 0; j < 3; j++) r.b[i][j] = ctx.cell.rlat[i][j];
+  }
+  ctx.cell.cov_to_cart(ctx.kA_cov, r.kA);
+  r.mask = ctx.fourier_mask;
+  const int G = ctx.plan->G_tile;
+  const long nelem = (long)((M + G - 1) / G) * G * ctx.N;
+  k_velocity_dot8<T><<<(int)std::min<long>((nelem + 255) / 256, 148L * 2), 256, 0, st>>>(
+      nelem, M, fb, pw, TileFourier{G, ctx.plan->y1, ctx.plan->y2}, r, acc);
+  INQB_CUDA_TRY(cudaGetLastError());
+  const ProjTables& t = ctx.proj;
+  const int nchunks = (int)t.chunk_atom.size();
+  if (t.nproj > 0 && nchunks > 0) {
+    if (ctx.d_nlpart.bytes < (size_t)nchunks * 4 * t.L * 16 * M * sizeof(double))
+      return fail(INQB_ERR_INVALID, "nonlocal moment workspace not reserved");
+    double* part = ctx.d_nlpart.as<double>();
+    k_nl_moments_pairs<T><<<dim3(nchunks, (M + 31) / 32, 4), 256, 0, st>>>(
+        t.L, M, b, t.d_chunk_atom.as<int>(), t.d_chunk_beg.as<int>(), t.d_atom_ptr.as<int>(),
+        t.d_adj_rec.as<AdjRec<T>>(), part);
+    INQB_CUDA_TRY(cudaGetLastError());
+    k_nl_combine8<<<dim3(t.nproj, t.L, (M + 31) / 32), 512, 0, st>>>(t.L, M, t.d_atom_chunk_ptr.as<int>(), part,
+                                                                   t.d_scale.as<double>(), pw, acc);
+    INQB_CUDA_TRY(cudaGetLastError());
+  }
+  k_finish_dA<<<1, 32, 0, st>>>(acc, 1.0 / (double)ctx.N, 2.0, 0.0, gA);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_half_grad(const inqb_ctx& ctx, const void* const Lam[4], const long ldL[4], const void* const Phi[4],
+                     long ldP, const void* const FL[4], const void* const FP[4], const double w[4][4][2], int M,
+                     double* gV, double* gA, void* stream) {
+  return ctx.precision == INQB_FP64
+             ? half_grad_impl<double>(ctx, Lam, ldL, Phi, ldP, FL, FP, w, M, gV, gA, (cudaStream_t)stream)
+             : half_grad_impl<float>(ctx, Lam, ldL, Phi, ldP, FL, FP, w, M, gV, gA, (cudaStream_t)stream);
+}
+
 static int grid_for(long n, int threads) { return (int)std::min<long>((n + threads - 1) / threads, 148L * 32); }
 
 template <typename T>

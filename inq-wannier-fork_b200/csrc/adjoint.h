@@ -19,4 +19,12 @@ int launch_vgrad(int precision, long N, int M, const void* u, const void* w, lon
 int launch_agrad(const inqb_ctx& ctx, const void* U, const void* W, const void* u, const void* w, long ld, int M,
                  double* acc, double cre, double cim, double* gA, void* stream, bool tiles = false);
 
+// The V and A gradient of one backward ETRS half step: Lam[0..3] (leading dimensions
+// ldL), Phi[0..3] (ldP), their forward coefficients FL, FP in the tile layout,
+// weights w[i][j] = conj(c_{i+j+1}) (i + j <= 3); with Xi_i = sum_j w[i][j] Lam_j,
+// gV += 2 Re sum_i conj(Xi_i) Phi_i and gA += 2 Re sum_i <Xi_i| dH/dA |Phi_i>.
+int launch_half_grad(const inqb_ctx& ctx, const void* const Lam[4], const long ldL[4], const void* const Phi[4],
+                     long ldP, const void* const FL[4], const void* const FP[4], const double w[4][4][2], int M,
+                     double* gV, double* gA, void* stream);
+
 }  // namespace inqb

@@ -864,10 +864,8 @@ int half_back(inqb_ctx* ctx, void* lam, long ld, int M, const double c[5][2], co
   const size_t fblk = nF * ctx->elem_bytes();
   char* w = static_cast<char*>(ctx->d_adjL.ptr);
   void* Lam[5] = {lam, w + blk, w + 2 * blk, w + 3 * blk, w + 4 * blk};
-  void* Xi = w + 5 * blk;
   char* wf = w + 6 * blk;
   void* FL[4] = {wf, wf + fblk, wf + 2 * fblk, wf + 3 * fblk};
-  void* FXi = wf + 4 * fblk;
   const long ldL[5] = {ld, Mi, Mi, Mi, Mi};
   const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
   for (int j = 1; j <= 4; j++)
@@ -878,25 +876,18 @@ int half_back(inqb_ctx* ctx, void* lam, long ld, int M, const double c[5][2], co
     cc[k][0] = c[k][0];
     cc[k][1] = -c[k][1];
   }
-  for (int i = 0; i < 4; i++) {
-    const int K = 4 - i;
-    double a[4][2];
-    const void* x[4];
-    const void* xf[4];
-    long ldx[4], ldf[4];
-    for (int j = 0; j < K; j++) {
-      a[j][0] = cc[i + j + 1][0];
-      a[j][1] = cc[i + j + 1][1];
-      x[j] = Lam[j];
-      ldx[j] = ldL[j];
-      xf[j] = FL[j];
-      ldf[j] = 1;
+  // gradients of the four (Xi_i, Phi_i) pairs in one pass over the eight blocks
+  double wgt[4][4][2] = {};
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j + i <= 3; j++) {
+      wgt[i][j][0] = cc[i + j + 1][0];
+      wgt[i][j][1] = cc[i + j + 1][1];
     }
-    INQB_TRY(launch_lincomb(ctx->precision, ctx->N, M, K, a, x, ldx, Xi, Mi, stream));
-    INQB_TRY(launch_lincomb(ctx->precision, (long)nF, 1, K, a, xf, ldf, FXi, 1, stream));
-    INQB_TRY(launch_vgrad(ctx->precision, ctx->N, M, Xi, Phi[i], Mi, 2.0, 0.0, gV, stream));
-    INQB_TRY(launch_agrad(*ctx, FXi, FPhi[i], Xi, Phi[i], Mi, M, ctx->d_red.as<double>(), 2.0, 0.0, gA, stream,
-                          true));
+  {
+    const void* L4[4] = {Lam[0], Lam[1], Lam[2], Lam[3]};
+    const long ld4[4] = {ldL[0], ldL[1], ldL[2], ldL[3]};
+    const void* F4[4] = {FL[0], FL[1], FL[2], FL[3]};
+    INQB_TRY(launch_half_grad(*ctx, L4, ld4, Phi, Mi, F4, FPhi, wgt, M, gV, gA, stream));
   }
   const void* x[5] = {Lam[0], Lam[1], Lam[2], Lam[3], Lam[4]};
   return launch_lincomb(ctx->precision, ctx->N, M, 5, cc, x, ldL, lam, ld, stream);
@@ -912,8 +903,9 @@ int adjoint_workspace(inqb_ctx* ctx, int M) {
   const size_t fblk = fourier_elems(ctx, M) * ctx->elem_bytes();
   INQB_TRY(ctx->d_adjL.ensure(6 * blk + 5 * fblk));
   INQB_TRY(ctx->d_red.ensure(256));
+  // per-chunk moments of four pairs of blocks
   INQB_TRY(ctx->d_nlpart.ensure(std::max<size_t>(
-      (size_t)ctx->proj.chunk_atom.size() * ctx->proj.L * 16 * M * sizeof(double), 16)));
+      (size_t)ctx->proj.chunk_atom.size() * 4 * ctx->proj.L * 16 * M * sizeof(double), 16)));
   return reserve(ctx, M);
 }
 
