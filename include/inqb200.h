@@ -110,7 +110,9 @@ int inqb_set_projectors(inqb_ctx* ctx, int nproj, int L, int smax, const int* co
  * with projector phases exp(+-i (k+A).r).  hpsi may alias psi. */
 int inqb_apply_h(inqb_ctx* ctx, const void* psi, void* hpsi, int M, int ld, void* stream);
 /* The same on HOST buffers ([N][M], ld = M): copies in, applies, copies out,
- * synchronous.  This is the call an INQ host-memory orbital_set would use. */
+ * synchronous.  This is the call an INQ host-memory orbital_set would use.  The
+ * orbitals go in chunks of at least 32 whose copy-in, H apply and copy-out overlap on
+ * three streams; page-locked host buffers let the copies run concurrently. */
 int inqb_apply_h_host(inqb_ctx* ctx, const void* psi_host, void* hpsi_host, int M);
 /* operations::transform::to_fourier / to_real (src/operations/transform.hpp:337-400):
  * forward unnormalised sign -1, backward sign +1 then 1/N.  out may alias in. */

@@ -368,6 +368,10 @@ int inqb_ctx_destroy(inqb_ctx* ctx) {
   DeviceGuard guard(ctx->device);
   cudaDeviceSynchronize();
   for (cudaEvent_t e : ctx->timing_events) cudaEventDestroy(e);
+  for (cudaStream_t s : ctx->host_streams)
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : ctx->host_events)
+    if (e) cudaEventDestroy(e);
   delete ctx;
   return INQB_OK;
 }
@@ -521,14 +525,46 @@ int inqb_apply_h_host(inqb_ctx* ctx, const void* psi_host, void* hpsi_host, int 
   INQB_CHECK_CTX(ctx);
   if (!psi_host || !hpsi_host || M <= 0) return fail(INQB_ERR_INVALID, "bad host buffers");
   INQB_GUARD(ctx);
-  const size_t bytes = (size_t)ctx->N * M * ctx->elem_bytes();
+  const size_t esz = ctx->elem_bytes();
+  const size_t bytes = (size_t)ctx->N * M * esz;
   INQB_TRY(ctx->d_work2.ensure(bytes));
-  cudaStream_t st = nullptr;
-  INQB_CUDA_TRY(cudaMemcpyAsync(ctx->d_work2.ptr, psi_host, bytes, cudaMemcpyHostToDevice, st));
+  INQB_TRY(ctx->d_work.ensure(bytes));
+  // Orbital chunks of at least 32 (rows of >= 256 bytes, up to 4 chunks): the copy-in
+  // of chunk c + 1, the H apply of chunk c and the copy-out of chunk c - 1 overlap on
+  // three streams, with pitched 2-D copies between the [N][M] host blocks and
+  // [N][chunk] device blocks.
+  const int G = ctx->plan->G_tile;
+  int C = std::max(32, (M + 3) / 4);
+  C = (C + G - 1) / G * G;
+  const int nchunks = (M + C - 1) / C;
+  for (int k = 0; k < 3; k++)
+    if (!ctx->host_streams[k]) INQB_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->host_streams[k], cudaStreamNonBlocking));
+  for (cudaEvent_t& e : ctx->host_events)
+    if (!e) INQB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaStream_t s_in = ctx->host_streams[0], s_comp = ctx->host_streams[1], s_out = ctx->host_streams[2];
   const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
-  INQB_TRY(apply(ctx, LaunchArgs::H, ctx->d_work2.ptr, M, ctx->d_work2.ptr, M, M, nullptr, 0, one, zero, st));
-  INQB_CUDA_TRY(cudaMemcpyAsync(hpsi_host, ctx->d_work2.ptr, bytes, cudaMemcpyDeviceToHost, st));
-  INQB_CUDA_TRY(cudaStreamSynchronize(st));
+  char* din = static_cast<char*>(ctx->d_work2.ptr);
+  char* dout = static_cast<char*>(ctx->d_work.ptr);
+  const char* hin = static_cast<const char*>(psi_host);
+  char* hout = static_cast<char*>(hpsi_host);
+  for (int c = 0; c < nchunks; c++) {
+    const int m0 = c * C, mc = std::min(C, M - m0);
+    char* di = din + (size_t)ctx->N * m0 * esz;
+    char* dq = dout + (size_t)ctx->N * m0 * esz;
+    cudaEvent_t ev_in = ctx->host_events[2 * (c % 4)], ev_done = ctx->host_events[2 * (c % 4) + 1];
+    INQB_CUDA_TRY(cudaMemcpy2DAsync(di, mc * esz, hin + m0 * esz, (size_t)M * esz, mc * esz, ctx->N,
+                                    cudaMemcpyHostToDevice, s_in));
+    INQB_CUDA_TRY(cudaEventRecord(ev_in, s_in));
+    INQB_CUDA_TRY(cudaStreamWaitEvent(s_comp, ev_in, 0));
+    INQB_TRY(apply(ctx, LaunchArgs::H, di, mc, dq, mc, mc, nullptr, 0, one, zero, s_comp));
+    INQB_CUDA_TRY(cudaEventRecord(ev_done, s_comp));
+    INQB_CUDA_TRY(cudaStreamWaitEvent(s_out, ev_done, 0));
+    INQB_CUDA_TRY(cudaMemcpy2DAsync(hout + m0 * esz, (size_t)M * esz, dq, mc * esz, mc * esz, ctx->N,
+                                    cudaMemcpyDeviceToHost, s_out));
+  }
+  INQB_CUDA_TRY(cudaStreamSynchronize(s_out));
+  INQB_CUDA_TRY(cudaStreamSynchronize(s_comp));
+  INQB_CUDA_TRY(cudaStreamSynchronize(s_in));
   return INQB_OK;
 }
 

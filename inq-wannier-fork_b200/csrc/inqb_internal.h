@@ -196,6 +196,10 @@ struct inqb_ctx {
   // by inqb_autotune or inqb_set_schedule; absent counts use the compiled default
   std::map<int, std::array<int, 4>> schedules;
 
+  // host-buffer applies: copy-in, compute and copy-out streams and chunk events
+  cudaStream_t host_streams[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t host_events[8] = {};
+
   // optional per-pass CUDA-event timing of H applications
   std::vector<cudaEvent_t> timing_events;  // 4 per recorded application
   int timing_capacity = 0, timing_count = 0;
