@@ -131,9 +131,12 @@ static int launch_h_impl(const LaunchArgs& a) {
   const int vout = aligned16(a.out, a.ld_out, esz);
   int ysplit = a.ysplit > 0 ? a.ysplit : TG::YSPLIT;
   if (TG::Y1 % ysplit != 0) return fail(INQB_ERR_INVALID, "schedule: ysplit must divide the tiles per plane");
+  // compiled defaults: 256 threads per CTA, except the x-line pass in FP64, which the
+  // autotuner measured faster with 128 (64^3: 295 -> 258 us)
+  const int thr_default[3] = {TG::THREADS, sizeof(T) == 8 ? 128 : TG::THREADS, TG::THREADS};
   int thr[3];
   for (int k = 0; k < 3; k++) {
-    thr[k] = a.threads[k] > 0 ? a.threads[k] : TG::THREADS;
+    thr[k] = a.threads[k] > 0 ? a.threads[k] : thr_default[k];
     if (thr[k] % 32 != 0 || thr[k] < 64 || thr[k] > TG::THREADS)
       return fail(INQB_ERR_INVALID, "schedule: threads per CTA must be a multiple of 32 in [64, 256]");
   }
