@@ -564,11 +564,12 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
   cp_async_commit();
   for (int i = threadIdx.x; i < NY; i += blockDim.x) twy[i] = tw_y[i];
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = tw_z[i];
-  // the tile's atom projections, in the tile precision
+  // the tile's atom projections, in the tile precision, as [segment][orbital][l]
+  // (a thread's orbitals read their LMAX values as whole 16-byte vectors)
   const bool pt_staged = nseg <= seg_cap;
   if (proj_on && pt_staged) {
     for (int i = threadIdx.x; i < nseg * LMAX * G; i += blockDim.x) {
-      const int j = i % G, l = (i / G) % LMAX, ts = i / (G * LMAX);
+      const int l = i % LMAX, j = (i / LMAX) % G, ts = i / (G * LMAX);
       cplx<T> v = mk<T>(0, 0);
       if (l < pj.L && j < gcount) {
         const double2 d = pj.proj[((long)pj.seg_atom[s0 + ts] * pj.L + l) * M + m0 + j];
@@ -687,7 +688,25 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
       cplx<T> h[PV];
 #pragma unroll
       for (int k = 0; k < PV; ++k) h[k] = S[sl + k];
-      if (proj_on) {
+      if (proj_on && pt_staged) {
+        for (int kk = k0[b]; kk < k1[b]; ++kk) {
+          const EntRec<T> re = (!TG::PREFETCH && kk == k0[b]) ? r0[b] : rec[kk + rbase];
+          const cplx<T> ph = mk<T>(re.ph[0], re.ph[1]);
+          const cplx<T>* pt = PT + (re.tseg * G + jb) * LMAX;
+#pragma unroll
+          for (int k = 0; k < PV; ++k) {
+            cplx<T> t = mk<T>(0, 0);
+#pragma unroll
+            for (int l = 0; l < LMAX; ++l) {
+              const cplx<T> pv = pt[k * LMAX + l];
+              t.x = fma(re.beta[l], pv.x, t.x);
+              t.y = fma(re.beta[l], pv.y, t.y);
+            }
+            h[k] = h[k] + mul_conj(t, ph);
+          }
+        }
+      } else if (proj_on) {
+        // more atom segments in this tile than staged: projections from global memory
         for (int kk = k0[b]; kk < k1[b]; ++kk) {
           const EntRec<T> re = (!TG::PREFETCH && kk == k0[b]) ? r0[b] : rec[kk + rbase];
           const cplx<T> ph = mk<T>(re.ph[0], re.ph[1]);
@@ -696,15 +715,10 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
             cplx<T> t = mk<T>(0, 0);
 #pragma unroll
             for (int l = 0; l < LMAX; ++l) {
-              cplx<T> pv;
-              if (pt_staged) {
-                pv = PT[(re.tseg * LMAX + l) * G + jb + k];
-              } else {
-                pv = mk<T>(0, 0);
-                if (l < pj.L && jb + k < gcount) {
-                  const double2 d = pj.proj[((long)pj.seg_atom[s0 + re.tseg] * pj.L + l) * M + m0 + jb + k];
-                  pv = mk<T>((T)d.x, (T)d.y);
-                }
+              cplx<T> pv = mk<T>(0, 0);
+              if (l < pj.L && jb + k < gcount) {
+                const double2 d = pj.proj[((long)pj.seg_atom[s0 + re.tseg] * pj.L + l) * M + m0 + jb + k];
+                pv = mk<T>((T)d.x, (T)d.y);
               }
               t.x = fma(re.beta[l], pv.x, t.x);
               t.y = fma(re.beta[l], pv.y, t.y);
