@@ -165,19 +165,22 @@ __global__ void __launch_bounds__(256)
     cp_async_wait<0>();
     __syncthreads();
 
-    // -- KB projection of the tile (projector_all.hpp:104-165): warp per atom
-    // segment, lanes = (orbital j, entry sub-lane)
+    // -- KB projection of the tile (projector_all.hpp:104-165): lanes = (orbital j,
+    // segment group); each group of G lanes walks one atom segment's entries, so a
+    // warp has 32 / G segments in flight and no cross-lane reduction is needed
     if (proj_on) {
-      constexpr int ESUB = 32 / G;
-      const int j = lane % G, es = lane / G;
+      constexpr int SGRP = 32 / G;
+      const int j = lane % G, sg = lane / G;
       const int tile = ix * Y1 + y1;
       const int s0 = pj.seg_ptr[tile], s1 = pj.seg_ptr[tile + 1];
-      for (int s = s0 + warp; s < s1; s += nw) {
+      for (int sb = s0 + warp * SGRP; sb < s1; sb += nw * SGRP) {
+        const int s = sb + sg;
+        if (s >= s1) continue;
         const int e0 = pj.seg_ent[s], e1 = pj.seg_ent[s + 1];
         cplx<T> a[LMAX];
 #pragma unroll
         for (int l = 0; l < LMAX; ++l) a[l] = mk<T>(0, 0);
-        for (int e = e0 + es; e < e1; e += ESUB) {
+        for (int e = e0; e < e1; ++e) {
           const EntRec<T>& re = rec[e - roff];
           const int off = re.off;
           const int r = off / NZ, z = off - r * NZ;
@@ -189,14 +192,7 @@ __global__ void __launch_bounds__(256)
             a[l].y = fma(b, x.y, a[l].y);
           }
         }
-#pragma unroll
-        for (int o = G; o < 32; o <<= 1)
-#pragma unroll
-          for (int l = 0; l < LMAX; ++l) {
-            a[l].x += __shfl_xor_sync(0xffffffffu, a[l].x, o);
-            a[l].y += __shfl_xor_sync(0xffffffffu, a[l].y, o);
-          }
-        if (es == 0 && j < gcount) {
+        if (j < gcount) {
           const int sl = pj.seg_local[s];
           if (sl < acc_cap) {
             // one segment per atom in a tile, tiles separated by barriers: no race
