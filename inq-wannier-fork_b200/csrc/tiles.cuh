@@ -70,8 +70,9 @@ struct TileGeom {
   // in FP32 the smaller footprint buys a third CTA per SM instead.
   static constexpr size_t TILE_BYTES = sizeof(cplx<T>) * (size_t)TILE;
   static constexpr bool PREFETCH = sizeof(T) == 8 && 2 * TILE_BYTES <= 150 * 1024;
-  // pass C in FP32 keeps four CTAs per SM (64 registers a thread) where they fit
-  static constexpr int INV_MIN_CTAS = (!PREFETCH && TILE_BYTES <= 40 * 1024) ? 4 : 1;
+  // pass C keeps four CTAs per SM in FP32 (64 registers a thread) and two with the
+  // FP64 orbital prefetch (128 registers), where the shared memory allows them
+  static constexpr int INV_MIN_CTAS = PREFETCH ? 2 : (TILE_BYTES <= 40 * 1024) ? 4 : 1;
   static constexpr size_t smem_inv(int rec_cap, int seg_cap) {
     return sizeof(cplx<T>) * ((size_t)TILE + (PREFETCH ? (size_t)PTS * G : 0) + NY + NZ) +
            sizeof(EntRec<T>) * (size_t)rec_cap + sizeof(int) * (size_t)PSTRIDE +
