@@ -231,6 +231,46 @@ int inqb_etrs_adjoint_step(inqb_ctx* ctx, void* lambda, int M, int ld, double dt
                            const double kA_tdt_cov[3], const void* powers, double* gV, double* gA_t,
                            double* gA_tdt, void* stream);
 
+/* ---------------------------------------------------------------- density -> potential
+ * solvers::poisson for a periodic cell (src/solvers/poisson.hpp:29-35,66-100,193-211),
+ * the field_set form: M complex fields [N][M] of the context precision,
+ * out(G) = 4 pi in(G) / |G|^2 with 0 at |G|^2 < 1e-6.  Three fused launches (the
+ * factor is applied inside the x-line transform pass).  out may alias in. */
+int inqb_poisson(inqb_ctx* ctx, const void* in, void* out, int M, int ld, void* stream);
+
+/* Theories of the density -> potential step (options::theory, src/options/theory.hpp:
+ * 31-62): non-interacting, Hartree only, and LDA (Hartree + XC_LDA_X + XC_LDA_C_PZ). */
+enum {
+  INQB_THEORY_NONE = 0,
+  INQB_THEORY_HARTREE = 1,
+  INQB_THEORY_LDA = 2
+};
+/* self_consistency::update_hamiltonian (src/hamiltonian/self_consistency.hpp:89-160)
+ * for an unpolarised density with no core density, no electric field and static
+ * ions: the context's local potential becomes vion + V_H[rho] + v_xc[max(rho, 0)]
+ * (xc_term.hpp:63-142), on the device.  rho and vion are FP64 device arrays [N];
+ * vion may be NULL (zero).  energies (host, may be NULL; non-NULL synchronises)
+ * receives {external, hartree, xc, nvxc}: dV sum rho vion, dV/2 sum rho V_H,
+ * dV sum e_xc n, dV sum rho v_xc, as hamiltonian::energy records them.  The
+ * exchange-correlation sums are FP64 in both precisions; V_H comes from
+ * inqb_poisson in the context precision. */
+int inqb_ks_potential(inqb_ctx* ctx, const double* rho, const double* vion, int theory, double energies[4],
+                      void* stream);
+/* real_time::etrs with its self-consistency loop (src/real_time/etrs.hpp:22-82), static
+ * ions, no induced vector potential, exchange off.  On entry the context's potential
+ * must be the Kohn-Sham potential of rho (inqb_ks_potential) and rho (FP64 device [N])
+ * the density of psi; on exit psi and rho are at t + dt and the potential is that of
+ * the last update.  Steps: save = T(i dt/2 H(kA_t)) psi and psi = T(i dt H(kA_t)) psi
+ * sharing the H^k psi (operations::exponential_2_for_1); rho = density(psi); update
+ * the potential; then for iscf < nscf: psi = T(i dt/2 H(kA_tdt)) save, rho =
+ * density(psi), delta = dV sum |rho - rho_old|, update the potential, stop when
+ * delta < threshold.  occ: FP64 device [M].  The reference uses nscf = 5 and
+ * threshold 5e-5.  Synchronises once per SCF iteration (delta is read back).
+ * iters and energies (host) may be NULL. */
+int inqb_etrs_scf_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                       const double kA_tdt_cov[3], const double* occ, double* rho, const double* vion, int theory,
+                       int nscf, double threshold, int* iters, double energies[4], void* stream);
+
 /* ---------------------------------------------------------------- launch schedules
  * (no counterpart in the reference; its kernels have fixed launch shapes).  A
  * schedule is {ysplit, threads of pass 1, of pass 2, of pass 3}: ysplit CTAs share

@@ -10,6 +10,7 @@
 #include "inqb_internal.h"
 #include "adjoint.h"
 #include "observables.h"
+#include "potential.h"
 #include "propagators.h"
 #include "plan.h"
 
@@ -204,6 +205,53 @@ int exponential(inqb_ctx* ctx, void* psi, int M, long ld, double fre, double fim
     INQB_TRY(apply(ctx, LaunchArgs::H, in, ldi, out, ldo, M, psi, ld, alpha, one, stream));
   }
   return INQB_OK;
+}
+
+// [N][M] block copy between leading dimensions (device to device)
+int copy_block(const void* src, long lds, void* dst, long ldd, int M, long N, size_t esz, void* stream) {
+  INQB_CUDA_TRY(cudaMemcpy2DAsync(dst, (size_t)ldd * esz, src, (size_t)lds * esz, (size_t)M * esz, (size_t)N,
+                                  cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return INQB_OK;
+}
+
+// Workspace of the density -> potential step, carved from ctx->d_pot.
+struct PotWork {
+  void* vh = nullptr;         // [N] complex, context precision (the Poisson field)
+  double* rho_old = nullptr;  // [N]
+  double* partial = nullptr;  // [kPotBlocks * 4]
+  double* sums = nullptr;     // [8]: the four potential sums, then sum |drho|
+};
+
+int pot_work(inqb_ctx* ctx, PotWork& w) {
+  const size_t N = (size_t)ctx->N;
+  const size_t vh = N * ctx->elem_bytes();
+  INQB_TRY(ctx->d_pot.ensure(vh + sizeof(double) * (N + (size_t)kPotBlocks * 4 + 8)));
+  char* b = static_cast<char*>(ctx->d_pot.ptr);
+  w.vh = b;
+  w.rho_old = reinterpret_cast<double*>(b + vh);
+  w.partial = w.rho_old + N;
+  w.sums = w.partial + (size_t)kPotBlocks * 4;
+  return INQB_OK;
+}
+
+// update_hamiltonian on the device: V_H by the Poisson passes, then one pass for
+// V = vion + V_H + v_xc and the four energy sums (w.sums[0..3], without dV).
+int ks_potential_dev(inqb_ctx* ctx, const double* rho, const double* vion, int theory, const PotWork& w,
+                     void* stream) {
+  if (theory >= INQB_THEORY_HARTREE) {
+    const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+    INQB_TRY(launch_pack_density(ctx->precision, rho, w.vh, ctx->N, stream));
+    INQB_TRY(apply(ctx, LaunchArgs::POISSON, w.vh, 1, w.vh, 1, 1, nullptr, 0, one, zero, stream));
+  }
+  return launch_ks_potential(ctx->precision, rho, vion, theory >= INQB_THEORY_HARTREE ? w.vh : nullptr, theory,
+                             ctx->N, ctx->d_V.ptr, w.partial, w.sums, stream);
+}
+
+void energies_from_sums(const inqb_ctx* ctx, const double s[4], double en[4]) {
+  en[0] = ctx->dV * s[0];
+  en[1] = 0.5 * ctx->dV * s[1];
+  en[2] = ctx->dV * s[2];
+  en[3] = ctx->dV * s[3];
 }
 
 }  // namespace
@@ -604,6 +652,97 @@ int inqb_etrs_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const dou
   INQB_TRY(exponential(ctx, psi, M, ld, 0.0, dt / 2.0, 4, stream));
   INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
   INQB_TRY(exponential(ctx, psi, M, ld, 0.0, dt / 2.0, 4, stream));
+  return INQB_OK;
+}
+
+int inqb_poisson(inqb_ctx* ctx, const void* in, void* out, int M, int ld, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, in, M, ld));
+  INQB_TRY(check_block(ctx, out, M, ld));
+  INQB_GUARD(ctx);
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  return apply(ctx, LaunchArgs::POISSON, in, ld, out, ld, M, nullptr, 0, one, zero, stream);
+}
+
+int inqb_ks_potential(inqb_ctx* ctx, const double* rho, const double* vion, int theory, double energies[4],
+                      void* stream) {
+  INQB_CHECK_CTX(ctx);
+  if (!rho) return fail(INQB_ERR_INVALID, "null density");
+  if (theory < INQB_THEORY_NONE || theory > INQB_THEORY_LDA) return fail(INQB_ERR_INVALID, "unknown theory");
+  INQB_GUARD(ctx);
+  PotWork w;
+  INQB_TRY(pot_work(ctx, w));
+  INQB_TRY(ks_potential_dev(ctx, rho, vion, theory, w, stream));
+  if (energies) {
+    double s[4];
+    INQB_CUDA_TRY(cudaMemcpyAsync(s, w.sums, sizeof(s), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    INQB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    energies_from_sums(ctx, s, energies);
+  }
+  return INQB_OK;
+}
+
+int inqb_etrs_scf_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                       const double kA_tdt_cov[3], const double* occ, double* rho, const double* vion, int theory,
+                       int nscf, double threshold, int* iters, double energies[4], void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!kA_t_cov || !kA_tdt_cov || !occ || !rho || !std::isfinite(dt) || nscf < 1 || !(threshold >= 0.0))
+    return fail(INQB_ERR_INVALID, "bad step arguments");
+  if (theory < INQB_THEORY_NONE || theory > INQB_THEORY_LDA) return fail(INQB_ERR_INVALID, "unknown theory");
+  INQB_GUARD(ctx);
+  INQB_TRY(reserve(ctx, M));
+  const long N = ctx->N;
+  const size_t esz = ctx->elem_bytes();
+  const size_t blk = (size_t)N * M * esz;
+  INQB_TRY(ctx->d_scf.ensure(2 * blk));
+  char* wb = static_cast<char*>(ctx->d_scf.ptr);
+  void* save = wb;
+  void* y = wb + blk;
+  PotWork w;
+  INQB_TRY(pot_work(ctx, w));
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+
+  // exponential_2_for_1(H(t), i dt/2, i dt): save = T(i dt/2 H) psi, psi = T(i dt H) psi,
+  // both from the same H^k psi (summed term by term, as the reference does)
+  INQB_TRY(set_kA(ctx, kA_t_cov, stream));
+  INQB_TRY(copy_block(psi, ld, save, M, M, N, esz, stream));
+  double c1[2] = {1.0, 0.0}, c2[2] = {1.0, 0.0};
+  for (int it = 1; it <= 4; it++) {
+    INQB_TRY(apply(ctx, LaunchArgs::H, it == 1 ? psi : y, it == 1 ? ld : M, y, M, M, nullptr, 0, one, zero,
+                   stream));
+    // c *= f / it with f = i dt/2 and i dt
+    const double h1 = 0.5 * dt / it, h2 = dt / it;
+    const double a1[2] = {-c1[1] * h1, c1[0] * h1}, a2[2] = {-c2[1] * h2, c2[0] * h2};
+    c1[0] = a1[0];
+    c1[1] = a1[1];
+    c2[0] = a2[0];
+    c2[1] = a2[1];
+    INQB_TRY(launch_shift2(ctx->precision, y, M, save, M, psi, ld, M, N, c1, c2, stream));
+  }
+  // density of the predicted step; the Hamiltonian moves to t + dt
+  INQB_TRY(launch_density(ctx->precision, psi, ld, M, N, occ, rho, stream));
+  INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
+  INQB_TRY(ks_potential_dev(ctx, rho, vion, theory, w, stream));
+
+  // the second half step with H(t + dt), self-consistently
+  double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  int done_iters = 0;
+  for (int iscf = 0; iscf < nscf; iscf++) {
+    INQB_TRY(copy_block(save, M, psi, ld, M, N, esz, stream));
+    INQB_TRY(exponential(ctx, psi, M, ld, 0.0, 0.5 * dt, 4, stream));
+    INQB_CUDA_TRY(cudaMemcpyAsync(w.rho_old, rho, sizeof(double) * N, cudaMemcpyDeviceToDevice,
+                                  (cudaStream_t)stream));
+    INQB_TRY(launch_density(ctx->precision, psi, ld, M, N, occ, rho, stream));
+    INQB_TRY(launch_absdiff(w.rho_old, rho, N, w.partial, w.sums + 4, stream));
+    INQB_TRY(ks_potential_dev(ctx, rho, vion, theory, w, stream));
+    INQB_CUDA_TRY(cudaMemcpyAsync(s, w.sums, sizeof(s), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    INQB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    done_iters = iscf + 1;
+    if (ctx->dV * s[4] < threshold) break;
+  }
+  if (iters) *iters = done_iters;
+  if (energies) energies_from_sums(ctx, s, energies);
   return INQB_OK;
 }
 

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <map>
 #include <tuple>
@@ -43,6 +44,10 @@ struct KinParams {
   int mask;   // zero the Laplacian term outside the Fourier sphere (|n/N|^2 > 1/4)
   int nr[3];
   T shift;    // 1/2 |k+A|^2 / N, moved to the epilogue when the mask is on
+  // Poisson mode when nonzero (k + A = 0, scale 1, so the quadratic is 1/2 |G|^2):
+  // the factor becomes pois / (1/2 |G|^2) = 4 pi / (N |G|^2), 0 where |G|^2 < 1e-6
+  // (solvers::poisson's periodic kernel, src/solvers/poisson.hpp:29-35,66-83)
+  T pois;
 };
 
 // INQ's fourier_space::outside_sphere (src/basis/fourier_space.hpp:87-93) in exact
@@ -155,6 +160,7 @@ static int launch_h_impl(const LaunchArgs& a) {
   kp.nr[0] = NX;
   kp.nr[1] = NY;
   kp.nr[2] = NZ;
+  kp.pois = (T)0;
 
   if (a.mode == LaunchArgs::H) {
     const int acc_cap = pj.nproj > 0 ? std::min(pj.max_plane_atoms, kAccAtomsMax) : 0;
@@ -191,6 +197,25 @@ static int launch_h_impl(const LaunchArgs& a) {
         tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv, seg_cap,
         vin && vout);
     if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
+  } else if (a.mode == LaunchArgs::POISSON) {
+    // solvers::poisson on M complex fields: forward z and inner y, then the outer y
+    // and x transforms with the 4 pi / (N |G|^2) factor, then the inverse (no 1/N:
+    // the factor holds it)
+    ProjView<T> none = pj;
+    none.nproj = 0;
+    k_tile_fwd<T, NX, NY, NZ><<<gfwd, thr[0], TG::smem_fwd(0, 0), st>>>(
+        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, none, 0, 0, ysplit, vin);
+    KinParams<T> kq = kp;
+    for (int d = 0; d < 3; d++) kq.kA[d] = (T)0;
+    kq.scale = (T)1;
+    kq.mask = 0;
+    kq.shift = (T)0;
+    kq.pois = (T)(2.0 * M_PI / ((double)NX * NY * NZ));
+    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kq, nullptr);
+    EpiParams<T> ep{};
+    ep.alpha = mk<T>((T)1, (T)0);
+    k_tile_inv<T, NX, NY, NZ, 0><<<ginv, thr[2], TG::smem_inv(0, 0), st>>>(
+        tmp, nullptr, 0, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, none, ep, 0, 0, vout);
   } else if (a.mode == LaunchArgs::FFT_FWD) {
     ProjView<T> none = pj;
     none.nproj = 0;

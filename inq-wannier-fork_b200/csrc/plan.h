@@ -4,7 +4,7 @@
 namespace inqb {
 
 struct LaunchArgs {
-  enum Mode { H = 0, FFT_FWD = 1, FFT_BWD = 2 };
+  enum Mode { H = 0, FFT_FWD = 1, FFT_BWD = 2, POISSON = 3 };
   int mode = H;
   const void* in = nullptr;
   long ld_in = 0;

@@ -358,6 +358,7 @@ __global__ void __launch_bounds__(256)
     const T f0 = (T)n0;
     T k = fma(fma(kinA, f0, kinB[kb]), f0, kinC[kb]);
     if (kp.mask) k = outside_sphere(kp.nr, n0, sym_freq(ka + Y2 * kb, NY), n2) ? (T)0 : k - kp.shift;
+    if (kp.pois != (T)0) k = ((T)2 * k < (T)1e-6) ? (T)0 : kp.pois / k;
     return k * v;
   });
   __syncthreads();

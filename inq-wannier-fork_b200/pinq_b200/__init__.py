@@ -3,10 +3,10 @@ Kohn-Sham Hamiltonian application and real-time propagators.
 
 It reaches the same C ABI as the C++ host adapter (``host/inq_b200.hpp``).
 """
-from ._lib import FP64, MIXED, InqbError, lib  # noqa: F401
+from ._lib import FP64, MIXED, THEORY_HARTREE, THEORY_LDA, THEORY_NONE, InqbError, lib  # noqa: F401
 from .hamiltonian import KSHamiltonian, build_gaussian_kb, gaussian_beta, grid_supported, sphere  # noqa: F401
 from . import systems  # noqa: F401
 from .batch import CellBatch  # noqa: F401
 
 __all__ = ["KSHamiltonian", "CellBatch", "build_gaussian_kb", "gaussian_beta", "grid_supported", "sphere", "systems",
-           "FP64", "MIXED", "InqbError", "lib"]
+           "FP64", "MIXED", "THEORY_NONE", "THEORY_HARTREE", "THEORY_LDA", "InqbError", "lib"]

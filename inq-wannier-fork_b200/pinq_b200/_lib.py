@@ -14,6 +14,10 @@ HEADER_PATH = os.path.join(os.path.dirname(_PKG), "include", "inqb200.h")
 
 FP64 = 0
 MIXED = 1
+# theories of the density -> potential step (INQB_THEORY_*)
+THEORY_NONE = 0
+THEORY_HARTREE = 1
+THEORY_LDA = 2
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -56,6 +60,10 @@ SIGNATURES = {
     "inqb_set_schedule": (ctypes.c_int, [_ctxp, ctypes.c_int, _ip]),
     "inqb_crank_nicolson_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
                                                 ctypes.c_int, ctypes.c_double, _ip, _dp, _vp]),
+    "inqb_poisson": (ctypes.c_int, [_ctxp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "inqb_ks_potential": (ctypes.c_int, [_ctxp, _vp, _vp, ctypes.c_int, _dp, _vp]),
+    "inqb_etrs_scf_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _vp,
+                                          _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _ip, _dp, _vp]),
     "inqb_etrs_powers_size": (ctypes.c_int, [_ctxp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "inqb_etrs_step_powers": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
                                              _vp, _vp]),

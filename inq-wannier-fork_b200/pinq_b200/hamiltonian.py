@@ -218,6 +218,53 @@ class KSHamiltonian:
         call("inqb_fft_backward", self._h, psi.data_ptr(), out.data_ptr(), psi.shape[1], psi.stride(0), self._stream())
         return out
 
+    # -- density -> potential (self_consistency.hpp:89-160)
+    def poisson(self, fields, out=None):
+        """solvers::poisson (periodic cell) of complex fields [N, M] in the context
+        precision: V(G) = 4 pi rho(G) / |G|^2, 0 at G = 0."""
+        fields = self._check(fields)
+        out = torch.empty_like(fields) if out is None else self._check(out)
+        call("inqb_poisson", self._h, fields.data_ptr(), out.data_ptr(), fields.shape[1], fields.stride(0),
+             self._stream())
+        return out
+
+    def _fp64_field(self, x, name):
+        if x is None:
+            return None
+        if x.dtype != torch.float64 or x.device.type != "cuda" or x.numel() != self.N or not x.is_contiguous():
+            raise TypeError(f"{name} must be a contiguous FP64 CUDA tensor of N values")
+        return x
+
+    def ks_potential(self, rho, vion=None, theory=2, energies=True):
+        """update_hamiltonian: the local potential becomes vion + V_H[rho] + v_xc[rho]
+        (theory 0 none, 1 Hartree, 2 LDA).  Returns the energies {external, hartree,
+        xc, nvxc} (synchronises) or None."""
+        rho = self._fp64_field(rho, "rho")
+        vion = self._fp64_field(vion, "vion")
+        en = np.zeros(4) if energies else None
+        call("inqb_ks_potential", self._h, rho.data_ptr(), vion.data_ptr() if vion is not None else None, int(theory),
+             dptr(en) if en is not None else None, self._stream())
+        return dict(zip(("external", "hartree", "xc", "nvxc"), en.tolist())) if en is not None else None
+
+    def etrs_scf_step_(self, psi, rho, dt, kA_t_cov, kA_tdt_cov, occ, vion=None, theory=2, nscf=5, threshold=5e-5):
+        """ETRS with the self-consistency loop of real_time::etrs, in place on psi and
+        rho (the potential must be the Kohn-Sham potential of rho on entry).
+        Returns (SCF iterations, energies of the last update)."""
+        psi = self._check(psi)
+        rho = self._fp64_field(rho, "rho")
+        vion = self._fp64_field(vion, "vion")
+        occ_t = torch.as_tensor(occ, dtype=torch.float64, device=self.device).contiguous()
+        if occ_t.numel() != psi.shape[1]:
+            raise ValueError("one occupation per orbital")
+        a = np.ascontiguousarray(kA_t_cov, np.float64).reshape(3)
+        b = np.ascontiguousarray(kA_tdt_cov, np.float64).reshape(3)
+        it = ctypes.c_int(0)
+        en = np.zeros(4)
+        call("inqb_etrs_scf_step", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), float(dt), dptr(a), dptr(b),
+             occ_t.data_ptr(), rho.data_ptr(), vion.data_ptr() if vion is not None else None, int(theory), int(nscf),
+             float(threshold), ctypes.byref(it), dptr(en), self._stream())
+        return it.value, dict(zip(("external", "hartree", "xc", "nvxc"), en.tolist()))
+
     def exponential_(self, psi, factor, order=4):
         """psi <- sum_k (factor H)^k / k! psi (in place)."""
         psi = self._check(psi)

@@ -69,6 +69,15 @@ def lib():
         L.orc_rvectors.argtypes = [ctypes.c_void_p, _dp]
         L.orc_orthonormalize.restype = ctypes.c_int
         L.orc_orthonormalize.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.orc_poisson.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.orc_lda_functional.restype = ctypes.c_double
+        L.orc_lda_functional.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.orc_ks_potential.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp, _dp]
+        L.orc_integral_sum_absdiff.restype = ctypes.c_double
+        L.orc_integral_sum_absdiff.argtypes = [ctypes.c_void_p, ctypes.c_long, _dp, _dp]
+        L.orc_etrs_scf_step.restype = ctypes.c_int
+        L.orc_etrs_scf_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp, _dp,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -247,3 +256,54 @@ class System:
         if info != 0:
             raise ArithmeticError(f"overlap matrix not positive definite at pivot {info - 1}")
         return out
+
+    # ---- density -> potential (self_consistency.hpp:89-160)
+
+    def poisson(self, fields):
+        """solvers::poisson (periodic) of complex fields [N] or [N][M]."""
+        f = np.asarray(fields, dtype=np.complex128)
+        shape = f.shape
+        f = np.ascontiguousarray(f.reshape(self.N, -1))
+        out = np.zeros_like(f)
+        lib().orc_poisson(self._h, f.shape[1], _d(f.view(np.float64)), _d(out.view(np.float64)))
+        return out.reshape(shape)
+
+    def lda_functional(self, func, rho):
+        """(v, efunc) of XC_LDA_X (func 1) or XC_LDA_C_PZ (func 9); rho [N] or [N][2]."""
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        nspin = 1 if rho.ndim == 1 else rho.shape[1]
+        if rho.shape[0] != self.N or nspin not in (1, 2):
+            raise ValueError("rho must be [N] or [N][2]")
+        v = np.zeros_like(rho)
+        e = lib().orc_lda_functional(self._h, int(func), int(nspin), _d(rho), _d(v))
+        return v, e
+
+    def ks_potential(self, rho, vion, theory):
+        """update_hamiltonian: sets V = vion + V_H + V_xc; returns (V, energies
+        {external, hartree, xc, nvxc}).  theory 0 none, 1 Hartree, 2 LDA."""
+        rho = np.ascontiguousarray(rho, np.float64).reshape(self.N)
+        vion = np.ascontiguousarray(vion, np.float64).reshape(self.N)
+        V = np.zeros(self.N)
+        en = np.zeros(4)
+        lib().orc_ks_potential(self._h, _d(rho), _d(vion), int(theory), _d(V), _d(en))
+        return V, en
+
+    def integral_sum_absdiff(self, a, b):
+        a = np.ascontiguousarray(a, np.float64).ravel()
+        b = np.ascontiguousarray(b, np.float64).ravel()
+        return lib().orc_integral_sum_absdiff(self._h, a.size, _d(a), _d(b))
+
+    def etrs_scf_step(self, psi, rho, dt, kA_t, kA_tdt, occ, vion, theory, nscf=5, threshold=5e-5):
+        """ETRS with its SCF loop (etrs.hpp:22-82).  The potential must already be the
+        Kohn-Sham potential of rho.  Returns (psi, rho, scf iterations, energies)."""
+        out = self._psi(psi).copy()
+        r = np.ascontiguousarray(rho, np.float64).reshape(self.N).copy()
+        a = np.ascontiguousarray(kA_t, np.float64).reshape(3)
+        b = np.ascontiguousarray(kA_tdt, np.float64).reshape(3)
+        occ = np.ascontiguousarray(occ, np.float64).reshape(out.shape[1])
+        vion = np.ascontiguousarray(vion, np.float64).reshape(self.N)
+        en = np.zeros(4)
+        it = lib().orc_etrs_scf_step(self._h, out.shape[1], float(dt), _d(a), _d(b), _d(occ), _d(vion),
+                                     int(theory), int(nscf), float(threshold), _d(out.view(np.float64)),
+                                     _d(r), _d(en))
+        return out, r, it, en

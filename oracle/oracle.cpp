@@ -454,6 +454,188 @@ void exponential_in_place(const System &s, int M, cd factor, cd *phi, int order)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Density -> potential (hamiltonian/self_consistency.hpp:89-160): the periodic
+// Poisson solve, LDA exchange and correlation, and the ETRS step with its
+// self-consistency loop.
+// ---------------------------------------------------------------------------
+
+// solvers::poisson with the 3-D periodic kernel (poisson.hpp:29-35,66-100):
+// rho(G) * (-4 pi / N) * (-1 / |G|^2) with 0 at |G|^2 < 1e-6, unnormalised
+// inverse transform.  M fields, [N][M] (the field_set form of in_place).
+void poisson_periodic(const Grid &g, int M, const cd *in, cd *out) {
+  const long N = g.npoints;
+  std::vector<cd> fs((size_t)N * M);
+  fft3d(g, M, in, fs.data(), -1, false);
+  const double scal = -4.0 * M_PI / (double)N;
+#pragma omp parallel for
+  for (int ix = 0; ix < g.nr[0]; ix++)
+    for (int iy = 0; iy < g.nr[1]; iy++)
+      for (int iz = 0; iz < g.nr[2]; iz++) {
+        v3 G{{g.sym(ix, 0) * 2.0 * M_PI, g.sym(iy, 1) * 2.0 * M_PI, g.sym(iz, 2) * 2.0 * M_PI}};
+        const double g2 = g.cell.norm_cov(G);
+        const double ker = (g2 < 1e-6) ? 0.0 : -1.0 / g2;
+        const long p = g.linear(ix, iy, iz);
+        for (int m = 0; m < M; m++) fs[(size_t)p * M + m] *= scal * ker;
+      }
+  fft3d(g, M, fs.data(), out, +1, false);
+}
+
+// LDA functionals, restated from their publications (libxc is not in the snapshot;
+// xc_term.hpp:276-287 calls xc_lda_exc_vxc).  Spin densities n[s], s < nspin.
+//   XC_LDA_X (id 1): Dirac-Slater exchange, e = -(3/4)(6/pi)^(1/3) sum_s n_s^(4/3) / n,
+//     v_s = -(6 n_s / pi)^(1/3)  (unpolarised: n_s = n / 2).
+//   XC_LDA_C_PZ (id 9): Perdew-Zunger, Phys. Rev. B 23, 5048 (1981), eqs. C1-C4 with
+//     the Ceperley-Alder fit of its Table XII: for rs >= 1 e = g / (1 + b1 sqrt(rs) + b2 rs),
+//     for rs < 1 e = A ln rs + B + C rs ln rs + D rs; between the unpolarised and the
+//     fully polarised fits the von Barth-Hedin interpolation f(zeta).
+// Points whose total density is below 1e-15 give e = v = 0.
+constexpr double kXcDensThreshold = 1e-15;
+
+struct PZParams {
+  double gamma, beta1, beta2, a, b, c, d;
+};
+constexpr PZParams kPZ[2] = {{-0.1423, 1.0529, 0.3334, 0.0311, -0.048, 0.0020, -0.0116},
+                             {-0.0843, 1.3981, 0.2611, 0.01555, -0.0269, 0.0007, -0.0048}};
+
+// e(rs) and de/drs of one Perdew-Zunger fit
+static void pz_fit(const PZParams &p, double rs, double &e, double &de) {
+  if (rs >= 1.0) {
+    const double sr = std::sqrt(rs), den = 1.0 + p.beta1 * sr + p.beta2 * rs;
+    e = p.gamma / den;
+    de = -p.gamma * (0.5 * p.beta1 / sr + p.beta2) / (den * den);
+  } else {
+    const double lr = std::log(rs);
+    e = p.a * lr + p.b + p.c * rs * lr + p.d * rs;
+    de = p.a / rs + p.c * (lr + 1.0) + p.d;
+  }
+}
+
+// energy per particle e and potentials v[s] at one point
+static void lda_point(int func, int nspin, const double *n, double &e, double *v) {
+  double nt = n[0] + (nspin == 2 ? n[1] : 0.0);
+  e = 0.0;
+  v[0] = 0.0;
+  if (nspin == 2) v[1] = 0.0;
+  if (nt < kXcDensThreshold) return;
+  if (func == 1) {
+    const double cx = std::cbrt(6.0 / M_PI);
+    if (nspin == 1) {
+      const double ns = 0.5 * nt, ns13 = std::cbrt(ns);
+      e = -0.75 * cx * 2.0 * ns * ns13 / nt;
+      v[0] = -cx * ns13;
+    } else {
+      double s4 = 0.0;
+      for (int s = 0; s < 2; s++) {
+        const double ns = std::max(n[s], 0.0), ns13 = std::cbrt(ns);
+        s4 += ns * ns13;
+        v[s] = -cx * ns13;
+      }
+      e = -0.75 * cx * s4 / nt;
+    }
+    return;
+  }
+  // func == 9
+  const double rs = std::cbrt(3.0 / (4.0 * M_PI * nt));
+  double eu, du;
+  pz_fit(kPZ[0], rs, eu, du);
+  if (nspin == 1) {
+    e = eu;
+    v[0] = eu - rs / 3.0 * du;
+    return;
+  }
+  double ep, dp;
+  pz_fit(kPZ[1], rs, ep, dp);
+  const double z = std::min(1.0, std::max(-1.0, (n[0] - n[1]) / nt));
+  const double fden = 2.0 * std::cbrt(2.0) - 2.0;
+  const double f = (std::pow(1.0 + z, 4.0 / 3.0) + std::pow(1.0 - z, 4.0 / 3.0) - 2.0) / fden;
+  const double df = 4.0 / 3.0 * (std::cbrt(1.0 + z) - std::cbrt(1.0 - z)) / fden;
+  e = eu + f * (ep - eu);
+  const double de_drs = du + f * (dp - du);
+  const double de_dz = df * (ep - eu);
+  const double vc = e - rs / 3.0 * de_drs;
+  v[0] = vc + (1.0 - z) * de_dz;
+  v[1] = vc - (1.0 + z) * de_dz;
+}
+
+// xc_term::evaluate_functional for an LDA (xc_term.hpp:276-287,316): v[p][s] of the
+// functional and efunc = dV sum_p e[p] n_total[p].
+static double lda_functional(const Grid &g, int func, int nspin, const double *rho, double *v) {
+  const long N = g.npoints;
+  double acc = 0.0;
+#pragma omp parallel for reduction(+ : acc)
+  for (long p = 0; p < N; p++) {
+    double e;
+    lda_point(func, nspin, rho + p * nspin, e, v + p * nspin);
+    acc += e * (rho[p * nspin] + (nspin == 2 ? rho[p * nspin + 1] : 0.0));
+  }
+  return g.volume_element() * acc;
+}
+
+// theory flags of update_hamiltonian (options/theory.hpp:31-62): 0 non-interacting,
+// 1 Hartree only, 2 LDA (Hartree + XC_LDA_X + XC_LDA_C_PZ)
+// self_consistency::update_hamiltonian for an unpolarised density with no core
+// density, no electric field and static ions (self_consistency.hpp:89-160,
+// xc_term.hpp:113-142): V = vion + V_H[rho] + V_xc[rho].  en = {external, hartree,
+// xc, nvxc}.
+void ks_potential(const Grid &g, const double *rho, const double *vion, int theory, double *V, double *en) {
+  const long N = g.npoints;
+  const double dV = g.volume_element();
+  double ext = 0.0;
+  for (long p = 0; p < N; p++) {
+    ext += rho[p] * vion[p];
+    V[p] = vion[p];
+  }
+  en[0] = dV * ext;
+  en[1] = en[2] = en[3] = 0.0;
+  if (theory >= 1) {
+    std::vector<cd> r(N), vh(N);
+    for (long p = 0; p < N; p++) r[p] = rho[p];
+    poisson_periodic(g, 1, r.data(), vh.data());
+    double eh = 0.0;
+    for (long p = 0; p < N; p++) {
+      eh += rho[p] * vh[p].real();
+      V[p] += vh[p].real();
+    }
+    en[1] = 0.5 * dV * eh;
+  }
+  if (theory >= 2) {
+    // process_density: negative values to zero (xc_term.hpp:82-91)
+    std::vector<double> full(N), vf(N), vxc(N, 0.0);
+    for (long p = 0; p < N; p++) full[p] = std::max(rho[p], 0.0);
+    for (int func : {1, 9}) {
+      en[2] += lda_functional(g, func, 1, full.data(), vf.data());
+      for (long p = 0; p < N; p++) vxc[p] += vf[p];
+    }
+    double nv = 0.0;
+    for (long p = 0; p < N; p++) {
+      V[p] += vxc[p];
+      nv += rho[p] * vxc[p];
+    }
+    en[3] = dV * nv;
+  }
+}
+
+// operations::exponential_2_for_1 (exponential.hpp:50-69): returns
+// T4(f1 H) phi in out and leaves T4(f2 H) phi in phi; both share the H^k phi.
+void exponential_2_for_1(const System &s, int M, cd f1, cd f2, cd *phi, cd *out) {
+  const long n = s.grid.npoints * M;
+  std::copy(phi, phi + n, out);
+  std::vector<cd> hn(n), tmp(n);
+  apply_h(s, M, phi, hn.data());
+  cd c1 = 1.0, c2 = 1.0;
+  for (int it = 1; it <= 4; it++) {
+    if (it > 1) {
+      apply_h(s, M, hn.data(), tmp.data());
+      std::swap(hn, tmp);
+    }
+    c1 *= f1 / (double)it;
+    c2 *= f2 / (double)it;
+    axpy(n, c1, hn.data(), out);
+    axpy(n, c2, hn.data(), phi);
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -722,6 +904,67 @@ int orc_orthonormalize(void *h, int M, double *psi_) {
     }
   }
   return 0;
+}
+
+// solvers::poisson::in_place on M complex fields [N][M] (periodic cell)
+void orc_poisson(void *h, int M, const double *in, double *out) {
+  poisson_periodic(((System *)h)->grid, M, (const cd *)in, (cd *)out);
+}
+
+// xc_term::evaluate_functional for func 1 (XC_LDA_X) or 9 (XC_LDA_C_PZ): v [N][nspin]
+// and the returned energy dV sum e n.  Returns NaN for another func id.
+double orc_lda_functional(void *h, int func, int nspin, const double *rho, double *v) {
+  if ((func != 1 && func != 9) || (nspin != 1 && nspin != 2)) return NAN;
+  return lda_functional(((System *)h)->grid, func, nspin, rho, v);
+}
+
+// update_hamiltonian: V = vion + V_H + V_xc becomes the system's potential, V_out
+// (optional) receives it, en = {external, hartree, xc, nvxc}
+void orc_ks_potential(void *h, const double *rho, const double *vion, int theory, double *V_out, double *en) {
+  auto *s = (System *)h;
+  ks_potential(s->grid, rho, vion, theory, s->V.data(), en);
+  if (V_out) std::memcpy(V_out, s->V.data(), sizeof(double) * s->grid.npoints);
+}
+
+// operations::integral_sum_absdiff (integral.hpp:113-126)
+double orc_integral_sum_absdiff(void *h, long n, const double *a, const double *b) {
+  double acc = 0.0;
+  for (long i = 0; i < n; i++) acc += std::fabs(a[i] - b[i]);
+  return ((System *)h)->grid.volume_element() * acc;
+}
+
+// real_time::etrs with its self-consistency loop (etrs.hpp:22-82), static ions, no
+// induced vector potential, exchange off.  On entry the system's potential is the
+// Kohn-Sham potential of the density at t (as update_hamiltonian left it); rho
+// [N] holds that density on entry and the density at t + dt on exit.  Returns the
+// SCF iterations run; en = energies of the last update_hamiltonian.
+int orc_etrs_scf_step(void *h, int M, double dt, const double *kA_t, const double *kA_tdt, const double *occ,
+                      const double *vion, int theory, int nscf, double threshold, double *psi_, double *rho,
+                      double *en) {
+  auto *s = (System *)h;
+  cd *psi = (cd *)psi_;
+  const long N = s->grid.npoints, n = N * (long)M;
+  std::vector<cd> save(n);
+  std::vector<double> old(N);
+  orc_set_vector_potential_cov(h, kA_t);
+  exponential_2_for_1(*s, M, cd(0.0, dt / 2.0), cd(0.0, dt), psi, save.data());
+  orc_density(h, M, psi_, occ, rho);
+  orc_set_vector_potential_cov(h, kA_tdt);
+  ks_potential(s->grid, rho, vion, theory, s->V.data(), en);
+  std::copy(save.begin(), save.end(), psi);
+  int iters = 0;
+  for (int iscf = 0; iscf < nscf; iscf++) {
+    if (iscf != 0) std::copy(save.begin(), save.end(), psi);
+    exponential_in_place(*s, M, cd(0.0, dt / 2.0), psi, 4);
+    std::copy(rho, rho + N, old.begin());
+    orc_density(h, M, psi_, occ, rho);
+    const double delta = orc_integral_sum_absdiff(h, N, old.data(), rho);
+    const bool done = (delta < threshold) || (iscf == nscf - 1);
+    ks_potential(s->grid, rho, vion, theory, s->V.data(), en);
+    iters = iscf + 1;
+    if (done) break;
+  }
+  return iters;
 }
 
 int orc_num_threads() {

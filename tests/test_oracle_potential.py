@@ -1,0 +1,200 @@
+"""The oracle's density -> potential step against the reference's own tests.
+
+Golden values:
+  * solvers::poisson, periodic point charge on a 10 x 10 x 13.7 cell with spacing
+    0.1 (src/solvers/poisson.hpp:228-300): sum |Re V| = 82.9383793318, V[0] =
+    -0.0241804443, Im V = 0; plane waves: V = 4 pi / k^2 rho (poisson.hpp:301-373).
+  * XC_LDA_X through xc_term::evaluate_functional on a 10.3 x 13.8 x 4.5 cell with
+    spacing 0.40557787 (src/hamiltonian/xc_term.hpp:339-418), unpolarised and
+    polarised energies and potentials at points 5439 and 4444.
+The Perdew-Zunger correlation has no golden value in the reference's unit tests
+(its tests of the LDA go through a ground-state run with pseudopotentials); it is
+checked here by v = d(n e)/dn and the continuity of the published fit at rs = 1.
+"""
+import numpy as np
+import pytest
+
+from helpers import make_oracle, small_system
+
+
+@pytest.fixture(scope="module")
+def poisson_cell(oracle_mod):
+    # real_space::calculate_dimensions: round(length / spacing) (real_space.hpp:183-193)
+    return oracle_mod.System(np.diag([10.0, 10.0, 13.7]), [100, 100, 137])
+
+
+def test_poisson_point_charge_golden(poisson_cell):
+    s = poisson_cell
+    rho = np.zeros((s.N, 2), complex)
+    rho[0, 0] = -1.0
+    rho[0, 1] = -2.0  # the field_set member 1 of the reference test, scaled by 1 + ist
+    V = s.poisson(rho)
+    assert np.abs(V[:, 0].real).sum() == pytest.approx(82.9383793318, abs=1e-10)
+    assert np.abs(V[:, 1].real).sum() / 2.0 == pytest.approx(82.9383793318, abs=1e-10)
+    assert np.abs(V.imag).sum() / 2.0 <= 5e-12
+    assert V[0, 0].real == pytest.approx(-0.0241804443, abs=1e-10)
+
+
+def test_poisson_plane_waves(poisson_cell):
+    s = poisson_cell
+    r = s.rvectors()
+    kk = 2.0 * np.pi / 10.0
+    d = np.exp(1j * kk * r[:, 0])
+    V = s.poisson(d)
+    assert np.abs(V - 4.0 * np.pi / kk**2 * d).sum() / s.N < 1e-13
+    kk = 8.0 * np.pi / 10.0
+    d = np.cos(kk * r[:, 1]).astype(complex)
+    V = s.poisson(d)
+    assert np.abs(V.real - 4.0 * np.pi / kk**2 * d.real).sum() / s.N < 1e-8
+
+
+@pytest.fixture(scope="module")
+def xc_case(oracle_mod):
+    lx, ly, lz = 10.3, 13.8, 4.5
+    nr = [int(round(l / 0.40557787)) for l in (lx, ly, lz)]
+    assert nr == [25, 34, 11]
+    s = oracle_mod.System(np.diag([lx, ly, lz]), nr)
+    r = s.rvectors()
+    kvec = 2.0 * np.pi * np.array([1.0 / lx, 1.0 / ly, 1.0 / lz])
+    ff = np.maximum(0.0, np.cos(r @ kvec) + 1.0)
+    dV = s.volume_element
+    unp = ff * 42.0 / (dV * ff.sum())                    # density::normalize(.., 42)
+    pol = np.sin((r * r).sum(1) / 100.0)                  # vector3 norm() is the squared length
+    dpol = np.stack([(1.0 - pol) * ff, pol * ff], 1)
+    dpol *= 42.0 / (dV * dpol.sum())
+    return s, unp, dpol
+
+
+def test_lda_x_golden(xc_case):
+    """The reference prints 10 decimal places: agreement to 1e-10 absolute."""
+    s, unp, dpol = xc_case
+    assert unp[5439] == pytest.approx(0.0024885602, abs=1e-10)
+    assert dpol[5439, 0] == pytest.approx(0.0009452194, abs=1e-10)
+    assert dpol[5439, 1] == pytest.approx(0.0015433408, abs=1e-10)
+    v, e = s.lda_functional(1, unp)
+    assert e == pytest.approx(-14.0558385758, abs=1e-10)
+    assert v[5439] == pytest.approx(-0.1334462916, abs=1e-10)
+    assert v[4444] == pytest.approx(-0.3276348215, abs=1e-10)
+    v, e = s.lda_functional(1, dpol)
+    assert e == pytest.approx(-15.1704508993, abs=1e-10)
+    assert v[5439, 0] == pytest.approx(-0.1217618773, abs=1e-10)
+    assert v[5439, 1] == pytest.approx(-0.1433797225, abs=1e-10)
+    assert v[4444, 0] == pytest.approx(-0.3784052378, abs=1e-10)
+    assert v[4444, 1] == pytest.approx(-0.2527984139, abs=1e-10)
+
+
+def _energy_density(s, func, rho):
+    """n e(n) for each value of rho: the functional's energy on a field that holds
+    the value at one point and zero elsewhere, divided by dV"""
+    out = np.zeros(len(rho))
+    for i, r in enumerate(rho):
+        f = np.zeros(s.N) if np.ndim(r) == 0 else np.zeros((s.N, 2))
+        f[0] = r
+        _, e = s.lda_functional(func, f)
+        out[i] = e / s.volume_element
+    return out
+
+
+@pytest.mark.parametrize("func", [1, 9])
+def test_lda_potential_is_derivative(oracle_mod, func):
+    """v = d(n e(n))/dn by central differences, across rs = 1 (n = 0.2387)."""
+    s = oracle_mod.System(np.diag([2.0, 2.0, 2.0]), [2, 2, 2])
+    n = np.array([1e-3, 0.05, 0.2, 0.3, 2.0])
+    h = 1e-6 * n
+    v = np.zeros(len(n))
+    for i in range(len(n)):
+        f = np.zeros(s.N)
+        f[0] = n[i]
+        vv, _ = s.lda_functional(func, f)
+        v[i] = vv[0]
+    ep = _energy_density(s, func, n + h)
+    em = _energy_density(s, func, n - h)
+    assert np.abs((ep - em) / (2 * h) - v).max() < 1e-6 * np.abs(v).max()
+
+
+def test_pz_spin_potentials_are_derivatives(oracle_mod):
+    s = oracle_mod.System(np.diag([2.0, 2.0, 2.0]), [2, 2, 2])
+    for nu, nd in [(0.01, 0.004), (0.3, 0.1), (0.02, 0.2)]:
+        f = np.zeros((s.N, 2))
+        f[0] = (nu, nd)
+        v, _ = s.lda_functional(9, f)
+        for spin in range(2):
+            h = 1e-6 * f[0, spin]
+            fp, fm = f.copy(), f.copy()
+            fp[0, spin] += h
+            fm[0, spin] -= h
+            _, ep = s.lda_functional(9, fp)
+            _, em = s.lda_functional(9, fm)
+            d = (ep - em) / (2 * h * s.volume_element)
+            assert abs(d - v[0, spin]) < 1e-6 * abs(v[0, spin])
+
+
+def test_pz_fit_continuity(oracle_mod):
+    """The published Perdew-Zunger parameters join to about 3e-5 Ha at rs = 1."""
+    s = oracle_mod.System(np.diag([2.0, 2.0, 2.0]), [2, 2, 2])
+    n1 = 3.0 / (4.0 * np.pi)  # rs = 1
+    es = []
+    for n in (n1 * (1 + 1e-9), n1 * (1 - 1e-9)):
+        f = np.zeros(s.N)
+        f[0] = n
+        _, e = s.lda_functional(9, f)
+        es.append(e / (s.volume_element * n))
+    assert abs(es[0] - es[1]) < 5e-5
+    assert es[0] == pytest.approx(-0.048 - 0.0116, rel=1e-6)                 # rs < 1: B + D
+    assert es[1] == pytest.approx(-0.1423 / (1 + 1.0529 + 0.3334), rel=1e-6)  # rs > 1
+
+
+def test_ks_potential_composition(oracle_mod):
+    sysd = small_system(None, n=16, a=8.0, M=2, seed=3, with_proj=False, ecut=8.0)
+    o = make_oracle(oracle_mod, sysd)
+    rho = o.density(sysd["psi"], [2.0, 2.0])
+    vion = sysd["V"]
+    V0, e0 = o.ks_potential(rho, vion, 0)
+    assert np.array_equal(V0, vion) and e0[1] == e0[2] == e0[3] == 0.0
+    V1, e1 = o.ks_potential(rho, vion, 1)
+    vh = o.poisson(rho.astype(complex)).real
+    assert np.abs(V1 - vion - vh).max() < 1e-13
+    assert e1[1] == pytest.approx(0.5 * o.volume_element * (rho * vh).sum(), rel=1e-12)
+    V2, e2 = o.ks_potential(rho, vion, 2)
+    vx, ex = o.lda_functional(1, rho)
+    vc, ec = o.lda_functional(9, rho)
+    assert np.abs(V2 - vion - vh - vx - vc).max() < 1e-13
+    assert e2[2] == pytest.approx(ex + ec, rel=1e-12)
+    assert e2[3] == pytest.approx(o.volume_element * (rho * (vx + vc)).sum(), rel=1e-12)
+
+
+def test_etrs_scf_noninteracting_is_plain_etrs(oracle_mod):
+    """With a density-independent H the SCF loop stops at its second pass
+    (delta = 0) and the step equals T(H(t+dt)) T(H(t)) psi."""
+    sysd = small_system(None, n=16, a=8.0, M=3, seed=4, ecut=8.0)
+    sysd["positions"] = sysd["positions"][:2]
+    o = make_oracle(oracle_mod, sysd)
+    psi = sysd["psi"]
+    occ = np.array([2.0, 2.0, 1.0])
+    k1 = o.cart_to_cov(np.array([0.01, 0.0, 0.0]))
+    k2 = o.cart_to_cov(np.array([0.02, 0.0, 0.0]))
+    ref = o.etrs_step(psi, 0.05, k1, k2)
+    o.set_potential(sysd["V"])
+    rho = o.density(psi, occ)
+    out, rho2, iters, _ = o.etrs_scf_step(psi, rho, 0.05, k1, k2, occ, sysd["V"], 0)
+    assert iters == 2
+    assert np.array_equal(out, ref)
+    assert np.abs(rho2 - o.density(ref, occ)).max() == 0.0
+
+
+def test_etrs_scf_lda_conserves_norm(oracle_mod):
+    sysd = small_system(None, n=16, a=8.0, M=3, seed=5, ecut=8.0)
+    sysd["positions"] = sysd["positions"][:2]
+    o = make_oracle(oracle_mod, sysd)
+    occ = np.array([2.0, 2.0, 2.0])
+    psi = sysd["psi"]
+    rho = o.density(psi, occ)
+    o.ks_potential(rho, sysd["V"], 2)
+    k = np.zeros(3)
+    n0 = o.volume_element * (np.abs(psi) ** 2).sum(0)
+    for _ in range(2):
+        psi, rho, iters, en = o.etrs_scf_step(psi, rho, 0.05, k, k, occ, sysd["V"], 2)
+        assert 1 <= iters <= 5
+        assert np.all(np.isfinite(en)) and en[2] < 0.0
+    n1 = o.volume_element * (np.abs(psi) ** 2).sum(0)
+    assert np.abs(n1 - n0).max() < 1e-6
