@@ -8,7 +8,9 @@
 // Parity pinning: the golden values of the reference's own unit tests are
 // reproduced by tests/test_oracle_golden.py (harmonic oscillator 0.0051420503,
 // sphere of 257 points, dipole 2.6692428234, plane-wave kinetic energies, FFT
-// round trip, Taylor exponentials on diagonal operators, orthonormalisation).
+// round trip, Taylor exponentials on diagonal operators, orthonormalisation) and
+// tests/test_oracle_potential.py (Poisson point charge 82.9383793318 and
+// -0.0241804443, plane waves, LDA exchange energies and potentials).
 // The reference itself cannot be compiled here (its submodules multi, mpi3,
 // libxc and pseudopod are empty and FFTW/BLAS/MPI are absent), so the projector
 // tables (pseudopod's sharmonic) and the ETRS/CN steps (empty unit tests in the
@@ -39,6 +41,12 @@
 //   * overlap + Cholesky + rotate                  src/operations/overlap.hpp:41,
 //                                                  src/matrix/cholesky.hpp:28-89,
 //                                                  src/operations/rotate.hpp:147-157
+//   * periodic Poisson solve                       src/solvers/poisson.hpp:29-35,66-100
+//   * update_hamiltonian (V_ion + V_H + V_xc,
+//     energies), LDA evaluation                    src/hamiltonian/self_consistency.hpp:89-160,
+//                                                  src/hamiltonian/xc_term.hpp:63-142,276-323
+//   * exponential_2_for_1, ETRS with SCF loop      src/operations/exponential.hpp:50-69,
+//                                                  src/real_time/etrs.hpp:22-82
 //
 // Third-party arithmetic the reference delegates (not vendored in the snapshot):
 //   * boost-multi FFT adaptors -> FFTW3 / cuFFT (pinned version unknown): restated
@@ -47,6 +55,10 @@
 //   * pseudopod sharmonic (pinned version unknown): real spherical harmonics
 //     Y00 = 1/sqrt(4pi), (Y1-1, Y10, Y11) = sqrt(3/4pi) (y, z, x)/r, Y1m(0) = 0.
 //   * BLAS gemm / LAPACK zpotrf: restated as plain loops.
+//   * libxc XC_LDA_X and XC_LDA_C_PZ (pinned version unknown): restated from their
+//     publications (Dirac-Slater exchange; Perdew-Zunger 1981).  XC_LDA_X is pinned
+//     to the reference's xc_term test values; the Perdew-Zunger fit has no golden
+//     value in the reference's unit tests.
 
 #include <algorithm>
 #include <cmath>
