@@ -580,6 +580,38 @@ def run_ours(args):
     ms_e2e = max_over_ranks(dist, s2.elapsed_time(e2))
     wall_e2e = time.perf_counter() - t0
 
+    # -- checkpoint in INQ's restart layout: all 128 orbitals (complex128 files) + density
+    ckpt = None
+    if rank == 0:
+        import shutil
+
+        from pinq_b200.checkpoint import RealTimeResults, load_checkpoint, save_checkpoint
+
+        cdir = tempfile.mkdtemp(prefix="inqb_ckpt_")
+        try:
+            occ_c = np.full(x64.shape[1], 2.0)
+            rho_c = h64.density(x64, occ_c)
+            res_c = RealTimeResults()
+            res_c.record(0, 0.0, 0.0, (0.0, 0.0, 0.0))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            save_checkpoint(cdir, h64, x64, occ_c, rho_c, res_c)
+            t_save = time.perf_counter() - t0
+            back_c = torch.empty_like(x64)
+            rho_b = torch.empty_like(rho_c)
+            t0 = time.perf_counter()
+            load_checkpoint(cdir, h64, back_c, rho_b)
+            torch.cuda.synchronize()
+            t_load = time.perf_counter() - t0
+            nbytes = x64.numel() * 16 + rho_c.numel() * 8
+            ckpt = {"bytes": int(nbytes), "save_s": t_save, "load_s": t_load,
+                    "save_GBps": nbytes / t_save / 1e9, "load_GBps": nbytes / t_load / 1e9,
+                    "exact_round_trip": bool(torch.equal(back_c, x64) and torch.equal(rho_b, rho_c)),
+                    "layout": "INQ restart layout (one complex128 file per state + occupations + density)",
+                    "storage": "local temporary directory of the GPU host"}
+        finally:
+            shutil.rmtree(cdir, ignore_errors=True)
+
     cells = bench_cells(args, local) if args.cells else None
     adj = bench_adjoint(args, local) if args.adjoint else None
     big = bench_cfg4(args, local) if args.cfg4 else None
@@ -640,6 +672,7 @@ def run_ours(args):
                  "H_applies_per_step": 8, "dt": 0.05},
         "crank_nicolson": cn,
         "etrs_scf": scf,
+        "checkpoint": ckpt,
         "error": {"mixed_vs_fp64_gpu_rel_norm": err_fp64, "vs_oracle": err_oracle},
     }
     if cells is not None:

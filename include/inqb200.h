@@ -36,7 +36,8 @@ enum inqb_status {
   INQB_ERR_NOMEM = 4,         /* device allocation failed */
   INQB_ERR_NONFINITE = 5,     /* NaN or Inf found in an input */
   INQB_ERR_NOT_POSITIVE_DEFINITE = 6, /* overlap matrix failed Cholesky */
-  INQB_ERR_TIMEOUT = 7        /* a bounded device-side wait gave up */
+  INQB_ERR_TIMEOUT = 7,       /* a bounded device-side wait gave up */
+  INQB_ERR_IO = 8             /* a checkpoint file is missing, short or unwritable */
 };
 
 enum inqb_precision {
@@ -270,6 +271,27 @@ int inqb_ks_potential(inqb_ctx* ctx, const double* rho, const double* vion, int 
 int inqb_etrs_scf_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
                        const double kA_tdt_cov[3], const double* occ, double* rho, const double* vion, int theory,
                        int nscf, double threshold, int* iters, double energies[4], void* stream);
+
+/* ---------------------------------------------------------------- checkpoints
+ * INQ's restart layout, so that runs resume from their own checkpoints and exchange
+ * orbitals with INQ (operations::io::save/load, src/operations/io.hpp:42-177, as
+ * systems::electrons::save/try_load arranges them, src/systems/electrons.hpp:323-375):
+ *   <dir>/kpin<kpin>/states/<state>_0000000000   raw complex128 [N] per state,
+ *                                                 grid order p = (ix ny + iy) nz + iz
+ *   <dir>/kpin<kpin>/occupations/array           raw FP64, this block at offset first_state
+ *   <dir>/spin_density/0000000000                raw FP64 [N]
+ * with numbers written "%010ld" (utils::num_to_str, src/utils/num_str.hpp:20-24).
+ * The files are complex128 in both precisions (a mixed context widens on save and
+ * rounds on load).  psi holds states first_state .. first_state + M - 1 (a rank's
+ * block when the states are sharded); occ is a host array of M values or NULL.
+ * Loading a missing or short file returns INQB_ERR_IO, as io::load returns false.
+ * Synchronous. */
+int inqb_save_orbitals(inqb_ctx* ctx, const char* dirname, int kpin, const void* psi, int M, int ld,
+                       int first_state, const double* occ, void* stream);
+int inqb_load_orbitals(inqb_ctx* ctx, const char* dirname, int kpin, void* psi, int M, int ld, int first_state,
+                       double* occ, void* stream);
+int inqb_save_density(inqb_ctx* ctx, const char* dirname, const double* rho, void* stream);
+int inqb_load_density(inqb_ctx* ctx, const char* dirname, double* rho, void* stream);
 
 /* ---------------------------------------------------------------- launch schedules
  * (no counterpart in the reference; its kernels have fixed launch shapes).  A

@@ -9,6 +9,7 @@
 
 #include "inqb_internal.h"
 #include "adjoint.h"
+#include "checkpoint.h"
 #include "observables.h"
 #include "potential.h"
 #include "propagators.h"
@@ -744,6 +745,40 @@ int inqb_etrs_scf_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const
   if (iters) *iters = done_iters;
   if (energies) energies_from_sums(ctx, s, energies);
   return INQB_OK;
+}
+
+int inqb_save_orbitals(inqb_ctx* ctx, const char* dirname, int kpin, const void* psi, int M, int ld,
+                       int first_state, const double* occ, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!dirname || kpin < 0 || first_state < 0) return fail(INQB_ERR_INVALID, "bad checkpoint arguments");
+  INQB_GUARD(ctx);
+  INQB_TRY(ctx->d_io.ensure(checkpoint_staging_bytes(ctx->N, M)));
+  return save_states(ctx->precision, dirname, kpin, psi, ld, M, ctx->N, first_state, occ, ctx->d_io.ptr, stream);
+}
+
+int inqb_load_orbitals(inqb_ctx* ctx, const char* dirname, int kpin, void* psi, int M, int ld, int first_state,
+                       double* occ, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!dirname || kpin < 0 || first_state < 0) return fail(INQB_ERR_INVALID, "bad checkpoint arguments");
+  INQB_GUARD(ctx);
+  INQB_TRY(ctx->d_io.ensure(checkpoint_staging_bytes(ctx->N, M)));
+  return load_states(ctx->precision, dirname, kpin, psi, ld, M, ctx->N, first_state, occ, ctx->d_io.ptr, stream);
+}
+
+int inqb_save_density(inqb_ctx* ctx, const char* dirname, const double* rho, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  if (!dirname || !rho) return fail(INQB_ERR_INVALID, "bad checkpoint arguments");
+  INQB_GUARD(ctx);
+  return save_density(dirname, rho, ctx->N, stream);
+}
+
+int inqb_load_density(inqb_ctx* ctx, const char* dirname, double* rho, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  if (!dirname || !rho) return fail(INQB_ERR_INVALID, "bad checkpoint arguments");
+  INQB_GUARD(ctx);
+  return load_density(dirname, rho, ctx->N, stream);
 }
 
 int inqb_crank_nicolson_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],

@@ -18,6 +18,8 @@ MIXED = 1
 THEORY_NONE = 0
 THEORY_HARTREE = 1
 THEORY_LDA = 2
+# status of a missing, short or unwritable checkpoint file
+ERR_IO = 8
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -64,6 +66,12 @@ SIGNATURES = {
     "inqb_ks_potential": (ctypes.c_int, [_ctxp, _vp, _vp, ctypes.c_int, _dp, _vp]),
     "inqb_etrs_scf_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _vp,
                                           _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _ip, _dp, _vp]),
+    "inqb_save_orbitals": (ctypes.c_int, [_ctxp, ctypes.c_char_p, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, _dp, _vp]),
+    "inqb_load_orbitals": (ctypes.c_int, [_ctxp, ctypes.c_char_p, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, _dp, _vp]),
+    "inqb_save_density": (ctypes.c_int, [_ctxp, ctypes.c_char_p, _vp, _vp]),
+    "inqb_load_density": (ctypes.c_int, [_ctxp, ctypes.c_char_p, _vp, _vp]),
     "inqb_etrs_powers_size": (ctypes.c_int, [_ctxp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "inqb_etrs_step_powers": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
                                              _vp, _vp]),

@@ -7,6 +7,7 @@ kernels through the C ABI.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 import torch
@@ -264,6 +265,34 @@ class KSHamiltonian:
              occ_t.data_ptr(), rho.data_ptr(), vion.data_ptr() if vion is not None else None, int(theory), int(nscf),
              float(threshold), ctypes.byref(it), dptr(en), self._stream())
         return it.value, dict(zip(("external", "hartree", "xc", "nvxc"), en.tolist()))
+
+    # -- checkpoints in INQ's restart layout (operations/io.hpp, systems/electrons.hpp)
+    def save_orbitals(self, dirname, psi, occ=None, kpin=0, first_state=0):
+        """Write states first_state.. of k-point block kpin (and the occupations)
+        under the electrons directory dirname, as complex128 files."""
+        psi = self._check(psi)
+        o = None if occ is None else np.ascontiguousarray(occ, np.float64).reshape(psi.shape[1])
+        call("inqb_save_orbitals", self._h, os.fsencode(dirname), int(kpin), psi.data_ptr(), psi.shape[1],
+             psi.stride(0), int(first_state), dptr(o) if o is not None else None, self._stream())
+
+    def load_orbitals(self, dirname, psi, kpin=0, first_state=0, with_occupations=True):
+        """Fill psi [N, M] from the files; returns the occupations (or None).  Raises
+        InqbError (status ERR_IO) when a file is missing or short."""
+        psi = self._check(psi)
+        o = np.zeros(psi.shape[1]) if with_occupations else None
+        call("inqb_load_orbitals", self._h, os.fsencode(dirname), int(kpin), psi.data_ptr(), psi.shape[1],
+             psi.stride(0), int(first_state), dptr(o) if o is not None else None, self._stream())
+        return o
+
+    def save_density(self, dirname, rho):
+        rho = self._fp64_field(rho, "rho")
+        call("inqb_save_density", self._h, os.fsencode(dirname), rho.data_ptr(), self._stream())
+
+    def load_density(self, dirname, rho=None):
+        rho = torch.empty(self.N, dtype=torch.float64, device=self.device) if rho is None else \
+            self._fp64_field(rho, "rho")
+        call("inqb_load_density", self._h, os.fsencode(dirname), rho.data_ptr(), self._stream())
+        return rho
 
     def exponential_(self, psi, factor, order=4):
         """psi <- sum_k (factor H)^k / k! psi (in place)."""

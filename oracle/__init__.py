@@ -307,3 +307,40 @@ class System:
                                      int(theory), int(nscf), float(threshold), _d(out.view(np.float64)),
                                      _d(r), _d(en))
         return out, r, it, en
+
+
+# ---- checkpoint layout (operations/io.hpp:42-177, systems/electrons.hpp:323-375)
+
+def num_to_str(n: int) -> str:
+    """utils::num_to_str (src/utils/num_str.hpp:20-24): "%010ld" into an 11-byte buffer."""
+    return ("%010d" % int(n))[:10]
+
+
+def save_orbitals_layout(dirname, psi, occ=None, kpin=0, first_state=0):
+    """The files systems::electrons::save writes for one k-point block: one raw
+    complex128 file per state (io::save(orbital_set), spinor 0) and the occupations
+    array written at offset first_state (io::save(array))."""
+    psi = np.asarray(psi)
+    kdir = os.path.join(dirname, "kpin" + num_to_str(kpin))
+    os.makedirs(os.path.join(kdir, "states"), exist_ok=True)
+    for j in range(psi.shape[1]):
+        name = num_to_str(first_state + j) + "_" + num_to_str(0)
+        np.ascontiguousarray(psi[:, j], dtype=np.complex128).tofile(os.path.join(kdir, "states", name))
+    if occ is not None:
+        os.makedirs(os.path.join(kdir, "occupations"), exist_ok=True)
+        path = os.path.join(kdir, "occupations", "array")
+        mode = "r+b" if os.path.exists(path) else "wb"
+        with open(path, mode) as f:
+            f.seek(8 * first_state)
+            f.write(np.ascontiguousarray(occ, dtype=np.float64).tobytes())
+
+
+def load_orbitals_layout(dirname, N, M, kpin=0, first_state=0):
+    """(psi [N, M] complex128, occupations [M]) read back from that layout."""
+    kdir = os.path.join(dirname, "kpin" + num_to_str(kpin))
+    psi = np.zeros((N, M), np.complex128)
+    for j in range(M):
+        name = num_to_str(first_state + j) + "_" + num_to_str(0)
+        psi[:, j] = np.fromfile(os.path.join(kdir, "states", name), dtype=np.complex128, count=N)
+    occ = np.fromfile(os.path.join(kdir, "occupations", "array"), dtype=np.float64)[first_state:first_state + M]
+    return psi, occ
