@@ -580,6 +580,62 @@ def run_ours(args):
     ms_e2e = max_over_ranks(dist, s2.elapsed_time(e2))
     wall_e2e = time.perf_counter() - t0
 
+    # -- TD-MLWF after a step (mlwf_properties::calculate): the six matrices, JADE, the
+    # rotation of all 128 orbitals, centres and spreads; per-phase CUDA-event times
+    # states: 128 Gaussians (sigma 1 bohr) on the 64 atoms and 64 bond midpoints,
+    # orthonormalised and mixed by a seeded unitary, built on the device
+    mlwf = {}
+    lat_t = torch.tensor(np.asarray(lattice, float).reshape(3, 3), dtype=torch.float64, device="cuda")
+    fr = [torch.tensor(np.where(np.arange(n) >= (n + 1) // 2, np.arange(n) - n, np.arange(n)) / n,
+                       dtype=torch.float64, device="cuda") for n in nr]
+    fx, fy, fz = torch.meshgrid(fr[0], fr[1], fr[2], indexing="ij")
+    rr = torch.stack([fx.reshape(-1), fy.reshape(-1), fz.reshape(-1)], 1) @ lat_t
+    centres_w = np.concatenate([pos, pos + 10.26 / 8.0])
+    loc = torch.empty((rr.shape[0], len(centres_w)), dtype=torch.complex128, device="cuda")
+    for j, c in enumerate(centres_w):
+        d = rr - torch.tensor(c, dtype=torch.float64, device="cuda")
+        d -= 20.52 * torch.round(d / 20.52)
+        loc[:, j] = torch.exp(-(d * d).sum(1) / 2.0)
+    h64.orthonormalize_(loc)
+    g_mix = torch.Generator(device="cpu").manual_seed(11)
+    qm, _ = torch.linalg.qr(torch.randn(len(centres_w), len(centres_w), dtype=torch.complex128, generator=g_mix))
+    loc = loc @ qm.to("cuda")
+    del rr, fx, fy, fz
+    for name, h, x in (("mixed", h32, loc.to(torch.complex64)), ("fp64", h64, loc)):
+        xm = x.clone()
+        t0 = time.perf_counter()
+        _, _, k_first = h.mlwf_step_(xm)  # the first transform un-mixes the states
+        torch.cuda.synchronize()
+        mlwf[f"{name}_first_ms"] = 1e3 * (time.perf_counter() - t0)
+        mlwf[f"{name}_first_jade_sweeps"] = k_first
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n_m = 3
+        sw = []
+        for _ in range(n_m):
+            _, spreads_m, k_ = h.mlwf_step_(xm)
+            sw.append(k_)
+        torch.cuda.synchronize()
+        mlwf[f"{name}_ms_per_step"] = 1e3 * (time.perf_counter() - t0) / n_m
+        mlwf[f"{name}_jade_sweeps"] = sw
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(n_m):
+            h.mlwf_matrices(xm)
+        s1.record()
+        torch.cuda.synchronize()
+        ms_g = s0.elapsed_time(s1) / n_m
+        M_ = xm.shape[1]
+        mlwf[f"{name}_matrices_ms"] = ms_g
+        # 3 weighted Gram products: 3 N M^2 complex multiply-adds = 24 N M^2 flops
+        mlwf[f"{name}_matrices_tflops"] = 24.0 * xm.shape[0] * M_ * M_ / (ms_g * 1e-3) / 1e12
+        mlwf[f"{name}_mean_spread"] = float(np.mean(spreads_m))
+    mlwf.update({"states": "128 Gaussians (sigma 1 bohr) on the 64 atoms and 64 bond midpoints, orthonormalised "
+                           "and mixed by a seeded unitary; steps after the first start in the localised gauge",
+                 "orbitals": int(x64.shape[1]), "maxsweep": 100, "tol": 1e-8,
+                 "timing": "step: wall clock around synchronised calls (one read-back per JADE sweep); "
+                           "matrices: CUDA events"})
+
     # -- checkpoint in INQ's restart layout: all 128 orbitals (complex128 files) + density
     ckpt = None
     if rank == 0:
@@ -673,6 +729,7 @@ def run_ours(args):
         "crank_nicolson": cn,
         "etrs_scf": scf,
         "checkpoint": ckpt,
+        "mlwf": mlwf,
         "error": {"mixed_vs_fp64_gpu_rel_norm": err_fp64, "vs_oracle": err_oracle},
     }
     if cells is not None:

@@ -293,6 +293,30 @@ int inqb_load_orbitals(inqb_ctx* ctx, const char* dirname, int kpin, void* psi, 
 int inqb_save_density(inqb_ctx* ctx, const char* dirname, const double* rho, void* stream);
 int inqb_load_density(inqb_ctx* ctx, const char* dirname, double* rho, void* stream);
 
+/* ---------------------------------------------------------------- TD-MLWF
+ * The fork's time-dependent maximally localised Wannier functions
+ * (observables::mlwf_properties::calculate, src/observables/mlwf_properties.hpp:28-44).
+ * inqb_mlwf_step = tdmlwf_trans::update + compute_transform + apply_transform and the
+ * centres and spreads: the six matrices a_k = <psi_m| t_k |psi_n> of the normalised
+ * states (t = cos, sin of 2 pi r_d / |a_d|; tdmlwf_trans.hpp:96-172), their joint
+ * diagonalisation by JADE (jade_complex.hpp:32-335; the reference calls it with
+ * maxsweep 100, tol 1e-8), psi <- psi u^H (operations::rotate), then per state the
+ * centre L t (t_d = atan2(Re adiag_sin, Re adiag_cos) / 2 pi, L's rows the lattice
+ * vectors, as tdmlwf_trans::center writes it) and the spread
+ * sqrt(sum_d (1 - |c_d|^2 - |s_d|^2) / |b_d|^2).  centres [M][3], spreads [M] and
+ * sweeps are host outputs and may be NULL.  Synchronises once per JADE sweep.
+ * FP64 matrices and rotations in both precisions; in the mixed precision the matrix
+ * products are FP32 summed over 16 points, then FP64. */
+int inqb_mlwf_step(inqb_ctx* ctx, void* psi, int M, int ld, int maxsweep, double tol, int* sweeps, double* centres,
+                   double* spreads, void* stream);
+/* The pieces, on device arrays of complex128: a [6][M][M] from psi
+ * (tdmlwf_trans::update); jade_complex on a (rotated in place), u [M][M], adiag [6][M];
+ * psi <- psi u^H. */
+int inqb_mlwf_matrices(inqb_ctx* ctx, const void* psi, int M, int ld, void* a, void* stream);
+int inqb_jade(inqb_ctx* ctx, int M, void* a, void* u, void* adiag, int maxsweep, double tol, int* sweeps,
+              void* stream);
+int inqb_mlwf_rotate(inqb_ctx* ctx, void* psi, int M, int ld, const void* u, void* stream);
+
 /* ---------------------------------------------------------------- launch schedules
  * (no counterpart in the reference; its kernels have fixed launch shapes).  A
  * schedule is {ysplit, threads of pass 1, of pass 2, of pass 3}: ysplit CTAs share

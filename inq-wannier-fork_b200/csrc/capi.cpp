@@ -13,6 +13,7 @@
 #include "observables.h"
 #include "potential.h"
 #include "propagators.h"
+#include "wannier.h"
 #include "plan.h"
 
 namespace inqb {
@@ -246,6 +247,139 @@ int ks_potential_dev(inqb_ctx* ctx, const double* rho, const double* vion, int t
   }
   return launch_ks_potential(ctx->precision, rho, vion, theory >= INQB_THEORY_HARTREE ? w.vh : nullptr, theory,
                              ctx->N, ctx->d_V.ptr, w.partial, w.sums, stream);
+}
+
+// TD-MLWF workspace carved from ctx->d_mlwf
+struct MlwfWork {
+  double2* a = nullptr;      // [6][M][M]
+  double2* u = nullptr;      // [M][M]
+  double2* adiag = nullptr;  // [6][M]
+  double* sums = nullptr;    // [3 M] band sums
+  double2* partial = nullptr;
+  int2* pairs = nullptr;     // [2 np - 1][np]
+  double* delta = nullptr;   // [2 np - 1][np]
+  double* change = nullptr;  // [1]
+};
+
+int mlwf_work(inqb_ctx* ctx, int M, bool with_gram, MlwfWork& w) {
+  const size_t MM = (size_t)M * M, np = (size_t)(M + 1) / 2, steps = 2 * np - 1;
+  const size_t slabs = with_gram ? mlwf_gram_slabs(ctx->N, M) : 0;
+  size_t off = 0;
+  auto take = [&off](size_t bytes) {
+    const size_t at = off;
+    off += (bytes + 255) / 256 * 256;
+    return at;
+  };
+  const size_t oa = take(sizeof(double2) * 6 * MM), ou = take(sizeof(double2) * MM),
+               od = take(sizeof(double2) * 6 * M), os = take(sizeof(double) * 3 * M),
+               op = take(sizeof(double2) * slabs * 3 * MM), opr = take(sizeof(int2) * steps * np),
+               ode = take(sizeof(double) * steps * np), oc = take(sizeof(double));
+  INQB_TRY(ctx->d_mlwf.ensure(off));
+  char* b = static_cast<char*>(ctx->d_mlwf.ptr);
+  w.a = reinterpret_cast<double2*>(b + oa);
+  w.u = reinterpret_cast<double2*>(b + ou);
+  w.adiag = reinterpret_cast<double2*>(b + od);
+  w.sums = reinterpret_cast<double*>(b + os);
+  w.partial = reinterpret_cast<double2*>(b + op);
+  w.pairs = reinterpret_cast<int2*>(b + opr);
+  w.delta = reinterpret_cast<double*>(b + ode);
+  w.change = reinterpret_cast<double*>(b + oc);
+  return INQB_OK;
+}
+
+// One JADE sweep (2 np - 1 rotation steps and the trace-change sum) as a CUDA graph:
+// captured once per call on a private stream, launched once per sweep (the sweep's
+// pair schedule is copied to the same buffer before each launch).
+struct SweepGraph {
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int capture(int M, double2* a, double2* u, const MlwfWork& w, int np, int steps) {
+    INQB_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    INQB_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    int rc = INQB_OK;
+    for (int s = 0; s < steps && rc == INQB_OK; s++)
+      rc = launch_jade_step(a, u, M, w.pairs + (size_t)s * np, np, w.delta + (size_t)s * np, cap);
+    if (rc == INQB_OK) rc = launch_jade_change(w.delta, steps, np, w.change, cap);
+    const cudaError_t e = cudaStreamEndCapture(cap, &graph);
+    if (rc != INQB_OK) return rc;
+    if (e != cudaSuccess) return fail(INQB_ERR_CUDA, std::string("JADE sweep capture: ") + cudaGetErrorString(e));
+    INQB_CUDA_TRY(cudaGraphInstantiate(&exec, graph, 0));
+    return INQB_OK;
+  }
+  ~SweepGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap) cudaStreamDestroy(cap);
+  }
+};
+
+// jade_complex on device arrays a [6][M][M] (rotated in place), u, adiag.  The pair
+// schedule of each sweep is made on the host (the reference's round-robin shift) and
+// copied before the sweep; the sweep's trace change is read back once per sweep.
+int jade_dev(int M, double2* a, double2* u, double2* adiag, int maxsweep, double tol, const MlwfWork& w, int* sweeps,
+             void* stream) {
+  const int np = (M + 1) / 2, steps = 2 * np - 1;
+  cudaStream_t st = (cudaStream_t)stream;
+  INQB_TRY(launch_identity(u, M, stream));
+  std::vector<int> top(np), bot(np);
+  for (int i = 0; i < np; i++) {
+    top[i] = i;
+    bot[np - i - 1] = np + i;
+  }
+  std::vector<int2> sched((size_t)steps * np);
+  SweepGraph graph;
+  int nsweep = 0;
+  for (;;) {
+    ++nsweep;
+    for (int s = 0; s < steps; s++) {
+      for (int i = 0; i < np; i++) sched[(size_t)s * np + i] = make_int2(top[i], bot[i]);
+      // the reference's shift: bot[j] <- bot[j+1], top[j+1] <- top[j] as one parallel
+      // move, then the ends, then one swap (jade_complex.hpp:296-322)
+      const int top_back = top[np - 1], bot_front = bot[0];
+      std::vector<int> t2 = top, b2 = bot;
+      for (int j = 0; j + 1 < np; j++) {
+        b2[j] = bot[j + 1];
+        t2[j + 1] = top[j];
+      }
+      b2[np - 1] = top_back;
+      t2[0] = bot_front;
+      if (np > 1)
+        std::swap(t2[0], t2[1]);
+      else
+        std::swap(t2[0], b2[0]);
+      top.swap(t2);
+      bot.swap(b2);
+    }
+    INQB_CUDA_TRY(cudaMemcpyAsync(w.pairs, sched.data(), sizeof(int2) * sched.size(), cudaMemcpyHostToDevice, st));
+    if (!graph.exec) INQB_TRY(graph.capture(M, a, u, w, np, steps));
+    INQB_CUDA_TRY(cudaGraphLaunch(graph.exec, st));
+    double change = 0.0;
+    INQB_CUDA_TRY(cudaMemcpyAsync(&change, w.change, sizeof(double), cudaMemcpyDeviceToHost, st));
+    INQB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (std::fabs(change) < tol || nsweep >= maxsweep) break;
+  }
+  INQB_TRY(launch_jade_adiag(a, u, M, adiag, stream));
+  if (sweeps) *sweeps = nsweep;
+  return INQB_OK;
+}
+
+// centres and spreads from adiag (tdmlwf_trans::center / spread2, tdmlwf_trans.hpp:196-312)
+void mlwf_centres(const inqb_ctx* ctx, int M, const double2* adiag, double* centres, double* spreads) {
+  const double (*L)[3] = ctx->cell.lat;
+  const double (*B)[3] = ctx->cell.rlat;
+  for (int i = 0; i < M; i++) {
+    double t[3], s2 = 0.0;
+    for (int d = 0; d < 3; d++) {
+      const double2 c = adiag[(size_t)(2 * d) * M + i], s = adiag[(size_t)(2 * d + 1) * M + i];
+      t[d] = std::atan2(s.x, c.x) / (2.0 * M_PI);
+      const double b2 = B[d][0] * B[d][0] + B[d][1] * B[d][1] + B[d][2] * B[d][2];
+      s2 += (1.0 - (c.x * c.x + c.y * c.y) - (s.x * s.x + s.y * s.y)) / b2;
+    }
+    if (centres)
+      for (int r = 0; r < 3; r++) centres[3 * i + r] = t[0] * L[r][0] + t[1] * L[r][1] + t[2] * L[r][2];
+    if (spreads) spreads[i] = std::sqrt(s2);
+  }
 }
 
 void energies_from_sums(const inqb_ctx* ctx, const double s[4], double en[4]) {
@@ -779,6 +913,67 @@ int inqb_load_density(inqb_ctx* ctx, const char* dirname, double* rho, void* str
   if (!dirname || !rho) return fail(INQB_ERR_INVALID, "bad checkpoint arguments");
   INQB_GUARD(ctx);
   return load_density(dirname, rho, ctx->N, stream);
+}
+
+int inqb_mlwf_matrices(inqb_ctx* ctx, const void* psi, int M, int ld, void* a, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!a) return fail(INQB_ERR_INVALID, "null matrix buffer");
+  INQB_GUARD(ctx);
+  MlwfWork w;
+  INQB_TRY(mlwf_work(ctx, M, true, w));
+  INQB_TRY(launch_band_sums(ctx->precision, psi, psi, ld, M, ctx->N, w.sums, stream));
+  return launch_mlwf_gram(ctx->precision, psi, ld, M, ctx->N, ctx->nr, ctx->cell.lat, w.sums, w.partial,
+                          static_cast<double2*>(a), stream);
+}
+
+int inqb_jade(inqb_ctx* ctx, int M, void* a, void* u, void* adiag, int maxsweep, double tol, int* sweeps,
+              void* stream) {
+  INQB_CHECK_CTX(ctx);
+  if (M < 1 || !a || !u || !adiag || maxsweep < 1 || !(tol > 0.0)) return fail(INQB_ERR_INVALID, "bad jade arguments");
+  INQB_GUARD(ctx);
+  MlwfWork w;
+  INQB_TRY(mlwf_work(ctx, M, false, w));
+  return jade_dev(M, static_cast<double2*>(a), static_cast<double2*>(u), static_cast<double2*>(adiag), maxsweep, tol,
+                  w, sweeps, stream);
+}
+
+int inqb_mlwf_rotate(inqb_ctx* ctx, void* psi, int M, int ld, const void* u, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!u) return fail(INQB_ERR_INVALID, "null rotation");
+  INQB_GUARD(ctx);
+  const size_t esz = ctx->elem_bytes();
+  INQB_TRY(ctx->d_work.ensure((size_t)ctx->N * M * esz));
+  INQB_TRY(launch_mlwf_rotate(ctx->precision, psi, ld, M, ctx->N, static_cast<const double2*>(u), ctx->d_work.ptr, M,
+                              stream));
+  return copy_block(ctx->d_work.ptr, M, psi, ld, M, ctx->N, esz, stream);
+}
+
+int inqb_mlwf_step(inqb_ctx* ctx, void* psi, int M, int ld, int maxsweep, double tol, int* sweeps, double* centres,
+                   double* spreads, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (maxsweep < 1 || !(tol > 0.0)) return fail(INQB_ERR_INVALID, "bad jade arguments");
+  INQB_GUARD(ctx);
+  MlwfWork w;
+  INQB_TRY(mlwf_work(ctx, M, true, w));
+  INQB_TRY(launch_band_sums(ctx->precision, psi, psi, ld, M, ctx->N, w.sums, stream));
+  INQB_TRY(launch_mlwf_gram(ctx->precision, psi, ld, M, ctx->N, ctx->nr, ctx->cell.lat, w.sums, w.partial, w.a,
+                            stream));
+  INQB_TRY(jade_dev(M, w.a, w.u, w.adiag, maxsweep, tol, w, sweeps, stream));
+  const size_t esz = ctx->elem_bytes();
+  INQB_TRY(ctx->d_work.ensure((size_t)ctx->N * M * esz));
+  INQB_TRY(launch_mlwf_rotate(ctx->precision, psi, ld, M, ctx->N, w.u, ctx->d_work.ptr, M, stream));
+  INQB_TRY(copy_block(ctx->d_work.ptr, M, psi, ld, M, ctx->N, esz, stream));
+  if (centres || spreads) {
+    std::vector<double2> h((size_t)6 * M);
+    INQB_CUDA_TRY(cudaMemcpyAsync(h.data(), w.adiag, sizeof(double2) * h.size(), cudaMemcpyDeviceToHost,
+                                  (cudaStream_t)stream));
+    INQB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    mlwf_centres(ctx, M, h.data(), centres, spreads);
+  }
+  return INQB_OK;
 }
 
 int inqb_crank_nicolson_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],

@@ -192,6 +192,7 @@ struct inqb_ctx {
   inqb::DevBuf d_cnred;         // Crank-Nicolson: 4 sums and the residual norm per orbital
   inqb::DevBuf d_scf;           // ETRS with self-consistency: the saved half step, H^k phi
   inqb::DevBuf d_io;            // checkpoint staging (complex128 rows of a chunk of states)
+  inqb::DevBuf d_mlwf;          // TD-MLWF: the six matrices, u, adiag, sums, slabs, pairs, deltas
   inqb::DevBuf d_pot;           // density -> potential: V_H field [N] (complex), previous
                                 // density [N], partial sums, sums
   size_t elem_bytes() const { return precision == INQB_FP64 ? 16 : 8; }

@@ -1,0 +1,561 @@
+// TD-MLWF: the Wannier transformation applied after each real-time step
+// (src/observables/mlwf_properties.hpp:28-44, src/wannier/tdmlwf_trans.hpp,
+// src/wannier/jade_complex.hpp).
+//
+//   gram     split over points: Z_d[m][n] = sum_p conj(psi_m) e^{i theta_d} psi_n for the
+//            three directions (theta_d = 2 pi r_d / |a_d|), per-slab partial sums in
+//            FP64 (FP32 products summed over 16-point chunks in the mixed precision)
+//   finish   sum of the slabs, normalisation 1/(|psi_m| |psi_n|), and the six matrices
+//            of tdmlwf_trans::update: cos = (Z + Z^H)/2, sin = (Z - Z^H)/(2i)
+//   jade     one CTA per pair and rotation step: the 18 pair elements, the 3 x 3
+//            Jacobi eigenproblem, the plane rotation of the pair's rows of the six
+//            matrices and of u, and the step's change of the traces.  The reference
+//            multiplies dense M x M rotation matrices (7 GEMMs per step); the pairs are
+//            disjoint, so rotating two rows per pair is the same product in O(M) per pair.
+//   adiag    adiag[k][i] = sum_j conj(a_k[i][j]) u[i][j]
+//   rotate   psi <- psi u^H (operations::rotate), tiled through shared memory
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "dft.cuh"
+#include "inqb_internal.h"
+#include "wannier.h"
+
+namespace inqb {
+
+namespace {
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+// ------------------------------------------------------------------ gram
+constexpr int kGT = 32;  // output tile (m and n)
+constexpr int kGP = 16;  // points per staged chunk (static shared memory stays under 48 KB)
+
+struct GramGeom {
+  int nr[3];
+  double frac_to_theta[3][3];  // theta_d = 2 pi sum_j f_j a_j[d] / |a_d|
+};
+
+template <typename T>
+struct GramAcc;
+template <>
+struct GramAcc<double> {
+  using R = double;
+};
+template <>
+struct GramAcc<float> {
+  using R = float;
+};
+
+// grid (tiles_m * tiles_n, ksplit); 256 threads as 16 x 16, each 2 x 2 outputs x 3 directions
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_mlwf_gram(const cplx<T>* __restrict__ psi, long ld, int M, long N, GramGeom geo, long pts_per_slab,
+                double2* __restrict__ partial) {
+  using R = typename GramAcc<T>::R;
+  __shared__ cplx<R> sA[kGP][kGT];
+  __shared__ cplx<R> sB[3][kGP][kGT];
+  __shared__ cplx<R> sW[3][kGP];
+  const int tiles = (M + kGT - 1) / kGT;
+  const int m0 = (blockIdx.x % tiles) * kGT, n0 = (blockIdx.x / tiles) * kGT;
+  const long p_beg = (long)blockIdx.y * pts_per_slab, p_end = min(N, p_beg + pts_per_slab);
+  const int tm = threadIdx.x % 16, tn = threadIdx.x / 16;
+  double acc[3][2][2][2];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) acc[d][a][b][0] = acc[d][a][b][1] = 0.0;
+  for (long pc = p_beg; pc < p_end; pc += kGP) {
+    // weights of the chunk's points
+    if (threadIdx.x < kGP) {
+      const long p = pc + threadIdx.x;
+      cplx<R> w[3] = {mk<R>(0, 0), mk<R>(0, 0), mk<R>(0, 0)};
+      if (p < p_end) {
+        const int iz = (int)(p % geo.nr[2]), iy = (int)((p / geo.nr[2]) % geo.nr[1]),
+                  ix = (int)(p / ((long)geo.nr[1] * geo.nr[2]));
+        const int id[3] = {ix, iy, iz};
+        double f[3];
+        for (int j = 0; j < 3; ++j) {
+          const int s = (id[j] >= (geo.nr[j] + 1) / 2) ? id[j] - geo.nr[j] : id[j];
+          f[j] = (double)s / geo.nr[j];
+        }
+        for (int d = 0; d < 3; ++d) {
+          const double th = geo.frac_to_theta[d][0] * f[0] + geo.frac_to_theta[d][1] * f[1] +
+                            geo.frac_to_theta[d][2] * f[2];  // in units of pi
+          double sn, cs;
+          sincospi(th, &sn, &cs);
+          w[d] = mk<R>((R)cs, (R)sn);
+        }
+      }
+      for (int d = 0; d < 3; ++d) sW[d][threadIdx.x] = w[d];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kGP * kGT; i += blockDim.x) {
+      const int q = i / kGT, j = i % kGT;
+      const long p = pc + q;
+      cplx<R> va = mk<R>(0, 0), vb = mk<R>(0, 0);
+      if (p < p_end) {
+        if (m0 + j < M) {
+          const cplx<T> x = psi[p * ld + m0 + j];
+          va = mk<R>((R)x.x, (R)x.y);
+        }
+        if (n0 + j < M) {
+          const cplx<T> x = psi[p * ld + n0 + j];
+          vb = mk<R>((R)x.x, (R)x.y);
+        }
+      }
+      sA[q][j] = va;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) sB[d][q][j] = sW[d][q] * vb;
+    }
+    __syncthreads();
+    // FP32 products are summed over the chunk in FP32 (mixed) then added in FP64; the
+    // FP64 path accumulates straight into acc
+    constexpr bool kSplit = sizeof(R) == 4;
+    R part[3][2][2][2];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) part[d][a][b][0] = part[d][a][b][1] = (R)0;
+    auto& tgt = *reinterpret_cast<R(*)[3][2][2][2]>(kSplit ? (void*)part : (void*)acc);
+#pragma unroll 4
+    for (int q = 0; q < kGP; ++q) {
+      const cplx<R> a0 = sA[q][tm], a1 = sA[q][tm + 16];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const cplx<R> b0 = sB[d][q][tn], b1 = sB[d][q][tn + 16];
+        const cplx<R> av[2] = {a0, a1}, bv[2] = {b0, b1};
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b) {
+            // conj(a) * b
+            tgt[d][a][b][0] = fma(av[a].x, bv[b].x, fma(av[a].y, bv[b].y, tgt[d][a][b][0]));
+            tgt[d][a][b][1] = fma(av[a].x, bv[b].y, fma(-av[a].y, bv[b].x, tgt[d][a][b][1]));
+          }
+      }
+    }
+    if (kSplit) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b) {
+            acc[d][a][b][0] += (double)part[d][a][b][0];
+            acc[d][a][b][1] += (double)part[d][a][b][1];
+          }
+    }
+    __syncthreads();
+  }
+  // partial[slab][d][m][n]
+  const size_t MM = (size_t)M * M;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const int m = m0 + tm + 16 * a, n = n0 + tn + 16 * b;
+        if (m < M && n < M)
+          partial[((size_t)blockIdx.y * 3 + d) * MM + (size_t)m * M + n] = make_double2(acc[d][a][b][0], acc[d][a][b][1]);
+      }
+}
+
+// a[2d][m][n] = (Z + Z^H)/2, a[2d+1][m][n] = (Z - Z^H)/(2i), Z the slab sum divided by
+// |psi_m| |psi_n| (norm2[3 m + 2] = sum_p |psi_m|^2 from the band sums)
+__global__ void k_mlwf_finish(const double2* __restrict__ partial, int nslab, int M, const double* __restrict__ sums,
+                              double2* __restrict__ a) {
+  const size_t MM = (size_t)M * M;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < 3 * (long)MM; e += (long)gridDim.x * blockDim.x) {
+    const int d = (int)(e / MM);
+    const int m = (int)((e % MM) / M), n = (int)(e % M);
+    double2 z = make_double2(0, 0), zt = make_double2(0, 0);
+    for (int s = 0; s < nslab; ++s) {
+      const double2 x = partial[((size_t)s * 3 + d) * MM + (size_t)m * M + n];
+      const double2 y = partial[((size_t)s * 3 + d) * MM + (size_t)n * M + m];
+      z.x += x.x;
+      z.y += x.y;
+      zt.x += y.x;
+      zt.y += y.y;
+    }
+    const double sc = 1.0 / sqrt(sums[3 * m + 2] * sums[3 * n + 2]);
+    // conj(Z[n][m]) = (zt.x, -zt.y)
+    a[(2 * d) * MM + (size_t)m * M + n] = make_double2(0.5 * sc * (z.x + zt.x), 0.5 * sc * (z.y - zt.y));
+    // (Z - conj(Z^T)) / (2i): (u + i v) / (2i) = (v - i u) / 2 with u + i v = Z - conj(Z[n][m])
+    const double ur = z.x - zt.x, vi = z.y + zt.y;
+    a[(2 * d + 1) * MM + (size_t)m * M + n] = make_double2(0.5 * sc * vi, -0.5 * sc * ur);
+  }
+}
+
+// ------------------------------------------------------------------ jade
+// Symmetric 3x3 eigenproblem by cyclic Jacobi rotations (the method of
+// wannier/jacobi_eigenvalue.hpp; the oracle restates the same steps); returns the
+// eigenvector of the largest eigenvalue with the sign the iteration leaves.
+__device__ void jacobi3_top(double S[3][3], double out[3]) {
+  double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  double d[3] = {S[0][0], S[1][1], S[2][2]};
+  double base[3] = {d[0], d[1], d[2]};
+  double inc[3] = {0, 0, 0};
+  for (int pass = 1; pass <= 10000; pass++) {
+    double off = 0.0;
+    for (int q = 0; q < 3; q++)
+      for (int p = 0; p < q; p++) off += S[p][q] * S[p][q];
+    const double thresh = sqrt(off) / 12.0;
+    if (thresh == 0.0) break;
+    for (int p = 0; p < 3; p++)
+      for (int q = p + 1; q < 3; q++) {
+        const double big = 10.0 * fabs(S[p][q]);
+        if (pass > 4 && big + fabs(d[p]) == fabs(d[p]) && big + fabs(d[q]) == fabs(d[q])) {
+          S[p][q] = 0.0;
+          continue;
+        }
+        if (fabs(S[p][q]) < thresh) continue;
+        double h = d[q] - d[p];
+        double t;
+        if (fabs(h) + big == fabs(h)) {
+          t = S[p][q] / h;
+        } else {
+          const double theta = 0.5 * h / S[p][q];
+          t = 1.0 / (fabs(theta) + sqrt(1.0 + theta * theta));
+          if (theta < 0.0) t = -t;
+        }
+        const double c = 1.0 / sqrt(1.0 + t * t), s = t * c, tau = s / (1.0 + c);
+        h = t * S[p][q];
+        inc[p] -= h;
+        inc[q] += h;
+        d[p] -= h;
+        d[q] += h;
+        S[p][q] = 0.0;
+#define INQB_JROT(x, y)                   \
+  {                                       \
+    const double g_ = (x), h_ = (y);      \
+    (x) = g_ - s * (h_ + g_ * tau);       \
+    (y) = h_ + s * (g_ - h_ * tau);       \
+  }
+        for (int j = 0; j < p; j++) INQB_JROT(S[j][p], S[j][q])
+        for (int j = p + 1; j < q; j++) INQB_JROT(S[p][j], S[j][q])
+        for (int j = q + 1; j < 3; j++) INQB_JROT(S[p][j], S[q][j])
+        for (int j = 0; j < 3; j++) INQB_JROT(V[j][p], V[j][q])
+#undef INQB_JROT
+      }
+    for (int i = 0; i < 3; i++) {
+      base[i] += inc[i];
+      d[i] = base[i];
+      inc[i] = 0.0;
+    }
+  }
+  for (int k = 0; k < 2; k++) {
+    int m = k;
+    for (int l = k + 1; l < 3; l++)
+      if (d[l] < d[m]) m = l;
+    if (m != k) {
+      const double t = d[m];
+      d[m] = d[k];
+      d[k] = t;
+      for (int i = 0; i < 3; i++) {
+        const double v = V[i][m];
+        V[i][m] = V[i][k];
+        V[i][k] = v;
+      }
+    }
+  }
+  for (int i = 0; i < 3; i++) out[i] = V[i][2];
+}
+
+constexpr int kJT = 128;  // threads of a pair's CTA
+
+// one CTA per pair of this rotation step; a [6][M][M], u [M][M]
+__global__ void __launch_bounds__(kJT)
+    k_jade_step(double2* __restrict__ a, double2* __restrict__ u, int M, const int2* __restrict__ pairs,
+                double* __restrict__ delta) {
+  __shared__ double red[kJT / 32][36];
+  __shared__ double rot[3];  // c, Re s, Im s
+  __shared__ double old_diag;
+  const int2 pq = pairs[blockIdx.x];
+  const int p = pq.x, q = pq.y;
+  if (p >= M || q >= M) {
+    if (threadIdx.x == 0) delta[blockIdx.x] = 0.0;
+    return;
+  }
+  const size_t MM = (size_t)M * M;
+  // the 18 pair elements: (sum conj(a_k[p][i]) u[q][i], sum conj(a_k[p][i]) u[p][i],
+  // sum conj(a_k[q][i]) u[q][i]) for k < 6
+  double s[36];
+#pragma unroll
+  for (int i = 0; i < 36; ++i) s[i] = 0.0;
+  for (int i = threadIdx.x; i < M; i += blockDim.x) {
+    const double2 up = u[(size_t)p * M + i], uq = u[(size_t)q * M + i];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const double2 ap = cconj(a[k * MM + (size_t)p * M + i]), aq = cconj(a[k * MM + (size_t)q * M + i]);
+      const double2 x0 = cmul(ap, uq), x1 = cmul(ap, up), x2 = cmul(aq, uq);
+      s[6 * k + 0] += x0.x;
+      s[6 * k + 1] += x0.y;
+      s[6 * k + 2] += x1.x;
+      s[6 * k + 3] += x1.y;
+      s[6 * k + 4] += x2.x;
+      s[6 * k + 5] += x2.y;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 36; ++i)
+    for (int o = 16; o > 0; o >>= 1) s[i] += __shfl_down_sync(0xffffffffu, s[i], o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int i = 0; i < 36; ++i) red[w][i] = s[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    double od = 0.0;
+    for (int k = 0; k < 6; ++k) {
+      double e[6];
+      for (int i = 0; i < 6; ++i) {
+        double v = 0.0;
+        for (int ww = 0; ww < kJT / 32; ++ww) v += red[ww][6 * k + i];
+        e[i] = v;
+      }
+      const double2 aij = make_double2(e[0], e[1]), aii = make_double2(e[2], e[3]), ajj = make_double2(e[4], e[5]);
+      // h = (aii - ajj, aij + conj(aij), i (aij - conj(aij))) = (.., (2 Re aij, 0), (-2 Im aij, 0))
+      const double2 h[3] = {make_double2(aii.x - ajj.x, aii.y - ajj.y), make_double2(2.0 * aij.x, 0.0),
+                            make_double2(-2.0 * aij.y, 0.0)};
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) G[r][c] += h[r].x * h[c].x + h[r].y * h[c].y;
+      od += a[k * MM + (size_t)p * M + p].x + a[k * MM + (size_t)q * M + q].x;
+    }
+    double v[3];
+    jacobi3_top(G, v);
+    double x = v[0], y = v[1], z = v[2];
+    if (v[0] < 0.0) {
+      x = -x;
+      y = -y;
+    }
+    const double r = sqrt((x + 1.0) / 2.0);
+    rot[0] = r;
+    rot[1] = y / (2.0 * r);
+    rot[2] = -z / (2.0 * r);
+    old_diag = od;
+  }
+  __syncthreads();
+  const double c = rot[0];
+  const double2 sv = make_double2(rot[1], rot[2]), sc = cconj(sv);
+  // rows p, q of a_k and u: row_p <- c row_p + conj(s) row_q, row_q <- -s row_p + c row_q
+  for (int e = threadIdx.x; e < 7 * M; e += blockDim.x) {
+    const int k = e / M, i = e % M;
+    double2* base = (k < 6) ? a + k * MM : u;
+    double2& rp = base[(size_t)p * M + i];
+    double2& rq = base[(size_t)q * M + i];
+    const double2 xv = rp, yv = rq;
+    const double2 t1 = cmul(sc, yv), t2 = cmul(sv, xv);
+    rp = make_double2(c * xv.x + t1.x, c * xv.y + t1.y);
+    rq = make_double2(c * yv.x - t2.x, c * yv.y - t2.y);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double nd = 0.0;
+    for (int k = 0; k < 6; ++k) nd += a[k * MM + (size_t)p * M + p].x + a[k * MM + (size_t)q * M + q].x;
+    delta[blockIdx.x] = nd - old_diag;
+  }
+}
+
+// out = sum_steps 2 |sum_pairs delta[step][pair]| (one block, fixed order)
+__global__ void k_jade_change(const double* __restrict__ delta, int nsteps, int np, double* __restrict__ out) {
+  __shared__ double part[256];
+  double acc = 0.0;
+  for (int s = threadIdx.x; s < nsteps; s += blockDim.x) {
+    double t = 0.0;
+    for (int i = 0; i < np; ++i) t += delta[(size_t)s * np + i];
+    acc += 2.0 * fabs(t);
+  }
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < (int)blockDim.x; ++i) t += part[i];
+    out[0] = t;
+  }
+}
+
+__global__ void k_identity(double2* __restrict__ u, int M) {
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < (long)M * M; e += (long)gridDim.x * blockDim.x)
+    u[e] = make_double2((e / M == e % M) ? 1.0 : 0.0, 0.0);
+}
+
+// adiag[k][i] = sum_j conj(a_k[i][j]) u[i][j]; grid (M, 6)
+__global__ void __launch_bounds__(128)
+    k_jade_adiag(const double2* __restrict__ a, const double2* __restrict__ u, int M, double2* __restrict__ adiag) {
+  __shared__ double red[4][2];
+  const int i = blockIdx.x, k = blockIdx.y;
+  const size_t MM = (size_t)M * M;
+  double sr = 0.0, si = 0.0;
+  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+    const double2 x = cmul(cconj(a[k * MM + (size_t)i * M + j]), u[(size_t)i * M + j]);
+    sr += x.x;
+    si += x.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sr += __shfl_down_sync(0xffffffffu, sr, o);
+    si += __shfl_down_sync(0xffffffffu, si, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5][0] = sr;
+    red[threadIdx.x >> 5][1] = si;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0, im = 0.0;
+    for (int w = 0; w < 4; ++w) {
+      r += red[w][0];
+      im += red[w][1];
+    }
+    adiag[(size_t)k * M + i] = make_double2(r, im);
+  }
+}
+
+// ------------------------------------------------------------------ rotate
+// out[p][i] = sum_j psi[p][j] conj(u[i][j]); 64 x 64 output tiles, 256 threads with
+// 4 x 4 outputs each, j in chunks of 8 through shared memory.
+constexpr int kRT = 64, kRK = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_mlwf_rotate(const cplx<T>* __restrict__ psi, long ld, int M, long N, const double2* __restrict__ u,
+                  cplx<T>* __restrict__ out, long ldo) {
+  using R = T;
+  __shared__ cplx<R> sP[kRK][kRT + 1];  // [j][point]
+  __shared__ cplx<R> sU[kRK][kRT];      // [j][i] = conj(u[i][j])
+  const long p0 = (long)blockIdx.x * kRT;
+  const int i0 = blockIdx.y * kRT;
+  const int tp = threadIdx.x % 16, ti = threadIdx.x / 16;
+  cplx<R> acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = mk<R>(0, 0);
+  for (int j0 = 0; j0 < M; j0 += kRK) {
+    for (int e = threadIdx.x; e < kRK * kRT; e += blockDim.x) {
+      const int jj = e % kRK, pp = e / kRK;
+      const long p = p0 + pp;
+      const int j = j0 + jj;
+      sP[jj][pp] = (p < N && j < M) ? psi[p * ld + j] : mk<R>(0, 0);
+      const int ii = e / kRK;  // same decomposition for u: [i][j] rows
+      const int i = i0 + ii;
+      if (i < M && j < M) {
+        const double2 x = u[(size_t)i * M + j];
+        sU[jj][ii] = mk<R>((R)x.x, (R)(-x.y));
+      } else {
+        sU[jj][ii] = mk<R>(0, 0);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < kRK; ++jj) {
+      cplx<R> pv[4], uv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) pv[a] = sP[jj][tp + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) uv[b] = sU[jj][ti + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          acc[a][b].x = fma(pv[a].x, uv[b].x, fma(-pv[a].y, uv[b].y, acc[a][b].x));
+          acc[a][b].y = fma(pv[a].x, uv[b].y, fma(pv[a].y, uv[b].x, acc[a][b].y));
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const long p = p0 + tp + 16 * a;
+      const int i = i0 + ti + 16 * b;
+      if (p < N && i < M) out[p * ldo + i] = acc[a][b];
+    }
+}
+
+}  // namespace
+
+size_t mlwf_gram_slabs(long N, int M) {
+  const long tiles = (long)((M + kGT - 1) / kGT) * ((M + kGT - 1) / kGT);
+  const long chunks = (N + kGP - 1) / kGP;
+  return (size_t)std::max<long>(1, std::min<long>(chunks, (148L * 4 + tiles - 1) / tiles));
+}
+
+int launch_mlwf_gram(int precision, const void* psi, long ld, int M, long N, const int nr[3], const double lat[3][3],
+                     const double* sums, double2* partial, double2* a, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  GramGeom g;
+  double len[3];
+  for (int d = 0; d < 3; ++d) {
+    g.nr[d] = nr[d];
+    len[d] = sqrt(lat[d][0] * lat[d][0] + lat[d][1] * lat[d][1] + lat[d][2] * lat[d][2]);
+  }
+  // theta_d / pi = 2 r_d / |a_d|, r = sum_j f_j a_j
+  for (int d = 0; d < 3; ++d)
+    for (int j = 0; j < 3; ++j) g.frac_to_theta[d][j] = 2.0 * lat[j][d] / len[d];
+  const int tiles = (M + kGT - 1) / kGT;
+  const long slabs = (long)mlwf_gram_slabs(N, M);
+  const long per = ((N + slabs - 1) / slabs + kGP - 1) / kGP * kGP;
+  const long nslab = (N + per - 1) / per;
+  const dim3 grid((unsigned)(tiles * tiles), (unsigned)nslab);
+  if (precision == INQB_FP64)
+    k_mlwf_gram<double><<<grid, 256, 0, st>>>((const cplx<double>*)psi, ld, M, N, g, per, partial);
+  else
+    k_mlwf_gram<float><<<grid, 256, 0, st>>>((const cplx<float>*)psi, ld, M, N, g, per, partial);
+  INQB_CUDA_TRY(cudaGetLastError());
+  const long work = 3L * M * M;
+  k_mlwf_finish<<<(unsigned)std::min<long>((work + 255) / 256, 148L * 8), 256, 0, st>>>(partial, (int)nslab, M, sums,
+                                                                                         a);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_identity(double2* u, int M, void* stream) {
+  k_identity<<<(unsigned)std::min<long>(((long)M * M + 255) / 256, 1024), 256, 0, (cudaStream_t)stream>>>(u, M);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_jade_step(double2* a, double2* u, int M, const int2* pairs, int np, double* delta, void* stream) {
+  k_jade_step<<<np, kJT, 0, (cudaStream_t)stream>>>(a, u, M, pairs, delta);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_jade_change(const double* delta, int nsteps, int np, double* out, void* stream) {
+  k_jade_change<<<1, 256, 0, (cudaStream_t)stream>>>(delta, nsteps, np, out);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_jade_adiag(const double2* a, const double2* u, int M, double2* adiag, void* stream) {
+  k_jade_adiag<<<dim3(M, 6), 128, 0, (cudaStream_t)stream>>>(a, u, M, adiag);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_mlwf_rotate(int precision, const void* psi, long ld, int M, long N, const double2* u, void* out, long ldo,
+                       void* stream) {
+  const dim3 grid((unsigned)((N + kRT - 1) / kRT), (unsigned)((M + kRT - 1) / kRT));
+  if (precision == INQB_FP64)
+    k_mlwf_rotate<double><<<grid, 256, 0, (cudaStream_t)stream>>>((const cplx<double>*)psi, ld, M, N, u,
+                                                                   (cplx<double>*)out, ldo);
+  else
+    k_mlwf_rotate<float><<<grid, 256, 0, (cudaStream_t)stream>>>((const cplx<float>*)psi, ld, M, N, u,
+                                                                  (cplx<float>*)out, ldo);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+}  // namespace inqb

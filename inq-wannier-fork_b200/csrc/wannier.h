@@ -1,0 +1,27 @@
+// Launchers of the TD-MLWF kernels (wannier.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+namespace inqb {
+
+// Number of point slabs the Gram kernel splits N into for M states (partial sums
+// take slabs * 3 * M * M complex128).
+size_t mlwf_gram_slabs(long N, int M);
+// a [6][M][M] complex128: the six matrices of tdmlwf_trans::update from psi; sums[3 m + 2]
+// = sum_p |psi_m|^2 (band sums); partial: mlwf_gram_slabs * 3 * M * M complex128.
+int launch_mlwf_gram(int precision, const void* psi, long ld, int M, long N, const int nr[3], const double lat[3][3],
+                     const double* sums, double2* partial, double2* a, void* stream);
+int launch_identity(double2* u, int M, void* stream);
+// one JADE rotation step over np pairs (int2 top, bottom; indices >= M are skipped);
+// delta[np] receives each pair's change of sum_k trace(a_k)
+int launch_jade_step(double2* a, double2* u, int M, const int2* pairs, int np, double* delta, void* stream);
+int launch_jade_change(const double* delta, int nsteps, int np, double* out, void* stream);
+int launch_jade_adiag(const double2* a, const double2* u, int M, double2* adiag, void* stream);
+// out = psi u^H (out must not alias psi)
+int launch_mlwf_rotate(int precision, const void* psi, long ld, int M, long N, const double2* u, void* out, long ldo,
+                       void* stream);
+
+}  // namespace inqb

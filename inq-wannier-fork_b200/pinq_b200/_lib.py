@@ -72,6 +72,11 @@ SIGNATURES = {
                                           ctypes.c_int, _dp, _vp]),
     "inqb_save_density": (ctypes.c_int, [_ctxp, ctypes.c_char_p, _vp, _vp]),
     "inqb_load_density": (ctypes.c_int, [_ctxp, ctypes.c_char_p, _vp, _vp]),
+    "inqb_mlwf_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _ip,
+                                      _dp, _dp, _vp]),
+    "inqb_mlwf_matrices": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "inqb_jade": (ctypes.c_int, [_ctxp, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, ctypes.c_double, _ip, _vp]),
+    "inqb_mlwf_rotate": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "inqb_etrs_powers_size": (ctypes.c_int, [_ctxp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "inqb_etrs_step_powers": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
                                              _vp, _vp]),

@@ -294,6 +294,47 @@ class KSHamiltonian:
         call("inqb_load_density", self._h, os.fsencode(dirname), rho.data_ptr(), self._stream())
         return rho
 
+    # -- TD-MLWF (wannier/tdmlwf_trans.hpp, observables/mlwf_properties.hpp)
+    def mlwf_step_(self, psi, maxsweep=100, tol=1e-8):
+        """update + compute_transform + apply_transform: psi is rotated in place to the
+        maximally localised gauge; returns (centres [M, 3], spreads [M], JADE sweeps)."""
+        psi = self._check(psi)
+        M = psi.shape[1]
+        centres = np.zeros((M, 3))
+        spreads = np.zeros(M)
+        sw = ctypes.c_int(0)
+        call("inqb_mlwf_step", self._h, psi.data_ptr(), M, psi.stride(0), int(maxsweep), float(tol), ctypes.byref(sw),
+             dptr(centres), dptr(spreads), self._stream())
+        return centres, spreads, sw.value
+
+    def mlwf_matrices(self, psi):
+        """The six [M, M] complex128 matrices of tdmlwf_trans::update (a CUDA tensor)."""
+        psi = self._check(psi)
+        M = psi.shape[1]
+        a = torch.empty((6, M, M), dtype=torch.complex128, device=self.device)
+        call("inqb_mlwf_matrices", self._h, psi.data_ptr(), M, psi.stride(0), a.data_ptr(), self._stream())
+        return a
+
+    def jade(self, a, maxsweep=100, tol=1e-8):
+        """jade_complex on a [6, M, M] complex128 CUDA tensor (rotated in place);
+        returns (u, adiag, sweeps)."""
+        if a.dtype != torch.complex128 or a.device.type != "cuda" or not a.is_contiguous() or a.shape[0] != 6:
+            raise TypeError("a must be a contiguous [6, M, M] complex128 CUDA tensor")
+        M = a.shape[1]
+        u = torch.empty((M, M), dtype=torch.complex128, device=self.device)
+        adiag = torch.empty((6, M), dtype=torch.complex128, device=self.device)
+        sw = ctypes.c_int(0)
+        call("inqb_jade", self._h, M, a.data_ptr(), u.data_ptr(), adiag.data_ptr(), int(maxsweep), float(tol),
+             ctypes.byref(sw), self._stream())
+        return u, adiag, sw.value
+
+    def mlwf_rotate_(self, psi, u):
+        """psi <- psi u^H (operations::rotate) with u an [M, M] complex128 CUDA tensor."""
+        psi = self._check(psi)
+        u = u.contiguous()
+        call("inqb_mlwf_rotate", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), u.data_ptr(), self._stream())
+        return psi
+
     def exponential_(self, psi, factor, order=4):
         """psi <- sum_k (factor H)^k / k! psi (in place)."""
         psi = self._check(psi)

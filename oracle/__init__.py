@@ -78,6 +78,10 @@ def lib():
         L.orc_etrs_scf_step.restype = ctypes.c_int
         L.orc_etrs_scf_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp, _dp,
                                         ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
+        L.orc_mlwf_matrices.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.orc_jade.restype = ctypes.c_int
+        L.orc_jade.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]
+        L.orc_mlwf_rotate.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -293,6 +297,23 @@ class System:
         b = np.ascontiguousarray(b, np.float64).ravel()
         return lib().orc_integral_sum_absdiff(self._h, a.size, _d(a), _d(b))
 
+    # ---- TD-MLWF (wannier/tdmlwf_trans.hpp)
+
+    def mlwf_matrices(self, psi):
+        """tdmlwf_trans::update: the six [M][M] matrices of the normalised states."""
+        psi = self._psi(psi)
+        M = psi.shape[1]
+        a = np.zeros((6, M, M), np.complex128)
+        lib().orc_mlwf_matrices(self._h, M, _d(psi.view(np.float64)), _d(a.view(np.float64)))
+        return a
+
+    def mlwf_rotate(self, psi, u):
+        """apply_transform: psi u^H (operations::rotate)."""
+        out = self._psi(psi).copy()
+        u = np.ascontiguousarray(u, np.complex128)
+        lib().orc_mlwf_rotate(self._h, out.shape[1], _d(out.view(np.float64)), _d(u.view(np.float64)))
+        return out
+
     def etrs_scf_step(self, psi, rho, dt, kA_t, kA_tdt, occ, vion, theory, nscf=5, threshold=5e-5):
         """ETRS with its SCF loop (etrs.hpp:22-82).  The potential must already be the
         Kohn-Sham potential of rho.  Returns (psi, rho, scf iterations, energies)."""
@@ -344,3 +365,37 @@ def load_orbitals_layout(dirname, N, M, kpin=0, first_state=0):
         psi[:, j] = np.fromfile(os.path.join(kdir, "states", name), dtype=np.complex128, count=N)
     occ = np.fromfile(os.path.join(kdir, "occupations", "array"), dtype=np.float64)[first_state:first_state + M]
     return psi, occ
+
+
+# ---- TD-MLWF (wannier/jade_complex.hpp, tdmlwf_trans.hpp:196-330)
+
+def jade(a, maxsweep=100, tol=1e-8):
+    """jade_complex: (a rotated, u, adiag, sweeps) for a [6][M][M] complex."""
+    a = np.ascontiguousarray(a, np.complex128).copy()
+    M = a.shape[1]
+    u = np.zeros((M, M), np.complex128)
+    adiag = np.zeros((6, M), np.complex128)
+    sw = lib().orc_jade(int(maxsweep), float(tol), M, _d(a.view(np.float64)), _d(u.view(np.float64)),
+                        _d(adiag.view(np.float64)))
+    return a, u, adiag, sw
+
+
+def mlwf_center(adiag, i, lattice):
+    """tdmlwf_trans::center (tdmlwf_trans.hpp:196-220): t_d = atan2(Re s_d, Re c_d) / 2 pi,
+    r = L t with L's rows the lattice vectors, as the reference writes it."""
+    L = np.asarray(lattice, float).reshape(3, 3)
+    t = [np.arctan2(adiag[2 * d + 1][i].real, adiag[2 * d][i].real) / (2 * np.pi) for d in range(3)]
+    return np.array([t[0] * L[0, 0] + t[1] * L[0, 1] + t[2] * L[0, 2],
+                     t[0] * L[1, 0] + t[1] * L[1, 1] + t[2] * L[1, 2],
+                     t[0] * L[2, 0] + t[1] * L[2, 1] + t[2] * L[2, 2]])
+
+
+def mlwf_spread(adiag, i, lattice):
+    """tdmlwf_trans::spread (tdmlwf_trans.hpp:286-312): sqrt(sum_d (1 - |c_d|^2 - |s_d|^2) / |b_d|^2)."""
+    L = np.asarray(lattice, float).reshape(3, 3)
+    B = 2 * np.pi * np.linalg.inv(L).T  # rows: reciprocal vectors (cell.hpp:50-52)
+    s2 = 0.0
+    for d in range(3):
+        c, s = adiag[2 * d][i], adiag[2 * d + 1][i]
+        s2 += (1.0 - abs(c) ** 2 - abs(s) ** 2) / (B[d] @ B[d])
+    return np.sqrt(s2)

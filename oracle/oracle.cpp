@@ -47,6 +47,9 @@
 //                                                  src/hamiltonian/xc_term.hpp:63-142,276-323
 //   * exponential_2_for_1, ETRS with SCF loop      src/operations/exponential.hpp:50-69,
 //                                                  src/real_time/etrs.hpp:22-82
+//   * TD-MLWF matrices, JADE, rotation, centres    src/wannier/tdmlwf_trans.hpp:63-346,
+//                                                  src/wannier/jade_complex.hpp:32-335,
+//                                                  src/observables/mlwf_properties.hpp:28-44
 //
 // Third-party arithmetic the reference delegates (not vendored in the snapshot):
 //   * boost-multi FFT adaptors -> FFTW3 / cuFFT (pinned version unknown): restated
@@ -648,6 +651,250 @@ void exponential_2_for_1(const System &s, int M, cd f1, cd f2, cd *phi, cd *out)
   }
 }
 
+// ---------------------------------------------------------------------------
+// TD-MLWF: the Wannier transformation the fork applies after each real-time step
+// (observables/mlwf_properties.hpp:28-44, wannier/tdmlwf_trans.hpp,
+// wannier/jade_complex.hpp).
+// ---------------------------------------------------------------------------
+
+// tdmlwf_trans::update (tdmlwf_trans.hpp:63-172): on copies of the states normalised
+// to sum_p |psi|^2 = 1 (no volume element), a[k][m][n] = sum_p conj(psi_m) psi_n t_k
+// with t = cos, sin of 2 pi x/|a0|, 2 pi y/|a1|, 2 pi z/|a2| (cartesian grid coordinates
+// in the symmetric range, |a_d| the lattice vector lengths).  a: [6][M][M].
+void mlwf_matrices(const Grid &g, int M, const cd *psi, cd *a) {
+  const long N = g.npoints;
+  std::vector<double> nrm(M, 0.0);
+  for (long p = 0; p < N; p++)
+    for (int m = 0; m < M; m++) nrm[m] += std::norm(psi[p * M + m]);
+  for (int m = 0; m < M; m++) nrm[m] = 1.0 / std::sqrt(nrm[m]);
+  double len[3];
+  for (int d = 0; d < 3; d++) len[d] = std::sqrt(dot(g.cell.lat[d], g.cell.lat[d]));
+  std::fill(a, a + (size_t)6 * M * M, cd(0.0));
+#pragma omp parallel for schedule(dynamic)
+  for (int m = 0; m < M; m++) {
+    std::vector<cd> acc((size_t)6 * M, 0.0);
+    for (int ix = 0; ix < g.nr[0]; ix++)
+      for (int iy = 0; iy < g.nr[1]; iy++)
+        for (int iz = 0; iz < g.nr[2]; iz++) {
+          const v3 r = g.rvector_cart(ix, iy, iz);
+          double t[6];
+          for (int d = 0; d < 3; d++) {
+            t[2 * d] = std::cos(2.0 * M_PI * r[d] / len[d]);
+            t[2 * d + 1] = std::sin(2.0 * M_PI * r[d] / len[d]);
+          }
+          const long p = g.linear(ix, iy, iz);
+          const cd cm = std::conj(psi[p * M + m]) * nrm[m];
+          for (int n = 0; n < M; n++) {
+            const cd x = cm * psi[p * M + n] * nrm[n];
+            for (int k = 0; k < 6; k++) acc[(size_t)k * M + n] += x * t[k];
+          }
+        }
+    for (int k = 0; k < 6; k++)
+      for (int n = 0; n < M; n++) a[((size_t)k * M + m) * M + n] = acc[(size_t)k * M + n];
+  }
+}
+
+// Eigen-decomposition of a symmetric 3x3 matrix by cyclic Jacobi rotations, the
+// published method jade_complex uses (wannier/jacobi_eigenvalue.hpp, John Burkardt's
+// jacobi_eigenvalue after Numerical Recipes): each pass sets the threshold
+// sqrt(sum_{p<q} s_pq^2) / 12; after four passes an element negligible beside both
+// diagonal entries is zeroed; otherwise an element at or above the threshold is
+// rotated away with t = sgn(theta) / (|theta| + sqrt(1 + theta^2)) (or s_pq / h when h
+// dwarfs it), updating the off-diagonal upper triangle and the eigenvector columns
+// through tau = s / (1 + c); diagonal increments are gathered per pass.  Returns the
+// eigenvector of the largest eigenvalue (column 2 after the ascending sort), with the
+// sign the iteration leaves on it.
+void jacobi3_top_vector(double S[3][3], double out[3]) {
+  double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  double d[3] = {S[0][0], S[1][1], S[2][2]};
+  double base[3] = {d[0], d[1], d[2]};
+  double inc[3] = {0, 0, 0};
+  for (int pass = 1; pass <= 10000; pass++) {
+    double off = 0.0;
+    for (int q = 0; q < 3; q++)
+      for (int p = 0; p < q; p++) off += S[p][q] * S[p][q];
+    const double thresh = std::sqrt(off) / 12.0;
+    if (thresh == 0.0) break;
+    for (int p = 0; p < 3; p++)
+      for (int q = p + 1; q < 3; q++) {
+        const double big = 10.0 * std::fabs(S[p][q]);
+        if (pass > 4 && big + std::fabs(d[p]) == std::fabs(d[p]) && big + std::fabs(d[q]) == std::fabs(d[q])) {
+          S[p][q] = 0.0;
+          continue;
+        }
+        if (std::fabs(S[p][q]) < thresh) continue;
+        double h = d[q] - d[p];
+        double t;
+        if (std::fabs(h) + big == std::fabs(h)) {
+          t = S[p][q] / h;
+        } else {
+          const double theta = 0.5 * h / S[p][q];
+          t = 1.0 / (std::fabs(theta) + std::sqrt(1.0 + theta * theta));
+          if (theta < 0.0) t = -t;
+        }
+        const double c = 1.0 / std::sqrt(1.0 + t * t), s = t * c, tau = s / (1.0 + c);
+        h = t * S[p][q];
+        inc[p] -= h;
+        inc[q] += h;
+        d[p] -= h;
+        d[q] += h;
+        S[p][q] = 0.0;
+        auto rot = [s, tau](double &x, double &y) {
+          const double g = x, hh = y;
+          x = g - s * (hh + g * tau);
+          y = hh + s * (g - hh * tau);
+        };
+        for (int j = 0; j < p; j++) rot(S[j][p], S[j][q]);
+        for (int j = p + 1; j < q; j++) rot(S[p][j], S[j][q]);
+        for (int j = q + 1; j < 3; j++) rot(S[p][j], S[q][j]);
+        for (int j = 0; j < 3; j++) rot(V[j][p], V[j][q]);
+      }
+    for (int i = 0; i < 3; i++) {
+      base[i] += inc[i];
+      d[i] = base[i];
+      inc[i] = 0.0;
+    }
+  }
+  // ascending selection sort of the eigenvalues, columns of V follow
+  for (int k = 0; k < 2; k++) {
+    int m = k;
+    for (int l = k + 1; l < 3; l++)
+      if (d[l] < d[m]) m = l;
+    if (m != k) {
+      std::swap(d[m], d[k]);
+      for (int i = 0; i < 3; i++) std::swap(V[i][m], V[i][k]);
+    }
+  }
+  for (int i = 0; i < 3; i++) out[i] = V[i][2];
+}
+
+// The plane rotation of one pair from its 3 x 6 matrix elements (jade_complex.hpp:
+// 103-280): apq[k] = (a_pq, a_pp, a_qq) of matrix k as the reference forms them;
+// G = sum_k Re(conj(h) h^T) with h = (a_pp - a_qq, a_pq + conj(a_pq), i (a_pq - conj(a_pq)));
+// (x, y, z) its top eigenvector, with x and y negated when x < 0; c = sqrt((x + 1) / 2),
+// s = (y - i z) / (2 c).
+void jade_pair_rotation(const cd apq[6][3], double &c, cd &s) {
+  double G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int k = 0; k < 6; k++) {
+    const cd aij = apq[k][0], aii = apq[k][1], ajj = apq[k][2];
+    const cd h[3] = {aii - ajj, aij + std::conj(aij), cd(0.0, 1.0) * (aij - std::conj(aij))};
+    for (int r = 0; r < 3; r++)
+      for (int q = 0; q < 3; q++) G[r][q] += (std::conj(h[r]) * h[q]).real();
+  }
+  double v[3];
+  jacobi3_top_vector(G, v);
+  double x = v[0], y = v[1], z = v[2];
+  if (v[0] < 0.0) {
+    x = -x;
+    y = -y;
+  }
+  const double r = std::sqrt((x + 1.0) / 2.0);
+  c = r;
+  s = cd(y / (2.0 * r), -z / (2.0 * r));
+}
+
+// Round-robin pairing of jade_complex (jade_complex.hpp:52-61,296-322): pair i is
+// (top[i], bot[i]); after each rotation step the arrays shift as one parallel move
+// (bot[j] <- bot[j+1], top[j+1] <- top[j]), the old top[np-1] goes to bot[np-1] and
+// the old bot[0] to top[0], then top[0] <-> top[1] (or top[0] <-> bot[0] when np = 1).
+void jade_shift_pairs(std::vector<int> &top, std::vector<int> &bot) {
+  const int np = (int)top.size();
+  if (np == 0) return;
+  const int top_back = top[np - 1], bot_front = bot[0];
+  std::vector<int> t2 = top, b2 = bot;
+  for (int j = 0; j + 1 < np; j++) {
+    b2[j] = bot[j + 1];
+    t2[j + 1] = top[j];
+  }
+  b2[np - 1] = top_back;
+  t2[0] = bot_front;
+  if (np > 1)
+    std::swap(t2[0], t2[1]);
+  else
+    std::swap(t2[0], b2[0]);
+  top = t2;
+  bot = b2;
+}
+
+// jade_complex (jade_complex.hpp:32-335): joint approximate diagonalisation of the
+// six M x M matrices a ([6][M][M], rotated in place: a_k <- R a_k, as the reference
+// does), u ([M][M]) the accumulated rotation, adiag[k][i] = sum_j conj(a_k[i][j]) u[i][j].
+// Each step rotates every pair with the pair elements taken as
+// (sum_i conj(a_k[p][i]) u[q][i], sum_i conj(a_k[p][i]) u[p][i], sum_i conj(a_k[q][i]) u[q][i]);
+// a sweep is 2 np - 1 steps and ends when 2 sum_steps |change of sum_k trace(a_k)| < tol
+// or maxsweep sweeps ran.  Returns the sweeps run.
+int jade(int maxsweep, double tol, int M, cd *a, cd *u, cd *adiag) {
+  for (int i = 0; i < M; i++)
+    for (int j = 0; j < M; j++) u[(size_t)i * M + j] = (i == j) ? 1.0 : 0.0;
+  const int np = (M + 1) / 2;
+  std::vector<int> top(np), bot(np);
+  for (int i = 0; i < np; i++) {
+    top[i] = i;
+    bot[np - i - 1] = np + i;
+  }
+  auto trace = [&]() {
+    double s = 0.0;
+    for (int k = 0; k < 6; k++)
+      for (int i = 0; i < M; i++) s += a[((size_t)k * M + i) * M + i].real();
+    return s;
+  };
+  int nsweep = 0;
+  bool done = false;
+  std::vector<double> cs(np);
+  std::vector<cd> ss(np);
+  while (!done) {
+    ++nsweep;
+    double change = 0.0;
+    for (int step = 0; step < 2 * np - 1; step++) {
+      const double t0 = trace();
+      for (int ip = 0; ip < np; ip++) {
+        const int p = top[ip], q = bot[ip];
+        if (p >= M || q >= M) continue;
+        cd apq[6][3];
+        for (int k = 0; k < 6; k++) {
+          cd s0 = 0.0, s1 = 0.0, s2 = 0.0;
+          const cd *ap = &a[((size_t)k * M + p) * M], *aq = &a[((size_t)k * M + q) * M];
+          for (int i = 0; i < M; i++) {
+            s0 += std::conj(ap[i]) * u[(size_t)q * M + i];
+            s1 += std::conj(ap[i]) * u[(size_t)p * M + i];
+            s2 += std::conj(aq[i]) * u[(size_t)q * M + i];
+          }
+          apq[k][0] = s0;
+          apq[k][1] = s1;
+          apq[k][2] = s2;
+        }
+        jade_pair_rotation(apq, cs[ip], ss[ip]);
+      }
+      // R: R[p][p] = R[q][q] = c, R[p][q] = conj(s), R[q][p] = -s; rows p, q of every a_k and u
+      for (int ip = 0; ip < np; ip++) {
+        const int p = top[ip], q = bot[ip];
+        if (p >= M || q >= M) continue;
+        const double c = cs[ip];
+        const cd s = ss[ip];
+        auto rows = [&](cd *rp, cd *rq) {
+          for (int i = 0; i < M; i++) {
+            const cd x = rp[i], y = rq[i];
+            rp[i] = c * x + std::conj(s) * y;
+            rq[i] = -s * x + c * y;
+          }
+        };
+        for (int k = 0; k < 6; k++) rows(&a[((size_t)k * M + p) * M], &a[((size_t)k * M + q) * M]);
+        rows(&u[(size_t)p * M], &u[(size_t)q * M]);
+      }
+      change += 2.0 * std::fabs(trace() - t0);
+      jade_shift_pairs(top, bot);
+    }
+    done = (std::fabs(change) < tol) || (nsweep >= maxsweep);
+  }
+  for (int k = 0; k < 6; k++)
+    for (int i = 0; i < M; i++) {
+      cd s = 0.0;
+      for (int j = 0; j < M; j++) s += std::conj(a[((size_t)k * M + i) * M + j]) * u[(size_t)i * M + j];
+      adiag[(size_t)k * M + i] = s;
+    }
+  return nsweep;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -977,6 +1224,33 @@ int orc_etrs_scf_step(void *h, int M, double dt, const double *kA_t, const doubl
     if (done) break;
   }
   return iters;
+}
+
+// tdmlwf_trans::update: a [6][M][M] complex
+void orc_mlwf_matrices(void *h, int M, const double *psi, double *a) {
+  mlwf_matrices(((System *)h)->grid, M, (const cd *)psi, (cd *)a);
+}
+
+// jade_complex on a [6][M][M] (rotated in place), u [M][M], adiag [6][M]; returns sweeps
+int orc_jade(int maxsweep, double tol, int M, double *a, double *u, double *adiag) {
+  return jade(maxsweep, tol, M, (cd *)a, (cd *)u, (cd *)adiag);
+}
+
+// tdmlwf_trans::apply_transform = operations::rotate(u, phi): phi <- phi u^H
+// (operations/rotate.hpp:61)
+void orc_mlwf_rotate(void *h, int M, double *psi_, const double *u_) {
+  auto *s = (System *)h;
+  cd *psi = (cd *)psi_;
+  const cd *u = (const cd *)u_;
+#pragma omp parallel for
+  for (long p = 0; p < s->grid.npoints; p++) {
+    std::vector<cd> row(psi + p * M, psi + p * M + M);
+    for (int i = 0; i < M; i++) {
+      cd acc = 0.0;
+      for (int j = 0; j < M; j++) acc += row[j] * std::conj(u[(size_t)i * M + j]);
+      psi[p * M + i] = acc;
+    }
+  }
 }
 
 int orc_num_threads() {
