@@ -255,7 +255,7 @@ struct MlwfWork {
   double2* u = nullptr;      // [M][M]
   double2* adiag = nullptr;  // [6][M]
   double* sums = nullptr;    // [3 M] band sums
-  double2* partial = nullptr;
+  void* partial = nullptr;   // per-slab Gram partial sums
   int2* pairs = nullptr;     // [2 np - 1][np]
   double* delta = nullptr;   // [2 np - 1][np]
   double* change = nullptr;  // [1]
@@ -263,7 +263,7 @@ struct MlwfWork {
 
 int mlwf_work(inqb_ctx* ctx, int M, bool with_gram, MlwfWork& w) {
   const size_t MM = (size_t)M * M, np = (size_t)(M + 1) / 2, steps = 2 * np - 1;
-  const size_t slabs = with_gram ? mlwf_gram_slabs(ctx->N, M) : 0;
+  const size_t partial_bytes = with_gram ? mlwf_partial_bytes(ctx->N, M) : 0;
   size_t off = 0;
   auto take = [&off](size_t bytes) {
     const size_t at = off;
@@ -272,7 +272,7 @@ int mlwf_work(inqb_ctx* ctx, int M, bool with_gram, MlwfWork& w) {
   };
   const size_t oa = take(sizeof(double2) * 6 * MM), ou = take(sizeof(double2) * MM),
                od = take(sizeof(double2) * 6 * M), os = take(sizeof(double) * 3 * M),
-               op = take(sizeof(double2) * slabs * 3 * MM), opr = take(sizeof(int2) * steps * np),
+               op = take(partial_bytes), opr = take(sizeof(int2) * steps * np),
                ode = take(sizeof(double) * steps * np), oc = take(sizeof(double));
   INQB_TRY(ctx->d_mlwf.ensure(off));
   char* b = static_cast<char*>(ctx->d_mlwf.ptr);
@@ -280,7 +280,7 @@ int mlwf_work(inqb_ctx* ctx, int M, bool with_gram, MlwfWork& w) {
   w.u = reinterpret_cast<double2*>(b + ou);
   w.adiag = reinterpret_cast<double2*>(b + od);
   w.sums = reinterpret_cast<double*>(b + os);
-  w.partial = reinterpret_cast<double2*>(b + op);
+  w.partial = b + op;
   w.pairs = reinterpret_cast<int2*>(b + opr);
   w.delta = reinterpret_cast<double*>(b + ode);
   w.change = reinterpret_cast<double*>(b + oc);

@@ -3,8 +3,8 @@
 // src/wannier/jade_complex.hpp).
 //
 //   gram     split over points: Z_d[m][n] = sum_p conj(psi_m) e^{i theta_d} psi_n for the
-//            three directions (theta_d = 2 pi r_d / |a_d|), per-slab partial sums in
-//            FP64 (FP32 products summed over 16-point chunks in the mixed precision)
+//            three directions (theta_d = 2 pi r_d / |a_d|), one partial per slab of points
+//            (FP64 slabs in FP64; FP32 slabs of 1024 points in the mixed precision)
 //   finish   sum of the slabs, normalisation 1/(|psi_m| |psi_n|), and the six matrices
 //            of tdmlwf_trans::update: cos = (Z + Z^H)/2, sin = (Z - Z^H)/(2i)
 //   jade     one CTA per pair and rotation step: the 18 pair elements, the 3 x 3
@@ -33,47 +33,60 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 
 // ------------------------------------------------------------------ gram
-constexpr int kGT = 32;  // output tile (m and n)
-constexpr int kGP = 16;  // points per staged chunk (static shared memory stays under 48 KB)
+// 256 threads as 16 x 16; thread (tm, tn) holds outputs m = m0 + tm + 16 a (a < TMX),
+// n = n0 + tn + 16 b (b < TNX) for the three directions; CTA tile (16 TMX) x (16 TNX).
+// FP64 contexts accumulate in FP64 over the CTA's slab (few slabs).  The mixed context
+// accumulates FP32 products in FP32 over a slab of at most kSlabF32 points and keeps one
+// FP32 partial per slab; the finish kernel adds the slabs in FP64 (the FP32 rounding of
+// a slab sum is about 6e-8 sqrt(kSlabF32) of its size, about 1e-7 of the total after the
+// FP64 sum over slabs).  Freeing the FP64 registers lets the FP32 tile be 4 x 2.
+constexpr long kSlabF32 = 1024;    // points per slab in the mixed precision
 
 struct GramGeom {
   int nr[3];
-  double frac_to_theta[3][3];  // theta_d = 2 pi sum_j f_j a_j[d] / |a_d|
+  double frac_to_theta[3][3];  // theta_d / pi = sum_j f_j frac_to_theta[d][j]
 };
 
 template <typename T>
-struct GramAcc;
+struct GramCfg;
 template <>
-struct GramAcc<double> {
-  using R = double;
+struct GramCfg<double> {
+  static constexpr int TMX = 2, TNX = 2, GP = 16, MINB = 2;  // GP: points per staged chunk
+  using P = double2;                                         // partial type
 };
 template <>
-struct GramAcc<float> {
-  using R = float;
+struct GramCfg<float> {
+  static constexpr int TMX = 4, TNX = 2, GP = 32, MINB = 3;
+  using P = float2;
 };
 
-// grid (tiles_m * tiles_n, ksplit); 256 threads as 16 x 16, each 2 x 2 outputs x 3 directions
+__device__ __forceinline__ void store_partial(double2* p, double x, double y) { *p = make_double2(x, y); }
+__device__ __forceinline__ void store_partial(float2* p, float x, float y) { *p = make_float2(x, y); }
+
+// grid (tiles_m * tiles_n, nslab)
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, GramCfg<T>::MINB)
     k_mlwf_gram(const cplx<T>* __restrict__ psi, long ld, int M, long N, GramGeom geo, long pts_per_slab,
-                double2* __restrict__ partial) {
-  using R = typename GramAcc<T>::R;
-  __shared__ cplx<R> sA[kGP][kGT];
-  __shared__ cplx<R> sB[3][kGP][kGT];
+                typename GramCfg<T>::P* __restrict__ partial) {
+  using R = T;
+  constexpr int TMX = GramCfg<T>::TMX, TNX = GramCfg<T>::TNX, kGP = GramCfg<T>::GP;
+  constexpr int TILE_M = 16 * TMX, TILE_N = 16 * TNX;
+  __shared__ cplx<R> sA[kGP][TILE_M];
+  __shared__ cplx<R> sB[3][kGP][TILE_N];
   __shared__ cplx<R> sW[3][kGP];
-  const int tiles = (M + kGT - 1) / kGT;
-  const int m0 = (blockIdx.x % tiles) * kGT, n0 = (blockIdx.x / tiles) * kGT;
+  const int tiles_m = (M + TILE_M - 1) / TILE_M;
+  const int m0 = (blockIdx.x % tiles_m) * TILE_M, n0 = (blockIdx.x / tiles_m) * TILE_N;
   const long p_beg = (long)blockIdx.y * pts_per_slab, p_end = min(N, p_beg + pts_per_slab);
   const int tm = threadIdx.x % 16, tn = threadIdx.x / 16;
-  double acc[3][2][2][2];
+  R acc[3][TMX][TNX][2];
 #pragma unroll
   for (int d = 0; d < 3; ++d)
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < TMX; ++a)
 #pragma unroll
-      for (int b = 0; b < 2; ++b) acc[d][a][b][0] = acc[d][a][b][1] = 0.0;
+      for (int b = 0; b < TNX; ++b) acc[d][a][b][0] = acc[d][a][b][1] = (R)0;
   for (long pc = p_beg; pc < p_end; pc += kGP) {
-    // weights of the chunk's points
+    // weights of the chunk's points, e^{i theta_d}
     if (threadIdx.x < kGP) {
       const long p = pc + threadIdx.x;
       cplx<R> w[3] = {mk<R>(0, 0), mk<R>(0, 0), mk<R>(0, 0)};
@@ -83,12 +96,12 @@ __global__ void __launch_bounds__(256)
         const int id[3] = {ix, iy, iz};
         double f[3];
         for (int j = 0; j < 3; ++j) {
-          const int s = (id[j] >= (geo.nr[j] + 1) / 2) ? id[j] - geo.nr[j] : id[j];
-          f[j] = (double)s / geo.nr[j];
+          const int sy = (id[j] >= (geo.nr[j] + 1) / 2) ? id[j] - geo.nr[j] : id[j];
+          f[j] = (double)sy / geo.nr[j];
         }
         for (int d = 0; d < 3; ++d) {
           const double th = geo.frac_to_theta[d][0] * f[0] + geo.frac_to_theta[d][1] * f[1] +
-                            geo.frac_to_theta[d][2] * f[2];  // in units of pi
+                            geo.frac_to_theta[d][2] * f[2];
           double sn, cs;
           sincospi(th, &sn, &cs);
           w[d] = mk<R>((R)cs, (R)sn);
@@ -97,63 +110,38 @@ __global__ void __launch_bounds__(256)
       for (int d = 0; d < 3; ++d) sW[d][threadIdx.x] = w[d];
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kGP * kGT; i += blockDim.x) {
-      const int q = i / kGT, j = i % kGT;
+    for (int i = threadIdx.x; i < kGP * TILE_M; i += blockDim.x) {
+      const int q = i / TILE_M, j = i % TILE_M;
       const long p = pc + q;
-      cplx<R> va = mk<R>(0, 0), vb = mk<R>(0, 0);
-      if (p < p_end) {
-        if (m0 + j < M) {
-          const cplx<T> x = psi[p * ld + m0 + j];
-          va = mk<R>((R)x.x, (R)x.y);
-        }
-        if (n0 + j < M) {
-          const cplx<T> x = psi[p * ld + n0 + j];
-          vb = mk<R>((R)x.x, (R)x.y);
-        }
-      }
-      sA[q][j] = va;
+      sA[q][j] = (p < p_end && m0 + j < M) ? psi[p * ld + m0 + j] : mk<R>(0, 0);
+    }
+    for (int i = threadIdx.x; i < kGP * TILE_N; i += blockDim.x) {
+      const int q = i / TILE_N, j = i % TILE_N;
+      const long p = pc + q;
+      const cplx<R> vb = (p < p_end && n0 + j < M) ? psi[p * ld + n0 + j] : mk<R>(0, 0);
 #pragma unroll
       for (int d = 0; d < 3; ++d) sB[d][q][j] = sW[d][q] * vb;
     }
     __syncthreads();
-    // FP32 products are summed over the chunk in FP32 (mixed) then added in FP64; the
-    // FP64 path accumulates straight into acc
-    constexpr bool kSplit = sizeof(R) == 4;
-    R part[3][2][2][2];
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) part[d][a][b][0] = part[d][a][b][1] = (R)0;
-    auto& tgt = *reinterpret_cast<R(*)[3][2][2][2]>(kSplit ? (void*)part : (void*)acc);
-#pragma unroll 4
+#pragma unroll 2
     for (int q = 0; q < kGP; ++q) {
-      const cplx<R> a0 = sA[q][tm], a1 = sA[q][tm + 16];
+      cplx<R> av[TMX];
+#pragma unroll
+      for (int a = 0; a < TMX; ++a) av[a] = sA[q][tm + 16 * a];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const cplx<R> b0 = sB[d][q][tn], b1 = sB[d][q][tn + 16];
-        const cplx<R> av[2] = {a0, a1}, bv[2] = {b0, b1};
+        cplx<R> bv[TNX];
 #pragma unroll
-        for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < TNX; ++b) bv[b] = sB[d][q][tn + 16 * b];
 #pragma unroll
-          for (int b = 0; b < 2; ++b) {
+        for (int a = 0; a < TMX; ++a)
+#pragma unroll
+          for (int b = 0; b < TNX; ++b) {
             // conj(a) * b
-            tgt[d][a][b][0] = fma(av[a].x, bv[b].x, fma(av[a].y, bv[b].y, tgt[d][a][b][0]));
-            tgt[d][a][b][1] = fma(av[a].x, bv[b].y, fma(-av[a].y, bv[b].x, tgt[d][a][b][1]));
+            acc[d][a][b][0] = fma(av[a].x, bv[b].x, fma(av[a].y, bv[b].y, acc[d][a][b][0]));
+            acc[d][a][b][1] = fma(av[a].x, bv[b].y, fma(-av[a].y, bv[b].x, acc[d][a][b][1]));
           }
       }
-    }
-    if (kSplit) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-          for (int b = 0; b < 2; ++b) {
-            acc[d][a][b][0] += (double)part[d][a][b][0];
-            acc[d][a][b][1] += (double)part[d][a][b][1];
-          }
     }
     __syncthreads();
   }
@@ -162,37 +150,39 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int d = 0; d < 3; ++d)
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < TMX; ++a)
 #pragma unroll
-      for (int b = 0; b < 2; ++b) {
+      for (int b = 0; b < TNX; ++b) {
         const int m = m0 + tm + 16 * a, n = n0 + tn + 16 * b;
         if (m < M && n < M)
-          partial[((size_t)blockIdx.y * 3 + d) * MM + (size_t)m * M + n] = make_double2(acc[d][a][b][0], acc[d][a][b][1]);
+          store_partial(&partial[((size_t)blockIdx.y * 3 + d) * MM + (size_t)m * M + n], acc[d][a][b][0],
+                        acc[d][a][b][1]);
       }
 }
 
-// a[2d][m][n] = (Z + Z^H)/2, a[2d+1][m][n] = (Z - Z^H)/(2i), Z the slab sum divided by
-// |psi_m| |psi_n| (norm2[3 m + 2] = sum_p |psi_m|^2 from the band sums)
-__global__ void k_mlwf_finish(const double2* __restrict__ partial, int nslab, int M, const double* __restrict__ sums,
+// a[2d][m][n] = (Z + Z^H)/2, a[2d+1][m][n] = (Z - Z^H)/(2i), Z the slab sum (FP64) divided
+// by |psi_m| |psi_n| (sums[3 m + 2] = sum_p |psi_m|^2 from the band sums)
+template <typename P>
+__global__ void k_mlwf_finish(const P* __restrict__ partial, int nslab, int M, const double* __restrict__ sums,
                               double2* __restrict__ a) {
   const size_t MM = (size_t)M * M;
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < 3 * (long)MM; e += (long)gridDim.x * blockDim.x) {
     const int d = (int)(e / MM);
     const int m = (int)((e % MM) / M), n = (int)(e % M);
-    double2 z = make_double2(0, 0), zt = make_double2(0, 0);
+    double zx = 0, zy = 0, tx = 0, ty = 0;
     for (int s = 0; s < nslab; ++s) {
-      const double2 x = partial[((size_t)s * 3 + d) * MM + (size_t)m * M + n];
-      const double2 y = partial[((size_t)s * 3 + d) * MM + (size_t)n * M + m];
-      z.x += x.x;
-      z.y += x.y;
-      zt.x += y.x;
-      zt.y += y.y;
+      const P x = partial[((size_t)s * 3 + d) * MM + (size_t)m * M + n];
+      const P y = partial[((size_t)s * 3 + d) * MM + (size_t)n * M + m];
+      zx += (double)x.x;
+      zy += (double)x.y;
+      tx += (double)y.x;
+      ty += (double)y.y;
     }
     const double sc = 1.0 / sqrt(sums[3 * m + 2] * sums[3 * n + 2]);
-    // conj(Z[n][m]) = (zt.x, -zt.y)
-    a[(2 * d) * MM + (size_t)m * M + n] = make_double2(0.5 * sc * (z.x + zt.x), 0.5 * sc * (z.y - zt.y));
-    // (Z - conj(Z^T)) / (2i): (u + i v) / (2i) = (v - i u) / 2 with u + i v = Z - conj(Z[n][m])
-    const double ur = z.x - zt.x, vi = z.y + zt.y;
+    // conj(Z[n][m]) = (tx, -ty)
+    a[(2 * d) * MM + (size_t)m * M + n] = make_double2(0.5 * sc * (zx + tx), 0.5 * sc * (zy - ty));
+    // (Z - conj(Z[n][m])) / (2i) = (v - i u) / 2 with u + i v = Z - conj(Z[n][m])
+    const double ur = zx - tx, vi = zy + ty;
     a[(2 * d + 1) * MM + (size_t)m * M + n] = make_double2(0.5 * sc * vi, -0.5 * sc * ur);
   }
 }
@@ -486,15 +476,43 @@ __global__ void __launch_bounds__(256)
 
 }  // namespace
 
-size_t mlwf_gram_slabs(long N, int M) {
-  const long tiles = (long)((M + kGT - 1) / kGT) * ((M + kGT - 1) / kGT);
+namespace {
+template <typename T>
+long gram_slabs(long N, int M) {
+  constexpr int TM = 16 * GramCfg<T>::TMX, TN = 16 * GramCfg<T>::TNX, kGP = GramCfg<T>::GP;
+  const long tiles = (long)((M + TM - 1) / TM) * ((M + TN - 1) / TN);
   const long chunks = (N + kGP - 1) / kGP;
-  return (size_t)std::max<long>(1, std::min<long>(chunks, (148L * 4 + tiles - 1) / tiles));
+  if (sizeof(T) == 4) return std::max<long>(1, (N + kSlabF32 - 1) / kSlabF32);
+  return std::max<long>(1, std::min<long>(chunks, (148L * 4 + tiles - 1) / tiles));
+}
+}  // namespace
+
+size_t mlwf_partial_bytes(long N, int M) {
+  const size_t MM = (size_t)M * M;
+  return std::max((size_t)gram_slabs<double>(N, M) * 3 * MM * sizeof(double2),
+                  (size_t)gram_slabs<float>(N, M) * 3 * MM * sizeof(float2));
+}
+
+template <typename T>
+static int gram_impl(const void* psi, long ld, int M, long N, const GramGeom& g, const double* sums, void* partial,
+                     double2* a, cudaStream_t st) {
+  using P = typename GramCfg<T>::P;
+  constexpr int TM = 16 * GramCfg<T>::TMX, TN = 16 * GramCfg<T>::TNX, kGP = GramCfg<T>::GP;
+  const long slabs = gram_slabs<T>(N, M);
+  const long per = ((N + slabs - 1) / slabs + kGP - 1) / kGP * kGP;
+  const long nslab = (N + per - 1) / per;
+  const dim3 grid((unsigned)(((M + TM - 1) / TM) * ((M + TN - 1) / TN)), (unsigned)nslab);
+  k_mlwf_gram<T><<<grid, 256, 0, st>>>((const cplx<T>*)psi, ld, M, N, g, per, (P*)partial);
+  INQB_CUDA_TRY(cudaGetLastError());
+  const long work = 3L * M * M;
+  k_mlwf_finish<P><<<(unsigned)std::min<long>((work + 255) / 256, 148L * 8), 256, 0, st>>>((const P*)partial,
+                                                                                          (int)nslab, M, sums, a);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
 }
 
 int launch_mlwf_gram(int precision, const void* psi, long ld, int M, long N, const int nr[3], const double lat[3][3],
-                     const double* sums, double2* partial, double2* a, void* stream) {
-  cudaStream_t st = (cudaStream_t)stream;
+                     const double* sums, void* partial, double2* a, void* stream) {
   GramGeom g;
   double len[3];
   for (int d = 0; d < 3; ++d) {
@@ -504,21 +522,8 @@ int launch_mlwf_gram(int precision, const void* psi, long ld, int M, long N, con
   // theta_d / pi = 2 r_d / |a_d|, r = sum_j f_j a_j
   for (int d = 0; d < 3; ++d)
     for (int j = 0; j < 3; ++j) g.frac_to_theta[d][j] = 2.0 * lat[j][d] / len[d];
-  const int tiles = (M + kGT - 1) / kGT;
-  const long slabs = (long)mlwf_gram_slabs(N, M);
-  const long per = ((N + slabs - 1) / slabs + kGP - 1) / kGP * kGP;
-  const long nslab = (N + per - 1) / per;
-  const dim3 grid((unsigned)(tiles * tiles), (unsigned)nslab);
-  if (precision == INQB_FP64)
-    k_mlwf_gram<double><<<grid, 256, 0, st>>>((const cplx<double>*)psi, ld, M, N, g, per, partial);
-  else
-    k_mlwf_gram<float><<<grid, 256, 0, st>>>((const cplx<float>*)psi, ld, M, N, g, per, partial);
-  INQB_CUDA_TRY(cudaGetLastError());
-  const long work = 3L * M * M;
-  k_mlwf_finish<<<(unsigned)std::min<long>((work + 255) / 256, 148L * 8), 256, 0, st>>>(partial, (int)nslab, M, sums,
-                                                                                         a);
-  INQB_CUDA_TRY(cudaGetLastError());
-  return INQB_OK;
+  return precision == INQB_FP64 ? gram_impl<double>(psi, ld, M, N, g, sums, partial, a, (cudaStream_t)stream)
+                                : gram_impl<float>(psi, ld, M, N, g, sums, partial, a, (cudaStream_t)stream);
 }
 
 int launch_identity(double2* u, int M, void* stream) {

@@ -7,13 +7,12 @@
 
 namespace inqb {
 
-// Number of point slabs the Gram kernel splits N into for M states (partial sums
-// take slabs * 3 * M * M complex128).
-size_t mlwf_gram_slabs(long N, int M);
+// Bytes of the Gram kernel's per-slab partial sums for M states (either precision).
+size_t mlwf_partial_bytes(long N, int M);
 // a [6][M][M] complex128: the six matrices of tdmlwf_trans::update from psi; sums[3 m + 2]
-// = sum_p |psi_m|^2 (band sums); partial: mlwf_gram_slabs * 3 * M * M complex128.
+// = sum_p |psi_m|^2 (band sums); partial: mlwf_partial_bytes.
 int launch_mlwf_gram(int precision, const void* psi, long ld, int M, long N, const int nr[3], const double lat[3][3],
-                     const double* sums, double2* partial, double2* a, void* stream);
+                     const double* sums, void* partial, double2* a, void* stream);
 int launch_identity(double2* u, int M, void* stream);
 // one JADE rotation step over np pairs (int2 top, bottom; indices >= M are skipped);
 // delta[np] receives each pair's change of sum_k trace(a_k)
