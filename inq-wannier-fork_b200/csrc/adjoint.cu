@@ -287,17 +287,22 @@ __global__ void __launch_bounds__(256)
 }
 
 // The moments of the four pairs (Lambda_j, Phi_j), pair j = blockIdx.z, into
-// part[chunk][pair][l][q][M] (the same sums as k_nl_moments).
-template <typename T>
+// part[chunk][pair][l][q][M] (the same sums as k_nl_moments).  Warps are (projector l,
+// half h); a lane holds orbital m = blockIdx.y * MW + lane % MW and walks the entry
+// stream (lane / MW) + (32 / MW) h, so that fewer than 32 orbitals still fill the warp
+// (MW = 16 for M <= 16), with four entries in flight per lane.
+template <typename T, int MW>
 __global__ void __launch_bounds__(256)
     k_nl_moments_pairs(int L, int M, EightBlocks<T> b, const int* __restrict__ chunk_atom,
                        const int* __restrict__ chunk_beg, const int* __restrict__ atom_ptr,
                        const AdjRec<T>* __restrict__ adj, double* __restrict__ part) {
-  constexpr int LM = 4, Q = 16;
+  constexpr int LM = 4, Q = 16, SUB = 32 / MW, STREAMS = 2 * SUB;
   __shared__ double red[LM][32][Q + 1];
   const int c = blockIdx.x, pr = blockIdx.z;
-  const int m = blockIdx.y * 32 + (threadIdx.x & 31);
-  const int l = (threadIdx.x >> 5) & (LM - 1), es = threadIdx.x >> 7;
+  const int lane = threadIdx.x & 31;
+  const int m = blockIdx.y * MW + (lane % MW);
+  const int l = (threadIdx.x >> 5) & (LM - 1), h = threadIdx.x >> 7;
+  const int stream = lane / MW + SUB * h;
   const int a = chunk_atom[c];
   const int i0 = chunk_beg[c], i1 = min(i0 + kNlChunk, atom_ptr[a + 1]);
   const cplx<T>* u = b.L[pr];
@@ -307,8 +312,8 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int q = 0; q < Q; ++q) s[q] = 0.0;
   if (m < M && l < L) {
-#pragma unroll 2
-    for (int i = i0 + es; i < i1; i += 2) {
+#pragma unroll 4
+    for (int i = i0 + stream; i < i1; i += STREAMS) {
       const AdjRec<T> r = adj[i];
       const cplx<T> uu = u[(long)r.pt * ldu + m], ww = w[(long)r.pt * ldw + m];
       const double bb = (double)r.beta[l];
@@ -322,15 +327,21 @@ __global__ void __launch_bounds__(256)
       s[10] += x0 * wr; s[11] += x0 * wi; s[12] += x1 * wr; s[13] += x1 * wi; s[14] += x2 * wr; s[15] += x2 * wi;
     }
   }
-  if (es == 1) {
+  // the SUB streams of a warp meet by shuffles (lane % MW keeps the orbital), then the
+  // two halves in shared memory
 #pragma unroll
-    for (int q = 0; q < Q; ++q) red[l][threadIdx.x & 31][q] = s[q];
+  for (int o = 16; o >= MW; o >>= 1)
+#pragma unroll
+    for (int q = 0; q < Q; ++q) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
+  if (h == 1 && lane < MW) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) red[l][lane][q] = s[q];
   }
   __syncthreads();
-  if (es == 0 && m < M && l < L) {
+  if (h == 0 && lane < MW && m < M && l < L) {
 #pragma unroll
     for (int q = 0; q < Q; ++q)
-      part[((((long)c * 4 + pr) * L + l) * Q + q) * M + m] = s[q] + red[l][threadIdx.x & 31][q];
+      part[((((long)c * 4 + pr) * L + l) * Q + q) * M + m] = s[q] + red[l][lane][q];
   }
 }
 
@@ -514,21 +525,28 @@ __global__ void __launch_bounds__(512)
   const int mi = threadIdx.x & 31, q = threadIdx.x >> 5;
   const int m = blockIdx.z * 32 + mi;
   const int c0 = atom_chunk_ptr[a], c1 = atom_chunk_ptr[a + 1];
+  // the four pairs' chunk sums, four loads in flight per pair (fixed order: deterministic)
+  double v[4][4];
 #pragma unroll
-  for (int pr = 0; pr < 4; ++pr) {
-    double v0 = 0.0, v1 = 0.0;
-    if (m < M) {
-      const long stride = 4L * L * Q * M;
-      const double* pp = part + (((long)c0 * 4 + pr) * L + l) * Q * M + (long)q * M + m;
-      int c = c0;
-      for (; c + 1 < c1; c += 2, pp += 2 * stride) {
-        v0 += pp[0];
-        v1 += pp[stride];
+  for (int pr = 0; pr < 4; ++pr) v[pr][0] = v[pr][1] = v[pr][2] = v[pr][3] = 0.0;
+  if (m < M) {
+    const long stride = 4L * L * Q * M;
+    const double* pp = part + ((long)c0 * 4 * L + l) * Q * M + (long)q * M + m;
+    const long pstride = (long)L * Q * M;  // next pair of the same chunk
+    int c = c0;
+    for (; c + 1 < c1; c += 2, pp += 2 * stride) {
+#pragma unroll
+      for (int pr = 0; pr < 4; ++pr) {
+        v[pr][0] += pp[pr * pstride];
+        v[pr][1] += pp[pr * pstride + stride];
       }
-      if (c < c1) v0 += pp[0];
     }
-    mom[pr][q][mi] = v0 + v1;
+    if (c < c1)
+#pragma unroll
+      for (int pr = 0; pr < 4; ++pr) v[pr][2] += pp[pr * pstride];
   }
+#pragma unroll
+  for (int pr = 0; pr < 4; ++pr) mom[pr][q][mi] = (v[pr][0] + v[pr][1]) + (v[pr][2] + v[pr][3]);
   __syncthreads();
   if (q != 0) return;  // warp 0 goes on whole (lanes past M add zeros)
   const double S = scale[a * L + l];
@@ -625,9 +643,14 @@ static int half_grad_impl(const inqb_ctx& ctx, const void* const Lam[4], const l
     if (ctx.d_nlpart.bytes < (size_t)nchunks * 4 * t.L * 16 * M * sizeof(double))
       return fail(INQB_ERR_INVALID, "nonlocal moment workspace not reserved");
     double* part = ctx.d_nlpart.as<double>();
-    k_nl_moments_pairs<T><<<dim3(nchunks, (M + 31) / 32, 4), 256, 0, st>>>(
-        t.L, M, b, t.d_chunk_atom.as<int>(), t.d_chunk_beg.as<int>(), t.d_atom_ptr.as<int>(),
-        t.d_adj_rec.as<AdjRec<T>>(), part);
+    if (M <= 16)
+      k_nl_moments_pairs<T, 16><<<dim3(nchunks, (M + 15) / 16, 4), 256, 0, st>>>(
+          t.L, M, b, t.d_chunk_atom.as<int>(), t.d_chunk_beg.as<int>(), t.d_atom_ptr.as<int>(),
+          t.d_adj_rec.as<AdjRec<T>>(), part);
+    else
+      k_nl_moments_pairs<T, 32><<<dim3(nchunks, (M + 31) / 32, 4), 256, 0, st>>>(
+          t.L, M, b, t.d_chunk_atom.as<int>(), t.d_chunk_beg.as<int>(), t.d_atom_ptr.as<int>(),
+          t.d_adj_rec.as<AdjRec<T>>(), part);
     INQB_CUDA_TRY(cudaGetLastError());
     k_nl_combine8<<<dim3(t.nproj, t.L, (M + 31) / 32), 512, 0, st>>>(t.L, M, t.d_atom_chunk_ptr.as<int>(), part,
                                                                    t.d_scale.as<double>(), pw, acc);
