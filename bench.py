@@ -646,6 +646,38 @@ def run_ours(args):
                  "timing": "step: wall clock around synchronised calls (one read-back per JADE sweep); "
                            "matrices: CUDA events"})
 
+    # -- the oracle (CPU, FP64, all host threads) on bounded samples of the same two
+    # workloads, reported beside them: one SCF ETRS step of 16 orbitals, and the TD-MLWF
+    # matrices + JADE for 32 of the localised states
+    if rank == 0:
+        import oracle
+
+        o = oracle.System(lattice, nr)
+        o.set_potential(V)
+        o.set_projectors(o.build_gaussian_kb(pos))
+        ps = np.ascontiguousarray(x64[:, :16].cpu().numpy())
+        occ16 = np.full(16, 2.0)
+        rho16 = o.density(ps, occ16)
+        o.ks_potential(rho16, V, 2)
+        t0 = time.perf_counter()
+        _, _, it_c, _ = o.etrs_scf_step(ps, rho16, 0.05, cov[1], cov[2], occ16, V, 2)
+        t_c = time.perf_counter() - t0
+        scf["cpu_reference"] = {"kind": "port", "cores": oracle.num_threads(), "sample": "one SCF ETRS step of 16 of "
+                                "the 128 orbitals (oracle, FP64)", "seconds": t_c, "scf_iterations": it_c,
+                                "orbital_steps_per_s": 16 / t_c}
+        scf["mixed_orbital_steps_per_s"] = scf["mixed_steps_per_s"] * x64.shape[1]
+        # 32 of the states as the TD-MLWF steps left them (localised gauge, FP64)
+        ls = np.ascontiguousarray(xm[:, :32].cpu().numpy())
+        t0 = time.perf_counter()
+        a_c = o.mlwf_matrices(ls)
+        t1 = time.perf_counter()
+        _, _, _, sw_c = oracle.jade(a_c)
+        t2 = time.perf_counter()
+        mlwf["cpu_reference"] = {"kind": "port", "cores": oracle.num_threads(), "sample": "matrices and JADE for 32 of "
+                                 "the 128 states in the localised gauge (oracle, FP64)", "matrices_s": t1 - t0, "jade_s": t2 - t1,
+                                 "jade_sweeps": sw_c}
+        del o
+
     # -- checkpoint in INQ's restart layout: all 128 orbitals (complex128 files) + density
     ckpt = None
     if rank == 0:

@@ -271,6 +271,14 @@ int inqb_ks_potential(inqb_ctx* ctx, const double* rho, const double* vion, int 
 int inqb_etrs_scf_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
                        const double kA_tdt_cov[3], const double* occ, double* rho, const double* vion, int theory,
                        int nscf, double threshold, int* iters, double energies[4], void* stream);
+/* The exchange step of an orbital-sharded run (one block of states per GPU): INQ sums
+ * the density over its states communicator (src/observables/density.hpp:77-95).  When
+ * set, inqb_etrs_scf_step calls fn(rho, N, user) after each density of its own orbitals,
+ * with the stream synchronised; fn must leave the sum over all ranks in rho (device
+ * memory) and return 0 when the reduction is complete; nonzero ends the step with
+ * INQB_ERR_INVALID.  fn NULL removes it. */
+typedef int (*inqb_density_reduce_fn)(double* rho, long n, void* user);
+int inqb_set_density_reduce(inqb_ctx* ctx, inqb_density_reduce_fn fn, void* user);
 
 /* ---------------------------------------------------------------- checkpoints
  * INQ's restart layout, so that runs resume from their own checkpoints and exchange

@@ -817,6 +817,27 @@ int inqb_ks_potential(inqb_ctx* ctx, const double* rho, const double* vion, int 
   return INQB_OK;
 }
 
+int inqb_set_density_reduce(inqb_ctx* ctx, inqb_density_reduce_fn fn, void* user) {
+  INQB_CHECK_CTX(ctx);
+  ctx->density_reduce = fn;
+  ctx->density_reduce_user = fn ? user : nullptr;
+  return INQB_OK;
+}
+
+namespace inqb {
+namespace {
+// the density of this rank's orbitals, then (when set) the sum over the ranks
+int sharded_density(inqb_ctx* ctx, const void* psi, long ld, int M, const double* occ, double* rho, void* stream) {
+  INQB_TRY(launch_density(ctx->precision, psi, ld, M, ctx->N, occ, rho, stream));
+  if (!ctx->density_reduce) return INQB_OK;
+  INQB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  if (ctx->density_reduce(rho, ctx->N, ctx->density_reduce_user) != 0)
+    return fail(INQB_ERR_INVALID, "the density reduction callback failed");
+  return INQB_OK;
+}
+}  // namespace
+}  // namespace inqb
+
 int inqb_etrs_scf_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
                        const double kA_tdt_cov[3], const double* occ, double* rho, const double* vion, int theory,
                        int nscf, double threshold, int* iters, double energies[4], void* stream) {
@@ -856,7 +877,7 @@ int inqb_etrs_scf_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const
     INQB_TRY(launch_shift2(ctx->precision, y, M, save, M, psi, ld, M, N, c1, c2, stream));
   }
   // density of the predicted step; the Hamiltonian moves to t + dt
-  INQB_TRY(launch_density(ctx->precision, psi, ld, M, N, occ, rho, stream));
+  INQB_TRY(sharded_density(ctx, psi, ld, M, occ, rho, stream));
   INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
   INQB_TRY(ks_potential_dev(ctx, rho, vion, theory, w, stream));
 
@@ -868,7 +889,7 @@ int inqb_etrs_scf_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const
     INQB_TRY(exponential(ctx, psi, M, ld, 0.0, 0.5 * dt, 4, stream));
     INQB_CUDA_TRY(cudaMemcpyAsync(w.rho_old, rho, sizeof(double) * N, cudaMemcpyDeviceToDevice,
                                   (cudaStream_t)stream));
-    INQB_TRY(launch_density(ctx->precision, psi, ld, M, N, occ, rho, stream));
+    INQB_TRY(sharded_density(ctx, psi, ld, M, occ, rho, stream));
     INQB_TRY(launch_absdiff(w.rho_old, rho, N, w.partial, w.sums + 4, stream));
     INQB_TRY(ks_potential_dev(ctx, rho, vion, theory, w, stream));
     INQB_CUDA_TRY(cudaMemcpyAsync(s, w.sums, sizeof(s), cudaMemcpyDeviceToHost, (cudaStream_t)stream));

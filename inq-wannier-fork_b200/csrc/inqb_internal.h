@@ -191,6 +191,8 @@ struct inqb_ctx {
   inqb::DevBuf d_cn;            // Crank-Nicolson: rhs, residual, (1 + i dt/2 H) residual
   inqb::DevBuf d_cnred;         // Crank-Nicolson: 4 sums and the residual norm per orbital
   inqb::DevBuf d_scf;           // ETRS with self-consistency: the saved half step, H^k phi
+  inqb_density_reduce_fn density_reduce = nullptr;  // cross-rank density sum (orbital sharding)
+  void* density_reduce_user = nullptr;
   inqb::DevBuf d_io;            // checkpoint staging (complex128 rows of a chunk of states)
   inqb::DevBuf d_mlwf;          // TD-MLWF: the six matrices, u, adiag, sums, slabs, pairs, deltas
   inqb::DevBuf d_pot;           // density -> potential: V_H field [N] (complex), previous

@@ -20,6 +20,8 @@ THEORY_HARTREE = 1
 THEORY_LDA = 2
 # status of a missing, short or unwritable checkpoint file
 ERR_IO = 8
+# int (*)(double* rho, long n, void* user): the cross-rank density sum of a sharded SCF step
+DENSITY_REDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p)
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -77,6 +79,7 @@ SIGNATURES = {
     "inqb_mlwf_matrices": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "inqb_jade": (ctypes.c_int, [_ctxp, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, ctypes.c_double, _ip, _vp]),
     "inqb_mlwf_rotate": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "inqb_set_density_reduce": (ctypes.c_int, [_ctxp, _vp, _vp]),
     "inqb_etrs_powers_size": (ctypes.c_int, [_ctxp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "inqb_etrs_step_powers": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
                                              _vp, _vp]),

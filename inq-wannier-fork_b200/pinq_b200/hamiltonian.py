@@ -261,10 +261,31 @@ class KSHamiltonian:
         b = np.ascontiguousarray(kA_tdt_cov, np.float64).reshape(3)
         it = ctypes.c_int(0)
         en = np.zeros(4)
-        call("inqb_etrs_scf_step", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), float(dt), dptr(a), dptr(b),
-             occ_t.data_ptr(), rho.data_ptr(), vion.data_ptr() if vion is not None else None, int(theory), int(nscf),
-             float(threshold), ctypes.byref(it), dptr(en), self._stream())
+        cb = None
+        reducer = getattr(self, "_density_reducer", None)
+        if reducer is not None:
+            def _reduce(ptr, n, user, _rho=rho):
+                try:
+                    reducer(_rho)
+                    return 0
+                except Exception:  # reported to the caller as the step's failure
+                    return 1
+            cb = _lib.DENSITY_REDUCE_FN(_reduce)
+            call("inqb_set_density_reduce", self._h, ctypes.cast(cb, ctypes.c_void_p), None)
+        try:
+            call("inqb_etrs_scf_step", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), float(dt), dptr(a),
+                 dptr(b), occ_t.data_ptr(), rho.data_ptr(), vion.data_ptr() if vion is not None else None,
+                 int(theory), int(nscf), float(threshold), ctypes.byref(it), dptr(en), self._stream())
+        finally:
+            if cb is not None:
+                call("inqb_set_density_reduce", self._h, None, None)
         return it.value, dict(zip(("external", "hartree", "xc", "nvxc"), en.tolist()))
+
+    def set_density_reducer(self, reducer):
+        """Orbital-sharded SCF: reducer(rho) must replace rho (an FP64 CUDA tensor) by
+        its sum over the ranks before returning, e.g. parallel.density_reducer(group).
+        None removes it."""
+        self._density_reducer = reducer
 
     # -- checkpoints in INQ's restart layout (operations/io.hpp, systems/electrons.hpp)
     def save_orbitals(self, dirname, psi, occ=None, kpin=0, first_state=0):

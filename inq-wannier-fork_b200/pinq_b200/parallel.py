@@ -50,3 +50,18 @@ def sharded_density(ham, psi_local, occ_local, group=None):
     FP64 all-reduce.  ham is anything with density(psi, occ) -> FP64 tensor [N]."""
     rho = ham.density(psi_local, occ_local)
     return allreduce_sum_(rho, group)
+
+
+def density_reducer(group=None):
+    """The exchange step of an orbital-sharded SCF step (KSHamiltonian.set_density_reducer):
+    an in-place SUM of the density over the ranks, finished before it returns (the
+    library's next kernels read the tensor on its own stream)."""
+    import torch
+
+    def reduce_(rho):
+        allreduce_sum_(rho, group)
+        if rho.is_cuda:
+            torch.cuda.current_stream(rho.device).synchronize()
+        return rho
+
+    return reduce_

@@ -129,3 +129,70 @@ def test_etrs_scf_noninteracting_equals_etrs(pb, oracle_mod, sysd):
     h.etrs_step_(b, 0.05, k1, k2)
     assert it == 2
     assert rel_max(a.cpu().numpy(), b.cpu().numpy()) < 1e-12
+
+
+def test_etrs_scf_sharded_two_blocks_equals_whole(pb, oracle_mod, sysd):
+    """Orbital sharding of the SCF step: two contexts, each with half of the orbitals,
+    run the step concurrently in two host threads; the density-reduction hook sums
+    their densities (the exchange step).  The union equals the one-context step."""
+    import threading
+
+    occ = np.array([2.0, 2.0, 2.0, 2.0])
+    k1 = np.zeros(3)
+    k2 = np.array([0.01, 0.0, 0.0])
+    vion = _dev(sysd["V"], torch.float64)
+    whole = make_product(pb, sysd, "fp64")
+    x = _dev(sysd["psi"])
+    rho = whole.density(x, occ)
+    whole.ks_potential(rho, vion, 2, energies=False)
+    it_ref, en_ref = whole.etrs_scf_step_(x, rho, 0.05, k1, k2, occ, vion, 2)
+
+    halves = [make_product(pb, sysd, "fp64") for _ in range(2)]
+    xs = [_dev(sysd["psi"][:, :2]), _dev(sysd["psi"][:, 2:])]
+    rhos = [h.density(xx, occ[:2]) for h, xx in zip(halves, xs)]
+    total = rhos[0] + rhos[1]
+    for h, r in zip(halves, rhos):
+        r.copy_(total)
+        h.ks_potential(r, vion, 2, energies=False)
+    torch.cuda.synchronize()
+    bar = threading.Barrier(2, timeout=60)
+    calls = [0, 0]
+
+    def make_reducer(i):
+        def reduce_(r):
+            calls[i] += 1
+            torch.cuda.synchronize()
+            bar.wait()
+            if i == 0:
+                s = rhos[0] + rhos[1]
+                torch.cuda.synchronize()
+                reduce_.shared[0] = s
+            bar.wait()
+            r.copy_(reduce_.shared[0])
+            torch.cuda.synchronize()
+            bar.wait()
+            return r
+        return reduce_
+
+    shared = [None]
+    out = [None, None]
+    for i, h in enumerate(halves):
+        red = make_reducer(i)
+        red.shared = shared
+        h.set_density_reducer(red)
+
+    def run(i):
+        out[i] = halves[i].etrs_scf_step_(xs[i], rhos[i], 0.05, k1, k2, occ[:2], vion, 2)
+
+    ts = [threading.Thread(target=run, args=(i,)) for i in range(2)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(120)
+    assert out[0] is not None and out[1] is not None
+    assert out[0][0] == out[1][0] == it_ref and calls == [it_ref + 1, it_ref + 1]
+    both = torch.cat(xs, 1).cpu().numpy()
+    assert rel_max(both, x.cpu().numpy()) < 1e-12
+    assert rel_max(rhos[0].cpu().numpy(), rho.cpu().numpy()) < 1e-12
+    for k in ("external", "hartree", "xc", "nvxc"):
+        assert abs(out[0][1][k] - en_ref[k]) < 1e-11 * max(1.0, abs(en_ref[k]))

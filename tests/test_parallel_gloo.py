@@ -49,6 +49,33 @@ def _rank_main(rank, world, port, M, out_dir):
         dist.destroy_process_group()
 
 
+def _reducer_main(rank, world, port, out_dir):
+    import datetime
+
+    import torch.distributed as dist
+
+    from pinq_b200.parallel import density_reducer
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        rho = torch.arange(6, dtype=torch.float64) * (rank + 1)
+        out = density_reducer()(rho)
+        assert out is rho  # in place, as the library's callback requires
+        np.save(os.path.join(out_dir, f"red{rank}.npy"), rho.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_density_reducer_sums_in_place(tmp_path):
+    """The exchange step of a sharded SCF step (KSHamiltonian.set_density_reducer)."""
+    mp.start_processes(_reducer_main, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    for r in range(2):
+        assert np.array_equal(np.load(tmp_path / f"red{r}.npy"), np.arange(6) * 3.0)
+
+
 def test_orbital_range_partitions():
     for M in (0, 1, 7, 16, 128, 131):
         for world in (1, 2, 3, 8):
