@@ -232,6 +232,13 @@ int inqb_etrs_adjoint_step(inqb_ctx* ctx, void* lambda, int M, int ld, double dt
                            const double kA_tdt_cov[3], const void* powers, double* gV, double* gA_t,
                            double* gA_tdt, void* stream);
 
+/* perturbations::kick (src/perturbations/kick.hpp:20-61): the zero-time kick of a
+ * length-gauge run, psi *= exp(-i kick . r) with kick a cartesian field and r the
+ * grid point in the symmetric range.  In a periodic cell INQ uses the velocity gauge
+ * instead, where the kick is the constant vector potential A = -kick (pass it as k + A
+ * to the propagators) and zero_step leaves the orbitals unchanged. */
+int inqb_kick(inqb_ctx* ctx, void* psi, int M, int ld, const double kick_cart[3], void* stream);
+
 /* ---------------------------------------------------------------- density -> potential
  * solvers::poisson for a periodic cell (src/solvers/poisson.hpp:29-35,66-100,193-211),
  * the field_set form: M complex fields [N][M] of the context precision,

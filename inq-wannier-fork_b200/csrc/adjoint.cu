@@ -84,6 +84,24 @@ __global__ void k_position_scale(long N, int M, const cplx<T>* __restrict__ psi,
   }
 }
 
+// perturbations::kick::zero_step in the length gauge (src/perturbations/kick.hpp:20-61):
+// psi *= exp(i E . r) with E = -kick field, r the cartesian point (symmetric range).
+template <typename T>
+__global__ void k_phase_kick(long N, int M, cplx<T>* __restrict__ psi, long ld, Lat g, double e0, double e1,
+                             double e2) {
+  const long total = N * M;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const long p = i / M;
+    const int m = (int)(i - p * M);
+    const double ph = e0 * rcomp(g, p, 0) + e1 * rcomp(g, p, 1) + e2 * rcomp(g, p, 2);
+    double sn, cs;
+    sincos(ph, &sn, &cs);
+    cplx<T>& v = psi[p * ld + m];
+    const double x = v.x, y = v.y;
+    v = mk<T>((T)(cs * x - sn * y), (T)(cs * y + sn * x));
+  }
+}
+
 // gV[p] += Re(c sum_m conj(u) w), one warp per grid point.
 template <typename T>
 __global__ void k_vgrad(long N, int M, const cplx<T>* __restrict__ u, const cplx<T>* __restrict__ w, long ld,
@@ -723,6 +741,25 @@ int launch_position_scale(int precision, const inqb_ctx& ctx, const void* psi, l
   else
     k_position_scale<float><<<grid_for(n, 256), 256, 0, st>>>(ctx.N, M, (const cplx<float>*)psi, ld,
                                                               (cplx<float>*)out, ldo, g, dir, occ, s);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_phase_kick(int precision, const inqb_ctx& ctx, void* psi, long ld, int M, const double kick[3],
+                      void* stream) {
+  Lat g;
+  for (int i = 0; i < 3; i++) {
+    g.nr[i] = ctx.nr[i];
+    for (int j = 0; j < 3; j++) g.lat[i][j] = ctx.cell.lat[i][j];
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const long n = ctx.N * M;
+  if (precision == INQB_FP64)
+    k_phase_kick<double><<<grid_for(n, 256), 256, 0, st>>>(ctx.N, M, (cplx<double>*)psi, ld, g, -kick[0], -kick[1],
+                                                           -kick[2]);
+  else
+    k_phase_kick<float><<<grid_for(n, 256), 256, 0, st>>>(ctx.N, M, (cplx<float>*)psi, ld, g, -kick[0], -kick[1],
+                                                          -kick[2]);
   INQB_CUDA_TRY(cudaGetLastError());
   return INQB_OK;
 }

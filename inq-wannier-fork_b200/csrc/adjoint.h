@@ -12,6 +12,9 @@ int launch_lincomb(int precision, long N, int M, int K, const double (*a)[2], co
                    void* y, long ldy, void* stream);
 int launch_position_scale(int precision, const inqb_ctx& ctx, const void* psi, long ld, void* out, long ldo, int M,
                           int dir, const double* occ, double s, void* stream);
+// psi *= exp(-i kick . r) (the length-gauge kick)
+int launch_phase_kick(int precision, const inqb_ctx& ctx, void* psi, long ld, int M, const double kick[3],
+                      void* stream);
 int launch_vgrad(int precision, long N, int M, const void* u, const void* w, long ld, double cre, double cim,
                  double* gV, void* stream);
 // gA += Re(c <u| dH/dA |w>) from the forward coefficients U, W of u, w: natural order

@@ -790,6 +790,16 @@ int inqb_etrs_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const dou
   return INQB_OK;
 }
 
+int inqb_kick(inqb_ctx* ctx, void* psi, int M, int ld, const double kick_cart[3], void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!kick_cart) return fail(INQB_ERR_INVALID, "null kick");
+  for (int d = 0; d < 3; d++)
+    if (!std::isfinite(kick_cart[d])) return fail(INQB_ERR_NONFINITE, "kick is not finite");
+  INQB_GUARD(ctx);
+  return launch_phase_kick(ctx->precision, *ctx, psi, ld, M, kick_cart, stream);
+}
+
 int inqb_poisson(inqb_ctx* ctx, const void* in, void* out, int M, int ld, void* stream) {
   INQB_CHECK_CTX(ctx);
   INQB_TRY(check_block(ctx, in, M, ld));

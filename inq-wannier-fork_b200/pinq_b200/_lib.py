@@ -64,6 +64,7 @@ SIGNATURES = {
     "inqb_set_schedule": (ctypes.c_int, [_ctxp, ctypes.c_int, _ip]),
     "inqb_crank_nicolson_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
                                                 ctypes.c_int, ctypes.c_double, _ip, _dp, _vp]),
+    "inqb_kick": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _dp, _vp]),
     "inqb_poisson": (ctypes.c_int, [_ctxp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "inqb_ks_potential": (ctypes.c_int, [_ctxp, _vp, _vp, ctypes.c_int, _dp, _vp]),
     "inqb_etrs_scf_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _vp,

@@ -219,6 +219,13 @@ class KSHamiltonian:
         call("inqb_fft_backward", self._h, psi.data_ptr(), out.data_ptr(), psi.shape[1], psi.stride(0), self._stream())
         return out
 
+    def kick_(self, psi, kick_cart):
+        """perturbations::kick::zero_step in the length gauge: psi *= exp(-i kick . r)."""
+        psi = self._check(psi)
+        k = np.ascontiguousarray(kick_cart, np.float64).reshape(3)
+        call("inqb_kick", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), dptr(k), self._stream())
+        return psi
+
     # -- density -> potential (self_consistency.hpp:89-160)
     def poisson(self, fields, out=None):
         """solvers::poisson (periodic cell) of complex fields [N, M] in the context

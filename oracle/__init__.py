@@ -82,6 +82,7 @@ def lib():
         L.orc_jade.restype = ctypes.c_int
         L.orc_jade.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]
         L.orc_mlwf_rotate.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
+        L.orc_kick.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -296,6 +297,13 @@ class System:
         a = np.ascontiguousarray(a, np.float64).ravel()
         b = np.ascontiguousarray(b, np.float64).ravel()
         return lib().orc_integral_sum_absdiff(self._h, a.size, _d(a), _d(b))
+
+    def kick(self, psi, kick_cart):
+        """perturbations::kick::zero_step, length gauge: psi exp(-i kick . r)."""
+        out = self._psi(psi).copy()
+        k = np.ascontiguousarray(kick_cart, np.float64).reshape(3)
+        lib().orc_kick(self._h, out.shape[1], _d(out.view(np.float64)), _d(k))
+        return out
 
     # ---- TD-MLWF (wannier/tdmlwf_trans.hpp)
 

@@ -1253,6 +1253,23 @@ void orc_mlwf_rotate(void *h, int M, double *psi_, const double *u_) {
   }
 }
 
+// perturbations::kick::zero_step, length gauge (kick.hpp:20-61): psi *= exp(i E . r),
+// E = -kick (cartesian), r the cartesian grid point
+void orc_kick(void *h, int M, double *psi_, const double *kick) {
+  auto *s = (System *)h;
+  const Grid &g = s->grid;
+  cd *psi = (cd *)psi_;
+  for (int ix = 0; ix < g.nr[0]; ix++)
+    for (int iy = 0; iy < g.nr[1]; iy++)
+      for (int iz = 0; iz < g.nr[2]; iz++) {
+        const v3 r = g.rvector_cart(ix, iy, iz);
+        const double ph = -(kick[0] * r[0] + kick[1] * r[1] + kick[2] * r[2]);
+        const cd f = std::polar(1.0, ph);
+        const long p = g.linear(ix, iy, iz);
+        for (int m = 0; m < M; m++) psi[p * M + m] *= f;
+      }
+}
+
 int orc_num_threads() {
 #ifdef _OPENMP
   return omp_get_max_threads();

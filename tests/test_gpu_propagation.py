@@ -134,3 +134,14 @@ def test_crank_nicolson_converges_and_keeps_norms(pb, oracle_mod, sysd):
     o = make_oracle(oracle_mod, sysd)
     e = o.etrs_step(sysd["psi"], -0.01, np.zeros(3), np.zeros(3))
     assert rel_norm(x.cpu().numpy(), e) < 1e-3
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_kick_matches_oracle(pb, oracle_mod, sysd, precision):
+    o = make_oracle(oracle_mod, sysd)
+    h = make_product(pb, sysd, precision)
+    k = np.array([0.05, -0.02, 0.1])
+    dt = torch.complex128 if precision == "fp64" else torch.complex64
+    x = h.kick_(_dev(sysd["psi"], dt), k).cpu().numpy()
+    ref = o.kick(sysd["psi"], k)
+    assert rel_max(x, ref) < (1e-14 if precision == "fp64" else 1e-6)

@@ -198,3 +198,15 @@ def test_etrs_scf_lda_conserves_norm(oracle_mod):
         assert np.all(np.isfinite(en)) and en[2] < 0.0
     n1 = o.volume_element * (np.abs(psi) ** 2).sum(0)
     assert np.abs(n1 - n0).max() < 1e-6
+
+
+def test_kick_shifts_plane_waves(oracle_mod):
+    """kick::zero_step (length gauge): exp(-i k.r) moves a plane wave e^{i q.r} to
+    e^{i (q - k).r} (kick.hpp:49-57)."""
+    s = oracle_mod.System(np.diag([8.0, 8.0, 8.0]), [12, 12, 12])
+    r = s.rvectors()
+    q = 2 * np.pi / 8.0 * np.array([1.0, 2.0, 0.0])
+    k = np.array([0.1, -0.2, 0.05])
+    psi = np.exp(1j * (r @ q))[:, None]
+    out = s.kick(psi, k)
+    assert np.abs(out[:, 0] - np.exp(1j * (r @ (q - k)))).max() < 1e-13
