@@ -528,6 +528,35 @@ def run_ours(args):
     ms_etrs32 = timed(lambda: etrs(h32, xe32), args.etrs_steps, W)
     ms_etrs64 = timed(lambda: etrs(h64, xe64), args.etrs_steps, W)
 
+    # -- the 3-D FFT alone: the library's forward transform (tile passes) against cuFFT's
+    # batched C2C (torch.fft.fftn over the three grid axes of the same [N][M] block), a
+    # comparison point only; 2 N M b algorithmic bytes per transform
+    fft = {}
+    Kf = max(5, K // 10)
+    for name, h, x in (("mixed", h32, x32), ("fp64", h64, x64)):
+        yf = torch.empty_like(x)
+        ms_ours = timed(lambda: h.to_fourier(x, yf), Kf, W)
+        xv = x.view(nr[0], nr[1], nr[2], x.shape[1])
+        ms_cufft = timed(lambda: torch.fft.fftn(xv, dim=(0, 1, 2)), Kf, W)
+        nb = 2.0 * x.numel() * x.element_size()
+        fft[name] = {"ours_ms": ms_ours / Kf, "cufft_ms": ms_cufft / Kf,
+                     "ours_GBps": nb / (ms_ours / Kf * 1e-3) / 1e9, "cufft_GBps": nb / (ms_cufft / Kf * 1e-3) / 1e9,
+                     "cufft_over_ours": ms_cufft / ms_ours}
+        del yf
+    if rank == 0:
+        import scipy.fft
+
+        xs16 = x64[:, :16].cpu().numpy().reshape(nr[0], nr[1], nr[2], 16)
+        nthr = os.cpu_count() or 1
+        scipy.fft.fftn(xs16, axes=(0, 1, 2), workers=nthr)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            scipy.fft.fftn(xs16, axes=(0, 1, 2), workers=nthr)
+        t_sp = (time.perf_counter() - t0) / 3
+        fft["cpu_scipy"] = {"kind": "scipy.fft twin", "cores": nthr, "sample": "16 of the 128 orbitals, complex128",
+                            "ms": 1e3 * t_sp, "orbital_transforms_per_s": 16 / t_sp}
+    fft["timing"] = "CUDA events over device-resident blocks; cuFFT plan made in the warm-up"
+
     # -- Crank-Nicolson steps (steepest-descent sweeps to a residual of 1e-10), 2 steps each
     cn = {}
     for name, h, x in (("mixed", h32, x32), ("fp64", h64, x64)):
@@ -768,6 +797,7 @@ def run_ours(args):
         "etrs": {"mixed_steps_per_s": world * args.etrs_steps / (ms_etrs32 * 1e-3),
                  "fp64_steps_per_s": world * args.etrs_steps / (ms_etrs64 * 1e-3),
                  "H_applies_per_step": 8, "dt": 0.05},
+        "fft": fft,
         "crank_nicolson": cn,
         "etrs_scf": scf,
         "checkpoint": ckpt,

@@ -652,7 +652,9 @@ static int half_grad_impl(const inqb_ctx& ctx, const void* const Lam[4], const l
   r.mask = ctx.fourier_mask;
   const int G = ctx.plan->G_tile;
   const long nelem = (long)((M + G - 1) / G) * G * ctx.N;
-  k_velocity_dot8<T><<<(int)std::min<long>((nelem + 255) / 256, 148L * 2), 256, 0, st>>>(
+  // six CTAs per SM keep enough coefficient loads in flight (the per-CTA sums end in
+  // six atomics each)
+  k_velocity_dot8<T><<<(int)std::min<long>((nelem + 255) / 256, 148L * 6), 256, 0, st>>>(
       nelem, M, fb, pw, TileFourier{G, ctx.plan->y1, ctx.plan->y2}, r, acc);
   INQB_CUDA_TRY(cudaGetLastError());
   const ProjTables& t = ctx.proj;
