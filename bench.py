@@ -180,6 +180,19 @@ def profiled_traffic():
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), recorded beside CPU timings."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
 def cpu_baseline(lattice, nr, pos, V, seconds, steps=None, warmup=0):
     """The oracle's FP64 H|psi> (C++, OpenMP over orbitals, all host threads) on a
     bounded sample of the same workload: as many orbitals as threads."""
@@ -207,7 +220,7 @@ def cpu_baseline(lattice, nr, pos, V, seconds, steps=None, warmup=0):
         if (steps is not None and n >= steps) or (steps is None and time.perf_counter() > t_end):
             break
     total = sum(times)
-    return {"value": Ms * n / total, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": Ms * n / total, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(), "kind": "port",
             "sample": f"oracle FP64 H|psi> on {Ms} of the 128 orbitals of the same 64^3 / 64-atom system, "
                       f"{n} applies ({total:.1f} s)"}, times
 
