@@ -296,7 +296,7 @@ def bench_adjoint(args, local):
     cfg = systems.config("cfg2")
     out = {"config": "cfg2: a=10.26, 32^3, 8 atoms, 16 orbitals, dt=0.05, 200 steps, checkpoint every 20, "
                      "Fourier sphere mask on", "steps": cfg["steps"],
-           "ratio": "(forward keeping what the backward needs + backward) / plain forward (best of 3)",
+           "ratio": "(forward keeping what the backward needs + backward, better of 2) / plain forward (best of 3)",
            "timing": "wall clock around device-synchronised calls"}
     for precision in ("fp64", "mixed"):
         h = pb.KSHamiltonian(cfg["lattice"], cfg["nr"], precision, device=local)
@@ -323,14 +323,19 @@ def bench_adjoint(args, local):
             prop = DipolePropagation(h, psi0, cfg["occ"], cfg["dt"], cfg["checkpoint_every"], store_powers=store)
             prop.forward(cfg["amplitudes"], keep=True)  # warm-up
             prop.backward()
-            torch.cuda.synchronize()
-            t1 = time.perf_counter()
-            d = prop.forward(cfg["amplitudes"], keep=True)
-            torch.cuda.synchronize()
-            t2 = time.perf_counter()
-            gA, gV = prop.backward()
-            torch.cuda.synchronize()
-            t3 = time.perf_counter()
+            best = None
+            for _ in range(2):  # the better of two (forward keeping + backward) runs
+                torch.cuda.synchronize()
+                t1 = time.perf_counter()
+                d = prop.forward(cfg["amplitudes"], keep=True)
+                torch.cuda.synchronize()
+                t2 = time.perf_counter()
+                gA, gV = prop.backward()
+                torch.cuda.synchronize()
+                t3 = time.perf_counter()
+                if best is None or t3 - t1 < best[2] - best[0]:
+                    best = (t1, t2, t3)
+            t1, t2, t3 = best
             res[mode] = {"forward_s": t_fwd, "forward_keep_s": t2 - t1, "backward_s": t3 - t2,
                          "total_over_forward": (t3 - t1) / t_fwd, "dipole": d,
                          "grad_amplitudes_norm": float(gA.norm()), "grad_V_norm": float(gV.norm()),

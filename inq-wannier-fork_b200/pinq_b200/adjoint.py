@@ -70,10 +70,18 @@ class DipolePropagation:
                 self.h.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)),
                                          self._kA(self._amp(amps, n + 1)), powers[n])
             self.powers = powers
+        elif keep:
+            # the same term-by-term step the backward recomputes each segment with, so
+            # that the recomputed trajectory is this one exactly (one scratch row)
+            scratch = self.h.powers_buffer(1, self.M)
+            for n in range(len(amps)):
+                if n % self.every == 0:
+                    cps[n] = psi.clone()
+                self.h.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)),
+                                         self._kA(self._amp(amps, n + 1)), scratch[0])
+            del scratch
         else:
             for n in range(len(amps)):
-                if keep and n % self.every == 0:
-                    cps[n] = psi.clone()
                 self.h.etrs_step_(psi, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)))
         rho = self.h.density(psi, self.occ)
         d = float(self.h.dipole(rho)[self.direction])
