@@ -416,8 +416,10 @@ __global__ void __launch_bounds__(128)
 // 4 x 4 outputs each, j in chunks of 8 through shared memory.
 constexpr int kRT = 64, kRK = 8;
 
+// FP64: 128 registers for two CTAs per SM (136 unbounded, one CTA: 2.98 -> 2.09 ms at
+// 64^3 x 128 states); FP32 runs best unbounded
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 1)
     k_mlwf_rotate(const cplx<T>* __restrict__ psi, long ld, int M, long N, const double2* __restrict__ u,
                   cplx<T>* __restrict__ out, long ldo) {
   using R = T;
