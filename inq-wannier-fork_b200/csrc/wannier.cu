@@ -198,11 +198,15 @@ __device__ void jacobi3_top(double S[3][3], double out[3]) {
   double inc[3] = {0, 0, 0};
   for (int pass = 1; pass <= 10000; pass++) {
     double off = 0.0;
+#pragma unroll
     for (int q = 0; q < 3; q++)
+#pragma unroll
       for (int p = 0; p < q; p++) off += S[p][q] * S[p][q];
     const double thresh = sqrt(off) / 12.0;
     if (thresh == 0.0) break;
+#pragma unroll
     for (int p = 0; p < 3; p++)
+#pragma unroll
       for (int q = p + 1; q < 3; q++) {
         const double big = 10.0 * fabs(S[p][q]);
         if (pass > 4 && big + fabs(d[p]) == fabs(d[p]) && big + fabs(d[q]) == fabs(d[q])) {
@@ -232,9 +236,13 @@ __device__ void jacobi3_top(double S[3][3], double out[3]) {
     (x) = g_ - s * (h_ + g_ * tau);       \
     (y) = h_ + s * (g_ - h_ * tau);       \
   }
+#pragma unroll
         for (int j = 0; j < p; j++) INQB_JROT(S[j][p], S[j][q])
+#pragma unroll
         for (int j = p + 1; j < q; j++) INQB_JROT(S[p][j], S[j][q])
+#pragma unroll
         for (int j = q + 1; j < 3; j++) INQB_JROT(S[p][j], S[q][j])
+#pragma unroll
         for (int j = 0; j < 3; j++) INQB_JROT(V[j][p], V[j][q])
 #undef INQB_JROT
       }
@@ -301,8 +309,10 @@ __global__ void __launch_bounds__(kJT)
   for (int i = 0; i < 36; ++i)
     for (int o = 16; o > 0; o >>= 1) s[i] += __shfl_down_sync(0xffffffffu, s[i], o);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0)
+  if (lane == 0) {
+#pragma unroll
     for (int i = 0; i < 36; ++i) red[w][i] = s[i];
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     double G[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
