@@ -7,6 +7,7 @@ from ._lib import FP64, MIXED, THEORY_HARTREE, THEORY_LDA, THEORY_NONE, InqbErro
 from .hamiltonian import KSHamiltonian, build_gaussian_kb, gaussian_beta, grid_supported, sphere  # noqa: F401
 from . import systems  # noqa: F401
 from .batch import CellBatch  # noqa: F401
+from .propagate import propagate  # noqa: F401
 
-__all__ = ["KSHamiltonian", "CellBatch", "build_gaussian_kb", "gaussian_beta", "grid_supported", "sphere", "systems",
+__all__ = ["KSHamiltonian", "CellBatch", "propagate", "build_gaussian_kb", "gaussian_beta", "grid_supported", "sphere", "systems",
            "FP64", "MIXED", "THEORY_NONE", "THEORY_HARTREE", "THEORY_LDA", "InqbError", "lib"]
