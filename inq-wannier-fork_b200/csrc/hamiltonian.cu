@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <map>
+#include <mutex>
 #include <tuple>
 
 #include "fft_tile.cuh"
@@ -105,24 +106,31 @@ template <typename T, int NX, int NY, int NZ>
 static int launch_h_impl(const LaunchArgs& a) {
   using TG = TileGeom<T, NX, NY, NZ>;
   constexpr int GT = TG::G;
-  static bool attr_done[64] = {};
+  // the kernels' shared-memory limits, set once per device (contexts on several host
+  // threads may launch for the first time together)
+  static std::once_flag attr_once[64];
   int dev = 0;
   INQB_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 64 && !attr_done[dev]) {
-    INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_fwd<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)std::min(TG::smem_fwd(kAccAtomsMax, kRecCapMax), TG::SMEM_MAX)));
-    INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)TG::SMEM_X));
-    INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x_fft<T, NX, NY, NZ, 0>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TG::SMEM_X));
-    INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x_fft<T, NX, NY, NZ, 1>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TG::SMEM_X));
-    INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_inv<T, NX, NY, NZ, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)std::min(TG::smem_inv(kRecCapMax, kAccAtomsMax), TG::SMEM_MAX)));
-    INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_inv<T, NX, NY, NZ, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)TG::smem_inv(0, 0)));
-    attr_done[dev] = true;
-  }
+  if (dev >= 64) return fail(INQB_ERR_UNSUPPORTED, "device index above 63");
+  int attr_rc = INQB_OK;
+  std::call_once(attr_once[dev], [&attr_rc] {
+    attr_rc = [] {
+      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_fwd<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)std::min(TG::smem_fwd(kAccAtomsMax, kRecCapMax), TG::SMEM_MAX)));
+      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)TG::SMEM_X));
+      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x_fft<T, NX, NY, NZ, 0>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TG::SMEM_X));
+      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x_fft<T, NX, NY, NZ, 1>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TG::SMEM_X));
+      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_inv<T, NX, NY, NZ, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)std::min(TG::smem_inv(kRecCapMax, kAccAtomsMax), TG::SMEM_MAX)));
+      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_inv<T, NX, NY, NZ, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)TG::smem_inv(0, 0)));
+      return (int)INQB_OK;
+    }();
+  });
+  if (attr_rc != INQB_OK) return attr_rc;
   const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(a.tw);
   const cplx<T>* twx = tw;
   const cplx<T>* twy = tw + NX;
