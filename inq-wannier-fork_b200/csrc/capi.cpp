@@ -470,6 +470,7 @@ const char* inqb_status_string(int status) {
     case INQB_ERR_NONFINITE: return "non-finite input";
     case INQB_ERR_NOT_POSITIVE_DEFINITE: return "matrix not positive definite";
     case INQB_ERR_TIMEOUT: return "device wait timed out";
+    case INQB_ERR_IO: return "checkpoint file missing, short or unwritable";
     default: return "unknown status";
   }
 }

@@ -36,6 +36,7 @@ def test_status_strings(pb):
     assert lib.inqb_version() >= 1
     assert lib.inqb_status_string(0) == b"ok"
     assert lib.inqb_status_string(6) == b"matrix not positive definite"
+    assert lib.inqb_status_string(8) == b"checkpoint file missing, short or unwritable"
 
 
 def test_grid_support_table(pb):
@@ -99,3 +100,19 @@ def test_setup_argument_errors(pb):
     bad = np.array([20, 0, 20], np.int32)
     assert pb.lib().inqb_sphere_size(_lib.dptr(lat), _lib.iptr(bad), _lib.dptr(c), 2.0, ctypes.byref(n)) == 1
     assert b"grid" in pb.lib().inqb_last_error()
+
+
+def test_new_entry_points_reject_a_null_context(pb):
+    """The density -> potential, checkpoint, TD-MLWF and kick entry points check their
+    context before touching a device."""
+    lib = pb.lib()
+    three = (ctypes.c_double * 3)(0.0, 0.0, 0.0)
+    assert lib.inqb_poisson(None, None, None, 1, 1, None) == 1
+    assert lib.inqb_ks_potential(None, None, None, 2, None, None) == 1
+    assert lib.inqb_set_density_reduce(None, None, None) == 1
+    assert lib.inqb_save_orbitals(None, b"x", 0, None, 1, 1, 0, None, None) == 1
+    assert lib.inqb_load_density(None, b"x", None, None) == 1
+    assert lib.inqb_mlwf_step(None, None, 1, 1, 100, 1e-8, None, None, None, None) == 1
+    assert lib.inqb_jade(None, 2, None, None, None, 100, 1e-8, None, None) == 1
+    assert lib.inqb_kick(None, None, 1, 1, three, None) == 1
+    assert b"null context" in lib.inqb_last_error()
