@@ -8,8 +8,12 @@
 // should let the caller decide).
 //
 //   inq::b200::device_orbitals   an [N][M] complex block in device memory
+//   inq::b200::device_field      an [N] FP64 field in device memory (density, potential)
 //   inq::b200::ks_hamiltonian    ks_hamiltonian<complex>::operator() (ks_hamiltonian.hpp:132-152)
 //   inq::b200::exponential_in_place / etrs    operations / real_time counterparts
+//   inq::b200::self_consistency / energy      update_hamiltonian (self_consistency.hpp:89-160)
+//   inq::b200::mlwf_properties   the fork's TD-MLWF step (mlwf_properties.hpp:28-44)
+//   inq::b200::io::save / load   checkpoints in INQ's restart layout (operations/io.hpp)
 #pragma once
 
 #include <cuda_runtime.h>
@@ -18,6 +22,7 @@
 #include <array>
 #include <complex>
 #include <cstddef>
+#include <ostream>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -256,6 +261,142 @@ void exponential_generic(const HamiltonianType& ham, std::complex<double> factor
   }
   if (cudaStreamSynchronize(nullptr) != cudaSuccess) throw std::runtime_error("exponential sync");
 }
+
+// An [N] FP64 field in device memory: the density or a potential of one spin component
+// (basis::field<real_space, double>).
+class device_field {
+ public:
+  explicit device_field(long npoints) : N_(npoints) {
+    if (cudaMalloc(&data_, sizeof(double) * N_) != cudaSuccess) throw std::runtime_error("cudaMalloc failed (field)");
+  }
+  device_field(const device_field&) = delete;
+  device_field& operator=(const device_field&) = delete;
+  ~device_field() {
+    if (data_) cudaFree(data_);
+  }
+  double* data() { return data_; }
+  const double* data() const { return data_; }
+  long size() const { return N_; }
+  void upload(const std::vector<double>& h) {
+    if ((long)h.size() != N_) throw std::invalid_argument("field size");
+    if (cudaMemcpy(data_, h.data(), sizeof(double) * N_, cudaMemcpyHostToDevice) != cudaSuccess)
+      throw std::runtime_error("field upload failed");
+  }
+  std::vector<double> download() const {
+    std::vector<double> h((size_t)N_);
+    if (cudaMemcpy(h.data(), data_, sizeof(double) * N_, cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw std::runtime_error("field download failed");
+    return h;
+  }
+
+ private:
+  double* data_ = nullptr;
+  long N_ = 0;
+};
+
+// observables::density::calculate (density.hpp:23-52): occupations on the device
+inline void density(ks_hamiltonian& ham, const device_orbitals& phi, const device_field& occ, device_field& rho) {
+  check(inqb_density(ham.handle(), phi.data(), phi.set_size(), phi.set_size(), occ.data(), rho.data(), nullptr),
+        "inqb_density");
+}
+
+// The energy terms update_hamiltonian records (hamiltonian/energy.hpp:26-56)
+struct energy {
+  double external = 0.0, hartree = 0.0, xc = 0.0, nvxc = 0.0;
+};
+
+// self_consistency for static ions, an unpolarised density, no core density
+// (self_consistency.hpp:28-160); theory: INQB_THEORY_NONE, _HARTREE or _LDA.
+class self_consistency {
+ public:
+  self_consistency(int theory, const device_field* vion) : theory_(theory), vion_(vion) {}
+  // update_hamiltonian (self_consistency.hpp:89-160): the potential of ham becomes
+  // vion + V_H[rho] + v_xc[rho]
+  void update_hamiltonian(ks_hamiltonian& ham, energy& en, const device_field& rho) const {
+    double e[4];
+    check(inqb_ks_potential(ham.handle(), rho.data(), vion_ ? vion_->data() : nullptr, theory_, e, nullptr),
+          "inqb_ks_potential");
+    en = energy{e[0], e[1], e[2], e[3]};
+  }
+  int theory() const { return theory_; }
+  const double* vion() const { return vion_ ? vion_->data() : nullptr; }
+
+ private:
+  int theory_;
+  const device_field* vion_;
+};
+
+// real_time::etrs with its self-consistency loop (etrs.hpp:22-82); rho is the density
+// of phi on entry and of the propagated phi on exit.  Returns the SCF iterations.
+inline int etrs(ks_hamiltonian& ham, double dt, const std::array<double, 3>& A_t, const std::array<double, 3>& A_tdt,
+                device_orbitals& phi, const device_field& occ, device_field& rho, const self_consistency& sc,
+                energy& en, int nscf = 5, double threshold = 5e-5) {
+  std::array<double, 3> c1, c2;
+  check(inqb_cart_to_cov(ham.handle(), A_t.data(), c1.data()), "inqb_cart_to_cov");
+  check(inqb_cart_to_cov(ham.handle(), A_tdt.data(), c2.data()), "inqb_cart_to_cov");
+  int iters = 0;
+  double e[4];
+  check(inqb_etrs_scf_step(ham.handle(), phi.data(), phi.set_size(), phi.set_size(), dt, c1.data(), c2.data(),
+                           occ.data(), rho.data(), sc.vion(), sc.theory(), nscf, threshold, &iters, e, nullptr),
+        "inqb_etrs_scf_step");
+  en = energy{e[0], e[1], e[2], e[3]};
+  return iters;
+}
+
+// observables::mlwf_properties::calculate (mlwf_properties.hpp:28-44): phi rotated in
+// place to the maximally localised gauge, then the reference's lines on out.
+class mlwf_properties {
+ public:
+  explicit mlwf_properties(int maxsweep = 100, double tol = 1e-8) : maxsweep_(maxsweep), tol_(tol) {}
+  void calculate(std::ostream& out, int time_step, ks_hamiltonian& ham, device_orbitals& phi) {
+    const int M = phi.set_size();
+    centres_.assign(3 * (size_t)M, 0.0);
+    spreads_.assign((size_t)M, 0.0);
+    check(inqb_mlwf_step(ham.handle(), phi.data(), M, M, maxsweep_, tol_, &sweeps_, centres_.data(), spreads_.data(),
+                         nullptr),
+          "inqb_mlwf_step");
+    out << "Time step: " << time_step + 1 << "\n";
+    out << "MLWFs:\n";
+    for (int i = 0; i < M; ++i)
+      out << "  WF " << i + 1 << ": " << centres_[3 * i] << "     " << centres_[3 * i + 1] << "     "
+          << centres_[3 * i + 2] << "     Spread: " << spreads_[i] << std::endl;
+  }
+  const std::vector<double>& centres() const { return centres_; }
+  const std::vector<double>& spreads() const { return spreads_; }
+  int sweeps() const { return sweeps_; }
+
+ private:
+  int maxsweep_;
+  double tol_;
+  int sweeps_ = 0;
+  std::vector<double> centres_, spreads_;
+};
+
+// Checkpoints in INQ's restart layout (operations/io.hpp:42-177,
+// systems/electrons.hpp:323-375): states and occupations of one k-point block
+// (first_state when the states are sharded), and the density.
+namespace io {
+inline void save(const std::string& dirname, ks_hamiltonian& ham, const device_orbitals& phi,
+                 const std::vector<double>& occ, const device_field& rho, int first_state = 0, int kpin = 0) {
+  check(inqb_save_orbitals(ham.handle(), dirname.c_str(), kpin, phi.data(), phi.set_size(), phi.set_size(),
+                           first_state, occ.empty() ? nullptr : occ.data(), nullptr),
+        "inqb_save_orbitals");
+  check(inqb_save_density(ham.handle(), dirname.c_str(), rho.data(), nullptr), "inqb_save_density");
+}
+// false when a file is missing or short (io::load returns false there)
+inline bool load(const std::string& dirname, ks_hamiltonian& ham, device_orbitals& phi, std::vector<double>& occ,
+                 device_field& rho, int first_state = 0, int kpin = 0) {
+  occ.assign((size_t)phi.set_size(), 0.0);
+  int st = inqb_load_orbitals(ham.handle(), dirname.c_str(), kpin, phi.data(), phi.set_size(), phi.set_size(),
+                              first_state, occ.data(), nullptr);
+  if (st == INQB_ERR_IO) return false;
+  check(st, "inqb_load_orbitals");
+  st = inqb_load_density(ham.handle(), dirname.c_str(), rho.data(), nullptr);
+  if (st == INQB_ERR_IO) return false;
+  check(st, "inqb_load_density");
+  return true;
+}
+}  // namespace io
 
 }  // namespace b200
 }  // namespace inq

@@ -1,17 +1,22 @@
 // C++ host-adapter check (built and run by tests/test_host_adapter.py).
 // Harmonic oscillator of ks_hamiltonian.hpp:356-397 through inq::b200::ks_hamiltonian,
 // then the generic INQ-style Taylor exponential written against HamiltonianType
-// against the library's fused exponential, and one ETRS step.
+// against the library's fused exponential, one ETRS step, one ETRS step with the LDA
+// self-consistency loop, the TD-MLWF step and a checkpoint round trip (directory in
+// argv[1]).
 #include <cmath>
 #include <complex>
 #include <cstdio>
+#include <sstream>
+#include <string>
 #include <vector>
 
 #include "../../inq-wannier-fork_b200/host/inq_b200.hpp"
 
 using cd = std::complex<double>;
 
-int main() {
+int main(int argc, char** argv) {
+  const std::string dir = argc > 1 ? argv[1] : "host_adapter_ckpt";
   namespace b2 = inq::b200;
   const std::array<double, 9> lat = {10, 0, 0, 0, 10, 0, 0, 0, 10};
   const std::array<int, 3> nr = {20, 20, 20};
@@ -57,5 +62,42 @@ int main() {
   double nrm = 0.0;
   for (auto& x : vc) nrm += std::norm(x);
   std::printf("etrs_norm %.12e\n", nrm * ham.volume_element());
+
+  // self-consistent ETRS with the LDA (self_consistency + etrs overload)
+  b2::device_field occ(M), rho(N), vion(N);
+  occ.upload(std::vector<double>(M, 2.0));
+  vion.upload(V);
+  b2::density(ham, b, occ, rho);
+  b2::self_consistency sc(INQB_THEORY_LDA, &vion);
+  b2::energy en;
+  sc.update_hamiltonian(ham, en, rho);
+  const int iters = b2::etrs(ham, 0.05, {0.0, 0.0, 0.0}, {0.01, 0.0, 0.0}, b, occ, rho, sc, en);
+  double q = 0.0;
+  for (double x : rho.download()) q += x;
+  std::printf("scf_iterations %d\n", iters);
+  std::printf("scf_charge %.12e\n", q * ham.volume_element());
+  std::printf("scf_xc %.12e\n", en.xc);
+
+  // TD-MLWF lines
+  b2::mlwf_properties mp;
+  std::ostringstream os;
+  mp.calculate(os, 0, ham, b);
+  int lines = 0;
+  for (char c : os.str()) lines += (c == '\n');
+  std::printf("mlwf_lines %d\n", lines);
+
+  // checkpoint round trip
+  b2::io::save(dir, ham, b, std::vector<double>(M, 2.0), rho);
+  b2::device_orbitals c = b.skeleton();
+  b2::device_field rho2(N);
+  std::vector<double> occ2;
+  const bool ok = b2::io::load(dir, ham, c, occ2, rho2);
+  const bool missing = b2::io::load(dir + "_absent", ham, c, occ2, rho2);
+  auto vb2 = b.download(), vc2 = c.download();
+  double d2 = 0.0;
+  for (long i = 0; i < N * M; i++) d2 = std::max(d2, std::abs(vb2[i] - vc2[i]));
+  std::printf("io_loaded %d\n", ok ? 1 : 0);
+  std::printf("io_missing_loaded %d\n", missing ? 1 : 0);
+  std::printf("io_maxdiff %.12e\n", d2);
   return 0;
 }
