@@ -278,9 +278,31 @@ int inqb_ks_potential(inqb_ctx* ctx, const double* rho, const double* vion, int 
 int inqb_etrs_scf_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
                        const double kA_tdt_cov[3], const double* occ, double* rho, const double* vion, int theory,
                        int nscf, double threshold, int* iters, double energies[4], void* stream);
+/* real_time::crank_nicolson with its self-consistency loop (src/real_time/crank_nicolson.hpp:41-114),
+ * static ions, no induced vector potential, exchange off.  Entry conditions as for
+ * inqb_etrs_scf_step: the potential is the Kohn-Sham potential of rho, the density of
+ * psi at t.  rhs = (1 - i dt/2 H(kA_t)) psi; then for istep < max_iter: update the
+ * potential from rho at kA_tdt; five steps of solvers::steepest_descent on
+ * (1 + i dt/2 H) psi = rhs from the current psi (as in inqb_crank_nicolson_step);
+ * new = density(psi); stop when dV sum |rho - new| / num_electrons < dens_tol;
+ * otherwise rho becomes the Broyden mix of rho and new (mixers::broyden with 4 steps
+ * and mixing 0.3, src/mixers/broyden.hpp:26-160) normalised to num_electrons
+ * (observables::density::normalize, src/observables/density.hpp:100-111).  On exit
+ * rho = density(psi) and the potential is updated from it.  The reference uses
+ * max_iter 300 and dens_tol 1e-5; num_electrons is the total over all ranks
+ * (electrons.states().num_electrons()).  The mixer's vectors are FP64 on the device;
+ * its small solve runs on the host.  Synchronises a few times per iteration.  occ:
+ * FP64 device [M]; vion may be NULL (zero); iters, residual (the solver's last
+ * largest dV <r|r>) and energies (host) may be NULL.  Calls the density-reduce
+ * callback like inqb_etrs_scf_step. */
+int inqb_crank_nicolson_scf_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                                 const double kA_tdt_cov[3], const double* occ, double num_electrons, double* rho,
+                                 const double* vion, int theory, int max_iter, double dens_tol, int* iters,
+                                 double* residual, double energies[4], void* stream);
 /* The exchange step of an orbital-sharded run (one block of states per GPU): INQ sums
  * the density over its states communicator (src/observables/density.hpp:77-95).  When
- * set, inqb_etrs_scf_step calls fn(rho, N, user) after each density of its own orbitals,
+ * set, inqb_etrs_scf_step and inqb_crank_nicolson_scf_step call fn(rho, N, user) after
+ * each density of their own orbitals,
  * with the stream synchronised; fn must leave the sum over all ranks in rho (device
  * memory) and return 0 when the reduction is complete; nonzero ends the step with
  * INQB_ERR_INVALID.  fn NULL removes it. */

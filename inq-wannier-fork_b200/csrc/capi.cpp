@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "inqb_internal.h"
+#include "broyden_host.h"
 #include "adjoint.h"
 #include "checkpoint.h"
 #include "observables.h"
@@ -234,6 +235,92 @@ int pot_work(inqb_ctx* ctx, PotWork& w) {
   w.partial = w.rho_old + N;
   w.sums = w.partial + (size_t)kPotBlocks * 4;
   return INQB_OK;
+}
+
+// Workspace of the Broyden density mixer, carved from ctx->d_mix
+struct MixWork {
+  static constexpr int kRing = 4;  // mixers::broyden(4, 0.3, ...) in crank_nicolson.hpp:68
+  double* df = nullptr;       // [kRing][N]
+  double* dv = nullptr;       // [kRing][N]
+  double* f_old = nullptr;    // [N]: the last vout - vin
+  double* vin_old = nullptr;  // [N]
+  double* fresh = nullptr;    // [N]: the density of the solved orbitals
+  double* partial = nullptr;  // [kPotBlocks * kMaxDots]
+  double* dots = nullptr;     // [kMaxDots + 1]: dot products, then the sum for the normalisation
+};
+
+int mix_work(inqb_ctx* ctx, MixWork& w) {
+  const size_t N = (size_t)ctx->N;
+  const size_t n = (2 * MixWork::kRing + 3) * N + (size_t)kPotBlocks * kMaxDots + kMaxDots + 1;
+  INQB_TRY(ctx->d_mix.ensure(sizeof(double) * n));
+  double* b = ctx->d_mix.as<double>();
+  w.df = b;
+  w.dv = w.df + MixWork::kRing * N;
+  w.f_old = w.dv + MixWork::kRing * N;
+  w.vin_old = w.f_old + N;
+  w.fresh = w.vin_old + N;
+  w.partial = w.fresh + N;
+  w.dots = w.partial + (size_t)kPotBlocks * kMaxDots;
+  return INQB_OK;
+}
+
+// nd dot products of device vectors, read back (synchronises the stream)
+int device_dots(const DotList& d, int nd, long n, const MixWork& w, double* out, void* stream) {
+  INQB_TRY(launch_dots(d, nd, n, w.partial, w.dots, stream));
+  INQB_CUDA_TRY(cudaMemcpyAsync(out, w.dots, sizeof(double) * nd, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  INQB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  return INQB_OK;
+}
+
+// One call of mixers::broyden (broyden.hpp:107-160) on the density, vin = rho and
+// vout = w.fresh, then observables::density::normalize(rho, nelec)
+// (density.hpp:100-111).  The vectors stay on the device; the ring bookkeeping and
+// the small solve are on the host (broyden_host.h).  Synchronises three times.
+int broyden_mix_density(inqb_ctx* ctx, BroydenRing& ring, double* rho, const MixWork& w, double nelec,
+                        void* stream) {
+  const long N = ctx->N;
+  const int pos = ring.begin();
+  double* dfp = pos >= 0 ? w.df + (size_t)pos * N : nullptr;
+  double* dvp = pos >= 0 ? w.dv + (size_t)pos * N : nullptr;
+  INQB_TRY(launch_broyden_diff(rho, w.fresh, w.f_old, w.vin_old, dfp, dvp, N, stream));
+  if (pos >= 0) {
+    DotList d{};
+    d.a[0] = dfp;
+    d.b[0] = dfp;
+    double g2 = 0.0;
+    INQB_TRY(device_dots(d, 1, N, w, &g2, stream));
+    const double gamma = std::max(1e-8, std::sqrt(g2));
+    INQB_TRY(launch_scale2(dfp, dvp, 1.0 / gamma, N, stream));
+    ring.filled(pos);
+  }
+  const int used = ring.used();
+  BroydenCoef c{};
+  if (used > 0) {
+    DotList d{};
+    int k = 0;
+    for (int i = 0; i < used; i++)
+      for (int j = i + 1; j < used; j++, k++) {
+        d.a[k] = w.df + (size_t)i * N;
+        d.b[k] = w.df + (size_t)j * N;
+      }
+    for (int i = 0; i < used; i++, k++) {
+      d.a[k] = w.df + (size_t)i * N;
+      d.b[k] = w.f_old;  // ff of this call
+    }
+    double dots[kMaxDots];
+    INQB_TRY(device_dots(d, k, N, w, dots, stream));
+    if (!broyden_coefficients(used, dots, c.c))
+      return fail(INQB_ERR_NONFINITE, "Broyden mixing: the history system is not finite");
+  }
+  INQB_TRY(launch_broyden_update(rho, w.f_old, w.df, w.dv, N, used, c, ring.mix, w.partial, w.dots + kMaxDots,
+                                 stream));
+  double q = 0.0;
+  INQB_CUDA_TRY(cudaMemcpyAsync(&q, w.dots + kMaxDots, sizeof(double), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  INQB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  q *= ctx->dV;
+  if (!(std::fabs(q) > 1e-16) || !std::isfinite(q))
+    return fail(INQB_ERR_NONFINITE, "density normalisation: the mixed density integrates to zero");
+  return launch_scale(rho, nelec / q, N, stream);
 }
 
 // update_hamiltonian on the device: V_H by the Poisson passes, then one pass for
@@ -1063,6 +1150,88 @@ int inqb_crank_nicolson_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt,
   }
   if (sweeps) *sweeps = k;
   if (residual) *residual = res;
+  return INQB_OK;
+}
+
+int inqb_crank_nicolson_scf_step(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                                 const double kA_tdt_cov[3], const double* occ, double num_electrons, double* rho,
+                                 const double* vion, int theory, int max_iter, double dens_tol, int* iters,
+                                 double* residual, double energies[4], void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!kA_t_cov || !kA_tdt_cov || !occ || !rho || !std::isfinite(dt) || max_iter < 1 || !(dens_tol >= 0.0) ||
+      !(num_electrons > 0.0) || !std::isfinite(num_electrons))
+    return fail(INQB_ERR_INVALID, "bad step arguments");
+  if (theory < INQB_THEORY_NONE || theory > INQB_THEORY_LDA) return fail(INQB_ERR_INVALID, "unknown theory");
+  INQB_GUARD(ctx);
+  INQB_TRY(reserve(ctx, M));
+  const long N = ctx->N;
+  const size_t blk = (size_t)N * M * ctx->elem_bytes();
+  INQB_TRY(ctx->d_cn.ensure(3 * blk));
+  INQB_TRY(ctx->d_cnred.ensure(sizeof(double) * 5 * (size_t)M));
+  char* wb = static_cast<char*>(ctx->d_cn.ptr);
+  void* rhs = wb;
+  void* r = wb + blk;
+  void* hsd = wb + 2 * blk;
+  double* acc = ctx->d_cnred.as<double>();
+  double* normres = acc + 4 * (size_t)M;
+  PotWork pw;
+  INQB_TRY(pot_work(ctx, pw));
+  MixWork mw;
+  INQB_TRY(mix_work(ctx, mw));
+  const long Mi = M;
+  cudaStream_t st = (cudaStream_t)stream;
+  const double one[2] = {1.0, 0.0};
+  const double fr[2] = {0.0, -0.5 * dt}, fl[2] = {0.0, 0.5 * dt};
+
+  // rhs = (1 - i dt/2 H(t)) psi with the potential of rho at t (crank_nicolson.hpp:47-56)
+  INQB_TRY(set_kA(ctx, kA_t_cov, stream));
+  INQB_TRY(apply(ctx, LaunchArgs::H, psi, ld, rhs, Mi, M, psi, ld, fr, one, stream));
+  INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
+
+  BroydenRing ring;  // mixers::broyden(4, 0.3, ...)
+  std::vector<double> hres(M);
+  double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  double res = 0.0;
+  int done_iters = 0;
+  for (int istep = 0; istep < max_iter; istep++) {
+    // update_hamiltonian(rho) at t + dt, then steepest_descent (five steps, as in
+    // inqb_crank_nicolson_step) from the current psi
+    INQB_TRY(ks_potential_dev(ctx, rho, vion, theory, pw, stream));
+    for (int step = 0; step < 5; step++) {
+      INQB_TRY(apply(ctx, LaunchArgs::H, psi, ld, r, Mi, M, psi, ld, fl, one, stream));
+      {
+        const double a[2][2] = {{1.0, 0.0}, {-1.0, 0.0}};
+        const void* x[2] = {r, rhs};
+        const long ldx[2] = {Mi, Mi};
+        INQB_TRY(launch_lincomb(ctx->precision, N, M, 2, a, x, ldx, r, Mi, stream));
+      }
+      INQB_TRY(apply(ctx, LaunchArgs::H, r, Mi, hsd, Mi, M, r, Mi, fl, one, stream));
+      INQB_TRY(launch_sd_sums(ctx->precision, r, hsd, Mi, M, N, acc, stream));
+      INQB_TRY(launch_sd_update(ctx->precision, psi, ld, r, Mi, M, N, acc, ctx->dV, normres, stream));
+    }
+    // the new density and dV sum |rho - new| / nelec (crank_nicolson.hpp:98-99)
+    INQB_TRY(sharded_density(ctx, psi, ld, M, occ, mw.fresh, stream));
+    INQB_TRY(launch_absdiff(rho, mw.fresh, N, pw.partial, pw.sums + 4, stream));
+    INQB_CUDA_TRY(cudaMemcpyAsync(hres.data(), normres, sizeof(double) * M, cudaMemcpyDeviceToHost, st));
+    INQB_CUDA_TRY(cudaMemcpyAsync(s, pw.sums, sizeof(s), cudaMemcpyDeviceToHost, st));
+    INQB_CUDA_TRY(cudaStreamSynchronize(st));
+    res = 0.0;
+    for (double v : hres) res = std::max(res, v);
+    if (!std::isfinite(res)) return fail(INQB_ERR_NONFINITE, "Crank-Nicolson residual is not finite");
+    done_iters = istep + 1;
+    if (ctx->dV * s[4] / num_electrons < dens_tol) break;
+    // mixer(rho, new) and normalize(rho, nelec) (crank_nicolson.hpp:107-108)
+    INQB_TRY(broyden_mix_density(ctx, ring, rho, mw, num_electrons, stream));
+  }
+  // rho = density(psi), update_hamiltonian(rho) (crank_nicolson.hpp:111-112)
+  INQB_TRY(sharded_density(ctx, psi, ld, M, occ, rho, stream));
+  INQB_TRY(ks_potential_dev(ctx, rho, vion, theory, pw, stream));
+  INQB_CUDA_TRY(cudaMemcpyAsync(s, pw.sums, sizeof(double) * 4, cudaMemcpyDeviceToHost, st));
+  INQB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (iters) *iters = done_iters;
+  if (residual) *residual = res;
+  if (energies) energies_from_sums(ctx, s, energies);
   return INQB_OK;
 }
 

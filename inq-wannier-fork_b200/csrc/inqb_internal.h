@@ -197,6 +197,8 @@ struct inqb_ctx {
   inqb::DevBuf d_mlwf;          // TD-MLWF: the six matrices, u, adiag, sums, slabs, pairs, deltas
   inqb::DevBuf d_pot;           // density -> potential: V_H field [N] (complex), previous
                                 // density [N], partial sums, sums
+  inqb::DevBuf d_mix;           // Crank-Nicolson with self-consistency: Broyden ring df, dv [4][N],
+                                // f_old, vin_old, the new density [N], partial sums, dot products
   size_t elem_bytes() const { return precision == INQB_FP64 ? 16 : 8; }
 
   // launch schedules per orbital count (ysplit, threads of the three passes), set

@@ -10,6 +10,10 @@
 //             deterministic
 //   shift2    a1 += c1 y, a2 += c2 y: the two accumulators of
 //             operations::exponential_2_for_1 (src/operations/exponential.hpp:50-69)
+//   broyden   the vector passes of mixers::broyden (src/mixers/broyden.hpp:107-160),
+//             the density mixer of the self-consistent Crank-Nicolson step: the
+//             differences, up to 16 dot products in a fixed order, the update with
+//             the sum for observables::density::normalize, and scalings
 //
 // The exchange-correlation functional is evaluated in FP64 in both precisions (it is
 // one pass over N points).  libxc, which the reference calls for it
@@ -160,6 +164,66 @@ __global__ void k_shift2(const cplx<T>* __restrict__ y, long ldy, cplx<T>* __res
   }
 }
 
+// ---- Broyden density mixer (src/mixers/broyden.hpp:107-160), FP64 vectors of n values
+
+// ff = vout - vin, kept in f_old (the reference sets f_old = ff after using the old
+// value); with a ring slot, df = ff - f_old and dv = vin - vin_old first; vin_old = vin.
+__global__ void __launch_bounds__(kThreads)
+    k_broyden_diff(const double* __restrict__ vin, const double* __restrict__ vout, double* __restrict__ f_old,
+                   double* __restrict__ vin_old, double* __restrict__ df, double* __restrict__ dv, long n) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double x = vin[i], f = vout[i] - x;
+    if (df) {
+      df[i] = f - f_old[i];
+      dv[i] = x - vin_old[i];
+    }
+    f_old[i] = f;
+    vin_old[i] = x;
+  }
+}
+
+// per-block partial sums of a_k . b_k for k < nd
+__global__ void __launch_bounds__(kThreads) k_dots(DotList d, int nd, long n, double* __restrict__ partial) {
+  double s[kMaxDots];
+#pragma unroll
+  for (int k = 0; k < kMaxDots; ++k) s[k] = 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < kMaxDots; ++k)
+      if (k < nd) s[k] += d.a[k][i] * d.b[k][i];
+  }
+  block_sum_store<kMaxDots>(s, partial + (long)kMaxDots * blockIdx.x);
+}
+
+__global__ void k_scale2(double* __restrict__ x, double* __restrict__ y, double s, long n) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    x[i] *= s;
+    y[i] *= s;
+  }
+}
+
+// vin += mix ff - sum_k c_k (mix df_k + dv_k) (broyden_extrapolation, broyden.hpp:95-101),
+// with per-block partial sums of the new vin
+__global__ void __launch_bounds__(kThreads)
+    k_broyden_update(double* __restrict__ vin, const double* __restrict__ ff, const double* __restrict__ df,
+                     const double* __restrict__ dv, long n, int used, BroydenCoef c, double mix,
+                     double* __restrict__ partial) {
+  double s[1] = {0.0};
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double v = vin[i] + mix * ff[i];
+#pragma unroll
+    for (int k = 0; k < kMaxBroyden; ++k)
+      if (k < used) v -= c.c[k] * (mix * df[(long)k * n + i] + dv[(long)k * n + i]);
+    vin[i] = v;
+    s[0] += v;
+  }
+  block_sum_store<1>(s, partial + blockIdx.x);
+}
+
+__global__ void k_scale(double* __restrict__ x, double s, long n) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) x[i] *= s;
+}
+
 int grid_for(long n) { return (int)std::max<long>(1, std::min<long>((n + kThreads - 1) / kThreads, kPotBlocks)); }
 
 }  // namespace
@@ -211,6 +275,49 @@ int launch_shift2(int precision, const void* y, long ldy, void* a1, long ld1, vo
   else
     k_shift2<float><<<nb, kThreads, 0, st>>>((const cplx<float>*)y, ldy, (cplx<float>*)a1, ld1,
                                               (cplx<float>*)a2, ld2, M, N, c1[0], c1[1], c2[0], c2[1]);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_broyden_diff(const double* vin, const double* vout, double* f_old, double* vin_old, double* df,
+                        double* dv, long n, void* stream) {
+  if ((df == nullptr) != (dv == nullptr)) return fail(INQB_ERR_INVALID, "Broyden ring slot: df and dv together");
+  k_broyden_diff<<<grid_for(n), kThreads, 0, (cudaStream_t)stream>>>(vin, vout, f_old, vin_old, df, dv, n);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_dots(const DotList& d, int nd, long n, double* partial, double* out, void* stream) {
+  if (nd < 1 || nd > kMaxDots) return fail(INQB_ERR_INVALID, "launch_dots: 1 to 16 products");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nb = grid_for(n);
+  k_dots<<<nb, kThreads, 0, st>>>(d, nd, n, partial);
+  INQB_CUDA_TRY(cudaGetLastError());
+  k_finish<<<1, kThreads, 0, st>>>(partial, nb, kMaxDots, out);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_scale2(double* x, double* y, double s, long n, void* stream) {
+  k_scale2<<<grid_for(n), kThreads, 0, (cudaStream_t)stream>>>(x, y, s, n);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_broyden_update(double* vin, const double* ff, const double* df, const double* dv, long n, int used,
+                          const BroydenCoef& c, double mix, double* partial, double* sum, void* stream) {
+  if (used < 0 || used > kMaxBroyden) return fail(INQB_ERR_INVALID, "Broyden update: 0 to 8 ring slots");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nb = grid_for(n);
+  k_broyden_update<<<nb, kThreads, 0, st>>>(vin, ff, df, dv, n, used, c, mix, partial);
+  INQB_CUDA_TRY(cudaGetLastError());
+  k_finish<<<1, kThreads, 0, st>>>(partial, nb, 1, sum);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_scale(double* x, double s, long n, void* stream) {
+  k_scale<<<grid_for(n), kThreads, 0, (cudaStream_t)stream>>>(x, s, n);
   INQB_CUDA_TRY(cudaGetLastError());
   return INQB_OK;
 }

@@ -20,4 +20,33 @@ int launch_absdiff(const double* a, const double* b, long N, double* partial, do
 int launch_shift2(int precision, const void* y, long ldy, void* a1, long ld1, void* a2, long ld2, int M, long N,
                   const double c1[2], const double c2[2], void* stream);
 
+
+// ---- Broyden density mixer (src/mixers/broyden.hpp:26-160) on FP64 device vectors of
+// n values.  The ring bookkeeping and the small solve are on the host
+// (broyden_host.h).
+constexpr int kMaxDots = 16;    // dot products per launch_dots call
+constexpr int kMaxBroyden = 8;  // ring slots the update kernel takes
+struct DotList {
+  const double* a[kMaxDots];
+  const double* b[kMaxDots];
+};
+struct BroydenCoef {
+  double c[kMaxBroyden];
+};
+// f_old = vout - vin and vin_old = vin; when df and dv are not null, first
+// df = (vout - vin) - f_old and dv = vin - vin_old.
+int launch_broyden_diff(const double* vin, const double* vout, double* f_old, double* vin_old, double* df,
+                        double* dv, long n, void* stream);
+// out[k] (device) = sum_i a_k[i] b_k[i] for k < nd <= kMaxDots, each in a fixed order.
+// partial: kPotBlocks * kMaxDots doubles.
+int launch_dots(const DotList& d, int nd, long n, double* partial, double* out, void* stream);
+// x *= s and y *= s
+int launch_scale2(double* x, double* y, double s, long n, void* stream);
+// vin += mix ff - sum_{k < used} c_k (mix df_k + dv_k), df and dv [used][n]; *sum (device)
+// = the sum of the new vin.  partial: kPotBlocks doubles.
+int launch_broyden_update(double* vin, const double* ff, const double* df, const double* dv, long n, int used,
+                          const BroydenCoef& c, double mix, double* partial, double* sum, void* stream);
+// x *= s
+int launch_scale(double* x, double s, long n, void* stream);
+
 }  // namespace inqb

@@ -10,7 +10,8 @@
 //   inq::b200::device_orbitals   an [N][M] complex block in device memory
 //   inq::b200::device_field      an [N] FP64 field in device memory (density, potential)
 //   inq::b200::ks_hamiltonian    ks_hamiltonian<complex>::operator() (ks_hamiltonian.hpp:132-152)
-//   inq::b200::exponential_in_place / etrs    operations / real_time counterparts
+//   inq::b200::exponential_in_place / etrs / crank_nicolson
+//                                 operations / real_time counterparts
 //   inq::b200::self_consistency / energy      update_hamiltonian (self_consistency.hpp:89-160)
 //   inq::b200::mlwf_properties   the fork's TD-MLWF step (mlwf_properties.hpp:28-44)
 //   inq::b200::io::save / load   checkpoints in INQ's restart layout (operations/io.hpp)
@@ -339,6 +340,27 @@ inline int etrs(ks_hamiltonian& ham, double dt, const std::array<double, 3>& A_t
   check(inqb_etrs_scf_step(ham.handle(), phi.data(), phi.set_size(), phi.set_size(), dt, c1.data(), c2.data(),
                            occ.data(), rho.data(), sc.vion(), sc.theory(), nscf, threshold, &iters, e, nullptr),
         "inqb_etrs_scf_step");
+  en = energy{e[0], e[1], e[2], e[3]};
+  return iters;
+}
+
+// real_time::crank_nicolson with its self-consistency loop and Broyden density mixing
+// (crank_nicolson.hpp:41-114); rho is the density of phi on entry and of the
+// propagated phi on exit; num_electrons is electrons.states().num_electrons().
+// Returns the iterations run.
+inline int crank_nicolson(ks_hamiltonian& ham, double dt, const std::array<double, 3>& A_t,
+                          const std::array<double, 3>& A_tdt, device_orbitals& phi, const device_field& occ,
+                          double num_electrons, device_field& rho, const self_consistency& sc, energy& en,
+                          int max_iter = 300, double dens_tol = 1e-5) {
+  std::array<double, 3> c1, c2;
+  check(inqb_cart_to_cov(ham.handle(), A_t.data(), c1.data()), "inqb_cart_to_cov");
+  check(inqb_cart_to_cov(ham.handle(), A_tdt.data(), c2.data()), "inqb_cart_to_cov");
+  int iters = 0;
+  double e[4];
+  check(inqb_crank_nicolson_scf_step(ham.handle(), phi.data(), phi.set_size(), phi.set_size(), dt, c1.data(),
+                                     c2.data(), occ.data(), num_electrons, rho.data(), sc.vion(), sc.theory(),
+                                     max_iter, dens_tol, &iters, nullptr, e, nullptr),
+        "inqb_crank_nicolson_scf_step");
   en = energy{e[0], e[1], e[2], e[3]};
   return iters;
 }

@@ -69,6 +69,9 @@ SIGNATURES = {
     "inqb_ks_potential": (ctypes.c_int, [_ctxp, _vp, _vp, ctypes.c_int, _dp, _vp]),
     "inqb_etrs_scf_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _vp,
                                           _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _ip, _dp, _vp]),
+    "inqb_crank_nicolson_scf_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp,
+                                                    _dp, _vp, ctypes.c_double, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_double, _ip, _dp, _dp, _vp]),
     "inqb_save_orbitals": (ctypes.c_int, [_ctxp, ctypes.c_char_p, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, _dp, _vp]),
     "inqb_load_orbitals": (ctypes.c_int, [_ctxp, ctypes.c_char_p, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,

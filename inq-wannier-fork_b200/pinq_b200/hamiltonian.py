@@ -80,6 +80,15 @@ def grid_supported(nr, precision="fp64") -> bool:
 
 
 # ------------------------------------------------------------------ the Hamiltonian
+class _DeviceDoubles:
+    """n FP64 values of device memory at ptr, exposed through __cuda_array_interface__
+    so torch.as_tensor makes a view of them (no copy)."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": "<f8", "data": (int(ptr), False),
+                                         "strides": None, "version": 3}
+
+
 class KSHamiltonian:
     """H|psi> and propagators for one cell/grid on one GPU (drop-in for ks_hamiltonian)."""
 
@@ -287,6 +296,58 @@ class KSHamiltonian:
             if cb is not None:
                 call("inqb_set_density_reduce", self._h, None, None)
         return it.value, dict(zip(("external", "hartree", "xc", "nvxc"), en.tolist()))
+
+    def crank_nicolson_scf_step_(self, psi, rho, dt, kA_t_cov, kA_tdt_cov, occ, vion=None, theory=2, max_iter=300,
+                                 dens_tol=1e-5, num_electrons=None):
+        """Crank-Nicolson with the self-consistency loop and Broyden density mixing of
+        real_time::crank_nicolson, in place on psi and rho (the potential must be the
+        Kohn-Sham potential of rho on entry).  num_electrons defaults to sum(occ); an
+        orbital-sharded run passes the total over the ranks.  Returns (iterations,
+        last solver residual, energies of the last update)."""
+        psi = self._check(psi)
+        rho = self._fp64_field(rho, "rho")
+        vion = self._fp64_field(vion, "vion")
+        occ_t = torch.as_tensor(occ, dtype=torch.float64, device=self.device).contiguous()
+        if occ_t.numel() != psi.shape[1]:
+            raise ValueError("one occupation per orbital")
+        nelec = float(np.sum(np.asarray(occ, np.float64))) if num_electrons is None else float(num_electrons)
+        a = np.ascontiguousarray(kA_t_cov, np.float64).reshape(3)
+        b = np.ascontiguousarray(kA_tdt_cov, np.float64).reshape(3)
+        it = ctypes.c_int(0)
+        res = ctypes.c_double(0.0)
+        en = np.zeros(4)
+        cb = self._install_density_reducer()
+        try:
+            call("inqb_crank_nicolson_scf_step", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), float(dt),
+                 dptr(a), dptr(b), occ_t.data_ptr(), nelec, rho.data_ptr(),
+                 vion.data_ptr() if vion is not None else None, int(theory), int(max_iter), float(dens_tol),
+                 ctypes.byref(it), ctypes.byref(res), dptr(en), self._stream())
+        finally:
+            if cb is not None:
+                call("inqb_set_density_reduce", self._h, None, None)
+        return it.value, res.value, dict(zip(("external", "hartree", "xc", "nvxc"), en.tolist()))
+
+    def _install_density_reducer(self):
+        """Registers the reducer set by set_density_reducer (if any) as the library's
+        density-reduce callback; returns the ctypes callback to keep alive, or None.
+        The reducer gets an FP64 tensor view of the buffer the library just filled
+        (the step's own density or its scratch copy), not a copy."""
+        reducer = getattr(self, "_density_reducer", None)
+        if reducer is None:
+            return None
+        device = self.device
+
+        def _reduce(ptr, n, user):
+            try:
+                with torch.cuda.device(device):
+                    view = torch.as_tensor(_DeviceDoubles(ptr, n), device=device)
+                reducer(view)
+                return 0
+            except Exception:  # reported to the caller as the step's failure
+                return 1
+        cb = _lib.DENSITY_REDUCE_FN(_reduce)
+        call("inqb_set_density_reduce", self._h, ctypes.cast(cb, ctypes.c_void_p), None)
+        return cb
 
     def set_density_reducer(self, reducer):
         """Orbital-sharded SCF: reducer(rho) must replace rho (an FP64 CUDA tensor) by

@@ -2,7 +2,8 @@
 
 One call runs the time loop the reference runs: the zero-time kick, the initial
 update of the Hamiltonian from the density, then per step the ETRS step (with its
-self-consistency loop when the theory is interacting) or the Crank-Nicolson step, the
+self-consistency loop when the theory is interacting) or the Crank-Nicolson step (with
+its Broyden-mixed self-consistency loop when the theory is interacting), the
 TD-MLWF transformation when asked (propagate.hpp:105-111), the energy, the
 real_time::results series, and a checkpoint every `checkpoint_every` steps
 (results.hpp:52-66).  Every numerical step is a library call; this module only
@@ -35,13 +36,16 @@ def _energy(ham, psi, occ, en):
 def propagate(ham, psi, occ, dt, num_steps, *, vion=None, theory=THEORY_NONE, propagator="etrs",
               vector_potential=None, kick=None, kick_gauge="velocity", tdmlwf=False, mlwf_out=None,
               results=None, checkpoint_dir=None, checkpoint_every=500, start_step=0, callback=None, nscf=5,
-              scf_threshold=5e-5, cn_max_sweeps=300, cn_tol=1e-10):
+              scf_threshold=5e-5, cn_max_sweeps=300, cn_tol=1e-10, cn_max_iter=300, cn_dens_tol=1e-5,
+              num_electrons=None):
     """Propagate psi ([N, M] CUDA tensor, in place) from start_step to num_steps.
 
     vion: FP64 CUDA tensor [N] of the ionic potential (the context's current potential
     when None and the theory is non-interacting).  theory: THEORY_NONE, THEORY_HARTREE or
-    THEORY_LDA.  propagator: "etrs" or "crank_nicolson" (the latter for a
-    density-independent Hamiltonian).  vector_potential: callable t -> cartesian A(t)
+    THEORY_LDA.  propagator: "etrs" or "crank_nicolson".  With an interacting theory, ETRS
+    runs its SCF loop (nscf, scf_threshold) and Crank-Nicolson its Broyden-mixed loop
+    (cn_max_iter, cn_dens_tol; num_electrons defaults to sum(occ)); without one,
+    Crank-Nicolson runs solver sweeps to cn_tol (cn_max_sweeps).  vector_potential: callable t -> cartesian A(t)
     (zero when None).  kick: cartesian kick field (perturbations::kick); in the velocity
     gauge it adds the constant vector potential -kick, in the length gauge it multiplies
     the orbitals by exp(-i kick . r) at step 0.  mlwf_out: open text file for the TD-MLWF
@@ -49,8 +53,6 @@ def propagate(ham, psi, occ, dt, num_steps, *, vion=None, theory=THEORY_NONE, pr
     psi, rho, energy) runs after step 0 and after every step.  Returns the results."""
     if propagator not in ("etrs", "crank_nicolson"):
         raise ValueError("propagator must be 'etrs' or 'crank_nicolson'")
-    if propagator == "crank_nicolson" and theory != THEORY_NONE:
-        raise NotImplementedError("Crank-Nicolson with a density-dependent potential (Broyden mixing) is not provided")
     if kick_gauge not in ("velocity", "length"):
         raise ValueError("kick_gauge must be 'velocity' or 'length'")
     occ = np.ascontiguousarray(occ, np.float64).reshape(psi.shape[1])
@@ -81,6 +83,9 @@ def propagate(ham, psi, occ, dt, num_steps, *, vion=None, theory=THEORY_NONE, pr
         k1, k2 = kA(t), kA(t + dt)
         if propagator == "etrs" and interacting:
             _, en = ham.etrs_scf_step_(psi, rho, dt, k1, k2, occ, vion, theory, nscf, scf_threshold)
+        elif interacting:
+            _, _, en = ham.crank_nicolson_scf_step_(psi, rho, dt, k1, k2, occ, vion, theory, cn_max_iter, cn_dens_tol,
+                                                    num_electrons)
         else:
             if propagator == "etrs":
                 ham.etrs_step_(psi, dt, k1, k2)

@@ -78,6 +78,16 @@ def lib():
         L.orc_etrs_scf_step.restype = ctypes.c_int
         L.orc_etrs_scf_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp, _dp,
                                         ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp]
+        L.orc_least_squares_sym.argtypes = [ctypes.c_int, _dp, _dp]
+        L.orc_broyden_create.restype = ctypes.c_void_p
+        L.orc_broyden_create.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_long]
+        L.orc_broyden_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_broyden_mix.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_density_normalize.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double]
+        L.orc_crank_nicolson_scf_step.restype = ctypes.c_int
+        L.orc_crank_nicolson_scf_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp,
+                                                  ctypes.c_double, _dp, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_double, _dp, _dp, _dp, _dp]
         L.orc_mlwf_matrices.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp]
         L.orc_jade.restype = ctypes.c_int
         L.orc_jade.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]
@@ -336,6 +346,65 @@ class System:
                                      int(theory), int(nscf), float(threshold), _d(out.view(np.float64)),
                                      _d(r), _d(en))
         return out, r, it, en
+
+
+    def density_normalize(self, rho, total):
+        """observables::density::normalize (density.hpp:100-111): rho * total / (dV sum rho)."""
+        r = np.ascontiguousarray(rho, np.float64).reshape(self.N).copy()
+        lib().orc_density_normalize(self._h, _d(r), float(total))
+        return r
+
+    def crank_nicolson_scf_step(self, psi, rho, dt, kA_t, kA_tdt, occ, vion, theory, nelec=None, max_iter=300,
+                                dens_tol=1e-5):
+        """Crank-Nicolson with its self-consistency loop and Broyden density mixing
+        (crank_nicolson.hpp:41-114).  The potential must already be the Kohn-Sham
+        potential of rho.  nelec defaults to sum(occ).  Returns (psi, rho, iterations,
+        energies, last solver residual)."""
+        out = self._psi(psi).copy()
+        r = np.ascontiguousarray(rho, np.float64).reshape(self.N).copy()
+        a = np.ascontiguousarray(kA_t, np.float64).reshape(3)
+        b = np.ascontiguousarray(kA_tdt, np.float64).reshape(3)
+        occ = np.ascontiguousarray(occ, np.float64).reshape(out.shape[1])
+        vion = np.ascontiguousarray(vion, np.float64).reshape(self.N)
+        nelec = float(occ.sum()) if nelec is None else float(nelec)
+        en = np.zeros(4)
+        res = np.zeros(1)
+        it = lib().orc_crank_nicolson_scf_step(self._h, out.shape[1], float(dt), _d(a), _d(b), _d(occ), nelec,
+                                               _d(vion), int(theory), int(max_iter), float(dens_tol),
+                                               _d(out.view(np.float64)), _d(r), _d(en), _d(res))
+        return out, r, it, en, float(res[0])
+
+
+def least_squares_sym(a, b):
+    """solvers::least_squares (least_squares.hpp:27-54, dgelsd with rcond -1) for a
+    symmetric matrix: the minimum-norm least-squares solution of a x = b."""
+    a = np.ascontiguousarray(a, np.float64).copy()
+    n = a.shape[0]
+    if a.shape != (n, n):
+        raise ValueError("a must be square")
+    x = np.ascontiguousarray(b, np.float64).reshape(n).copy()
+    lib().orc_least_squares_sym(n, _d(a), _d(x))
+    return x
+
+
+class Broyden:
+    """mixers::broyden (src/mixers/broyden.hpp:26-160) on a real vector of dim values:
+    mix(vin, vout) returns the new input."""
+
+    def __init__(self, steps, mix, dim):
+        self.dim = int(dim)
+        self._h = lib().orc_broyden_create(int(steps), float(mix), self.dim)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_broyden_destroy(self._h)
+            self._h = None
+
+    def mix(self, vin, vout):
+        vin = np.ascontiguousarray(vin, np.float64).reshape(self.dim).copy()
+        vout = np.ascontiguousarray(vout, np.float64).reshape(self.dim)
+        lib().orc_broyden_mix(self._h, _d(vin), _d(vout))
+        return vin
 
 
 # ---- checkpoint layout (operations/io.hpp:42-177, systems/electrons.hpp:323-375)

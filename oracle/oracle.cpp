@@ -47,6 +47,10 @@
 //                                                  src/hamiltonian/xc_term.hpp:63-142,276-323
 //   * exponential_2_for_1, ETRS with SCF loop      src/operations/exponential.hpp:50-69,
 //                                                  src/real_time/etrs.hpp:22-82
+//   * Broyden density mixer, normalisation,
+//     Crank-Nicolson with self-consistency        src/mixers/broyden.hpp:26-160,
+//                                                  src/observables/density.hpp:100-111,
+//                                                  src/real_time/crank_nicolson.hpp:41-114
 //   * TD-MLWF matrices, JADE, rotation, centres    src/wannier/tdmlwf_trans.hpp:63-346,
 //                                                  src/wannier/jade_complex.hpp:32-335,
 //                                                  src/observables/mlwf_properties.hpp:28-44
@@ -58,6 +62,12 @@
 //   * pseudopod sharmonic (pinned version unknown): real spherical harmonics
 //     Y00 = 1/sqrt(4pi), (Y1-1, Y10, Y11) = sqrt(3/4pi) (y, z, x)/r, Y1m(0) = 0.
 //   * BLAS gemm / LAPACK zpotrf: restated as plain loops.
+//   * LAPACK dgelsd with rcond -1 (solvers/least_squares.hpp:27-54, the Broyden
+//     mixer's small system): the minimum-norm least-squares solution from an SVD,
+//     singular values at or below machine epsilon times the largest dropped.  The
+//     matrix is symmetric, so its SVD comes from a cyclic Jacobi eigendecomposition.
+//     The mixer is pinned to the reference's broyden test values
+//     (tests/test_oracle_mixer.py).
 //   * libxc XC_LDA_X and XC_LDA_C_PZ (pinned version unknown): restated from their
 //     publications (Dirac-Slater exchange; Perdew-Zunger 1981).  XC_LDA_X is pinned
 //     to the reference's xc_term test values; the Perdew-Zunger fit has no golden
@@ -68,6 +78,7 @@
 #include <complex>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -895,6 +906,137 @@ int jade(int maxsweep, double tol, int M, cd *a, cd *u, cd *adiag) {
   return nsweep;
 }
 
+// ---- Broyden density mixing (src/mixers/broyden.hpp:26-160)
+
+// solvers::least_squares (least_squares.hpp:27-54) is LAPACK dgelsd with rcond -1: the
+// minimum-norm least-squares solution from an SVD, dropping singular values at or
+// below machine epsilon times the largest.  For the symmetric matrices the mixer
+// builds, the SVD comes from the eigendecomposition: cyclic Jacobi rotations (a
+// rotation in (p, q) with t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)),
+// theta = (a_qq - a_pp) / (2 a_pq), zeroes a_pq), then
+// x = sum_i v_i (v_i . b) / lambda_i over the kept eigenpairs.  a [n][n] is
+// overwritten; b becomes x.
+void symmetric_least_squares(int n, std::vector<double> &a, std::vector<double> &b) {
+  std::vector<double> v((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) v[(size_t)i * n + i] = 1.0;
+  for (int sweep = 0; sweep < 60; sweep++) {
+    double off = 0.0, diag = 0.0;
+    for (int p = 0; p < n; p++) {
+      diag += a[(size_t)p * n + p] * a[(size_t)p * n + p];
+      for (int q = p + 1; q < n; q++) off += a[(size_t)p * n + q] * a[(size_t)p * n + q];
+    }
+    if (off <= 1e-34 * diag) break;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) {
+        const double apq = a[(size_t)p * n + q];
+        if (apq == 0.0) continue;
+        const double theta = (a[(size_t)q * n + q] - a[(size_t)p * n + p]) / (2.0 * apq);
+        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < n; k++) {  // A J: columns p and q
+          const double akp = a[(size_t)k * n + p], akq = a[(size_t)k * n + q];
+          a[(size_t)k * n + p] = c * akp - s * akq;
+          a[(size_t)k * n + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; k++) {  // J^T (A J): rows p and q
+          const double apk = a[(size_t)p * n + k], aqk = a[(size_t)q * n + k];
+          a[(size_t)p * n + k] = c * apk - s * aqk;
+          a[(size_t)q * n + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; k++) {  // V J
+          const double vkp = v[(size_t)k * n + p], vkq = v[(size_t)k * n + q];
+          v[(size_t)k * n + p] = c * vkp - s * vkq;
+          v[(size_t)k * n + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  double smax = 0.0;
+  for (int i = 0; i < n; i++) smax = std::max(smax, std::fabs(a[(size_t)i * n + i]));
+  std::vector<double> x(n, 0.0);
+  for (int i = 0; i < n; i++) {
+    const double lam = a[(size_t)i * n + i];
+    if (!(std::fabs(lam) > std::numeric_limits<double>::epsilon() * smax)) continue;
+    double vb = 0.0;
+    for (int k = 0; k < n; k++) vb += v[(size_t)k * n + i] * b[k];
+    for (int k = 0; k < n; k++) x[k] += v[(size_t)k * n + i] * vb / lam;
+  }
+  b = x;
+}
+
+// mixers::broyden on a real field of dim values: history of max_size normalised
+// differences df, dv (a ring, filled in order 0, 1, ...), weights w0 = 0.01, ww = 5.
+struct Broyden {
+  int iter = 0, max_size, last_pos = -1;
+  double mix;
+  long dim;
+  std::vector<double> dv, df, f_old, vin_old;
+
+  Broyden(int steps, double mix_factor, long d)
+      : max_size(steps), mix(mix_factor), dim(d), dv((size_t)steps * d, NAN), df((size_t)steps * d, NAN),
+        f_old(d, NAN), vin_old(d, NAN) {}
+
+  double dot(const double *a, const double *b) const {
+    double s = 0.0;
+    for (long p = 0; p < dim; p++) s += a[p] * b[p];
+    return s;
+  }
+
+  // broyden_extrapolation (broyden.hpp:59-103), one process
+  void extrapolate(double *in, int used, const std::vector<double> &ff) const {
+    const double w0 = 0.01, ww = 5.0;
+    if (used == 0) {
+      for (long p = 0; p < dim; p++) in[p] += mix * ff[p];
+      return;
+    }
+    std::vector<double> beta((size_t)used * used), work(used);
+    for (int i = 0; i < used; i++)
+      for (int j = 0; j < used; j++) beta[(size_t)i * used + j] = ww * ww * dot(&df[(size_t)i * dim], &df[(size_t)j * dim]);
+    for (int i = 0; i < used; i++) beta[(size_t)i * used + i] = w0 * w0 + ww * ww;
+    for (int i = 0; i < used; i++) work[i] = dot(&df[(size_t)i * dim], ff.data());
+    symmetric_least_squares(used, beta, work);
+    for (long p = 0; p < dim; p++) {
+      double v = in[p] + mix * ff[p];
+      for (int i = 0; i < used; i++)
+        v -= ww * ww * work[i] * (mix * df[(size_t)i * dim + p] + dv[(size_t)i * dim + p]);
+      in[p] = v;
+    }
+  }
+
+  // operator() (broyden.hpp:107-160): in is the input density, replaced by the mix
+  void operator()(double *in, const double *out) {
+    iter++;
+    std::vector<double> ff(dim);
+    for (long p = 0; p < dim; p++) ff[p] = out[p] - in[p];
+    if (iter > 1) {
+      const int pos = (last_pos + 1) % max_size;
+      double *dfp = &df[(size_t)pos * dim], *dvp = &dv[(size_t)pos * dim];
+      for (long p = 0; p < dim; p++) {
+        dfp[p] = ff[p] - f_old[p];
+        dvp[p] = in[p] - vin_old[p];
+      }
+      const double gamma = std::max(1e-8, std::sqrt(dot(dfp, dfp)));
+      const double inv = 1.0 / gamma;
+      for (long p = 0; p < dim; p++) {
+        dfp[p] *= inv;
+        dvp[p] *= inv;
+      }
+      last_pos = pos;
+    }
+    std::copy(in, in + dim, vin_old.begin());
+    f_old = ff;
+    extrapolate(in, std::min(iter - 1, max_size), ff);
+  }
+};
+
+// observables::density::normalize (density.hpp:100-111): rho *= total / (dV sum rho)
+void density_normalize(const Grid &g, double *rho, double total) {
+  double q = 0.0;
+  for (long p = 0; p < g.npoints; p++) q += rho[p];
+  q *= g.volume_element();
+  const double f = total / q;
+  for (long p = 0; p < g.npoints; p++) rho[p] *= f;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1223,6 +1365,64 @@ int orc_etrs_scf_step(void *h, int M, double dt, const double *kA_t, const doubl
     iters = iscf + 1;
     if (done) break;
   }
+  return iters;
+}
+
+// solvers::least_squares (least_squares.hpp:27-54) for a symmetric n x n matrix a
+// (overwritten); b [n] becomes the solution
+void orc_least_squares_sym(int n, double *a, double *b) {
+  std::vector<double> av(a, a + (size_t)n * n), bv(b, b + n);
+  symmetric_least_squares(n, av, bv);
+  std::copy(av.begin(), av.end(), a);
+  std::copy(bv.begin(), bv.end(), b);
+}
+
+// mixers::broyden(steps, mix, dim) (broyden.hpp:26-160) as an opaque handle
+void *orc_broyden_create(int steps, double mix, long dim) { return new Broyden(steps, mix, dim); }
+void orc_broyden_destroy(void *m) { delete (Broyden *)m; }
+void orc_broyden_mix(void *m, double *in, const double *out) { (*(Broyden *)m)(in, out); }
+void orc_density_normalize(void *h, double *rho, double total) { density_normalize(((System *)h)->grid, rho, total); }
+
+// real_time::crank_nicolson with its self-consistency loop (crank_nicolson.hpp:41-114),
+// static ions, no induced vector potential, exchange off (so its exchange-energy test
+// always passes and the loop ends on the density alone).  On entry the system's
+// potential is the Kohn-Sham potential of rho, the density of psi at t.
+//   rhs = (1 - i dt/2 H(t)) psi; the vector potential moves to t + dt;
+//   a Broyden mixer (4 steps, mix 0.3) on the density;
+//   for istep < max_iter: update_hamiltonian(rho); steepest_descent (five steps) on
+//     (1 + i dt/2 H) psi = rhs from the current psi; new = density(psi);
+//     stop if dV sum |rho - new| / nelec < dens_tol; rho = mix(rho, new), normalised
+//     to nelec;
+//   rho = density(psi); update_hamiltonian(rho).
+// The reference uses max_iter 300 and dens_tol 1e-5.  Returns the iterations run;
+// en = energies of the last update_hamiltonian, residual = the solver's last value.
+int orc_crank_nicolson_scf_step(void *h, int M, double dt, const double *kA_t, const double *kA_tdt,
+                                const double *occ, double nelec, const double *vion, int theory, int max_iter,
+                                double dens_tol, double *psi_, double *rho, double *en, double *residual) {
+  auto *s = (System *)h;
+  cd *psi = (cd *)psi_;
+  const long N = s->grid.npoints, n = N * (long)M;
+  std::vector<cd> rhs(n);
+  orc_set_vector_potential_cov(h, kA_t);
+  cn_op(*s, M, cd(0.0, -0.5 * dt), psi, rhs.data());
+  orc_set_vector_potential_cov(h, kA_tdt);
+  Broyden mixer(4, 0.3, N);
+  std::vector<double> fresh(N);
+  int iters = 0;
+  double res = 0.0;
+  for (int istep = 0; istep < max_iter; istep++) {
+    ks_potential(s->grid, rho, vion, theory, s->V.data(), en);
+    res = steepest_descent(*s, M, cd(0.0, 0.5 * dt), rhs.data(), psi);
+    orc_density(h, M, psi_, occ, fresh.data());
+    const double diff = orc_integral_sum_absdiff(h, N, rho, fresh.data()) / nelec;
+    iters = istep + 1;
+    if (diff < dens_tol) break;
+    mixer(rho, fresh.data());
+    density_normalize(s->grid, rho, nelec);
+  }
+  orc_density(h, M, psi_, occ, rho);
+  ks_potential(s->grid, rho, vion, theory, s->V.data(), en);
+  if (residual) *residual = res;
   return iters;
 }
 

@@ -78,6 +78,15 @@ int main(int argc, char** argv) {
   std::printf("scf_charge %.12e\n", q * ham.volume_element());
   std::printf("scf_xc %.12e\n", en.xc);
 
+  // self-consistent Crank-Nicolson with Broyden mixing (crank_nicolson overload); the
+  // electron count is the charge the orbitals carry now
+  const int cn_iters = b2::crank_nicolson(ham, 0.05, {0.01, 0.0, 0.0}, {0.02, 0.0, 0.0}, b, occ,
+                                          q * ham.volume_element(), rho, sc, en, 60);
+  double q2 = 0.0;
+  for (double x : rho.download()) q2 += x;
+  std::printf("cn_scf_iterations %d\n", cn_iters);
+  std::printf("cn_scf_charge %.12e\n", q2 * ham.volume_element());
+
   // TD-MLWF lines
   b2::mlwf_properties mp;
   std::ostringstream os;

@@ -115,4 +115,6 @@ def test_new_entry_points_reject_a_null_context(pb):
     assert lib.inqb_mlwf_step(None, None, 1, 1, 100, 1e-8, None, None, None, None) == 1
     assert lib.inqb_jade(None, 2, None, None, None, 100, 1e-8, None, None) == 1
     assert lib.inqb_kick(None, None, 1, 1, three, None) == 1
+    assert lib.inqb_crank_nicolson_scf_step(None, None, 1, 1, 0.05, three, three, None, 2.0, None, None, 2, 300,
+                                            1e-5, None, None, None, None) == 1
     assert b"null context" in lib.inqb_last_error()

@@ -38,6 +38,10 @@ def test_host_adapter_runs(pb, tmp_path):
     assert 1 <= int(vals["scf_iterations"]) <= 5
     assert float(vals["scf_charge"]) == pytest.approx(2.0 * float(vals["etrs_norm"]), rel=1e-3)
     assert float(vals["scf_xc"]) < 0.0
+    # the Crank-Nicolson step with Broyden mixing: capped at 60 iterations, it keeps
+    # the charge to the solver's accuracy
+    assert 2 <= int(vals["cn_scf_iterations"]) <= 60
+    assert float(vals["cn_scf_charge"]) == pytest.approx(float(vals["scf_charge"]), rel=1e-3)
     assert int(vals["mlwf_lines"]) == 2 + 6
     assert vals["io_loaded"] == "1" and vals["io_missing_loaded"] == "0"
     assert float(vals["io_maxdiff"]) == 0.0

@@ -68,6 +68,12 @@ class RecordingHamiltonian:
         rho.copy_(self.density(psi, occ))
         return 2, dict(self.energies)
 
+    def crank_nicolson_scf_step_(self, psi, rho, dt, k1, k2, occ, vion, theory, max_iter, dens_tol, num_electrons):
+        self.log.append(("cn_scf", dt, tuple(k1), tuple(k2), theory, max_iter, dens_tol, num_electrons))
+        self._advance(psi)
+        rho.copy_(self.density(psi, occ))
+        return 3, 1e-9, dict(self.energies)
+
     def mlwf_step_(self, psi, maxsweep, tol):
         self.log.append(("mlwf", maxsweep, tol))
         return np.zeros((self.M, 3)), np.full(self.M, 1.5), 1
@@ -208,9 +214,24 @@ def test_callback_sees_every_step_from_zero():
     assert [t for _, t, _ in seen] == pytest.approx([0.0, 0.05, 0.1, 0.15])
 
 
+def test_crank_nicolson_with_a_density_dependent_potential_runs_the_mixed_loop():
+    from pinq_b200 import THEORY_HARTREE, propagate
+
+    occ = np.full(3, 2.0)
+    h = RecordingHamiltonian(3)
+    res = propagate(h, _psi(), occ, 0.1, 2, vion=torch.zeros(8, dtype=torch.float64), theory=THEORY_HARTREE,
+                    propagator="crank_nicolson", cn_max_iter=40, cn_dens_tol=1e-6, num_electrons=6.0,
+                    vector_potential=lambda t: (0.0, t, 0.0))
+    cn = _steps(h, "cn_scf")
+    assert len(cn) == 2 and not _steps(h, "cn") and not _steps(h, "etrs_scf")
+    for n, e in enumerate(cn):
+        assert e[1] == 0.1 and e[4:] == (THEORY_HARTREE, 40, 1e-6, 6.0)
+        assert e[2] == pytest.approx((0.0, 2 * n * 0.1, 0.0)) and e[3] == pytest.approx((0.0, 2 * (n + 1) * 0.1, 0.0))
+    assert res.total_energy == pytest.approx([18.0 - 1.25 + 0.5 - 0.75] * 3)
+
+
 @pytest.mark.parametrize("kwargs,exc", [
     ({"propagator": "rk4"}, ValueError),
-    ({"propagator": "crank_nicolson", "theory": 2}, NotImplementedError),
     ({"kick_gauge": "coulomb"}, ValueError),
 ])
 def test_argument_errors(kwargs, exc):
