@@ -15,12 +15,19 @@ sum_m occ_m eps_m - E_H - nvxc + E_xc, with eps_m = Re<psi_m|H|psi_m> / <psi_m|p
 """
 from __future__ import annotations
 
+import logging
+import time
+
 import numpy as np
 import torch
 
 from ._lib import THEORY_NONE
 from .checkpoint import RealTimeResults, save_checkpoint
 from .wannier import MLWFProperties
+
+# The reference's console lines (propagate.hpp:89-90,130,134), at INFO; the start and
+# end markers at DEBUG (the reference's trace level).
+log = logging.getLogger("pinq_b200.propagate")
 
 
 def _energy(ham, psi, occ, en):
@@ -78,6 +85,9 @@ def propagate(ham, psi, occ, dt, num_steps, *, vion=None, theory=THEORY_NONE, pr
             callback(0, 0.0, psi, rho, energy)
     mlwf = MLWFProperties(ham) if tdmlwf else None
 
+    log.debug("starting real-time propagation")
+    log.info("step %9d :  t =  %9.3f  e = %.12f", start_step, start_step * dt, energy)
+    t_last = time.perf_counter()
     for istep in range(start_step, num_steps):
         t = istep * dt
         k1, k2 = kA(t), kA(t + dt)
@@ -102,4 +112,8 @@ def propagate(ham, psi, occ, dt, num_steps, *, vion=None, theory=THEORY_NONE, pr
             save_checkpoint(checkpoint_dir, ham, psi, occ, rho, results)
         if callback:
             callback(istep + 1, tt, psi, rho, energy)
+        now = time.perf_counter()
+        log.info("step %9d :  t =  %9.3f  e = %.12f  wtime = %9.3f", istep + 1, tt, energy, now - t_last)
+        t_last = now
+    log.debug("real-time propagation ended normally")
     return results

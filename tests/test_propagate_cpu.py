@@ -241,3 +241,21 @@ def test_argument_errors(kwargs, exc):
     with pytest.raises(exc):
         propagate(h, _psi(), np.full(3, 2.0), 0.05, 1, **kwargs)
     assert h.log == []
+
+
+def test_console_lines_follow_the_reference(caplog):
+    """propagate.hpp:89-90,130: one line at the start step, one per step with the wall
+    time of that step."""
+    import logging
+    import re
+
+    from pinq_b200 import propagate
+
+    h = RecordingHamiltonian(3)
+    with caplog.at_level(logging.DEBUG, logger="pinq_b200.propagate"):
+        propagate(h, _psi(), np.full(3, 2.0), 0.05, 2)
+    msgs = [r.getMessage() for r in caplog.records if r.name == "pinq_b200.propagate"]
+    assert msgs[0] == "starting real-time propagation" and msgs[-1] == "real-time propagation ended normally"
+    assert msgs[1] == "step         0 :  t =      0.000  e = 18.000000000000"
+    for n, m in enumerate(msgs[2:4], start=1):
+        assert re.fullmatch(rf"step {n:9d} :  t =  {n * 0.05:9.3f}  e = 18\.000000000000  wtime = +\d+\.\d{{3}}", m), m
