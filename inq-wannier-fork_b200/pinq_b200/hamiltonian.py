@@ -310,7 +310,7 @@ class KSHamiltonian:
         occ_t = torch.as_tensor(occ, dtype=torch.float64, device=self.device).contiguous()
         if occ_t.numel() != psi.shape[1]:
             raise ValueError("one occupation per orbital")
-        nelec = float(np.sum(np.asarray(occ, np.float64))) if num_electrons is None else float(num_electrons)
+        nelec = float(occ_t.sum().item()) if num_electrons is None else float(num_electrons)
         a = np.ascontiguousarray(kA_t_cov, np.float64).reshape(3)
         b = np.ascontiguousarray(kA_tdt_cov, np.float64).reshape(3)
         it = ctypes.c_int(0)
