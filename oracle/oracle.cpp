@@ -57,8 +57,9 @@
 //
 // Third-party arithmetic the reference delegates (not vendored in the snapshot):
 //   * boost-multi FFT adaptors -> FFTW3 / cuFFT (pinned version unknown): restated
-//     here as a textbook mixed-radix Cooley-Tukey DFT (any radix, direct DFT for
-//     prime factors).
+//     here as a textbook mixed-radix Cooley-Tukey DFT in the Stockham autosort
+//     arrangement (radix 4 and 2 butterflies, a direct sum for 3, 5 and prime
+//     factors), run over contiguous rows with the orbitals as the batch.
 //   * pseudopod sharmonic (pinned version unknown): real spherical harmonics
 //     Y00 = 1/sqrt(4pi), (Y1-1, Y10, Y11) = sqrt(3/4pi) (y, z, x)/r, Y1m(0) = 0.
 //   * BLAS gemm / LAPACK zpotrf: restated as plain loops.
@@ -176,13 +177,15 @@ struct Grid {
 };
 
 // ---------------------------------------------------------------------------
-// FFT: mixed-radix decimation-in-time Cooley-Tukey, any length. Restates what
-// FFTW/cuFFT compute for transform.hpp (sign -1 forward, +1 backward).
+// FFT: mixed-radix decimation-in-time Cooley-Tukey, any length, in the Stockham
+// autosort arrangement. Restates what FFTW/cuFFT compute for transform.hpp (sign -1
+// forward, +1 backward).
 // ---------------------------------------------------------------------------
 struct Plan1D {
   int n;
-  std::vector<int> factors;
-  std::vector<cd> wfwd;  // exp(-2 pi i t / n)
+  std::vector<int> factors;            // radices, first applied first
+  std::vector<cd> wfwd;                // exp(-2 pi i t / n), t < n
+  std::vector<std::vector<cd>> stage;  // per stage: w_{pL}^{r k} at [k * p + r]
 
   explicit Plan1D(int n_) : n(n_) {
     int m = n;
@@ -206,76 +209,111 @@ struct Plan1D {
       double a = -2.0 * M_PI * (double)tt / (double)n;
       wfwd[t] = cd(std::cos(a), std::sin(a));
     }
+    long L = 1;
+    for (int p : factors) {
+      const long scale = n / (L * p);  // w_{pL}^e = w_n^(e n / (pL))
+      std::vector<cd> tw((size_t)L * p);
+      for (long k = 0; k < L; k++)
+        for (int r = 0; r < p; r++) tw[(size_t)k * p + r] = wfwd[(size_t)(((long)r * k * scale) % n)];
+      stage.push_back(std::move(tw));
+      L *= p;
+    }
   }
   cd w(long t, int sign) const {
     cd v = wfwd[(size_t)(((t % n) + n) % n)];
     return sign < 0 ? v : std::conj(v);
   }
-  // y[0..len) = DFT_len of x[0], x[xs], ..., computed recursively
-  void rec(const cd *x, long xs, cd *y, int len, int fi, int sign, cd *tmp) const {
-    if (len == 1) {
-      y[0] = x[0];
-      return;
-    }
-    int p = factors[fi];
-    int m = len / p;
-    for (int r = 0; r < p; r++) rec(x + r * xs, xs * p, y + r * m, m, fi + 1, sign, tmp);
-    long step_len = n / len;  // exponent scale: w_len^e = w_n^(e*n/len)
-    long step_p = n / p;
-    cd t[64];
-    std::vector<cd> tv;
-    cd *tb = t;
-    if (p > 64) {
-      tv.resize(p);
-      tb = tv.data();
-    }
-    for (int k = 0; k < m; k++) {
-      for (int r = 0; r < p; r++) tb[r] = y[r * m + k] * w((long)r * k * step_len, sign);
-      for (int q = 0; q < p; q++) {
-        cd s = 0.0;
-        for (int r = 0; r < p; r++) s += tb[r] * w((long)r * q * step_p, sign);
-        tmp[k + m * q] = s;
+
+  // B sequences stored as rows: element i of sequence b at x[i * ld + b] (i < n,
+  // b < B).  Each stage combines p DFTs of length L into DFTs of length pL:
+  //   X_{pL}[k + L u] = sum_r w_p^{r u} (w_{pL}^{r k} X_L^{(r)}[k]),
+  // with the stage's input at row k R + R' r + q and its output at row
+  // (k + L u) R' + q (R = n / L, R' = R / p, q < R'), so every inner loop runs over
+  // whole rows of B contiguous values.  w1, w2: scratch of n B values each.
+  void exec_rows(cd *x, long ld, long B, int sign, std::vector<cd> &w1, std::vector<cd> &w2) const {
+    if (n == 1 || B == 0) return;
+    if ((long)w1.size() < n * B) w1.resize((size_t)n * B);
+    if ((long)w2.size() < n * B) w2.resize((size_t)n * B);
+    const cd *src = x;
+    long sld = ld;
+    cd *dst = w1.data();
+    long L = 1, R = n;
+    std::vector<cd> a, wp;
+    for (size_t s = 0; s < factors.size(); s++) {
+      const int p = factors[s];
+      const long Rp = R / p;
+      wp.resize(p);
+      for (int t = 0; t < p; t++) wp[t] = w((long)t * (n / p), sign);
+      a.resize((size_t)p);
+      for (long k = 0; k < L; k++) {
+        const cd *tk = &stage[s][(size_t)k * p];
+        for (long q = 0; q < Rp; q++)
+          for (long b = 0; b < B; b++) {
+            for (int r = 0; r < p; r++) {
+              const cd v = src[(k * R + Rp * r + q) * sld + b];
+              a[r] = (k == 0 || r == 0) ? v : v * (sign < 0 ? tk[r] : std::conj(tk[r]));
+            }
+            cd *o = dst + ((k * Rp) + q) * B + b;  // row (k + L u) R' + q at o[u L R' B]
+            const long ostep = L * Rp * B;
+            if (p == 2) {
+              o[0] = a[0] + a[1];
+              o[ostep] = a[0] - a[1];
+            } else if (p == 4) {
+              const cd s02 = a[0] + a[2], d02 = a[0] - a[2], s13 = a[1] + a[3], d13 = a[1] - a[3];
+              // -i d13 forward (w_4 = -i), +i d13 backward
+              const cd j13 = sign < 0 ? cd(d13.imag(), -d13.real()) : cd(-d13.imag(), d13.real());
+              o[0] = s02 + s13;
+              o[ostep] = d02 + j13;
+              o[2 * ostep] = s02 - s13;
+              o[3 * ostep] = d02 - j13;
+            } else {
+              for (int u = 0; u < p; u++) {
+                cd acc = a[0];
+                for (int r = 1; r < p; r++) acc += wp[(size_t)((r * u) % p)] * a[r];
+                o[u * ostep] = acc;
+              }
+            }
+          }
       }
+      src = dst;
+      sld = B;
+      dst = (dst == w1.data()) ? w2.data() : w1.data();
+      L *= p;
+      R = Rp;
     }
-    for (int i = 0; i < len; i++) y[i] = tmp[i];
-  }
-  void exec(const cd *x, long xs, cd *y, int sign) const {
-    thread_local std::vector<cd> tmp;
-    if ((int)tmp.size() < n) tmp.resize(n);
-    rec(x, xs, y, n, 0, sign, tmp.data());
+    for (long i = 0; i < n; i++)
+      for (long b = 0; b < B; b++) x[i * ld + b] = src[i * B + b];
   }
 };
 
 // Batched 3-D FFT of a [N][M] orbital-fastest array (transform.hpp:129-133:
-// dft over the three grid dimensions, orbital index is the batch).
+// dft over the three grid dimensions, orbital index is the batch).  The array is
+// transformed as rows: along z each (x, y) block is [nz][M], along y each x plane is
+// [ny][nz M], along x the whole array is [nx][ny nz M] (split into column chunks).
 void fft3d(const Grid &g, int M, const cd *in, cd *out, int sign, bool normalize) {
   Plan1D px(g.nr[0]), py(g.nr[1]), pz(g.nr[2]);
-  const int nx = g.nr[0], ny = g.nr[1], nz = g.nr[2];
-  const long N = g.npoints;
-#pragma omp parallel for schedule(dynamic)
-  for (int m = 0; m < M; m++) {
-    std::vector<cd> a(N), line(std::max(nx, std::max(ny, nz))), res(line.size());
-    for (long p = 0; p < N; p++) a[p] = in[p * M + m];
-    for (int ix = 0; ix < nx; ix++)
-      for (int iy = 0; iy < ny; iy++) {
-        cd *base = &a[g.linear(ix, iy, 0)];
-        pz.exec(base, 1, res.data(), sign);
-        for (int iz = 0; iz < nz; iz++) base[iz] = res[iz];
-      }
-    for (int ix = 0; ix < nx; ix++)
-      for (int iz = 0; iz < nz; iz++) {
-        cd *base = &a[g.linear(ix, 0, iz)];
-        py.exec(base, nz, res.data(), sign);
-        for (int iy = 0; iy < ny; iy++) base[(long)iy * nz] = res[iy];
-      }
-    for (int iy = 0; iy < ny; iy++)
-      for (int iz = 0; iz < nz; iz++) {
-        cd *base = &a[g.linear(0, iy, iz)];
-        px.exec(base, (long)ny * nz, res.data(), sign);
-        for (int ix = 0; ix < nx; ix++) base[(long)ix * ny * nz] = res[ix];
-      }
-    double f = normalize ? 1.0 / (double)N : 1.0;
-    for (long p = 0; p < N; p++) out[p * M + m] = a[p] * f;
+  const long nx = g.nr[0], ny = g.nr[1], nz = g.nr[2];
+  const long N = g.npoints, total = N * M;
+  if (out != in) std::copy(in, in + total, out);
+  const long rowx = ny * nz * M, chunk = 1024;
+  const long nchunks = (rowx + chunk - 1) / chunk;
+#pragma omp parallel
+  {
+    std::vector<cd> w1, w2;
+#pragma omp for schedule(static)
+    for (long xy = 0; xy < nx * ny; xy++) pz.exec_rows(out + xy * nz * M, M, M, sign, w1, w2);
+#pragma omp for schedule(static)
+    for (long ix = 0; ix < nx; ix++) py.exec_rows(out + ix * ny * nz * M, nz * M, nz * M, sign, w1, w2);
+#pragma omp for schedule(static)
+    for (long c = 0; c < nchunks; c++) {
+      const long c0 = c * chunk;
+      px.exec_rows(out + c0, rowx, std::min(chunk, rowx - c0), sign, w1, w2);
+    }
+    if (normalize) {
+      const double f = 1.0 / (double)N;
+#pragma omp for schedule(static)
+      for (long i = 0; i < total; i++) out[i] *= f;
+    }
   }
 }
 

@@ -99,6 +99,21 @@ def test_fft_matches_numpy(oracle_mod):
         assert np.abs(o.fft3d(psi, -1) - ref).max() < 1e-12 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("nr,M", [((32, 32, 32), 2), ((64, 8, 45), 3), ((7, 12, 30), 1), ((25, 36, 16), 5),
+                                  ((2, 3, 49), 4)])
+def test_fft_forward_and_inverse_match_numpy(oracle_mod, nr, M):
+    """Radices 4, 2, 3, 5, 7 and a prime, with the orbitals as the batch: sign -1
+    unnormalised (to_fourier) and sign +1 with 1/N (to_real, transform.hpp:325-331)."""
+    o = oracle_mod.System(np.diag([5.0, 6.0, 7.0]), nr)
+    rng = np.random.default_rng(sum(nr) + M)
+    psi = rng.standard_normal((o.N, M)) + 1j * rng.standard_normal((o.N, M))
+    grid = psi.reshape(*nr, M)
+    fwd = np.fft.fftn(grid, axes=(0, 1, 2)).reshape(o.N, M)
+    inv = np.fft.ifftn(grid, axes=(0, 1, 2)).reshape(o.N, M)
+    assert np.abs(o.fft3d(psi, -1) - fwd).max() < 1e-13 * np.abs(fwd).max()
+    assert np.abs(o.fft3d(psi, +1, normalize=True) - inv).max() < 1e-13 * np.abs(inv).max()
+
+
 @pytest.mark.parametrize("center", [(0, 0, 0), (-5, 0, 0), (5, 0, 0), (-5, -5, -5), (5, 5, 5), (2.5, 2.5, 2.5)])
 def test_sphere_257_points(oracle_mod, center):
     """spherical_grid.hpp:264-376: radius 2 on a 10 bohr / 0.4967 grid -> 257 points,
