@@ -1,6 +1,10 @@
-"""Size-independent properties at the benchmark sizes, where the oracle would take too
-long: the 64-atom cell (64^3, all 128 orbitals, 256 projectors) and the large cell
-(144^3, 480 orbitals, 960 projectors).
+"""The benchmark sizes: the 64-atom cell (64^3, all 128 orbitals, 256 projectors) and
+the large cell (144^3, 480 orbitals, 960 projectors).
+
+On the 64-atom cell H|psi> of all 128 orbitals is compared with the oracle directly
+(FP64 1e-12 max-relative; mixed 1e-6 relative in norm, the mixed-precision bound).
+Beside that, size-independent properties, which also cover the large cell, where the
+oracle would take too long:
 
   * H is Hermitian: dV Psi^H (H Psi) equals its conjugate transpose (the kinetic term,
     the local potential and the Kleinman-Bylander projectors are each Hermitian).
@@ -43,6 +47,24 @@ def _herm_defect(h, psi, hpsi, chunk=1 << 18):
         a += psi[p0:p0 + chunk].to(torch.complex128).conj().T @ hpsi[p0:p0 + chunk].to(torch.complex128)
     a *= h.volume_element
     return float((a - a.conj().T).norm() / a.norm())
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 1e-6)])
+def test_h_cfg1_all_orbitals_matches_oracle(pb, oracle_mod, precision, tol):
+    from pinq_b200 import systems
+
+    h, psi = _cell(pb, "cfg1", precision, 128)
+    hpsi = h.apply(psi).to(torch.complex128).cpu().numpy()
+    lat = systems.cubic(20.52)
+    pos = systems.diamond_positions(10.26, 2)
+    o = oracle_mod.System(lat, (64, 64, 64))
+    o.set_potential(systems.gaussian_potential_device(lat, (64, 64, 64), pos))
+    o.set_projectors(o.build_gaussian_kb(pos))
+    ref = o.apply_h(psi.to(torch.complex128).cpu().numpy())
+    if precision == "fp64":
+        assert np.abs(hpsi - ref).max() / np.abs(ref).max() < tol
+    else:
+        assert np.linalg.norm(hpsi - ref) / np.linalg.norm(ref) < tol
 
 
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 2e-6)])
