@@ -341,6 +341,8 @@ class KSHamiltonian:
             try:
                 with torch.cuda.device(device):
                     view = torch.as_tensor(_DeviceDoubles(ptr, n), device=device)
+                if view.data_ptr() != int(ptr):  # a copy would not reach the library's buffer
+                    return 1
                 reducer(view)
                 return 0
             except Exception:  # reported to the caller as the step's failure
