@@ -173,7 +173,9 @@ int inqb_orthonormalize(inqb_ctx* ctx, void* psi, int M, int ld, void* stream);
  * hooks, or a service whose device memory budget is fixed after start-up.
  *   - M <= 256 orbitals; larger M returns INQB_ERR_UNSUPPORTED.
  *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.  The
+ *     address is kept until the process exits, so, like every context of this
+ *     library, it does not survive a cudaDeviceReset of that device.
  *   - All calls on a device share the array: calls that overlap on the GPU (from
  *     different streams or threads) race.  Each call clears what it accumulates.
  *   - Synchronous, like inqb_orthonormalize; the context itself was created earlier. */
