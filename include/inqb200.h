@@ -165,6 +165,29 @@ int inqb_band_energies(inqb_ctx* ctx, const void* psi, const void* hpsi, int M, 
 /* operations::orthogonalize (src/operations/orthogonalize.hpp:25-32): FP64
  * overlap S = dV psi^H psi, Cholesky S = U^H U, psi <- psi U^-1; synchronous. */
 int inqb_orthonormalize(inqb_ctx* ctx, void* psi, int M, int ld, void* stream);
+/* Orbital-sharded orthonormalisation, the pieces of operations::orthogonalize when
+ * the states are split over ranks (src/operations/orthogonalize.hpp:25-32).  Each rank
+ * holds a block of orbitals; the caller circulates the blocks and sums the matrices
+ * (pinq_b200.parallel.sharded_orthonormalize_ does it over torch.distributed).
+ * S, R: FP64 complex device matrices, interleaved (re, im), row-major with row stride
+ * lds / ldr in complex elements.
+ * inqb_overlap_block: S = dV a^H b for an Ma-orbital block a and an Mb-orbital block
+ * b: one block of operations::overlap's set-parallel branch
+ * (src/operations/overlap.hpp:47-72), which circulates the blocks and all-reduces
+ * the zero-padded matrix.  S is overwritten. */
+int inqb_overlap_block(inqb_ctx* ctx, const void* a, int Ma, int lda, const void* b, int Mb, int ldb, double* S,
+                       int lds, void* stream);
+/* matrix::cholesky then matrix::invert_triangular (src/matrix/cholesky.hpp:28-100,
+ * src/operations/rotate.hpp:147-157) of the M x M Hermitian S in place: on return
+ * S = U^-1, upper triangular (the strict lower part zero), where S = U^H U.
+ * INQB_ERR_NOT_POSITIVE_DEFINITE when a pivot fails; synchronous. */
+int inqb_cholesky_inverse(inqb_ctx* ctx, double* S, int M, int lds, void* stream);
+/* out = a R: a is an Ma-orbital block, R the Ma x Mo FP64 block, out an Mo-orbital
+ * block in the context precision (FP64 sums); out must not overlap a.  One term of
+ * operations::rotate's set-parallel branch (src/operations/rotate.hpp:100-125), whose
+ * terms are summed on the rank that owns the output orbitals. */
+int inqb_rotate_block(inqb_ctx* ctx, const void* a, int Ma, int lda, const double* R, int ldr, int Mo, void* out,
+                      int ldo, void* stream);
 /* The same orthonormalisation without any device allocation (no counterpart in the
  * reference).  inqb_orthonormalize allocates its M x M scratch on every call; this
  * one uses a fixed array of 2 MiB compiled into the library, which every GPU that

@@ -1286,6 +1286,45 @@ int inqb_orthonormalize(inqb_ctx* ctx, void* psi, int M, int ld, void* stream) {
                                info.as<int>(), stream);
 }
 
+int inqb_overlap_block(inqb_ctx* ctx, const void* a, int Ma, int lda, const void* b, int Mb, int ldb, double* S,
+                       int lds, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, a, Ma, lda));
+  INQB_TRY(check_block(ctx, b, Mb, ldb));
+  if (!S || lds < Mb) return fail(INQB_ERR_INVALID, "overlap block: need S and lds >= Mb");
+  INQB_GUARD(ctx);
+  return launch_overlap_block(ctx->precision, a, lda, Ma, b, ldb, Mb, ctx->N, ctx->dV,
+                              reinterpret_cast<double2*>(S), lds, stream);
+}
+
+int inqb_cholesky_inverse(inqb_ctx* ctx, double* S, int M, int lds, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  if (!S || M <= 0 || lds < M) return fail(INQB_ERR_INVALID, "cholesky inverse: need S, M > 0 and lds >= M");
+  if (((uintptr_t)S) % 16 != 0) return fail(INQB_ERR_INVALID, "cholesky inverse: S must be 16-byte aligned");
+  INQB_GUARD(ctx);
+  DevBuf X, info;
+  INQB_TRY(X.ensure(sizeof(double2) * (size_t)M * M));
+  INQB_TRY(info.ensure(sizeof(int)));
+  return launch_cholesky_inverse(reinterpret_cast<double2*>(S), M, lds, X.as<double2>(), info.as<int>(), stream);
+}
+
+int inqb_rotate_block(inqb_ctx* ctx, const void* a, int Ma, int lda, const double* R, int ldr, int Mo, void* out,
+                      int ldo, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, a, Ma, lda));
+  INQB_TRY(check_block(ctx, out, Mo, ldo));
+  if (!R || ldr < Mo) return fail(INQB_ERR_INVALID, "rotate block: need R and ldr >= Mo");
+  if (((uintptr_t)R) % 16 != 0) return fail(INQB_ERR_INVALID, "rotate block: R must be 16-byte aligned");
+  const size_t esz = ctx->elem_bytes();
+  const char* a0 = static_cast<const char*>(a);
+  const char* o0 = static_cast<const char*>(out);
+  const size_t span_a = ((size_t)(ctx->N - 1) * lda + Ma) * esz, span_o = ((size_t)(ctx->N - 1) * ldo + Mo) * esz;
+  if (o0 < a0 + span_a && a0 < o0 + span_o) return fail(INQB_ERR_INVALID, "rotate block: out overlaps a");
+  INQB_GUARD(ctx);
+  return launch_rotate_block(ctx->precision, a, lda, Ma, reinterpret_cast<const double2*>(R), ldr, Mo, out, ldo,
+                             ctx->N, stream);
+}
+
 int inqb_batch_create(inqb_ctx* const* cells, int ncells, inqb_batch** out) {
   if (!cells || !out || ncells <= 0) return fail(INQB_ERR_INVALID, "bad batch arguments");
   *out = nullptr;

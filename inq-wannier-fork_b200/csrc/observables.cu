@@ -77,10 +77,13 @@ __global__ void k_dipole(const double* __restrict__ rho, long N, LatticeView g, 
   }
 }
 
-// S[i][j] += dV sum_{p in chunk} conj(psi[p][i]) psi[p][j] ; 32x32 tile per CTA.
+// S[i][j] += dV sum_{p in chunk} conj(a[p][i]) b[p][j] ; 32x32 tile per CTA.  The
+// square overlap passes the same block twice; an orbital-sharded caller passes two
+// blocks (one block of operations::overlap's set-parallel branch).
 template <typename T>
-__global__ void __launch_bounds__(1024) k_overlap(const cplx<T>* __restrict__ psi, long ld, int M, long N,
-                                                  long chunk, double dV, double2* __restrict__ S) {
+__global__ void __launch_bounds__(1024) k_overlap(const cplx<T>* __restrict__ pa, long lda, int Ma,
+                                                  const cplx<T>* __restrict__ pb_, long ldb, int Mb, long N,
+                                                  long chunk, double dV, double2* __restrict__ S, long lds) {
   constexpr int TP = 32;  // points staged per round
   __shared__ double2 a[TP][33], b[TP][33];
   const int ti = threadIdx.y, tj = threadIdx.x;
@@ -88,16 +91,16 @@ __global__ void __launch_bounds__(1024) k_overlap(const cplx<T>* __restrict__ ps
   const long p0 = (long)blockIdx.z * chunk, p1 = min(N, p0 + chunk);
   double re = 0.0, im = 0.0;
   for (long pb = p0; pb < p1; pb += TP) {
-    // thread (ti, tj) loads point pb+ti, orbital i0+tj / j0+tj
+    // thread (ti, tj) loads point pb+ti, orbital i0+tj of a / j0+tj of b
     const long p = pb + ti;
     double2 va = make_double2(0, 0), vb = make_double2(0, 0);
     if (p < p1) {
-      if (i0 + tj < M) {
-        cplx<T> v = psi[p * ld + i0 + tj];
+      if (i0 + tj < Ma) {
+        cplx<T> v = pa[p * lda + i0 + tj];
         va = make_double2(v.x, v.y);
       }
-      if (j0 + tj < M) {
-        cplx<T> v = psi[p * ld + j0 + tj];
+      if (j0 + tj < Mb) {
+        cplx<T> v = pb_[p * ldb + j0 + tj];
         vb = make_double2(v.x, v.y);
       }
     }
@@ -112,21 +115,21 @@ __global__ void __launch_bounds__(1024) k_overlap(const cplx<T>* __restrict__ ps
     }
     __syncthreads();
   }
-  if (i0 + ti < M && j0 + tj < M) {
-    atomicAdd(&S[(long)(i0 + ti) * M + j0 + tj].x, dV * re);
-    atomicAdd(&S[(long)(i0 + ti) * M + j0 + tj].y, dV * im);
+  if (i0 + ti < Ma && j0 + tj < Mb) {
+    atomicAdd(&S[(long)(i0 + ti) * lds + j0 + tj].x, dV * re);
+    atomicAdd(&S[(long)(i0 + ti) * lds + j0 + tj].y, dV * im);
   }
 }
 
 // In-place Cholesky of the Hermitian S (upper triangle used): on exit the upper
 // triangle holds U with S = U^H U.  One CTA; info[0] = first failing pivot + 1.
-__global__ void __launch_bounds__(1024) k_cholesky(double2* __restrict__ S, int M, int* __restrict__ info) {
+__global__ void __launch_bounds__(1024) k_cholesky(double2* __restrict__ S, int M, long lds, int* __restrict__ info) {
   __shared__ int bad;
   if (threadIdx.x == 0) bad = 0;
   __syncthreads();
   for (int k = 0; k < M; k++) {
     __syncthreads();
-    const double d = S[(long)k * M + k].x;
+    const double d = S[(long)k * lds + k].x;
     if (!(d > 0.0)) {
       if (threadIdx.x == 0) {
         bad = 1;
@@ -138,8 +141,8 @@ __global__ void __launch_bounds__(1024) k_cholesky(double2* __restrict__ S, int 
     const double u = sqrt(d);
     __syncthreads();
     for (int j = k + threadIdx.x; j < M; j += blockDim.x) {
-      double2 v = S[(long)k * M + j];
-      S[(long)k * M + j] = j == k ? make_double2(u, 0.0) : make_double2(v.x / u, v.y / u);
+      double2 v = S[(long)k * lds + j];
+      S[(long)k * lds + j] = j == k ? make_double2(u, 0.0) : make_double2(v.x / u, v.y / u);
     }
     __syncthreads();
     // trailing update: S[i][j] -= conj(U[k][i]) U[k][j], k < i <= j
@@ -147,29 +150,29 @@ __global__ void __launch_bounds__(1024) k_cholesky(double2* __restrict__ S, int 
     for (long t = threadIdx.x; t < (long)n * n; t += blockDim.x) {
       const int i = k + 1 + (int)(t / n), j = k + 1 + (int)(t % n);
       if (j < i) continue;
-      const double2 ui = S[(long)k * M + i], uj = S[(long)k * M + j];
-      double2 s = S[(long)i * M + j];
+      const double2 ui = S[(long)k * lds + i], uj = S[(long)k * lds + j];
+      double2 s = S[(long)i * lds + j];
       s.x -= ui.x * uj.x + ui.y * uj.y;
       s.y -= ui.x * uj.y - ui.y * uj.x;
-      S[(long)i * M + j] = s;
+      S[(long)i * lds + j] = s;
     }
   }
   (void)bad;
 }
 
 // X = U^-1 (upper triangular), one thread per column j, back substitution.
-__global__ void k_triangular_inverse(const double2* __restrict__ U, int M, double2* __restrict__ X) {
+__global__ void k_triangular_inverse(const double2* __restrict__ U, int M, long ldu, double2* __restrict__ X) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= M) return;
   for (int i = 0; i < M; i++) X[(long)i * M + j] = make_double2(0, 0);
   for (int i = j; i >= 0; i--) {
     double2 s = make_double2(i == j ? 1.0 : 0.0, 0.0);
     for (int k = i + 1; k <= j; k++) {
-      const double2 u = U[(long)i * M + k], x = X[(long)k * M + j];
+      const double2 u = U[(long)i * ldu + k], x = X[(long)k * M + j];
       s.x -= u.x * x.x - u.y * x.y;
       s.y -= u.x * x.y + u.y * x.x;
     }
-    const double uii = U[(long)i * M + i].x;
+    const double uii = U[(long)i * ldu + i].x;
     X[(long)i * M + j] = make_double2(s.x / uii, s.y / uii);
   }
 }
@@ -193,6 +196,32 @@ __global__ void k_rotate_upper(cplx<T>* __restrict__ psi, long ld, int M, long N
         im += a.x * x.y + a.y * x.x;
       }
       psi[p * ld + j] = mk<T>((T)re, (T)im);
+    }
+  }
+}
+
+// out[p][j] = sum_{i < Ma} a[p][i] R[i][j], j < Mo: one block of operations::rotate's
+// set-parallel branch (src/operations/rotate.hpp:100-125), FP64 arithmetic, a row of a
+// staged in shared memory per point.
+template <typename T>
+__global__ void k_rotate_block(const cplx<T>* __restrict__ a, long lda, int Ma, const double2* __restrict__ R,
+                               long ldr, int Mo, cplx<T>* __restrict__ out, long ldo, long N) {
+  extern __shared__ double2 row[];
+  for (long p = blockIdx.x; p < N; p += gridDim.x) {
+    __syncthreads();
+    for (int m = threadIdx.x; m < Ma; m += blockDim.x) {
+      const cplx<T> v = a[p * lda + m];
+      row[m] = make_double2(v.x, v.y);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < Mo; j += blockDim.x) {
+      double re = 0.0, im = 0.0;
+      for (int i = 0; i < Ma; i++) {
+        const double2 x = row[i], r = R[(long)i * ldr + j];
+        re += x.x * r.x - x.y * r.y;
+        im += x.x * r.y + x.y * r.x;
+      }
+      out[p * ldo + j] = mk<T>((T)re, (T)im);
     }
   }
 }
@@ -287,10 +316,10 @@ static int orthonormalize_impl(void* psi, long ld, int M, long N, double dV, dou
   long nchunks = std::max<long>(1, std::min<long>(N / 1024, (148L * 8) / (tiles * tiles) + 1));
   const long chunk = (N + nchunks - 1) / nchunks;
   nchunks = (N + chunk - 1) / chunk;
-  k_overlap<T><<<dim3(tiles, tiles, (unsigned)nchunks), dim3(32, 32), 0, st>>>((const cplx<T>*)psi, ld, M, N, chunk,
-                                                                              dV, S);
+  k_overlap<T><<<dim3(tiles, tiles, (unsigned)nchunks), dim3(32, 32), 0, st>>>(
+      (const cplx<T>*)psi, ld, M, (const cplx<T>*)psi, ld, M, N, chunk, dV, S, M);
   INQB_CUDA_TRY(cudaGetLastError());
-  k_cholesky<<<1, 1024, 0, st>>>(S, M, info);
+  k_cholesky<<<1, 1024, 0, st>>>(S, M, M, info);
   INQB_CUDA_TRY(cudaGetLastError());
   int h_info = 0;
   INQB_CUDA_TRY(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -298,7 +327,7 @@ static int orthonormalize_impl(void* psi, long ld, int M, long N, double dV, dou
   if (h_info != 0)
     return fail(INQB_ERR_NOT_POSITIVE_DEFINITE,
                 "overlap matrix is not positive definite at pivot " + std::to_string(h_info - 1));
-  k_triangular_inverse<<<(M + 127) / 128, 128, 0, st>>>(S, M, X);
+  k_triangular_inverse<<<(M + 127) / 128, 128, 0, st>>>(S, M, M, X);
   INQB_CUDA_TRY(cudaGetLastError());
   const int blocks = (int)std::min<long>(N, 148L * 16);
   k_rotate_upper<T><<<blocks, 128, sizeof(double2) * M, st>>>((cplx<T>*)psi, ld, M, N, X);
@@ -312,6 +341,68 @@ int launch_orthonormalize(int precision, void* psi, long ld, int M, long N, doub
   return precision == INQB_FP64
              ? orthonormalize_impl<double>(psi, ld, M, N, dV, S, X, info, (cudaStream_t)stream)
              : orthonormalize_impl<float>(psi, ld, M, N, dV, S, X, info, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------- orbital-sharded orthonormalisation
+// The pieces of operations::orthogonalize over a states communicator: blocks of the
+// overlap, the Cholesky factor's inverse of the summed matrix, and blocks of the
+// rotation.  The caller moves the blocks between ranks.
+template <typename T>
+static int overlap_block_impl(const void* a, long lda, int Ma, const void* b, long ldb, int Mb, long N, double dV,
+                              double2* S, long lds, cudaStream_t st) {
+  INQB_CUDA_TRY(cudaMemset2DAsync(S, sizeof(double2) * lds, 0, sizeof(double2) * Mb, Ma, st));
+  const int ti = (Ma + 31) / 32, tj = (Mb + 31) / 32;
+  long nchunks = std::max<long>(1, std::min<long>(N / 1024, (148L * 8) / (ti * tj) + 1));
+  const long chunk = (N + nchunks - 1) / nchunks;
+  nchunks = (N + chunk - 1) / chunk;
+  k_overlap<T><<<dim3(tj, ti, (unsigned)nchunks), dim3(32, 32), 0, st>>>((const cplx<T>*)a, lda, Ma,
+                                                                          (const cplx<T>*)b, ldb, Mb, N, chunk, dV,
+                                                                          S, lds);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_overlap_block(int precision, const void* a, long lda, int Ma, const void* b, long ldb, int Mb, long N,
+                         double dV, double2* S, long lds, void* stream) {
+  return precision == INQB_FP64
+             ? overlap_block_impl<double>(a, lda, Ma, b, ldb, Mb, N, dV, S, lds, (cudaStream_t)stream)
+             : overlap_block_impl<float>(a, lda, Ma, b, ldb, Mb, N, dV, S, lds, (cudaStream_t)stream);
+}
+
+int launch_cholesky_inverse(double2* S, int M, long lds, double2* X, int* info, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  INQB_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
+  k_cholesky<<<1, 1024, 0, st>>>(S, M, lds, info);
+  INQB_CUDA_TRY(cudaGetLastError());
+  int h_info = 0;
+  INQB_CUDA_TRY(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, st));
+  INQB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h_info != 0)
+    return fail(INQB_ERR_NOT_POSITIVE_DEFINITE,
+                "overlap matrix is not positive definite at pivot " + std::to_string(h_info - 1));
+  k_triangular_inverse<<<(M + 127) / 128, 128, 0, st>>>(S, M, lds, X);
+  INQB_CUDA_TRY(cudaGetLastError());
+  INQB_CUDA_TRY(cudaMemcpy2DAsync(S, sizeof(double2) * lds, X, sizeof(double2) * M, sizeof(double2) * M, M,
+                                  cudaMemcpyDeviceToDevice, st));
+  INQB_CUDA_TRY(cudaStreamSynchronize(st));
+  return INQB_OK;
+}
+
+template <typename T>
+static int rotate_block_impl(const void* a, long lda, int Ma, const double2* R, long ldr, int Mo, void* out,
+                             long ldo, long N, cudaStream_t st) {
+  const int blocks = (int)std::min<long>(N, 148L * 16);
+  k_rotate_block<T><<<blocks, 128, sizeof(double2) * Ma, st>>>((const cplx<T>*)a, lda, Ma, R, ldr, Mo,
+                                                               (cplx<T>*)out, ldo, N);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
+}
+
+int launch_rotate_block(int precision, const void* a, long lda, int Ma, const double2* R, long ldr, int Mo,
+                        void* out, long ldo, long N, void* stream) {
+  return precision == INQB_FP64
+             ? rotate_block_impl<double>(a, lda, Ma, R, ldr, Mo, out, ldo, N, (cudaStream_t)stream)
+             : rotate_block_impl<float>(a, lda, Ma, R, ldr, Mo, out, ldo, N, (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------- orthonormalisation without allocation

@@ -60,6 +60,11 @@ SIGNATURES = {
     "inqb_orthonormalize": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "inqb_band_energies": (ctypes.c_int, [_ctxp, _vp, _vp, ctypes.c_int, ctypes.c_int, _dp, _vp]),
     "inqb_orthonormalize_noalloc": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "inqb_overlap_block": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
+                                          _vp, ctypes.c_int, _vp]),
+    "inqb_cholesky_inverse": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "inqb_rotate_block": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
+                                         _vp, ctypes.c_int, _vp]),
     "inqb_autotune": (ctypes.c_int, [_ctxp, ctypes.c_int, _vp, _ip]),
     "inqb_set_schedule": (ctypes.c_int, [_ctxp, ctypes.c_int, _ip]),
     "inqb_crank_nicolson_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,

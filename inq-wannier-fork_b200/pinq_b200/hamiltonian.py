@@ -573,3 +573,36 @@ class KSHamiltonian:
         psi = self._check(psi)
         call("inqb_orthonormalize", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), self._stream())
         return psi
+
+    # -- the pieces of an orbital-sharded orthonormalisation (parallel.sharded_orthonormalize_)
+    def overlap_block(self, a, b) -> torch.Tensor:
+        """dV a^H b in FP64: a [N, Ma], b [N, Mb] -> complex128 [Ma, Mb] on the device
+        (one block of operations::overlap's set-parallel branch)."""
+        a = self._check(a)
+        b = self._check(b)
+        S = torch.empty((a.shape[1], b.shape[1]), dtype=torch.complex128, device=a.device)
+        call("inqb_overlap_block", self._h, a.data_ptr(), a.shape[1], a.stride(0), b.data_ptr(), b.shape[1],
+             b.stride(0), S.data_ptr(), S.stride(0), self._stream())
+        return S
+
+    def cholesky_inverse_(self, S: torch.Tensor) -> torch.Tensor:
+        """S (complex128 [M, M] on the device, Hermitian) <- U^-1 where S = U^H U."""
+        if S.dtype != torch.complex128 or not S.is_cuda or S.dim() != 2 or S.shape[0] != S.shape[1] \
+                or S.stride(1) != 1:
+            raise ValueError("S must be a square row-major complex128 CUDA matrix")
+        call("inqb_cholesky_inverse", self._h, S.data_ptr(), S.shape[0], S.stride(0), self._stream())
+        return S
+
+    def rotate_block(self, a, R: torch.Tensor, out=None) -> torch.Tensor:
+        """a R: a [N, Ma] in the context precision, R complex128 [Ma, Mo] on the device."""
+        a = self._check(a)
+        if R.dtype != torch.complex128 or not R.is_cuda or R.dim() != 2 or R.shape[0] != a.shape[1]:
+            raise ValueError("R must be a complex128 CUDA matrix with a.shape[1] rows")
+        R = R.contiguous()
+        if out is None:
+            out = torch.empty((a.shape[0], R.shape[1]), dtype=a.dtype, device=a.device)
+        out = self._check(out)
+        if R.shape[1] > 0:
+            call("inqb_rotate_block", self._h, a.data_ptr(), a.shape[1], a.stride(0), R.data_ptr(), R.stride(0),
+                 R.shape[1], out.data_ptr(), out.stride(0), self._stream())
+        return out

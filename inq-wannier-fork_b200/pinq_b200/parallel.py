@@ -65,3 +65,107 @@ def density_reducer(group=None):
         return rho
 
     return reduce_
+
+
+def _peer(group, r):
+    import torch.distributed as dist
+
+    return r if group is None else dist.get_global_rank(group, r)
+
+
+def _block_counts(M_local: int, device, group=None) -> list[int]:
+    """Orbital counts of every rank's block (an all-gather of one integer)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(group) == 1:
+        return [int(M_local)]
+    t = torch.tensor([int(M_local)], dtype=torch.int64, device=device)
+    out = [torch.zeros_like(t) for _ in range(dist.get_world_size(group))]
+    dist.all_gather(out, t, group=group)
+    return [int(x.item()) for x in out]
+
+
+def _ring_shift(blk, recv_count: int, group=None):
+    """Send blk to the next rank and take a block of recv_count orbitals from the
+    previous one (one step of the block circulation of
+    src/parallel/block_array_iterator.hpp)."""
+    import torch
+    import torch.distributed as dist
+
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    nxt, prv = _peer(group, (rank + 1) % world), _peer(group, (rank - 1) % world)
+    recv = torch.empty((blk.shape[0], recv_count), dtype=blk.dtype, device=blk.device)
+    ops = []
+    if blk.shape[1] > 0:
+        ops.append(dist.P2POp(dist.isend, torch.view_as_real(blk.contiguous()), nxt, group))
+    if recv_count > 0:
+        rr = torch.view_as_real(recv)
+        ops.append(dist.P2POp(dist.irecv, rr, prv, group))
+    if ops:
+        for req in dist.batch_isend_irecv(ops):
+            req.wait()
+    return recv
+
+
+def sharded_overlap(ham, psi_local, group=None):
+    """The full FP64 overlap dV Psi^H Psi of all ranks' orbitals, on every rank, as
+    operations::overlap's set-parallel branch forms it (src/operations/overlap.hpp:47-72):
+    the orbital blocks circulate around the ranks, each rank fills the rows of the
+    block it holds against the columns of its own, and an all-reduce sums the
+    zero-padded matrix.  Returns (S, counts)."""
+    import torch
+    import torch.distributed as dist
+
+    counts = _block_counts(psi_local.shape[1], psi_local.device, group)
+    starts = [sum(counts[:i]) for i in range(len(counts))]
+    world = len(counts)
+    rank = dist.get_rank(group) if world > 1 else 0
+    Mt = sum(counts)
+    S = torch.zeros((Mt, Mt), dtype=torch.complex128, device=psi_local.device)
+    c0, c1 = starts[rank], starts[rank] + counts[rank]
+    blk, src = psi_local, rank
+    for step in range(world):
+        if counts[src] > 0 and counts[rank] > 0:
+            S[starts[src]:starts[src] + counts[src], c0:c1] = ham.overlap_block(blk, psi_local)
+        if step < world - 1:
+            src = (src - 1) % world
+            blk = _ring_shift(blk, counts[src], group)
+    allreduce_sum_(torch.view_as_real(S), group)
+    return S, counts
+
+
+def sharded_orthonormalize_(ham, psi_local, group=None):
+    """operations::orthogonalize (src/operations/orthogonalize.hpp:25-32) of orbitals
+    split over ranks in blocks: the overlap of all of them (sharded_overlap), its
+    Cholesky factor S = U^H U and U^-1 on every rank (FP64, the same summed matrix
+    everywhere), then Psi <- Psi U^-1 as operations::rotate's set-parallel branch does
+    it (src/operations/rotate.hpp:100-125): each rank multiplies its block by its rows
+    of U^-1 for every rank's columns, and those terms are summed on the owner.
+    ham provides overlap_block, cholesky_inverse_ and rotate_block (KSHamiltonian does,
+    through the C ABI).  psi_local is overwritten; it is returned."""
+    import torch
+    import torch.distributed as dist
+
+    S, counts = sharded_overlap(ham, psi_local, group)
+    ham.cholesky_inverse_(S)
+    world = len(counts)
+    rank = dist.get_rank(group) if world > 1 else 0
+    starts = [sum(counts[:i]) for i in range(world)]
+    r0, r1 = starts[rank], starts[rank] + counts[rank]
+    mine = None  # the sum for this rank's own orbitals; psi_local is read until the last term
+    for s in range(world):
+        if counts[s] == 0:
+            continue
+        cols = slice(starts[s], starts[s] + counts[s])
+        if counts[rank] > 0:
+            part = ham.rotate_block(psi_local, S[r0:r1, cols])
+        else:
+            part = torch.zeros((psi_local.shape[0], counts[s]), dtype=psi_local.dtype, device=psi_local.device)
+        if world > 1:
+            dist.reduce(torch.view_as_real(part), dst=_peer(group, s), op=dist.ReduceOp.SUM, group=group)
+        if s == rank:
+            mine = part
+    if mine is not None:
+        psi_local.copy_(mine)
+    return psi_local
