@@ -398,11 +398,33 @@ int inqb_set_schedule(inqb_ctx* ctx, int M, const int schedule[4]);
  * on the stream the kernels run on; the counterpart of INQ's scoped timers
  * (CALI_CXX_MARK_SCOPE, src/utils/profiling.hpp:12, external_libs/kalimotxo/cali.h).
  * inqb_timing_stop waits for the recorded events and returns the summed
- * milliseconds of the three passes (z and inner y transforms + projection,
+ * milliseconds of the three passes (KB projection + z and inner y transforms,
  * outer y and x transforms + kinetic, inverse transforms + potential/nonlocal
- * epilogue). */
+ * epilogue).  inqb_timing_passes returns the same with the projection kernel
+ * apart: [projection, first pass, second pass, third pass]. */
 int inqb_timing_start(inqb_ctx* ctx, int max_applies);
 int inqb_timing_stop(inqb_ctx* ctx, double ms_per_pass[3], int* napplies);
+int inqb_timing_passes(inqb_ctx* ctx, double ms[4], int* napplies);
+
+/* ---------------------------------------------------------------- projection and device status
+ * How H|psi> forms the KB projections proj[a][l][m] of projector_all::project
+ * (src/hamiltonian/projector_all.hpp:98-216):
+ *   INQB_PROJECTION_KERNEL (default): a kernel of its own before the tile passes,
+ *     one CTA per (atom, block of orbitals) summing that atom's sphere points in a
+ *     fixed order: deterministic.  In the mixed precision it is a tcgen05 tensor-core
+ *     contraction (TF32 with a split-precision correction, FP64 sums per chunk of 32
+ *     points); in FP64 it runs on the CUDA cores.  Orbital blocks whose complex64
+ *     rows are not 16-byte aligned (odd ld) use the fused form instead.
+ *   INQB_PROJECTION_FUSED: summed inside the first tile pass, per-plane FP64
+ *     partials flushed with atomics (summation order varies from run to run). */
+enum inqb_projection_mode { INQB_PROJECTION_KERNEL = 0, INQB_PROJECTION_FUSED = 1 };
+int inqb_set_projection_mode(inqb_ctx* ctx, int mode);
+/* Kernels with a bounded device-side wait record a failed wait in a device word of
+ * the context instead of waiting forever.  This synchronises `stream`, returns
+ * INQB_ERR_TIMEOUT (and clears the word) if one gave up since the last call, whose
+ * results are then not valid, else INQB_OK.  No counterpart in the reference (its
+ * gpu::run synchronises after every kernel, external_libs/gpurun/include/gpu/run.hpp:76). */
+int inqb_device_status(inqb_ctx* ctx, void* stream);
 
 #ifdef __cplusplus
 }

@@ -16,6 +16,7 @@
 #include "propagators.h"
 #include "wannier.h"
 #include "plan.h"
+#include "project.h"
 
 namespace inqb {
 const char* last_error();
@@ -79,6 +80,11 @@ ProjView<T> proj_view(inqb_ctx* ctx) {
   v.ent_phase = t.d_ent_phase.ptr;
   v.scale = t.d_scale.as<double>();
   v.proj = ctx->d_projacc.as<double2>();
+  v.pc_ptr = t.d_pc_ptr.as<int>();
+  v.pc_pt = t.d_pc_pt.as<int>();
+  v.pc_table = t.pc_chunks > 0 ? t.d_pc_table.ptr : nullptr;
+  v.err = ctx->d_err.as<int>();
+  v.proj_mode = ctx->proj_mode;
   return v;
 }
 
@@ -101,10 +107,12 @@ int reserve(inqb_ctx* ctx, int M) {
 
 int update_phases(inqb_ctx* ctx, void* stream) {
   if (ctx->proj.nproj == 0 || ctx->proj.nent == 0) return INQB_OK;
-  return launch_phases(ctx->precision, ctx->proj.nent, ctx->proj.d_ent_relpos.as<float>(), ctx->kA_cov,
-                       ctx->proj.d_ent_phase.ptr, ctx->proj.d_ent_rec.ptr, ctx->proj.d_ent_rec_pt.ptr,
-                       ctx->proj.d_pt_pos.as<int>(), ctx->proj.d_adj_rec.ptr, ctx->proj.d_atom_pos.as<int>(),
-                       stream);
+  INQB_TRY(launch_phases(ctx->precision, ctx->proj.nent, ctx->proj.d_ent_relpos.as<float>(), ctx->kA_cov,
+                         ctx->proj.d_ent_phase.ptr, ctx->proj.d_ent_rec.ptr, ctx->proj.d_ent_rec_pt.ptr,
+                         ctx->proj.d_pt_pos.as<int>(), ctx->proj.d_adj_rec.ptr, ctx->proj.d_atom_pos.as<int>(),
+                         stream));
+  return launch_project_table(ctx->precision, ctx->proj.pc_chunks, ctx->proj.d_pc_relpos.as<float>(),
+                              ctx->proj.d_pc_beta.as<double>(), ctx->kA_cov, ctx->proj.d_pc_table.ptr, stream);
 }
 
 int set_kA(inqb_ctx* ctx, const double kA[3], void* stream) {
@@ -153,7 +161,7 @@ int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long l
     for (int k = 0; k < 3; k++) a.threads[k] = sched->second[1 + k];
   }
   if (ctx->timing_on && mode == LaunchArgs::H && ctx->timing_count < ctx->timing_capacity) {
-    for (int i = 0; i < 4; i++) a.events[i] = ctx->timing_events[4 * ctx->timing_count + i];
+    for (int i = 0; i < 5; i++) a.events[i] = ctx->timing_events[5 * ctx->timing_count + i];
     ctx->timing_count++;
   }
   ProjView<double> v64;
@@ -170,7 +178,7 @@ int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long l
 
 // One H application with the four pass events recorded (used by the autotuner).
 int apply_events(inqb_ctx* ctx, const void* in, void* out, int M, const double alpha[2], const double beta[2],
-                 void* stream, cudaEvent_t ev[4]) {
+                 void* stream, cudaEvent_t ev[5]) {
   INQB_TRY(reserve(ctx, M));
   if (!ctx->proj_phases_valid) {
     INQB_TRY(update_phases(ctx, stream));
@@ -180,7 +188,7 @@ int apply_events(inqb_ctx* ctx, const void* in, void* out, int M, const double a
   const int cap = ctx->timing_capacity, count = ctx->timing_count;
   std::vector<cudaEvent_t> saved;
   saved.swap(ctx->timing_events);
-  ctx->timing_events.assign(ev, ev + 4);
+  ctx->timing_events.assign(ev, ev + 5);
   ctx->timing_on = true;
   ctx->timing_capacity = 1;
   ctx->timing_count = 0;
@@ -626,6 +634,11 @@ int inqb_ctx_create(const double lattice[9], int nx, int ny, int nz, int precisi
     if (st == INQB_OK && cudaMemset(ctx->d_V.ptr, 0, ctx->d_V.bytes) != cudaSuccess)
       st = fail(INQB_ERR_CUDA, "potential init failed");
   }
+  if (st == INQB_OK) {
+    st = ctx->d_err.ensure(sizeof(int));
+    if (st == INQB_OK && cudaMemset(ctx->d_err.ptr, 0, sizeof(int)) != cudaSuccess)
+      st = fail(INQB_ERR_CUDA, "error word init failed");
+  }
   if (st != INQB_OK) {
     delete ctx;
     return st;
@@ -651,7 +664,7 @@ int inqb_timing_start(inqb_ctx* ctx, int max_applies) {
   INQB_CHECK_CTX(ctx);
   INQB_GUARD(ctx);
   if (max_applies <= 0) return fail(INQB_ERR_INVALID, "max_applies must be positive");
-  while ((int)ctx->timing_events.size() < 4 * max_applies) {
+  while ((int)ctx->timing_events.size() < 5 * max_applies) {
     cudaEvent_t e;
     INQB_CUDA_TRY(cudaEventCreate(&e));
     ctx->timing_events.push_back(e);
@@ -662,22 +675,53 @@ int inqb_timing_start(inqb_ctx* ctx, int max_applies) {
   return INQB_OK;
 }
 
-int inqb_timing_stop(inqb_ctx* ctx, double ms_per_pass[3], int* napplies) {
+int inqb_set_projection_mode(inqb_ctx* ctx, int mode) {
+  INQB_CHECK_CTX(ctx);
+  if (mode != INQB_PROJECTION_KERNEL && mode != INQB_PROJECTION_FUSED)
+    return fail(INQB_ERR_INVALID, "unknown projection mode");
+  ctx->proj_mode = mode;
+  return INQB_OK;
+}
+
+int inqb_device_status(inqb_ctx* ctx, void* stream) {
   INQB_CHECK_CTX(ctx);
   INQB_GUARD(ctx);
-  if (!ms_per_pass || !napplies) return fail(INQB_ERR_INVALID, "null output");
+  cudaStream_t st = (cudaStream_t)stream;
+  int word = 0;
+  INQB_CUDA_TRY(cudaMemcpyAsync(&word, ctx->d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  INQB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (word == 0) return INQB_OK;
+  INQB_CUDA_TRY(cudaMemsetAsync(ctx->d_err.ptr, 0, sizeof(int), st));
+  INQB_CUDA_TRY(cudaStreamSynchronize(st));
+  return fail(INQB_ERR_TIMEOUT, "a device-side wait of a kernel gave up (its results are not valid)");
+}
+
+int inqb_timing_passes(inqb_ctx* ctx, double ms[4], int* napplies) {
+  INQB_CHECK_CTX(ctx);
+  INQB_GUARD(ctx);
+  if (!ms || !napplies) return fail(INQB_ERR_INVALID, "null output");
   ctx->timing_on = false;
-  for (int k = 0; k < 3; k++) ms_per_pass[k] = 0.0;
+  for (int k = 0; k < 4; k++) ms[k] = 0.0;
   *napplies = ctx->timing_count;
   for (int i = 0; i < ctx->timing_count; i++) {
-    INQB_CUDA_TRY(cudaEventSynchronize(ctx->timing_events[4 * i + 3]));
-    for (int k = 0; k < 3; k++) {
-      float ms = 0.f;
-      INQB_CUDA_TRY(cudaEventElapsedTime(&ms, ctx->timing_events[4 * i + k], ctx->timing_events[4 * i + k + 1]));
-      ms_per_pass[k] += ms;
+    INQB_CUDA_TRY(cudaEventSynchronize(ctx->timing_events[5 * i + 4]));
+    for (int k = 0; k < 4; k++) {
+      float t = 0.f;
+      INQB_CUDA_TRY(cudaEventElapsedTime(&t, ctx->timing_events[5 * i + k], ctx->timing_events[5 * i + k + 1]));
+      ms[k] += t;
     }
   }
   ctx->timing_count = 0;
+  return INQB_OK;
+}
+
+int inqb_timing_stop(inqb_ctx* ctx, double ms_per_pass[3], int* napplies) {
+  if (!ms_per_pass) return fail(INQB_ERR_INVALID, "null output");
+  double ms[4];
+  INQB_TRY(inqb_timing_passes(ctx, ms, napplies));
+  ms_per_pass[0] = ms[0] + ms[1];
+  ms_per_pass[1] = ms[2];
+  ms_per_pass[2] = ms[3];
   return INQB_OK;
 }
 
@@ -1643,7 +1687,7 @@ int inqb_autotune(inqb_ctx* ctx, int M, void* stream, int schedule[4]) {
   INQB_TRY(out.ensure(bytes));
   cudaStream_t st = (cudaStream_t)stream;
   INQB_CUDA_TRY(cudaMemsetAsync(in.ptr, 0, bytes, st));
-  cudaEvent_t ev[4];
+  cudaEvent_t ev[5];
   for (auto& e : ev) INQB_CUDA_TRY(cudaEventCreate(&e));
   const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
   const bool saved_timing = ctx->timing_on;
@@ -1655,11 +1699,12 @@ int inqb_autotune(inqb_ctx* ctx, int M, void* stream, int schedule[4]) {
     for (int k = 0; k < 3; k++) out_ms[k] = 1e30f;
     for (int rep = 0; rep < 4; rep++) {
       INQB_TRY(apply_events(ctx, in.ptr, out.ptr, M, one, zero, stream, ev));
-      INQB_CUDA_TRY(cudaEventSynchronize(ev[3]));
+      INQB_CUDA_TRY(cudaEventSynchronize(ev[4]));
       if (rep == 0) continue;
+      // the three tile passes (the projection kernel before them is not scheduled)
       for (int k = 0; k < 3; k++) {
         float t = 0.f;
-        INQB_CUDA_TRY(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+        INQB_CUDA_TRY(cudaEventElapsedTime(&t, ev[k + 1], ev[k + 2]));
         out_ms[k] = std::min(out_ms[k], t);
       }
     }

@@ -19,6 +19,7 @@
 #include "fft_tile.cuh"
 #include "inqb_internal.h"
 #include "plan.h"
+#include "project.h"
 #include "sizes.h"
 
 namespace inqb {
@@ -171,22 +172,35 @@ static int launch_h_impl(const LaunchArgs& a) {
   kp.pois = (T)0;
 
   if (a.mode == LaunchArgs::H) {
-    const int acc_cap = pj.nproj > 0 ? std::min(pj.max_plane_atoms, kAccAtomsMax) : 0;
+    // the KB projection: its own deterministic kernel (project.cu) where the tables and
+    // the block's alignment allow, else fused into the first tile pass with FP64 atomics
+    const bool sep = pj.nproj > 0 && pj.proj_mode == 0 && pj.pc_table != nullptr &&
+                     project_supported(sizeof(T) == 8 ? INQB_FP64 : INQB_MIXED, a.in, a.ld_in);
+    ProjView<T> pjA = pj;
+    if (sep) pjA.nproj = 0;
+    const int acc_cap = pjA.nproj > 0 ? std::min(pj.max_plane_atoms, kAccAtomsMax) : 0;
     const int seg_cap = pj.nproj > 0 ? std::min(pj.max_tile_seg, kAccAtomsMax) : 0;
     // stage a tile's records only when all of them fit beside the tile (the kernel
     // reads them from global memory otherwise)
     int rec_cap = (pj.nproj > 0 && pj.max_tile_ent <= kRecCapMax) ? pj.max_tile_ent : 0;
+    const int rec_cap_fwd = pjA.nproj > 0 ? rec_cap : 0;
     if (TG::smem_fwd(acc_cap, rec_cap) > TG::SMEM_MAX) rec_cap = 0;
+    const int rec_cap_a = (TG::smem_fwd(acc_cap, rec_cap_fwd) > TG::SMEM_MAX) ? 0 : rec_cap_fwd;
     if (pj.nproj > 0 && pj.pt_stride != TG::PSTRIDE)
       return fail(INQB_ERR_INVALID, "projector tables were built for another tiling of this grid");
-    if (pj.nproj > 0)
-      INQB_CUDA_TRY(cudaMemsetAsync(pj.proj, 0, sizeof(double2) * (size_t)pj.nproj * pj.L * a.M, st));
     if (a.events[0]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[0], st));
-    k_tile_fwd<T, NX, NY, NZ><<<gfwd, thr[0], TG::smem_fwd(acc_cap, rec_cap), st>>>(
-        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pj, acc_cap, rec_cap, ysplit, vin);
+    if (sep) {
+      INQB_TRY(launch_project(sizeof(T) == 8 ? INQB_FP64 : INQB_MIXED, a.in, a.ld_in, a.M, pj.nproj, pj.L,
+                              pj.pc_ptr, pj.pc_pt, pj.pc_table, pj.scale, pj.proj, pj.err, st));
+    } else if (pj.nproj > 0) {
+      INQB_CUDA_TRY(cudaMemsetAsync(pj.proj, 0, sizeof(double2) * (size_t)pj.nproj * pj.L * a.M, st));
+    }
     if (a.events[1]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[1], st));
-    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out);
+    k_tile_fwd<T, NX, NY, NZ><<<gfwd, thr[0], TG::smem_fwd(acc_cap, rec_cap_a), st>>>(
+        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pjA, acc_cap, rec_cap_a, ysplit, vin);
     if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
+    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out);
+    if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
     EpiParams<T> ep;
     ep.V = (const T*)a.V;
     ep.vshift = a.fourier_mask ? (T)(0.5 * kA2) : (T)0;
@@ -204,7 +218,7 @@ static int launch_h_impl(const LaunchArgs& a) {
     k_tile_inv<T, NX, NY, NZ, 1><<<ginv, thr[2], TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
         tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv, seg_cap,
         vin && vout);
-    if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
+    if (a.events[4]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[4], st));
   } else if (a.mode == LaunchArgs::POISSON) {
     // solvers::poisson on M complex fields: forward z and inner y, then the outer y
     // and x transforms with the 4 pi / (N |G|^2) factor, then the inverse (no 1/N:

@@ -117,6 +117,16 @@ struct ProjTables {
   // the unit of work of the nonlocal moment kernel of the adjoint
   std::vector<int> chunk_atom, chunk_beg, atom_chunk_ptr;
   std::vector<int> atom_pos;        // [nent] position of entry e in atom-major order
+  // per-atom chunks of kProjChunk entries (atom-major, the last chunk of an atom padded)
+  // for the projection kernels: pc_ptr [nproj+1] chunk offsets, pc_pt [chunks * 32]
+  // linear grid point (-1 = padding), pc_beta [chunks * 32][4] (zero past L and for
+  // padding), pc_relpos [chunks * 32][3] contravariant float relative position
+  int pc_chunks = 0;
+  std::vector<int> pc_ptr, pc_pt;
+  std::vector<double> pc_beta;
+  std::vector<float> pc_relpos;
+  DevBuf d_pc_ptr, d_pc_pt, d_pc_beta, d_pc_relpos;
+  DevBuf d_pc_table;                // coefficient table beta exp(+i (k+A).r) for the current k + A
   DevBuf d_adj_rec, d_atom_pos;     // [nent] AdjRec<T> in atom-major order
   // device copies
   DevBuf d_seg_ptr, d_seg_atom, d_seg_ent, d_seg_local, d_plane_ptr, d_plane_atom, d_ent_off, d_ent_atom;
@@ -153,6 +163,12 @@ struct ProjView {
   const int* pt_ptr;            // [tiles][pt_stride]
   const double* scale;
   double2* proj;          // [nproj][L][M] accumulators (FP64 in both precisions)
+  // the projection kernels' chunk tables (project.h)
+  const int* pc_ptr;
+  const int* pc_pt;
+  const void* pc_table;
+  int* err;               // device error word (a device-side wait gave up)
+  int proj_mode;          // 0: projection kernel, 1: projection fused into the first tile pass
 };
 
 constexpr int kNlChunk = 64;  // sphere entries per chunk of the adjoint's nonlocal moments
@@ -197,6 +213,8 @@ struct inqb_ctx {
   inqb::DevBuf d_mlwf;          // TD-MLWF: the six matrices, u, adiag, sums, slabs, pairs, deltas
   inqb::DevBuf d_pot;           // density -> potential: V_H field [N] (complex), previous
                                 // density [N], partial sums, sums
+  inqb::DevBuf d_err;           // one int: set by a kernel whose bounded device-side wait gave up
+  int proj_mode = 0;            // INQB_PROJECTION_KERNEL (0) or INQB_PROJECTION_FUSED (1)
   inqb::DevBuf d_mix;           // Crank-Nicolson with self-consistency: Broyden ring df, dv [4][N],
                                 // f_old, vin_old, the new density [N], partial sums, dot products
   size_t elem_bytes() const { return precision == INQB_FP64 ? 16 : 8; }
@@ -210,7 +228,7 @@ struct inqb_ctx {
   cudaEvent_t host_events[8] = {};
 
   // optional per-pass CUDA-event timing of H applications
-  std::vector<cudaEvent_t> timing_events;  // 4 per recorded application
+  std::vector<cudaEvent_t> timing_events;  // 5 per recorded application
   int timing_capacity = 0, timing_count = 0;
   bool timing_on = false;
 };

@@ -11,6 +11,7 @@
 #include <numeric>
 
 #include "inqb_internal.h"
+#include "project.h"
 #include "sizes.h"
 
 namespace inqb {
@@ -343,6 +344,23 @@ int build_proj_tables(const inqb_ctx& ctx, int nproj, int L, int smax, const int
     }
   }
   t.atom_chunk_ptr[nproj] = (int)t.chunk_atom.size();
+  // chunks of the projection kernels, in atom-major entry order
+  t.pc_ptr.assign(nproj + 1, 0);
+  for (int a = 0; a < nproj; a++)
+    t.pc_ptr[a + 1] = t.pc_ptr[a] + (t.atom_ptr[a + 1] - t.atom_ptr[a] + kProjChunk - 1) / kProjChunk;
+  t.pc_chunks = t.pc_ptr[nproj];
+  const size_t pcn = (size_t)t.pc_chunks * kProjChunk;
+  t.pc_pt.assign(pcn, -1);
+  t.pc_beta.assign(pcn * 4, 0.0);
+  t.pc_relpos.assign(pcn * 3, 0.0f);
+  for (int a = 0; a < nproj; a++)
+    for (int i = t.atom_ptr[a]; i < t.atom_ptr[a + 1]; i++) {
+      const size_t q = (size_t)t.pc_ptr[a] * kProjChunk + (i - t.atom_ptr[a]);
+      const int ee = t.atom_ent[i];
+      t.pc_pt[q] = t.ent_pt[ee];
+      for (int l = 0; l < L && l < 4; l++) t.pc_beta[4 * q + l] = t.ent_beta[(size_t)ee * L + l];
+      for (int d = 0; d < 3; d++) t.pc_relpos[3 * q + d] = t.ent_relpos[3 * (size_t)ee + d];
+    }
   t.scale.resize((size_t)nproj * L);
   for (int a = 0; a < nproj; a++)
     for (int l = 0; l < L; l++) t.scale[(size_t)a * L + l] = ctx.dV * coeff[(size_t)a * L + l];
@@ -428,6 +446,11 @@ int upload_proj_tables(const inqb_ctx& ctx, ProjTables& t) {
     INQB_TRY(upload(t.d_adj_rec, adj_records<float>(t)));
   }
   INQB_TRY(upload(t.d_pt_ptr, t.pt_ptr));
+  INQB_TRY(upload(t.d_pc_ptr, t.pc_ptr));
+  INQB_TRY(upload(t.d_pc_pt, t.pc_pt));
+  INQB_TRY(upload(t.d_pc_beta, t.pc_beta));
+  INQB_TRY(upload(t.d_pc_relpos, t.pc_relpos));
+  INQB_TRY(t.d_pc_table.ensure(std::max<size_t>(project_table_bytes(ctx.precision, t.pc_chunks), 16)));
   return INQB_OK;
 }
 

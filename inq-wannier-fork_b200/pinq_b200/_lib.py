@@ -60,6 +60,9 @@ SIGNATURES = {
     "inqb_orthonormalize": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "inqb_band_energies": (ctypes.c_int, [_ctxp, _vp, _vp, ctypes.c_int, ctypes.c_int, _dp, _vp]),
     "inqb_orthonormalize_noalloc": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "inqb_set_projection_mode": (ctypes.c_int, [_ctxp, ctypes.c_int]),
+    "inqb_device_status": (ctypes.c_int, [_ctxp, _vp]),
+    "inqb_timing_passes": (ctypes.c_int, [_ctxp, _dp, _ip]),
     "inqb_overlap_block": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
                                           _vp, ctypes.c_int, _vp]),
     "inqb_cholesky_inverse": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),

@@ -549,11 +549,30 @@ class KSHamiltonian:
         call("inqb_timing_start", self._h, int(max_applies))
 
     def timing_stop(self):
-        """(summed ms of [tile_fwd, tile_x, tile_inv], number of timed applies)."""
+        """(summed ms of [projection + tile_fwd, tile_x, tile_inv], number of timed applies)."""
         ms = np.zeros(3)
         n = ctypes.c_int(0)
         call("inqb_timing_stop", self._h, dptr(ms), ctypes.byref(n))
         return ms, n.value
+
+    def timing_passes(self):
+        """(summed ms of [projection kernel, tile_fwd, tile_x, tile_inv], number of timed applies)."""
+        ms = np.zeros(4)
+        n = ctypes.c_int(0)
+        call("inqb_timing_passes", self._h, dptr(ms), ctypes.byref(n))
+        return ms, n.value
+
+    PROJECTION_KERNEL = 0
+    PROJECTION_FUSED = 1
+
+    def set_projection_mode(self, mode):
+        """INQB_PROJECTION_KERNEL (0, or "kernel") or INQB_PROJECTION_FUSED (1, or "fused")."""
+        m = {"kernel": 0, "fused": 1}.get(mode, mode)
+        call("inqb_set_projection_mode", self._h, int(m))
+
+    def device_status(self):
+        """Raise if a kernel's bounded device-side wait gave up since the last check."""
+        call("inqb_device_status", self._h, self._stream())
 
     def band_energies(self, psi, hpsi=None) -> np.ndarray:
         """eps[m] = Re<H psi_m|psi_m> / <psi_m|psi_m> (FP64 sums); H psi is applied
