@@ -10,10 +10,11 @@
 //
 //   mixed   k_project_tc: tcgen05 tensor-core MMAs, kind::tf32, FP32 accumulation in
 //           tensor memory, with a split-precision correction.  A chunk of 32 sphere
-//           points is gathered (cp.async, 512-byte orbital rows) straight into the
-//           MN-major operand layout; each value x becomes hi = tf32(x) and
-//           lo = tf32(x - hi), and the coefficient table holds the same split, so
-//           hi*hi + hi*lo + lo*hi + lo*lo restores FP32 products.  Each chunk's
+//           points is gathered (cp.async, whole 512-byte orbital rows) into a
+//           staging buffer, four chunks in flight; a pass over shared memory
+//           transposes it into the K-major operand and splits each value x into
+//           hi = tf32(x) and lo = tf32(x - hi).  The coefficient table holds the same
+//           split, so hi*hi + hi*lo + lo*hi + lo*lo restores FP32 products.  Each chunk's
 //           accumulator is added to FP64 registers (two accumulators in tensor
 //           memory alternate, so the MMAs of one chunk overlap the read-out of the
 //           previous one).
@@ -118,17 +119,19 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
                : "memory");
 }
-// 16 consecutive FP32 columns of this warp's 32 tensor-memory lanes.
+// 16 consecutive FP32 columns of this warp's 32 tensor-memory lanes.  The load and its
+// wait are one asm statement, so no use of the registers can be scheduled before the
+// wait.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
+      "%15}, [%16];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
         "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr)
       : "memory");
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
@@ -141,12 +144,13 @@ __device__ __forceinline__ float tf32_round(float x) {
 }
 
 // ---------------------------------------------------------------- tensor-core geometry
-//   MMA shape M = 128 (64 orbitals x (re, im)), N = 16, K = 8 per instruction.
-//   A (M x K, MN-major, no swizzle): element (row, k) at byte
-//     (row / 4) * 128 + (k % 8) * 16 + (k / 8) * 4096 + (row % 4) * 4,
-//   so a 16-byte piece of one orbital row (two complex64 orbitals at one sphere
-//   point) lands whole: the gather is one cp.async per piece.
-//   B (N x K, K-major, no swizzle): element (n, k) at byte
+//   MMA shape M = 128 (64 orbitals x (re, im)), N = 16, K = 8 per instruction; both
+//   operands K-major without swizzle (core matrices of 8 rows x 16 bytes).
+//   The gather lands each sphere point's 512-byte orbital row whole in a staging
+//   buffer ([point][128 floats]); the split pass transposes it into
+//   A (M x K): element (row, k) at byte
+//     (row % 8) * 16 + (row / 8) * 128 + (k % 4) * 4 + (k / 4) * 2048.
+//   B (N x K): element (n, k) at byte
 //     (n / 8) * 1024 + (k / 4) * 128 + (n % 8) * 16 + (k % 4) * 4,
 //   columns n = [Re B hi (l 0-3) | Im B hi | Re B lo | Im B lo], built by
 //   k_project_table in exactly this layout (one 2 KB piece per chunk).
@@ -154,15 +158,17 @@ constexpr int kRows = 2 * kProjOrbTC;            // 128
 constexpr int kN = 16;
 constexpr int kABytes = kProjChunk * kRows * 4;  // 16 KB per chunk
 constexpr int kBBytes = kProjChunk * kN * 4;     // 2 KB per chunk
-constexpr int kStages = 3;
-constexpr int kStageBytes = 2 * kABytes + kBBytes;  // A hi (the gathered rows, converted in place), A lo, B
+constexpr int kStages = 4;                       // gathered chunks in flight
+constexpr int kStageBytes = kABytes + kBBytes;   // staging rows + B
 constexpr int kTCThreads = 128;
-constexpr size_t kTCSmem = (size_t)kStages * kStageBytes + 64;
+// stages | A hi, A lo of two chunks (double-buffered against the MMAs) | barriers
+constexpr size_t kSplitOff = (size_t)kStages * kStageBytes;
+constexpr size_t kTCSmem = kSplitOff + 4 * (size_t)kABytes + 64;
 
-// c_format F32 (bits 4-5), a/b format TF32 (bits 7-9, 10-12), A MN-major (bit 15),
-// B K-major (bit 16), N >> 3 (bits 17-22), M >> 4 (bits 24-28)
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | ((uint32_t)(kN >> 3) << 17) |
-                            ((uint32_t)(kRows >> 4) << 24);
+// c_format F32 (bits 4-5), a/b format TF32 (bits 7-9, 10-12), A and B K-major (bits
+// 15, 16 clear), N >> 3 (bits 17-22), M >> 4 (bits 24-28)
+constexpr uint32_t kIdesc =
+    (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kN >> 3) << 17) | ((uint32_t)(kRows >> 4) << 24);
 
 __device__ __forceinline__ int b_index(int n, int k) {  // in floats
   return (n >> 3) * 256 + (k >> 2) * 32 + (n & 7) * 4 + (k & 3);
@@ -171,12 +177,12 @@ __device__ __forceinline__ int b_index(int n, int k) {  // in floats
 // A device-side wait that gives up: the kernel records it and returns.
 constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s
 
-__global__ void __launch_bounds__(kTCThreads, 2)
+__global__ void __launch_bounds__(kTCThreads, 1)
     k_project_tc(const cplx<float>* __restrict__ in, long ld, int M, const int* __restrict__ pc_ptr,
                  const int* __restrict__ pc_pt, const float* __restrict__ pc_b, const double* __restrict__ scale,
                  int L, double2* __restrict__ proj, int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + (size_t)kStages * kStageBytes);  // [2]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kSplitOff + 4 * (size_t)kABytes);  // [2]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
@@ -197,24 +203,25 @@ __global__ void __launch_bounds__(kTCThreads, 2)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  auto stage_a = [&](int s) { return smem + (size_t)s * kStageBytes; };
-  auto stage_lo = [&](int s) { return smem + (size_t)s * kStageBytes + kABytes; };
-  auto stage_b = [&](int s) { return smem + (size_t)s * kStageBytes + 2 * kABytes; };
+  auto stage_rows = [&](int s) { return smem + (size_t)s * kStageBytes; };
+  auto stage_b = [&](int s) { return smem + (size_t)s * kStageBytes + kABytes; };
+  auto split_hi = [&](int b) { return smem + kSplitOff + (size_t)(2 * b) * kABytes; };
+  auto split_lo = [&](int b) { return smem + kSplitOff + (size_t)(2 * b + 1) * kABytes; };
 
-  // gather of chunk c into stage s: 32 points x 32 pieces of 16 bytes, then the B piece
+  // gather of chunk c into stage s: 32 rows of 32 pieces of 16 bytes, then the B piece
   auto load_chunk = [&](int c, int s) {
     if (c < nch) {
       const int* pts = pc_pt + (size_t)(c0 + c) * kProjChunk;
-      unsigned char* A = stage_a(s);
+      unsigned char* R = stage_rows(s);
 #pragma unroll
       for (int i = 0; i < (kProjChunk * 32) / kTCThreads; i++) {
         const int idx = i * kTCThreads + tid;
-        const int kk = idx & 7, q = (idx >> 3) & 31, k = (idx >> 8) * 8 + kk;
+        const int q = idx & 31, k = idx >> 5;
         const int pt = pts[k];
         const int nval = M - m0 - 2 * q;  // orbitals of this piece inside the block
         const int bytes = (pt < 0 || nval <= 0) ? 0 : (nval >= 2 ? 16 : 8);
         const cplx<float>* src = bytes ? in + (long)pt * ld + m0 + 2 * q : in;
-        cp_async16_zfill(A + q * 128 + kk * 16 + (k >> 3) * 4096, src, bytes);
+        cp_async16_zfill(R + k * 512 + q * 16, src, bytes);
       }
       cp_async16_zfill(stage_b(s) + tid * 16, pc_b + (size_t)(c0 + c) * (kBBytes / 4) + tid * 4, 16);
     }
@@ -244,43 +251,45 @@ __global__ void __launch_bounds__(kTCThreads, 2)
 
   bool ok = true;
   for (int c = 0; c < nch; c++) {
-    const int s = c % kStages;
+    const int s = c % kStages, b = c & 1;
     cp_async_wait<kStages - 2>();
     __syncthreads();
-    // split in place: the gathered value becomes its TF32 head, the tail goes to A lo
+    // transpose into the K-major operand and split: hi = tf32(x), lo = tf32(x - hi).
+    // Buffer b was last read by the MMAs of chunk c - 2, which completed before its
+    // accumulator was read in the previous iteration.
     {
-      float4* A = reinterpret_cast<float4*>(stage_a(s));
-      float4* Lo = reinterpret_cast<float4*>(stage_lo(s));
+      const float* R = reinterpret_cast<const float*>(stage_rows(s));
+      unsigned char* H = split_hi(b);
+      unsigned char* Lo = split_lo(b);
+      const int row = tid;
 #pragma unroll
-      for (int i = 0; i < kABytes / 16 / kTCThreads; i++) {
-        const int idx = i * kTCThreads + tid;
-        float4 x = A[idx], h, t;
-        h.x = tf32_round(x.x);
-        h.y = tf32_round(x.y);
-        h.z = tf32_round(x.z);
-        h.w = tf32_round(x.w);
-        t.x = tf32_round(x.x - h.x);
-        t.y = tf32_round(x.y - h.y);
-        t.z = tf32_round(x.z - h.z);
-        t.w = tf32_round(x.w - h.w);
-        A[idx] = h;
-        Lo[idx] = t;
+      for (int kc = 0; kc < kProjChunk / 4; kc++) {
+        float x[4], h[4], t[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          x[j] = R[(4 * kc + j) * kRows + row];
+          h[j] = tf32_round(x[j]);
+          t[j] = tf32_round(x[j] - h[j]);
+        }
+        const int off = (row & 7) * 16 + (row >> 3) * 128 + kc * 2048;
+        *reinterpret_cast<float4*>(H + off) = make_float4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<float4*>(Lo + off) = make_float4(t[0], t[1], t[2], t[3]);
       }
     }
     fence_proxy_async_smem();
     __syncthreads();
     if (tid == 0) {
       tc_fence_after();
-      const uint32_t d = tmem + (uint32_t)((c & 1) * kN);
+      const uint32_t d = tmem + (uint32_t)(b * kN);
 #pragma unroll
       for (int kk = 0; kk < kProjChunk / 8; kk++) {
-        const uint64_t ah = smem_desc(stage_a(s) + kk * 4096, 4096, 128);
-        const uint64_t al = smem_desc(stage_lo(s) + kk * 4096, 4096, 128);
+        const uint64_t ah = smem_desc(split_hi(b) + kk * 4096, 2048, 128);
+        const uint64_t al = smem_desc(split_lo(b) + kk * 4096, 2048, 128);
         const uint64_t bd = smem_desc(stage_b(s) + kk * 256, 128, 1024);
         mma_tf32(d, ah, bd, kIdesc, kk > 0 ? 1u : 0u);
         mma_tf32(d, al, bd, kIdesc, 1u);
       }
-      mma_commit(&bar[c & 1]);
+      mma_commit(&bar[b]);
     }
     // the previous chunk's accumulator, while this chunk's MMAs run
     if (c > 0 && ok) ok = drain(c - 1);
@@ -290,7 +299,8 @@ __global__ void __launch_bounds__(kTCThreads, 2)
       ok = false;
       break;
     }
-    // stage (c - 1) % kStages is free: its MMAs completed before the drain above
+    // stage (c - 1) % kStages is free: its rows were split in the previous iteration
+    // and its B piece was read by MMAs that completed before the drain above
     load_chunk(c + kStages - 1, (c + kStages - 1) % kStages);
   }
   if (ok && nch > 0) ok = drain(nch - 1);

@@ -187,6 +187,16 @@ class KSHamiltonian:
     def _stream():
         return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
+    def _out_like(self, psi: torch.Tensor, out: torch.Tensor | None) -> torch.Tensor:
+        """An output block for a call that takes one leading dimension for its input
+        and output: psi's shape and row stride (a new block when out is None)."""
+        if out is None:
+            return torch.empty((psi.shape[0], psi.stride(0)), dtype=psi.dtype, device=psi.device)[:, :psi.shape[1]]
+        out = self._check(out)
+        if out.shape != psi.shape or out.stride(0) != psi.stride(0):
+            raise ValueError("out must have the shape and the leading dimension (row stride) of the input")
+        return out
+
     def empty(self, M: int) -> torch.Tensor:
         return torch.empty((self.N, M), dtype=self.dtype, device=self.device)
 
@@ -194,9 +204,7 @@ class KSHamiltonian:
     def apply(self, psi: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
         """out = H psi  (ks_hamiltonian::operator(); out may be psi)."""
         psi = self._check(psi)
-        if out is None:
-            out = torch.empty_like(psi)
-        self._check(out)
+        out = self._out_like(psi, out)
         call("inqb_apply_h", self._h, psi.data_ptr(), out.data_ptr(), psi.shape[1], psi.stride(0), self._stream())
         return out
 
@@ -206,6 +214,8 @@ class KSHamiltonian:
         """H psi on host memory (copies in and out inside the call)."""
         if torch.is_tensor(psi_host):
             src = psi_host
+            if not src.is_contiguous() or (out is not None and (not out.is_contiguous() or out.shape != src.shape)):
+                raise ValueError("host blocks must be contiguous [N, M] tensors of one shape")
             if out is None:
                 out = torch.empty_like(src)
             call("inqb_apply_h_host", self._h, src.data_ptr(), out.data_ptr(), src.shape[1])
@@ -218,13 +228,13 @@ class KSHamiltonian:
 
     def to_fourier(self, psi, out=None):
         psi = self._check(psi)
-        out = torch.empty_like(psi) if out is None else self._check(out)
+        out = self._out_like(psi, out)
         call("inqb_fft_forward", self._h, psi.data_ptr(), out.data_ptr(), psi.shape[1], psi.stride(0), self._stream())
         return out
 
     def to_real(self, psi, out=None):
         psi = self._check(psi)
-        out = torch.empty_like(psi) if out is None else self._check(out)
+        out = self._out_like(psi, out)
         call("inqb_fft_backward", self._h, psi.data_ptr(), out.data_ptr(), psi.shape[1], psi.stride(0), self._stream())
         return out
 
@@ -240,7 +250,7 @@ class KSHamiltonian:
         """solvers::poisson (periodic cell) of complex fields [N, M] in the context
         precision: V(G) = 4 pi rho(G) / |G|^2, 0 at G = 0."""
         fields = self._check(fields)
-        out = torch.empty_like(fields) if out is None else self._check(out)
+        out = self._out_like(fields, out)
         call("inqb_poisson", self._h, fields.data_ptr(), out.data_ptr(), fields.shape[1], fields.stride(0),
              self._stream())
         return out

@@ -86,3 +86,15 @@ def test_tensor_core_projection_close_to_fused(pb, sys70):
     h.set_projection_mode("fused")
     b = h(x).cpu().numpy()
     assert rel_norm(a, b) < 5e-7
+
+
+def test_output_takes_the_input_row_stride(pb, sys70):
+    """The C ABI takes one leading dimension for input and output: a new output block
+    gets the input's row stride, and an output with another stride is refused."""
+    h = make_product(pb, sys70, "mixed")
+    full = torch.as_tensor(sys70["psi"][:, :10]).to("cuda", torch.complex64)
+    view = full[:, 2:9]
+    out = h(view)
+    assert out.shape == view.shape and out.stride(0) == view.stride(0)
+    with pytest.raises(ValueError):
+        h.apply(view, out=torch.empty_like(view.contiguous()))
