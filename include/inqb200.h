@@ -408,16 +408,19 @@ int inqb_timing_passes(inqb_ctx* ctx, double ms[4], int* napplies);
 
 /* ---------------------------------------------------------------- projection and device status
  * How H|psi> forms the KB projections proj[a][l][m] of projector_all::project
- * (src/hamiltonian/projector_all.hpp:98-216):
- *   INQB_PROJECTION_KERNEL (default): a kernel of its own before the tile passes,
- *     one CTA per (atom, block of orbitals) summing that atom's sphere points in a
- *     fixed order: deterministic.  In the mixed precision it is a tcgen05 tensor-core
- *     contraction (TF32 with a split-precision correction, FP64 sums per chunk of 32
- *     points); in FP64 it runs on the CUDA cores.  Orbital blocks whose complex64
- *     rows are not 16-byte aligned (odd ld) use the fused form instead.
- *   INQB_PROJECTION_FUSED: summed inside the first tile pass, per-plane FP64
- *     partials flushed with atomics (summation order varies from run to run). */
-enum inqb_projection_mode { INQB_PROJECTION_KERNEL = 0, INQB_PROJECTION_FUSED = 1 };
+ * (src/hamiltonian/projector_all.hpp:98-216).  Both are deterministic: every partial
+ * sum has one owner and the partials are added in a fixed order.
+ *   INQB_PROJECTION_FUSED (default): summed inside the first tile pass while the tile
+ *     is in shared memory (FP32 products, FP64 sums), one partial per (x-plane, half
+ *     of its row classes, atom), added per atom by a small finish kernel.
+ *   INQB_PROJECTION_KERNEL: a kernel of its own before the tile passes, one CTA per
+ *     (atom, block of orbitals) that gathers the orbitals at the atom's sphere points.
+ *     In the mixed precision it is a tcgen05 tensor-core contraction (TF32 with a
+ *     split-precision correction, FP64 sums per chunk of 32 points); in FP64 it runs
+ *     on the CUDA cores.  It reads the sphere points' orbitals once more from memory,
+ *     and measures slower than the fused form; orbital blocks whose complex64 rows are
+ *     not 16-byte aligned (odd ld) take the fused form. */
+enum inqb_projection_mode { INQB_PROJECTION_FUSED = 0, INQB_PROJECTION_KERNEL = 1 };
 int inqb_set_projection_mode(inqb_ctx* ctx, int mode);
 /* Kernels with a bounded device-side wait record a failed wait in a device word of
  * the context instead of waiting forever.  This synchronises `stream`, returns

@@ -85,6 +85,9 @@ ProjView<T> proj_view(inqb_ctx* ctx) {
   v.pc_table = t.pc_chunks > 0 ? t.d_pc_table.ptr : nullptr;
   v.err = ctx->d_err.as<int>();
   v.proj_mode = ctx->proj_mode;
+  v.slots = ctx->d_slots.as<double2>();
+  v.aslot_ptr = t.d_aslot_ptr.as<int>();
+  v.aslot = t.d_aslot.as<int>();
   return v;
 }
 
@@ -160,8 +163,13 @@ int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long l
     a.ysplit = sched->second[0];
     for (int k = 0; k < 3; k++) a.threads[k] = sched->second[1 + k];
   }
+  // the fused projection's partial sums: one [4][M] slot per (plane, atom, half)
+  if (mode == LaunchArgs::H && ctx->proj.nproj > 0 && ctx->proj_mode == INQB_PROJECTION_FUSED) {
+    const int ys = a.ysplit > 0 ? a.ysplit : ctx->plan->ysplit;
+    INQB_TRY(ctx->d_slots.ensure(sizeof(double2) * (size_t)ctx->proj.aslot.size() * ys * 4 * M));
+  }
   if (ctx->timing_on && mode == LaunchArgs::H && ctx->timing_count < ctx->timing_capacity) {
-    for (int i = 0; i < 5; i++) a.events[i] = ctx->timing_events[5 * ctx->timing_count + i];
+    for (int i = 0; i < 6; i++) a.events[i] = ctx->timing_events[6 * ctx->timing_count + i];
     ctx->timing_count++;
   }
   ProjView<double> v64;
@@ -178,7 +186,7 @@ int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long l
 
 // One H application with the four pass events recorded (used by the autotuner).
 int apply_events(inqb_ctx* ctx, const void* in, void* out, int M, const double alpha[2], const double beta[2],
-                 void* stream, cudaEvent_t ev[5]) {
+                 void* stream, cudaEvent_t ev[6]) {
   INQB_TRY(reserve(ctx, M));
   if (!ctx->proj_phases_valid) {
     INQB_TRY(update_phases(ctx, stream));
@@ -188,7 +196,7 @@ int apply_events(inqb_ctx* ctx, const void* in, void* out, int M, const double a
   const int cap = ctx->timing_capacity, count = ctx->timing_count;
   std::vector<cudaEvent_t> saved;
   saved.swap(ctx->timing_events);
-  ctx->timing_events.assign(ev, ev + 5);
+  ctx->timing_events.assign(ev, ev + 6);
   ctx->timing_on = true;
   ctx->timing_capacity = 1;
   ctx->timing_count = 0;
@@ -639,6 +647,7 @@ int inqb_ctx_create(const double lattice[9], int nx, int ny, int nz, int precisi
     if (st == INQB_OK && cudaMemset(ctx->d_err.ptr, 0, sizeof(int)) != cudaSuccess)
       st = fail(INQB_ERR_CUDA, "error word init failed");
   }
+
   if (st != INQB_OK) {
     delete ctx;
     return st;
@@ -664,7 +673,7 @@ int inqb_timing_start(inqb_ctx* ctx, int max_applies) {
   INQB_CHECK_CTX(ctx);
   INQB_GUARD(ctx);
   if (max_applies <= 0) return fail(INQB_ERR_INVALID, "max_applies must be positive");
-  while ((int)ctx->timing_events.size() < 5 * max_applies) {
+  while ((int)ctx->timing_events.size() < 6 * max_applies) {
     cudaEvent_t e;
     INQB_CUDA_TRY(cudaEventCreate(&e));
     ctx->timing_events.push_back(e);
@@ -677,7 +686,7 @@ int inqb_timing_start(inqb_ctx* ctx, int max_applies) {
 
 int inqb_set_projection_mode(inqb_ctx* ctx, int mode) {
   INQB_CHECK_CTX(ctx);
-  if (mode != INQB_PROJECTION_KERNEL && mode != INQB_PROJECTION_FUSED)
+  if (mode != INQB_PROJECTION_FUSED && mode != INQB_PROJECTION_KERNEL)
     return fail(INQB_ERR_INVALID, "unknown projection mode");
   ctx->proj_mode = mode;
   return INQB_OK;
@@ -704,10 +713,14 @@ int inqb_timing_passes(inqb_ctx* ctx, double ms[4], int* napplies) {
   for (int k = 0; k < 4; k++) ms[k] = 0.0;
   *napplies = ctx->timing_count;
   for (int i = 0; i < ctx->timing_count; i++) {
-    INQB_CUDA_TRY(cudaEventSynchronize(ctx->timing_events[5 * i + 4]));
+    const cudaEvent_t* e = &ctx->timing_events[6 * i];
+    INQB_CUDA_TRY(cudaEventSynchronize(e[5]));
+    INQB_CUDA_TRY(cudaEventSynchronize(e[1]));
+    // projection: start -> its end (its own stream when concurrent); passes: their events
+    const int from[4] = {0, 2, 3, 4}, to[4] = {1, 3, 4, 5};
     for (int k = 0; k < 4; k++) {
       float t = 0.f;
-      INQB_CUDA_TRY(cudaEventElapsedTime(&t, ctx->timing_events[5 * i + k], ctx->timing_events[5 * i + k + 1]));
+      INQB_CUDA_TRY(cudaEventElapsedTime(&t, e[from[k]], e[to[k]]));
       ms[k] += t;
     }
   }
@@ -716,12 +729,25 @@ int inqb_timing_passes(inqb_ctx* ctx, double ms[4], int* napplies) {
 }
 
 int inqb_timing_stop(inqb_ctx* ctx, double ms_per_pass[3], int* napplies) {
-  if (!ms_per_pass) return fail(INQB_ERR_INVALID, "null output");
-  double ms[4];
-  INQB_TRY(inqb_timing_passes(ctx, ms, napplies));
-  ms_per_pass[0] = ms[0] + ms[1];
-  ms_per_pass[1] = ms[2];
-  ms_per_pass[2] = ms[3];
+  INQB_CHECK_CTX(ctx);
+  INQB_GUARD(ctx);
+  if (!ms_per_pass || !napplies) return fail(INQB_ERR_INVALID, "null output");
+  ctx->timing_on = false;
+  for (int k = 0; k < 3; k++) ms_per_pass[k] = 0.0;
+  *napplies = ctx->timing_count;
+  for (int i = 0; i < ctx->timing_count; i++) {
+    const cudaEvent_t* e = &ctx->timing_events[6 * i];
+    INQB_CUDA_TRY(cudaEventSynchronize(e[5]));
+    // first pass from the start (it includes a projection kernel run before it), then
+    // the second and third passes
+    const int from[3] = {0, 3, 4}, to[3] = {3, 4, 5};
+    for (int k = 0; k < 3; k++) {
+      float t = 0.f;
+      INQB_CUDA_TRY(cudaEventElapsedTime(&t, e[from[k]], e[to[k]]));
+      ms_per_pass[k] += t;
+    }
+  }
+  ctx->timing_count = 0;
   return INQB_OK;
 }
 
@@ -1687,7 +1713,7 @@ int inqb_autotune(inqb_ctx* ctx, int M, void* stream, int schedule[4]) {
   INQB_TRY(out.ensure(bytes));
   cudaStream_t st = (cudaStream_t)stream;
   INQB_CUDA_TRY(cudaMemsetAsync(in.ptr, 0, bytes, st));
-  cudaEvent_t ev[5];
+  cudaEvent_t ev[6];
   for (auto& e : ev) INQB_CUDA_TRY(cudaEventCreate(&e));
   const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
   const bool saved_timing = ctx->timing_on;
@@ -1699,12 +1725,12 @@ int inqb_autotune(inqb_ctx* ctx, int M, void* stream, int schedule[4]) {
     for (int k = 0; k < 3; k++) out_ms[k] = 1e30f;
     for (int rep = 0; rep < 4; rep++) {
       INQB_TRY(apply_events(ctx, in.ptr, out.ptr, M, one, zero, stream, ev));
-      INQB_CUDA_TRY(cudaEventSynchronize(ev[4]));
+      INQB_CUDA_TRY(cudaEventSynchronize(ev[5]));
       if (rep == 0) continue;
-      // the three tile passes (the projection kernel before them is not scheduled)
+      // the three tile passes (the projection kernel is not scheduled)
       for (int k = 0; k < 3; k++) {
         float t = 0.f;
-        INQB_CUDA_TRY(cudaEventElapsedTime(&t, ev[k + 1], ev[k + 2]));
+        INQB_CUDA_TRY(cudaEventElapsedTime(&t, ev[k + 2], ev[k + 3]));
         out_ms[k] = std::min(out_ms[k], t);
       }
     }

@@ -98,6 +98,26 @@ __global__ void k_phases(int nent, const float* __restrict__ relpos, double k0, 
   adj[atom_pos[e]].ph[1] = (T)s;
 }
 
+// ---------------------------------------------------------------- projection finish
+// proj[a][l][m] = dV ekb[a][l] sum over the atom's (plane, half) slots, in the order of
+// its planes and halves: the first tile pass writes one partial per slot, no atomics.
+template <typename T>
+__global__ void k_proj_finish(ProjView<T> pj, int M, int ysplit) {
+  const long n = (long)pj.nproj * pj.L * M;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int m = (int)(i % M), l = (int)((i / M) % pj.L), a = (int)(i / ((long)M * pj.L));
+    double sx = 0.0, sy = 0.0;
+    for (int q = pj.aslot_ptr[a]; q < pj.aslot_ptr[a + 1]; q++)
+      for (int h = 0; h < ysplit; h++) {
+        const double2 v = pj.slots[(((long)pj.aslot[q] * ysplit + h) * LMAX + l) * M + m];
+        sx += v.x;
+        sy += v.y;
+      }
+    const double sc = pj.scale[a * pj.L + l];
+    pj.proj[i] = make_double2(sc * sx, sc * sy);
+  }
+}
+
 // ---------------------------------------------------------------- launch
 static bool aligned16(const void* p, long ld, size_t esz) {
   return ((uintptr_t)p % 16 == 0) && ((ld * (long)esz) % 16 == 0);
@@ -174,7 +194,7 @@ static int launch_h_impl(const LaunchArgs& a) {
   if (a.mode == LaunchArgs::H) {
     // the KB projection: its own deterministic kernel (project.cu) where the tables and
     // the block's alignment allow, else fused into the first tile pass with FP64 atomics
-    const bool sep = pj.nproj > 0 && pj.proj_mode == 0 && pj.pc_table != nullptr &&
+    const bool sep = pj.nproj > 0 && pj.proj_mode == 1 && pj.pc_table != nullptr &&
                      project_supported(sizeof(T) == 8 ? INQB_FP64 : INQB_MIXED, a.in, a.ld_in);
     ProjView<T> pjA = pj;
     if (sep) pjA.nproj = 0;
@@ -192,15 +212,21 @@ static int launch_h_impl(const LaunchArgs& a) {
     if (sep) {
       INQB_TRY(launch_project(sizeof(T) == 8 ? INQB_FP64 : INQB_MIXED, a.in, a.ld_in, a.M, pj.nproj, pj.L,
                               pj.pc_ptr, pj.pc_pt, pj.pc_table, pj.scale, pj.proj, pj.err, st));
-    } else if (pj.nproj > 0) {
+    } else if (pj.nproj > 0 && pj.slots == nullptr) {
       INQB_CUDA_TRY(cudaMemsetAsync(pj.proj, 0, sizeof(double2) * (size_t)pj.nproj * pj.L * a.M, st));
     }
     if (a.events[1]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[1], st));
+    if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
     k_tile_fwd<T, NX, NY, NZ><<<gfwd, thr[0], TG::smem_fwd(acc_cap, rec_cap_a), st>>>(
         (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pjA, acc_cap, rec_cap_a, ysplit, vin);
-    if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
-    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out);
+    // the fused projection's per-(plane, half) partial sums, added per atom in a fixed order
+    if (!sep && pj.nproj > 0 && pj.slots != nullptr) {
+      const long n = (long)pj.nproj * pj.L * a.M;
+      k_proj_finish<<<(unsigned)std::min<long>((n + 255) / 256, 148L * 8), 256, 0, st>>>(pj, a.M, ysplit);
+    }
     if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
+    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out);
+    if (a.events[4]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[4], st));
     EpiParams<T> ep;
     ep.V = (const T*)a.V;
     ep.vshift = a.fourier_mask ? (T)(0.5 * kA2) : (T)0;
@@ -218,7 +244,7 @@ static int launch_h_impl(const LaunchArgs& a) {
     k_tile_inv<T, NX, NY, NZ, 1><<<ginv, thr[2], TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
         tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv, seg_cap,
         vin && vout);
-    if (a.events[4]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[4], st));
+    if (a.events[5]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[5], st));
   } else if (a.mode == LaunchArgs::POISSON) {
     // solvers::poisson on M complex fields: forward z and inner y, then the outer y
     // and x transforms with the 4 pi / (N |G|^2) factor, then the inverse (no 1/N:

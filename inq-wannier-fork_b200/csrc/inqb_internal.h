@@ -127,6 +127,9 @@ struct ProjTables {
   std::vector<float> pc_relpos;
   DevBuf d_pc_ptr, d_pc_pt, d_pc_beta, d_pc_relpos;
   DevBuf d_pc_table;                // coefficient table beta exp(+i (k+A).r) for the current k + A
+  // each atom's (plane, atom) slots of the fused projection, in plane order
+  std::vector<int> aslot_ptr, aslot;
+  DevBuf d_aslot_ptr, d_aslot;
   DevBuf d_adj_rec, d_atom_pos;     // [nent] AdjRec<T> in atom-major order
   // device copies
   DevBuf d_seg_ptr, d_seg_atom, d_seg_ent, d_seg_local, d_plane_ptr, d_plane_atom, d_ent_off, d_ent_atom;
@@ -168,7 +171,12 @@ struct ProjView {
   const int* pc_pt;
   const void* pc_table;
   int* err;               // device error word (a device-side wait gave up)
-  int proj_mode;          // 0: projection kernel, 1: projection fused into the first tile pass
+  int proj_mode;          // 0: fused into the first tile pass; 1: projection kernel
+  // the fused projection's partial sums: slot (plane_ptr[ix] + local atom) * ysplit + half
+  // holds [LMAX][M]; aslot_ptr / aslot list each atom's slots in plane order
+  double2* slots;         // null: flush with atomics instead
+  const int* aslot_ptr;
+  const int* aslot;
 };
 
 constexpr int kNlChunk = 64;  // sphere entries per chunk of the adjoint's nonlocal moments
@@ -214,7 +222,8 @@ struct inqb_ctx {
   inqb::DevBuf d_pot;           // density -> potential: V_H field [N] (complex), previous
                                 // density [N], partial sums, sums
   inqb::DevBuf d_err;           // one int: set by a kernel whose bounded device-side wait gave up
-  int proj_mode = 0;            // INQB_PROJECTION_KERNEL (0) or INQB_PROJECTION_FUSED (1)
+  int proj_mode = 0;            // INQB_PROJECTION_FUSED (0) or INQB_PROJECTION_KERNEL (1)
+  inqb::DevBuf d_slots;         // the fused projection's per-(plane, half) partial sums
   inqb::DevBuf d_mix;           // Crank-Nicolson with self-consistency: Broyden ring df, dv [4][N],
                                 // f_old, vin_old, the new density [N], partial sums, dot products
   size_t elem_bytes() const { return precision == INQB_FP64 ? 16 : 8; }

@@ -23,9 +23,9 @@ struct LaunchArgs {
   double beta[2] = {0.0, 0.0};
   void* stream = nullptr;
   int fourier_mask = 0;             // zero the kinetic term outside the Fourier sphere
-  // optional cudaEvent_t: before the projection kernel, before the first tile pass,
-  // and after each of the three passes
-  void* events[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  // optional cudaEvent_t: start, end of the projection kernel, start of the first tile
+  // pass, and after each of the three passes
+  void* events[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   // launch schedule (0 = the compiled default): CTAs sharing one x-plane in the first
   // pass (a divisor of the y split's Y1), and threads per CTA of the three passes
   int ysplit = 0;

@@ -158,9 +158,9 @@ constexpr int kRows = 2 * kProjOrbTC;            // 128
 constexpr int kN = 16;
 constexpr int kABytes = kProjChunk * kRows * 4;  // 16 KB per chunk
 constexpr int kBBytes = kProjChunk * kN * 4;     // 2 KB per chunk
-constexpr int kStages = 4;                       // gathered chunks in flight
+constexpr int kStages = 6;                       // gathered chunks in flight
 constexpr int kStageBytes = kABytes + kBBytes;   // staging rows + B
-constexpr int kTCThreads = 128;
+constexpr int kTCThreads = 512;  // 16 warps: four per scheduler hide the split pass's latencies
 // stages | A hi, A lo of two chunks (double-buffered against the MMAs) | barriers
 constexpr size_t kSplitOff = (size_t)kStages * kStageBytes;
 constexpr size_t kTCSmem = kSplitOff + 4 * (size_t)kABytes + 64;
@@ -208,31 +208,46 @@ __global__ void __launch_bounds__(kTCThreads, 1)
   auto split_hi = [&](int b) { return smem + kSplitOff + (size_t)(2 * b) * kABytes; };
   auto split_lo = [&](int b) { return smem + kSplitOff + (size_t)(2 * b + 1) * kABytes; };
 
-  // gather of chunk c into stage s: 32 rows of 32 pieces of 16 bytes, then the B piece
-  auto load_chunk = [&](int c, int s) {
-    if (c < nch) {
-      const int* pts = pc_pt + (size_t)(c0 + c) * kProjChunk;
-      unsigned char* R = stage_rows(s);
+  // A thread gathers the 16-byte pieces (point k = W i + warp, piece q = lane), i <
+  // kPer, of a chunk, W = warps per CTA.  Their grid points are read one chunk ahead of
+  // the gather, so the index load is off the critical path.
+  constexpr int kWarps = kTCThreads / 32;
+  constexpr int kPer = (kProjChunk * 32) / kTCThreads;  // pieces per thread
+  auto fetch_points = [&](int c, int (&pt)[kPer]) {
 #pragma unroll
-      for (int i = 0; i < (kProjChunk * 32) / kTCThreads; i++) {
-        const int idx = i * kTCThreads + tid;
-        const int q = idx & 31, k = idx >> 5;
-        const int pt = pts[k];
-        const int nval = M - m0 - 2 * q;  // orbitals of this piece inside the block
-        const int bytes = (pt < 0 || nval <= 0) ? 0 : (nval >= 2 ? 16 : 8);
-        const cplx<float>* src = bytes ? in + (long)pt * ld + m0 + 2 * q : in;
+    for (int i = 0; i < kPer; i++)
+      pt[i] = (c < nch) ? pc_pt[(size_t)(c0 + c) * kProjChunk + kWarps * i + warp] : -1;
+  };
+  // gather of chunk c into stage s: 32 rows of 32 pieces of 16 bytes, then the B piece
+  auto load_chunk = [&](int c, int s, const int (&pt)[kPer]) {
+    if (c < nch) {
+      unsigned char* R = stage_rows(s);
+      const int q = lane;
+      const int nval = M - m0 - 2 * q;  // orbitals of this piece inside the block
+#pragma unroll
+      for (int i = 0; i < kPer; i++) {
+        const int k = kWarps * i + warp;
+        const int bytes = (pt[i] < 0 || nval <= 0) ? 0 : (nval >= 2 ? 16 : 8);
+        const cplx<float>* src = bytes ? in + (long)pt[i] * ld + m0 + 2 * q : in;
         cp_async16_zfill(R + k * 512 + q * 16, src, bytes);
       }
-      cp_async16_zfill(stage_b(s) + tid * 16, pc_b + (size_t)(c0 + c) * (kBBytes / 4) + tid * 4, 16);
+      if (tid < kBBytes / 16)
+        cp_async16_zfill(stage_b(s) + tid * 16, pc_b + (size_t)(c0 + c) * (kBBytes / 4) + tid * 4, 16);
     }
     cp_async_commit();
   };
 
-  for (int c = 0; c < kStages - 1; c++) load_chunk(c, c);
+  int pts[kPer];
+  for (int c = 0; c < kStages - 1; c++) {
+    fetch_points(c, pts);
+    load_chunk(c, c, pts);
+  }
+  fetch_points(kStages - 1, pts);
 
   double accR[4] = {0, 0, 0, 0}, accI[4] = {0, 0, 0, 0};
   // read the accumulator of chunk c into the FP64 sums (every warp: its 32 rows)
   auto drain = [&](int c) -> bool {
+    if (warp >= 4) return true;  // warps 0-3 read the four lane quadrants
     const uint64_t deadline = globaltimer_ns() + kWaitLimitNs;
     if (!mbar_wait_warp(&bar[c & 1], (uint32_t)((c >> 1) & 1), deadline)) {
       *abort_flag = 1;
@@ -261,9 +276,10 @@ __global__ void __launch_bounds__(kTCThreads, 1)
       const float* R = reinterpret_cast<const float*>(stage_rows(s));
       unsigned char* H = split_hi(b);
       unsigned char* Lo = split_lo(b);
-      const int row = tid;
 #pragma unroll
-      for (int kc = 0; kc < kProjChunk / 4; kc++) {
+      for (int it = 0; it < (kRows * kProjChunk / 4) / kTCThreads; it++) {
+        const int item = it * kTCThreads + tid;
+        const int row = item % kRows, kc = item / kRows;  // four points kc of one operand row
         float x[4], h[4], t[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
@@ -301,7 +317,8 @@ __global__ void __launch_bounds__(kTCThreads, 1)
     }
     // stage (c - 1) % kStages is free: its rows were split in the previous iteration
     // and its B piece was read by MMAs that completed before the drain above
-    load_chunk(c + kStages - 1, (c + kStages - 1) % kStages);
+    load_chunk(c + kStages - 1, (c + kStages - 1) % kStages, pts);
+    fetch_points(c + kStages, pts);
   }
   if (ok && nch > 0) ok = drain(nch - 1);
   if (!ok) {
@@ -323,7 +340,7 @@ __global__ void __launch_bounds__(kTCThreads, 1)
     pI[l] = __shfl_xor_sync(0xffffffffu, accI[l], 1);
   }
   const int m = m0 + (warp * 32 + lane) / 2;
-  if ((lane & 1) == 0 && m < M) {
+  if (warp < 4 && (lane & 1) == 0 && m < M) {
     for (int l = 0; l < L && l < 4; l++) {
       const double sc = scale[a * L + l];
       // Re = sum Re B x - Im B y; Im = sum Re B y + Im B x
@@ -347,25 +364,46 @@ __global__ void __launch_bounds__(kF64Threads)
   const bool valid = m < M;
   const int e0 = pc_ptr[a] * kProjChunk, e1 = pc_ptr[a + 1] * kProjChunk;
   double pr[4] = {0, 0, 0, 0}, pi[4] = {0, 0, 0, 0};
-  constexpr int U = 4;  // entries in flight per warp
-  for (int eb = e0 + warp * U; eb < e1; eb += (kF64Threads / 32) * U) {
-    int pt[U];
-    cplx<double> x[U];
+  // Software-pipelined over steps of U entries per warp: the orbital values of step
+  // i + 1 are in flight while step i is summed, and the grid points of step i + 2
+  // are read meanwhile.
+  constexpr int U = 8;
+  constexpr int STEP = (kF64Threads / 32) * U;
+  auto points = [&](int eb, int (&pt)[U]) {
+#pragma unroll
+    for (int u = 0; u < U; u++) pt[u] = (eb + u < e1) ? pc_pt[eb + u] : -1;
+  };
+  auto values = [&](const int (&pt)[U], cplx<double> (&x)[U]) {
+#pragma unroll
+    for (int u = 0; u < U; u++) x[u] = (pt[u] >= 0 && valid) ? in[(long)pt[u] * ld + m] : mk<double>(0, 0);
+  };
+  int pt_cur[U], pt_nxt[U];
+  cplx<double> x_cur[U];
+  const int eb0 = e0 + warp * U;
+  points(eb0, pt_cur);
+  values(pt_cur, x_cur);
+  points(eb0 + STEP, pt_nxt);
+  for (int eb = eb0; eb < e1; eb += STEP) {
+    cplx<double> x_nxt[U];
+    values(pt_nxt, x_nxt);
+    int pt_after[U];
+    points(eb + 2 * STEP, pt_after);
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      pt[u] = (eb + u < e1) ? pc_pt[eb + u] : -1;
-      x[u] = (pt[u] >= 0 && valid) ? in[(long)pt[u] * ld + m] : mk<double>(0, 0);
-    }
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      if (pt[u] < 0) continue;
+      if (pt_cur[u] < 0) continue;
       const double* b = pc_b + (size_t)(eb + u) * 8;
 #pragma unroll
       for (int l = 0; l < 4; l++) {
         const double br = b[l], bi = b[4 + l];
-        pr[l] = fma(br, x[u].x, fma(-bi, x[u].y, pr[l]));
-        pi[l] = fma(br, x[u].y, fma(bi, x[u].x, pi[l]));
+        pr[l] = fma(br, x_cur[u].x, fma(-bi, x_cur[u].y, pr[l]));
+        pi[l] = fma(br, x_cur[u].y, fma(bi, x_cur[u].x, pi[l]));
       }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      x_cur[u] = x_nxt[u];
+      pt_cur[u] = pt_nxt[u];
+      pt_nxt[u] = pt_after[u];
     }
   }
 #pragma unroll

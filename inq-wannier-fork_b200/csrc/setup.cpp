@@ -361,6 +361,18 @@ int build_proj_tables(const inqb_ctx& ctx, int nproj, int L, int smax, const int
       for (int l = 0; l < L && l < 4; l++) t.pc_beta[4 * q + l] = t.ent_beta[(size_t)ee * L + l];
       for (int d = 0; d < 3; d++) t.pc_relpos[3 * q + d] = t.ent_relpos[3 * (size_t)ee + d];
     }
+  // each atom's slots of the fused projection's partial sums, in plane order
+  {
+    std::vector<std::vector<int>> lists(nproj);
+    for (int ix = 0; ix < nx; ix++)
+      for (int q = t.plane_ptr[ix]; q < t.plane_ptr[ix + 1]; q++) lists[t.plane_atom[q]].push_back(q);
+    t.aslot_ptr.assign(nproj + 1, 0);
+    t.aslot.clear();
+    for (int a = 0; a < nproj; a++) {
+      t.aslot.insert(t.aslot.end(), lists[a].begin(), lists[a].end());
+      t.aslot_ptr[a + 1] = (int)t.aslot.size();
+    }
+  }
   t.scale.resize((size_t)nproj * L);
   for (int a = 0; a < nproj; a++)
     for (int l = 0; l < L; l++) t.scale[(size_t)a * L + l] = ctx.dV * coeff[(size_t)a * L + l];
@@ -446,6 +458,8 @@ int upload_proj_tables(const inqb_ctx& ctx, ProjTables& t) {
     INQB_TRY(upload(t.d_adj_rec, adj_records<float>(t)));
   }
   INQB_TRY(upload(t.d_pt_ptr, t.pt_ptr));
+  INQB_TRY(upload(t.d_aslot_ptr, t.aslot_ptr));
+  INQB_TRY(upload(t.d_aslot, t.aslot));
   INQB_TRY(upload(t.d_pc_ptr, t.pc_ptr));
   INQB_TRY(upload(t.d_pc_pt, t.pc_pt));
   INQB_TRY(upload(t.d_pc_beta, t.pc_beta));

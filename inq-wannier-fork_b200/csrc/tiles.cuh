@@ -140,8 +140,17 @@ __global__ void __launch_bounds__(256)
   const bool proj_on = pj.nproj > 0;
   for (int i = threadIdx.x; i < NY; i += blockDim.x) twy[i] = tw_y[i];
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = tw_z[i];
-  if (proj_on)
+  if (proj_on) {
     for (int i = threadIdx.x; i < acc_cap * LMAX * G; i += blockDim.x) acc[i] = make_double2(0.0, 0.0);
+    // slots of the plane's atoms beyond the shared-memory accumulators start at zero
+    if (pj.slots) {
+      const int a0 = pj.plane_ptr[ix], na = pj.plane_ptr[ix + 1] - a0;
+      for (int i = threadIdx.x; i < max(0, na - acc_cap) * LMAX * G; i += blockDim.x) {
+        const int j = i % G, l = (i / G) % LMAX, sl = acc_cap + i / (G * LMAX);
+        if (j < gcount) pj.slots[(((long)(a0 + sl) * YS + yh) * LMAX + l) * M + m0 + j] = make_double2(0.0, 0.0);
+      }
+    }
+  }
 
   for (int y1 = yh * YPER; y1 < (yh + 1) * YPER; ++y1) {
     // -- rows y1 + Y1 r of plane ix, G orbitals per point
@@ -203,6 +212,17 @@ __global__ void __launch_bounds__(256)
               d.x += (double)a[l].x;
               d.y += (double)a[l].y;
             }
+          } else if (pj.slots) {
+            // beyond the shared-memory accumulators: this CTA's own slot in global
+            // memory (zeroed at the start), the same ownership
+            double2* d = pj.slots + (((long)(pj.plane_ptr[ix] + sl) * YS + yh) * LMAX) * M + m0 + j;
+#pragma unroll
+            for (int l = 0; l < LMAX; ++l) {
+              double2 v = d[(long)l * M];
+              v.x += (double)a[l].x;
+              v.y += (double)a[l].y;
+              d[(long)l * M] = v;
+            }
           } else {
             const int at = pj.seg_atom[s];
 #pragma unroll
@@ -253,19 +273,25 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
   }
 
-  // -- flush the plane accumulators: proj[a][l][m] += dV ekb * sum
+  // -- flush the plane accumulators: into this CTA's (plane, half) slots, which the
+  // finish kernel adds per atom in a fixed order; without slots, proj[a][l][m] +=
+  // dV ekb * sum with atomics
   if (proj_on) {
     const int a0 = pj.plane_ptr[ix];
     const int na = min(pj.plane_ptr[ix + 1] - a0, acc_cap);
     for (int i = threadIdx.x; i < na * LMAX * G; i += blockDim.x) {
       const int j = i % G, l = (i / G) % LMAX, sl = i / (G * LMAX);
-      if (l >= pj.L || j >= gcount) continue;
-      const int at = pj.plane_atom[a0 + sl];
-      const double sc = pj.scale[at * pj.L + l];
+      if (j >= gcount) continue;
       const double2 v = acc[i];
-      double2* dst = &pj.proj[((long)at * pj.L + l) * M + m0 + j];
-      atomicAdd(&dst->x, sc * v.x);
-      atomicAdd(&dst->y, sc * v.y);
+      if (pj.slots) {
+        pj.slots[(((long)(a0 + sl) * YS + yh) * LMAX + l) * M + m0 + j] = v;
+      } else if (l < pj.L) {
+        const int at = pj.plane_atom[a0 + sl];
+        const double sc = pj.scale[at * pj.L + l];
+        double2* dst = &pj.proj[((long)at * pj.L + l) * M + m0 + j];
+        atomicAdd(&dst->x, sc * v.x);
+        atomicAdd(&dst->y, sc * v.y);
+      }
     }
   }
 }

@@ -572,12 +572,14 @@ class KSHamiltonian:
         call("inqb_timing_passes", self._h, dptr(ms), ctypes.byref(n))
         return ms, n.value
 
-    PROJECTION_KERNEL = 0
-    PROJECTION_FUSED = 1
+    PROJECTION_FUSED = 0
+    PROJECTION_KERNEL = 1
 
     def set_projection_mode(self, mode):
-        """INQB_PROJECTION_KERNEL (0, or "kernel") or INQB_PROJECTION_FUSED (1, or "fused")."""
-        m = {"kernel": 0, "fused": 1}.get(mode, mode)
+        """INQB_PROJECTION_FUSED (0, "fused": inside the first tile pass, the default)
+        or INQB_PROJECTION_KERNEL (1, "kernel": its own gather-and-contract kernel, on
+        the tensor cores in the mixed precision)."""
+        m = {"fused": 0, "kernel": 1}.get(mode, mode)
         call("inqb_set_projection_mode", self._h, int(m))
 
     def device_status(self):

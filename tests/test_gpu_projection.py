@@ -1,14 +1,14 @@
-"""The KB projection kernel of H|psi> (csrc/project.cu; projector_all::project,
+"""The two forms of the KB projection of H|psi> (projector_all::project,
 src/hamiltonian/projector_all.hpp:98-216) against the oracle, through the C ABI:
 
-  * the default projection kernel (mixed: tcgen05 TF32 tensor cores with the
-    split-precision correction; FP64: CUDA cores) and the projection fused into the
-    first tile pass give H|psi> within the stated bounds of the FP64 oracle (FP64
-    1e-10 max-relative, mixed 1e-6 in norm);
+  * the projection fused into the first tile pass (the default) and the projection
+    kernel of csrc/project.cu (mixed: tcgen05 TF32 tensor cores with the
+    split-precision correction; FP64: CUDA cores) give H|psi> within the stated
+    bounds of the FP64 oracle (FP64 1e-10 max-relative, mixed 1e-6 in norm);
   * orbital counts that fill no block (M = 70: a 64-orbital block and a ragged one;
     odd M: a half 16-byte piece), a strided block, a nonzero k + A (the coefficient
     table is rebuilt with the phases);
-  * the projection kernel is deterministic: two applies agree bit for bit;
+  * both forms are deterministic: two applies agree bit for bit;
   * an odd leading dimension (complex64 rows not 16-byte aligned) takes the fused form
     and is still right;
   * no device-side wait gave up (inqb_device_status).
@@ -51,8 +51,10 @@ def test_projection_modes_match_oracle(pb, oracle_mod, sys70, precision, mode):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_projection_kernel_is_deterministic(pb, sys70, precision):
+@pytest.mark.parametrize("mode", ["kernel", "fused"])
+def test_projection_is_deterministic(pb, sys70, precision, mode):
     h = make_product(pb, sys70, precision)
+    h.set_projection_mode(mode)
     x = torch.as_tensor(sys70["psi"]).to("cuda", DT[precision])
     a = h(x)
     b = h(x)
@@ -61,14 +63,16 @@ def test_projection_kernel_is_deterministic(pb, sys70, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("mode", ["kernel", "fused"])
 @pytest.mark.parametrize("M,lo,hi", [(7, 2, 9), (33, 0, 33), (4, 0, 3)])
-def test_projection_ragged_and_strided(pb, oracle_mod, sys70, precision, M, lo, hi):
+def test_projection_ragged_and_strided(pb, oracle_mod, sys70, precision, mode, M, lo, hi):
     """Blocks [lo, hi) of a buffer of M + 3 orbitals: odd orbital counts (a half-filled
     16-byte piece), an offset block, and an odd leading dimension (7), whose complex64
     rows are not 16-byte aligned, so the mixed context takes the fused form."""
     s = sys70
     o = make_oracle(oracle_mod, s)
     h = make_product(pb, s, precision)
+    h.set_projection_mode(mode)
     full = torch.as_tensor(s["psi"][:, :M + 3]).to("cuda", DT[precision])
     view = full[:, lo:hi]
     out = h(view).cpu().numpy()
@@ -82,6 +86,7 @@ def test_tensor_core_projection_close_to_fused(pb, sys70):
     give H|psi> within the FP32 rounding of each other."""
     h = make_product(pb, sys70, "mixed")
     x = torch.as_tensor(sys70["psi"]).to("cuda", torch.complex64)
+    h.set_projection_mode("kernel")
     a = h(x).cpu().numpy()
     h.set_projection_mode("fused")
     b = h(x).cpu().numpy()
