@@ -40,9 +40,14 @@ def test_status_strings(pb):
 
 
 def test_grid_support_table(pb):
-    for n in (16, 20, 24, 32, 40, 48, 64):
-        assert pb.grid_supported((n, n, n), "fp64") and pb.grid_supported((n, n, n), "mixed")
+    """Every length of the FFT size table as a cubic grid, plus the compiled
+    orthorhombic and tetragonal grids; lengths outside the table are not compiled."""
+    for n in (12, 16, 18, 20, 24, 30, 32, 36, 40, 48, 60, 64, 72, 80, 96, 128, 144):
+        assert pb.grid_supported((n, n, n), "fp64") and pb.grid_supported((n, n, n), "mixed"), n
+    for nr in ((18, 24, 20), (36, 48, 60), (24, 24, 48), (32, 32, 48), (64, 64, 96)):
+        assert pb.grid_supported(nr, "fp64") and pb.grid_supported(nr, "mixed"), nr
     assert not pb.grid_supported((17, 17, 17), "fp64")
+    assert not pb.grid_supported((36, 60, 48), "mixed")
 
 
 def test_context_needs_a_gpu_or_reports_an_error(pb):
