@@ -81,39 +81,6 @@ struct EpiParams {
 
 namespace inqb {
 
-// ---------------------------------------------------------------- projection finish
-// proj[a][l][m] = dV ekb[a][l] sum over the atom's (plane, half) slots, in the order of
-// its planes and halves: the first tile pass writes one partial per slot, no atomics.
-template <typename T>
-__global__ void k_proj_finish(ProjView<T> pj, int M, int ysplit) {
-  const long n = (long)pj.nproj * pj.L * M;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    const int m = (int)(i % M), l = (int)((i / M) % pj.L), a = (int)(i / ((long)M * pj.L));
-    // the atom's partials in order (plane, half), eight loads in flight, added in order
-    const int q0 = pj.aslot_ptr[a] * ysplit, q1 = pj.aslot_ptr[a + 1] * ysplit;
-    double sx = 0.0, sy = 0.0;
-    for (int qb = q0; qb < q1; qb += 8) {
-      double2 v[8];
-#pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const int q = qb + u;
-        v[u] = make_double2(0.0, 0.0);
-        if (q < q1) {
-          const long slot = (long)pj.aslot[q / ysplit] * ysplit + q % ysplit;
-          v[u] = pj.slots[(slot * LMAX + l) * M + m];
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 8; u++) {
-        sx += v[u].x;
-        sy += v[u].y;
-      }
-    }
-    const double sc = pj.scale[a * pj.L + l];
-    pj.proj[i] = make_double2(sc * sx, sc * sy);
-  }
-}
-
 // ---------------------------------------------------------------- launch
 inline bool aligned16(const void* p, long ld, size_t esz) {
   return ((uintptr_t)p % 16 == 0) && ((ld * (long)esz) % 16 == 0);
@@ -215,13 +182,13 @@ int launch_h_impl(const LaunchArgs& a) {
     if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
     k_tile_fwd<T, NX, NY, NZ><<<gfwd, thr[0], TG::smem_fwd(acc_cap, rec_cap_a), st>>>(
         (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pjA, acc_cap, rec_cap_a, ysplit, vin);
-    // the fused projection's per-(plane, half) partial sums, added per atom in a fixed order
-    if (!sep && pj.nproj > 0 && pj.slots != nullptr) {
-      const long n = (long)pj.nproj * pj.L * a.M;
-      k_proj_finish<<<(unsigned)std::min<long>((n + 255) / 256, 148L * 8), 256, 0, st>>>(pj, a.M, ysplit);
-    }
     if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
-    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out);
+    // the second pass also adds the fused projection's partial sums per atom, in a
+    // fixed order (its first CTAs; the third pass reads the result)
+    ProjView<T> fin = pj;
+    if (sep || pj.nproj == 0) fin.slots = nullptr;
+    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out, fin, a.M,
+                                                             ysplit);
     if (a.events[4]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[4], st));
     EpiParams<T> ep;
     ep.V = (const T*)a.V;
@@ -255,7 +222,9 @@ int launch_h_impl(const LaunchArgs& a) {
     kq.mask = 0;
     kq.shift = (T)0;
     kq.pois = (T)(2.0 * M_PI / ((double)NX * NY * NZ));
-    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kq, nullptr);
+    ProjView<T> nofin = pj;
+    nofin.slots = nullptr;
+    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kq, nullptr, nofin, 0, 1);
     EpiParams<T> ep{};
     ep.alpha = mk<T>((T)1, (T)0);
     k_tile_inv<T, NX, NY, NZ, 0><<<ginv, thr[2], TG::smem_inv(0, 0), st>>>(

@@ -296,13 +296,52 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---------------------------------------------------------------- projection finish
+// proj[a][l][m] = dV ekb[a][l] sum over the atom's (plane, half) slots, in the order of
+// its planes and halves: pass A wrote one partial per slot, no atomics.  Item i =
+// (a * L + l) * M + m; eight loads in flight, added in order.
+template <typename T>
+__device__ __forceinline__ void proj_finish_item(const ProjView<T>& pj, int M, int ysplit, long i) {
+  const int m = (int)(i % M), l = (int)((i / M) % pj.L), a = (int)(i / ((long)M * pj.L));
+  const int q0 = pj.aslot_ptr[a] * ysplit, q1 = pj.aslot_ptr[a + 1] * ysplit;
+  double sx = 0.0, sy = 0.0;
+  for (int qb = q0; qb < q1; qb += 8) {
+    double2 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int q = qb + u;
+      v[u] = make_double2(0.0, 0.0);
+      if (q < q1) {
+        const long slot = (long)pj.aslot[q / ysplit] * ysplit + q % ysplit;
+        v[u] = pj.slots[(slot * LMAX + l) * M + m];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      sx += v[u].x;
+      sy += v[u].y;
+    }
+  }
+  const double sc = pj.scale[a * pj.L + l];
+  pj.proj[i] = make_double2(sc * sx, sc * sy);
+}
+
 // ---------------------------------------------------------------- pass B
 // One contiguous block tmp[g][ka][kz] = [ix][y1][G]; in shared memory the x
-// index goes to padded slots of stride XS and (y1, j) stays contiguous.
+// index goes to padded slots of stride XS and (y1, j) stays contiguous.  With
+// fin.slots set, the first CTAs also finish the fused projection (pass C reads it):
+// thread t of CTA b handles item b * blockDim + t, so the few CTAs that carry the
+// finish run beside thousands that do not.
 template <typename T, int NX, int NY, int NZ>
 __global__ void __launch_bounds__(256)
     k_tile_x(cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ tw_x, KinParams<T> kp,
-             cplx<T>* __restrict__ fout) {
+             cplx<T>* __restrict__ fout, ProjView<T> fin, int fin_M, int fin_ysplit) {
+  if (fin.slots) {
+    const long n = (long)fin.nproj * fin.L * fin_M;
+    const long stride = (long)gridDim.x * gridDim.y * blockDim.x;
+    for (long i = ((long)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+      proj_finish_item(fin, fin_M, fin_ysplit, i);
+  }
   using TG = TileGeom<T, NX, NY, NZ>;
   using AX = typename TG::AX;
   constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, XS = TG::XS;
