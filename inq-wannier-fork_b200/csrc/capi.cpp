@@ -460,6 +460,7 @@ int jade_dev(int M, double2* a, double2* u, double2* adiag, int maxsweep, double
     double change = 0.0;
     INQB_CUDA_TRY(cudaMemcpyAsync(&change, w.change, sizeof(double), cudaMemcpyDeviceToHost, st));
     INQB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!std::isfinite(change)) return fail(INQB_ERR_NONFINITE, "TD-MLWF matrices are not finite");
     if (std::fabs(change) < tol || nsweep >= maxsweep) break;
   }
   INQB_TRY(launch_jade_adiag(a, u, M, adiag, stream));

@@ -160,24 +160,37 @@ __global__ void __launch_bounds__(256, GramCfg<T>::MINB)
       }
 }
 
+// Z[e] = sum over the slabs of partial[slab][e] in FP64, e = (d, m, n): the slabs' sums
+// in slab order, reads coalesced along e, eight slabs in flight per thread.
+template <typename P>
+__global__ void k_mlwf_slab_sum(const P* __restrict__ partial, int nslab, long n, double2* __restrict__ Z) {
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    double zx = 0.0, zy = 0.0;
+    for (int s0 = 0; s0 < nslab; s0 += 8) {
+      P v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = (s0 + u < nslab) ? partial[(size_t)(s0 + u) * n + e] : P{0, 0};
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        zx += (double)v[u].x;
+        zy += (double)v[u].y;
+      }
+    }
+    Z[e] = make_double2(zx, zy);
+  }
+}
+
 // a[2d][m][n] = (Z + Z^H)/2, a[2d+1][m][n] = (Z - Z^H)/(2i), Z the slab sum (FP64) divided
 // by |psi_m| |psi_n| (sums[3 m + 2] = sum_p |psi_m|^2 from the band sums)
-template <typename P>
-__global__ void k_mlwf_finish(const P* __restrict__ partial, int nslab, int M, const double* __restrict__ sums,
+__global__ void k_mlwf_finish(const double2* __restrict__ Z, int M, const double* __restrict__ sums,
                               double2* __restrict__ a) {
   const size_t MM = (size_t)M * M;
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < 3 * (long)MM; e += (long)gridDim.x * blockDim.x) {
     const int d = (int)(e / MM);
     const int m = (int)((e % MM) / M), n = (int)(e % M);
-    double zx = 0, zy = 0, tx = 0, ty = 0;
-    for (int s = 0; s < nslab; ++s) {
-      const P x = partial[((size_t)s * 3 + d) * MM + (size_t)m * M + n];
-      const P y = partial[((size_t)s * 3 + d) * MM + (size_t)n * M + m];
-      zx += (double)x.x;
-      zy += (double)x.y;
-      tx += (double)y.x;
-      ty += (double)y.y;
-    }
+    const double2 x = Z[(size_t)d * MM + (size_t)m * M + n];
+    const double2 y = Z[(size_t)d * MM + (size_t)n * M + m];
+    const double zx = x.x, zy = x.y, tx = y.x, ty = y.y;
     const double sc = 1.0 / sqrt(sums[3 * m + 2] * sums[3 * n + 2]);
     // conj(Z[n][m]) = (tx, -ty)
     a[(2 * d) * MM + (size_t)m * M + n] = make_double2(0.5 * sc * (zx + tx), 0.5 * sc * (zy - ty));
@@ -203,7 +216,7 @@ __device__ void jacobi3_top(double S[3][3], double out[3]) {
 #pragma unroll
       for (int p = 0; p < q; p++) off += S[p][q] * S[p][q];
     const double thresh = sqrt(off) / 12.0;
-    if (thresh == 0.0) break;
+    if (!(thresh > 0.0)) break;  // converged, or a non-finite matrix (reported by the sweep's change)
 #pragma unroll
     for (int p = 0; p < 3; p++)
 #pragma unroll
@@ -499,10 +512,12 @@ long gram_slabs(long N, int M) {
 }
 }  // namespace
 
+// the slabs of the larger layout, then Z [3][M][M] (FP64) at a 256-byte boundary
 size_t mlwf_partial_bytes(long N, int M) {
   const size_t MM = (size_t)M * M;
-  return std::max((size_t)gram_slabs<double>(N, M) * 3 * MM * sizeof(double2),
-                  (size_t)gram_slabs<float>(N, M) * 3 * MM * sizeof(float2));
+  const size_t slabs = std::max((size_t)gram_slabs<double>(N, M) * 3 * MM * sizeof(double2),
+                                (size_t)gram_slabs<float>(N, M) * 3 * MM * sizeof(float2));
+  return (slabs + 255) / 256 * 256 + 3 * MM * sizeof(double2);
 }
 
 template <typename T>
@@ -517,8 +532,14 @@ static int gram_impl(const void* psi, long ld, int M, long N, const GramGeom& g,
   k_mlwf_gram<T><<<grid, 256, 0, st>>>((const cplx<T>*)psi, ld, M, N, g, per, (P*)partial);
   INQB_CUDA_TRY(cudaGetLastError());
   const long work = 3L * M * M;
-  k_mlwf_finish<P><<<(unsigned)std::min<long>((work + 255) / 256, 148L * 8), 256, 0, st>>>((const P*)partial,
-                                                                                          (int)nslab, M, sums, a);
+  const size_t slab_bytes =
+      std::max((size_t)gram_slabs<double>(N, M) * 3 * (size_t)M * M * sizeof(double2),
+               (size_t)gram_slabs<float>(N, M) * 3 * (size_t)M * M * sizeof(float2));
+  double2* Z = reinterpret_cast<double2*>(static_cast<char*>(partial) + (slab_bytes + 255) / 256 * 256);
+  k_mlwf_slab_sum<P><<<(unsigned)std::min<long>((work + 255) / 256, 148L * 32), 256, 0, st>>>((const P*)partial,
+                                                                                             (int)nslab, work, Z);
+  INQB_CUDA_TRY(cudaGetLastError());
+  k_mlwf_finish<<<(unsigned)std::min<long>((work + 255) / 256, 148L * 8), 256, 0, st>>>(Z, M, sums, a);
   INQB_CUDA_TRY(cudaGetLastError());
   return INQB_OK;
 }

@@ -97,3 +97,17 @@ def test_mlwf_output_file_format(pb, oracle_mod, tmp_path):
     assert lines[0] == "Time step: 7" and lines[1] == "MLWFs:"
     assert lines[2] == (f"  WF 1: {centres[0, 0]:g}     {centres[0, 1]:g}     {centres[0, 2]:g}     "
                         f"Spread: {spreads[0]:g}")
+
+
+def test_jade_rejects_non_finite_matrices(pb):
+    """A non-finite entry (an orbital block that blew up) ends JADE after its first sweep
+    with INQB_ERR_NONFINITE instead of iterating on NaN."""
+    h = pb.KSHamiltonian(np.eye(3) * 10.0, (16, 16, 16), "fp64")
+    rng = np.random.default_rng(2)
+    M = 6
+    x = rng.standard_normal((6, M, M)) + 1j * rng.standard_normal((6, M, M))
+    a = torch.as_tensor(x + np.conj(np.transpose(x, (0, 2, 1)))).to("cuda").contiguous()
+    a[2, 1, 3] = float("nan")
+    with pytest.raises(pb.InqbError) as e:
+        h.jade(a, maxsweep=100)
+    assert e.value.status == 5  # INQB_ERR_NONFINITE
