@@ -47,7 +47,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample length")
     ap.add_argument("--no-cells", dest="cells", action="store_false", help="skip the 16-cell batch measurement")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false", help="skip the adjoint measurement")
-    ap.add_argument("--cfg4", action="store_true", help="also run the large-cell (144^3, 480 orbitals) section")
+    ap.add_argument("--no-cfg4", dest="cfg4", action="store_false",
+                    help="skip the large-cell (144^3, 480 orbitals) section")
     return ap.parse_args()
 
 
@@ -358,11 +359,13 @@ def bench_adjoint(args, local):
 
 
 def bench_cfg4(args, local):
-    """Large cell (opt-in, --cfg4): cubic a=30, 144^3, 240 atoms on a jittered shell
-    (radius 6.7), 960 projectors, 480 orbitals (11.5 GB in complex64, 23 GB in
-    complex128), inputs made on the device.  H|psi> and ETRS steps/s in both
-    precisions, peak device memory, and the adjoint gradient (50 steps, checkpoints
-    every 10) of 16 of the orbitals in both precisions."""
+    """Large cell: cubic a=30, 144^3, 240 atoms on a jittered shell (radius 6.7), 960
+    projectors, 480 orbitals (11.5 GB in complex64, 23 GB in complex128), inputs made on
+    the device (plane waves within ecut 30 Ha, the library's inverse FFT and
+    orthonormalisation).  H|psi> and ETRS steps/s in both precisions, the LDA SCF ETRS
+    step and the TD-MLWF step in mixed precision, device memory, the mixed-vs-FP64
+    error of H|psi> on the same (complex64) input orbitals, and the adjoint gradient
+    (50 steps, checkpoints every 10) of 16 of the orbitals in both precisions."""
     import torch
 
     import pinq_b200 as pb
@@ -373,10 +376,13 @@ def bench_cfg4(args, local):
     nr = (144, 144, 144)
     pos = systems.shell_positions(240, 6.7, 0.05, (15.0, 15.0, 15.0), seed=0)
     V = systems.gaussian_potential_device(lattice, nr, pos, device=f"cuda:{local}")
+    vion_d = torch.as_tensor(V, dtype=torch.float64, device=f"cuda:{local}").contiguous()
     M = 480
     out = {"config": "cfg4: cubic a=30, 144^3, 240 atoms on a jittered shell r=6.7 (Fibonacci sphere), "
-                     "960 projectors, ecut 30 Ha, 480 orbitals", "timing": "CUDA events"}
-    ys = {}
+                     "960 projectors, ecut 30 Ha, 480 orbitals", "timing": "CUDA events; SCF ETRS and TD-MLWF: "
+                     "wall clock around synchronised calls"}
+    x_err = None  # the first 32 orbitals of the FP64 block, rounded to complex64: the common input
+    y_err = {}
     for precision in ("fp64", "mixed"):
         torch.cuda.empty_cache()
         torch.cuda.reset_peak_memory_stats()
@@ -384,20 +390,47 @@ def bench_cfg4(args, local):
         h.set_scalar_potential(V)
         kb = h.set_gaussian_projectors(pos, 3.0, 1.0, 1.5, -0.7)
         x = systems.random_orbitals_device(h, M, 30.0, seed=3)
+        if x_err is None:
+            x_err = x[:, :32].to(torch.complex64).cpu()
+        xe = x_err.to(device=x.device, dtype=x.dtype)
+        y_err[precision] = h.apply(xe).to(torch.complex128).cpu()
+        del xe
         y = torch.empty_like(x)
         for _ in range(2):
             h.apply(x, y)
         ms = _timed_ms(lambda: h.apply(x, y), 5, 1) / 5
-        ys[precision] = y[:, :32].to(torch.complex128).cpu()
-        cov = [h.cart_to_cov(np.array([a, 0.0, 0.0])) for a in (0.0, 0.01, -0.01)]
+        # the propagators need the Fourier-sphere mask on the kinetic term here: 1/2 |G_max|^2
+        # dt / 2 is about 8 on this grid, far past the Taylor step's stability bound
+        h.set_fourier_sphere_mask(True)
+        cov = [h.cart_to_cov(np.array([a, 0.0, 0.0])) for a in (0.0, 0.01, -0.01, 0.02)]
         ms_etrs = _timed_ms(lambda: h.etrs_step_(x, 0.05, cov[1], cov[2]), 2, 1) / 2
+        res = {"apply_ms": ms, "orbital_applies_per_s": M / (ms * 1e-3),
+               "etrs_steps_per_s": 1.0 / (ms_etrs * 1e-3), "sphere_points": int(kb["counts"].sum())}
+        if precision == "mixed":
+            occ = np.full(M, 2.0)
+            rho = h.density(x, occ)
+            h.ks_potential(rho, vion_d, 2, energies=False)
+            h.etrs_scf_step_(x, rho, 0.05, cov[0], cov[1], occ, vion_d, 2)  # warm-up
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            its = [h.etrs_scf_step_(x, rho, 0.05, cov[n], cov[n + 1], occ, vion_d, 2)[0] for n in (1, 2)]
+            torch.cuda.synchronize()
+            res["scf_etrs_lda"] = {"steps_per_s": 2 / (time.perf_counter() - t0), "scf_iterations": its}
+            t0 = time.perf_counter()
+            _, spreads, sweeps = h.mlwf_step_(x)
+            torch.cuda.synchronize()
+            res["tdmlwf_step"] = {"s": time.perf_counter() - t0, "jade_sweeps": sweeps, "maxsweep": 100,
+                                  "states": "random plane-wave states after 5 ETRS steps (delocalised: JADE "
+                                            "runs to maxsweep)"}
+        res["propagation"] = "Fourier-sphere mask on the kinetic term (inqb_set_fourier_sphere_mask)"
         free, total = torch.cuda.mem_get_info()
-        out[precision] = {"apply_ms": ms, "orbital_applies_per_s": M / (ms * 1e-3),
-                          "etrs_steps_per_s": 1.0 / (ms_etrs * 1e-3), "sphere_points": int(kb["counts"].sum()),
-                          "device_memory_in_use_gb": (total - free) / 1e9,
-                          "torch_peak_gb": torch.cuda.max_memory_allocated() / 1e9}
+        res.update({"device_memory_in_use_gb": (total - free) / 1e9,
+                    "torch_peak_gb": torch.cuda.max_memory_allocated() / 1e9})
+        out[precision] = res
         del x, y, h
-    out["mixed_vs_fp64_apply_rel_norm_32_orbitals"] = float((ys["mixed"] - ys["fp64"]).norm() / ys["fp64"].norm())
+    out["mixed_vs_fp64_apply_rel_norm_32_orbitals"] = float((y_err["mixed"] - y_err["fp64"]).norm() /
+                                                            y_err["fp64"].norm())
+    out["error_input"] = "the same 32 orbitals (the FP64 block rounded to complex64) through both precisions"
     # adjoint on 16 orbitals: 50 steps, checkpoints every 10
     amps = np.random.default_rng(9).normal(0.0, 0.01, 50)
     grads = {}
@@ -531,6 +564,32 @@ def run_ours(args):
     ms = max_over_ranks(dist, s.elapsed_time(e))
     clk = clocks.stop()
     pass_ms, napplies = h32.timing_stop()
+
+    # -- the two forms of the KB projection (deterministic both): fused into the first
+    # tile pass (the default, timed above) and its own gather-and-contract kernel
+    # (tcgen05 TF32 tensor cores with a split-precision correction in the mixed
+    # precision, CUDA cores in FP64); per-pass CUDA-event times
+    proj_forms = {}
+    Kp = max(5, K // 4)
+    for name, h, x, y in (("mixed", h32, x32, y32), ("fp64", h64, x64, y64)):
+        for form in ("fused", "kernel"):
+            h.set_projection_mode(form)
+            for _ in range(W):
+                h.apply(x, y)
+            torch.cuda.synchronize()
+            h.timing_start(Kp)
+            for _ in range(Kp):
+                h.apply(x, y)
+            pms, pn = h.timing_passes()
+            proj_forms[f"{name}_{form}"] = {"apply_ms": float(sum(pms)) / pn,
+                                            "passes_ms": {"projection_kernel": pms[0] / pn, "tile_fwd": pms[1] / pn,
+                                                          "tile_x": pms[2] / pn, "tile_inv": pms[3] / pn}}
+        h.set_projection_mode("fused")
+    proj_forms["engines"] = {"fused": "CUDA cores inside the first tile pass: FP32 products, FP64 sums per "
+                                      "(plane, half, atom), fixed-order finish in the second pass",
+                             "kernel_mixed": "tcgen05.mma kind::tf32, M=128 N=16, 3xTF32 split, FP64 sums per "
+                                             "32-point chunk",
+                             "kernel_fp64": "CUDA cores, FP64"}
 
     # -- FP64 H|psi>
     ms64 = timed(lambda: h64.apply(x64, y64), max(3, K // 2), W)
@@ -763,7 +822,7 @@ def run_ours(args):
 
     cells = bench_cells(args, local) if args.cells else None
     adj = bench_adjoint(args, local) if args.adjoint else None
-    big = bench_cfg4(args, local) if args.cfg4 else None
+    big = bench_cfg4(args, local) if args.cfg4 and world == 1 else None
 
     if rank != 0:
         if dist is not None:
@@ -820,6 +879,7 @@ def run_ours(args):
                  "fp64_steps_per_s": world * args.etrs_steps / (ms_etrs64 * 1e-3),
                  "H_applies_per_step": 8, "dt": 0.05},
         "fft": fft,
+        "projection_forms": proj_forms,
         "crank_nicolson": cn,
         "etrs_scf": scf,
         "checkpoint": ckpt,
