@@ -59,6 +59,13 @@ int inqb_grid_supported(int nx, int ny, int nz, int precision);
 int inqb_ctx_create(const double lattice[9], int nx, int ny, int nz, int precision, int device,
                     inqb_ctx** out);
 int inqb_ctx_destroy(inqb_ctx* ctx);
+/* A second context with src's cell, grid, precision, device, local potential (as it is
+ * on the device now, including a self-consistent update), vector potential, Fourier
+ * mask, projectors, projection form and launch schedules, and a workspace of its own:
+ * for work on another stream beside src (two calls on one context must not overlap).
+ * The density-reduce hook is not copied.  No counterpart in the reference, whose
+ * Hamiltonian is copied with its C++ copy constructor. */
+int inqb_ctx_clone(const inqb_ctx* src, inqb_ctx** out);
 /* Allocates the device workspace for blocks of up to M orbitals, so that the
  * later calls with M' <= M allocate nothing (INQ allocates per call from its
  * caching pool, external_libs/gpurun/include/gpu/array.hpp:66-116). */

@@ -657,6 +657,37 @@ int inqb_ctx_create(const double lattice[9], int nx, int ny, int nz, int precisi
   return INQB_OK;
 }
 
+int inqb_ctx_clone(const inqb_ctx* src, inqb_ctx** out) {
+  if (!src || !out) return fail(INQB_ERR_INVALID, "null argument");
+  *out = nullptr;
+  double lat[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) lat[3 * i + j] = src->cell.lat[i][j];
+  inqb_ctx* c = nullptr;
+  INQB_TRY(inqb_ctx_create(lat, src->nr[0], src->nr[1], src->nr[2], src->precision, src->device, &c));
+  auto undo = [&c](int st) {
+    inqb_ctx_destroy(c);
+    return st;
+  };
+  DeviceGuard guard(src->device);
+  if (guard.status != INQB_OK) return undo(guard.status);
+  c->V_host = src->V_host;
+  if (cudaMemcpy(c->d_V.ptr, src->d_V.ptr, src->d_V.bytes, cudaMemcpyDeviceToDevice) != cudaSuccess)
+    return undo(fail(INQB_ERR_CUDA, "potential copy failed"));
+  for (int d = 0; d < 3; d++) c->kA_cov[d] = src->kA_cov[d];
+  c->fourier_mask = src->fourier_mask;
+  c->proj_mode = src->proj_mode;
+  c->schedules = src->schedules;
+  const auto& ps = src->proj_src;
+  if (ps.nproj > 0) {
+    const int st = inqb_set_projectors(c, ps.nproj, ps.L, ps.smax, ps.counts.data(), ps.coords.data(),
+                                       ps.relpos.data(), ps.beta.data(), ps.coeff.data());
+    if (st != INQB_OK) return undo(st);
+  }
+  *out = c;
+  return INQB_OK;
+}
+
 int inqb_ctx_destroy(inqb_ctx* ctx) {
   if (!ctx) return INQB_OK;
   DeviceGuard guard(ctx->device);
@@ -847,6 +878,18 @@ int inqb_set_projectors(inqb_ctx* ctx, int nproj, int L, int smax, const int* co
   }
   INQB_CUDA_TRY(cudaDeviceSynchronize());
   ctx->proj = std::move(fresh);
+  {
+    auto& src = ctx->proj_src;
+    src.nproj = nproj;
+    src.L = L;
+    src.smax = smax;
+    const size_t ns = (size_t)nproj * smax;
+    src.counts.assign(counts, counts + (nproj > 0 ? nproj : 0));
+    src.coords.assign(coords, coords + (nproj > 0 ? 3 * ns : 0));
+    src.relpos.assign(relpos, relpos + (nproj > 0 ? 3 * ns : 0));
+    src.beta.assign(beta, beta + (nproj > 0 ? (size_t)L * ns : 0));
+    src.coeff.assign(coeff, coeff + (nproj > 0 ? (size_t)nproj * L : 0));
+  }
   ctx->proj_phases_valid = false;
   INQB_TRY(update_phases(ctx, nullptr));
   INQB_CUDA_TRY(cudaStreamSynchronize(nullptr));

@@ -198,6 +198,13 @@ struct inqb_ctx {
   int fourier_mask = 0;            // zero_outside_sphere on the kinetic term
 
   std::vector<double> V_host;
+  // the projector inputs as set (inqb_ctx_clone rebuilds the tables from them)
+  struct ProjSource {
+    int nproj = 0, L = 0, smax = 0;
+    std::vector<int> counts, coords;
+    std::vector<float> relpos;
+    std::vector<double> beta, coeff;
+  } proj_src;
   inqb::DevBuf d_V;       // [N] in context precision
   inqb::DevBuf d_tw;      // twiddles for x, y, z (context precision), N_d entries each
   inqb::ProjTables proj;

@@ -38,6 +38,7 @@ SIGNATURES = {
     "inqb_ctx_create": (ctypes.c_int, [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_void_p)]),
     "inqb_ctx_destroy": (ctypes.c_int, [_ctxp]),
+    "inqb_ctx_clone": (ctypes.c_int, [_ctxp, ctypes.POINTER(ctypes.c_void_p)]),
     "inqb_ctx_reserve": (ctypes.c_int, [_ctxp, ctypes.c_int]),
     "inqb_volume_element": (ctypes.c_double, [_ctxp]),
     "inqb_cart_to_cov": (ctypes.c_int, [_ctxp, _dp, _dp]),

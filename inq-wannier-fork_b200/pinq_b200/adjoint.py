@@ -21,7 +21,10 @@ checkpointed every `every` steps and recomputed segment by segment.
 
 The steps run in libinqb200 (inqb_etrs_step, inqb_etrs_step_powers,
 inqb_etrs_adjoint_step); torch holds device memory and supplies the autograd
-interface.
+interface.  With more than one checkpoint segment, the recompute of the segment before
+runs on a second CUDA stream, with a second context (inqb_ctx_clone), beside the
+backward walk of the current one: the recompute's launches fill the gaps of the
+backward's.
 """
 from __future__ import annotations
 
@@ -47,6 +50,9 @@ class DipolePropagation:
         self.direction = int(direction)
         self.store_powers = bool(store_powers)
         self.powers = None
+        self.overlap = True  # recompute the previous segment on a second stream
+        self._h2 = None
+        self._h2_version = None
 
     # -- helpers
     def _kA(self, a: float):
@@ -111,10 +117,13 @@ class DipolePropagation:
                 h.etrs_adjoint_step_(lam, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)),
                                      self.powers[n], gV, gA[n], gA[n2])
             return gA[:, self.direction].clone(), gV
+        segments = [(s0, min(s0 + self.every, nsteps)) for s0 in range(0, nsteps, self.every)][::-1]
+        if self.overlap and len(segments) > 1 and self.psi0.is_cuda:
+            self._backward_overlapped(segments, lam, gV, gA)
+            return gA[:, self.direction].clone(), gV
         seg = min(self.every, nsteps)
         store = h.powers_buffer(seg, self.M)
-        for s0 in reversed(range(0, nsteps, self.every)):
-            s1 = min(s0 + self.every, nsteps)
+        for s0, s1 in segments:
             psi = self.checkpoints[s0].clone()
             for n in range(s0, s1):
                 h.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)),
@@ -125,6 +134,56 @@ class DipolePropagation:
                                      store[n - s0], gV, gA[n], gA[n2])
         del store
         return gA[:, self.direction].clone(), gV
+
+    def _recompute_context(self):
+        """The second context for the recompute stream: a clone of the Hamiltonian,
+        made again whenever the Hamiltonian changed since."""
+        if self._h2 is None or self._h2_version != self.h.state_version:
+            self._h2 = self.h.clone()
+            self._h2_version = self.h.state_version
+        return self._h2
+
+    def _backward_overlapped(self, segments, lam, gV, gA):
+        """Segments in reverse time order; segment i + 1's recompute (second context,
+        second stream) overlaps segment i's backward walk.  Two powers buffers
+        alternate; events order each buffer's write after its previous read."""
+        h, h2 = self.h, self._recompute_context()
+        amps, nsteps = self.amps, len(self.amps)
+        dev = self.psi0.device
+        main = torch.cuda.current_stream(dev)
+        side = torch.cuda.Stream(device=dev)
+        seg = min(self.every, nsteps)
+        stores = [h.powers_buffer(seg, self.M), h.powers_buffer(seg, self.M)]
+        for b in stores:
+            b.record_stream(side)
+        ready = [torch.cuda.Event() for _ in segments]
+        done = [torch.cuda.Event() for _ in segments]
+        side.wait_stream(main)  # the checkpoints were written on the main stream
+
+        def recompute(i):
+            s0, s1 = segments[i]
+            buf = stores[i % 2]
+            with torch.cuda.stream(side):
+                if i >= 2:
+                    side.wait_event(done[i - 2])  # the buffer's previous segment is walked back
+                psi = self.checkpoints[s0].clone()
+                for n in range(s0, s1):
+                    h2.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)),
+                                         self._kA(self._amp(amps, n + 1)), buf[n - s0])
+                ready[i].record(side)
+
+        recompute(0)
+        for i, (s0, s1) in enumerate(segments):
+            if i + 1 < len(segments):
+                recompute(i + 1)
+            main.wait_event(ready[i])
+            buf = stores[i % 2]
+            for n in reversed(range(s0, s1)):
+                n2 = min(n + 1, nsteps - 1)
+                h.etrs_adjoint_step_(lam, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)),
+                                     buf[n - s0], gV, gA[n], gA[n2])
+            done[i].record(main)
+        main.wait_stream(side)
 
 
 class _ETRSDipoleFunction(torch.autograd.Function):

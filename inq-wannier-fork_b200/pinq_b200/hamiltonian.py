@@ -103,6 +103,24 @@ class KSHamiltonian:
         call("inqb_ctx_create", dptr(_lattice(lattice)), self.nr[0], self.nr[1], self.nr[2], self.precision,
              int(device), ctypes.byref(h))
         self._h = h
+        self.state_version = 0  # bumped by every call that changes the Hamiltonian (see clone)
+
+    def clone(self) -> "KSHamiltonian":
+        """A second context with this one's state (potential as it is on the device,
+        vector potential, mask, projectors, projection form, schedules) and its own
+        workspace, for work on another CUDA stream beside this one."""
+        other = KSHamiltonian.__new__(KSHamiltonian)
+        other.lattice = self.lattice.copy()
+        other.nr = self.nr
+        other.N = self.N
+        other.precision = self.precision
+        other.dtype = self.dtype
+        other.device = self.device
+        h = ctypes.c_void_p()
+        call("inqb_ctx_clone", self._h, ctypes.byref(h))
+        other._h = h
+        other.state_version = 0
+        return other
 
     def close(self):
         h = getattr(self, "_h", None)
@@ -128,6 +146,7 @@ class KSHamiltonian:
         return out
 
     def set_scalar_potential(self, V):
+        self.state_version += 1
         V = np.ascontiguousarray(torch.as_tensor(V).detach().cpu().numpy() if torch.is_tensor(V) else V,
                                  dtype=np.float64).reshape(self.N)
         call("inqb_set_local_potential", self._h, dptr(V))
@@ -141,9 +160,11 @@ class KSHamiltonian:
 
     def set_fourier_sphere_mask(self, enable: bool = True):
         """INQ's zero_outside_sphere on the kinetic term (off by default, as in INQ)."""
+        self.state_version += 1
         call("inqb_set_fourier_sphere_mask", self._h, int(bool(enable)))
 
     def set_projectors(self, kb):
+        self.state_version += 1
         nproj = len(kb["counts"])
         counts = np.ascontiguousarray(kb["counts"], np.int32)
         coords = np.ascontiguousarray(kb["coords"], np.int32)
@@ -161,12 +182,14 @@ class KSHamiltonian:
     def autotune(self, M: int) -> tuple:
         """Time the launch schedules for M orbitals and keep the fastest; returns
         (ysplit, threads of the three passes)."""
+        self.state_version += 1
         sched = (ctypes.c_int * 4)()
         call("inqb_autotune", self._h, int(M), self._stream(), sched)
         return tuple(sched)
 
     def set_schedule(self, M: int, schedule=None):
         """Use schedule (ysplit, t1, t2, t3) for M orbitals; None restores the default."""
+        self.state_version += 1
         arr = None if schedule is None else (ctypes.c_int * 4)(*[int(v) for v in schedule])
         call("inqb_set_schedule", self._h, int(M), arr)
 
@@ -266,6 +289,7 @@ class KSHamiltonian:
         """update_hamiltonian: the local potential becomes vion + V_H[rho] + v_xc[rho]
         (theory 0 none, 1 Hartree, 2 LDA).  Returns the energies {external, hartree,
         xc, nvxc} (synchronises) or None."""
+        self.state_version += 1
         rho = self._fp64_field(rho, "rho")
         vion = self._fp64_field(vion, "vion")
         en = np.zeros(4) if energies else None
@@ -277,6 +301,7 @@ class KSHamiltonian:
         """ETRS with the self-consistency loop of real_time::etrs, in place on psi and
         rho (the potential must be the Kohn-Sham potential of rho on entry).
         Returns (SCF iterations, energies of the last update)."""
+        self.state_version += 1
         psi = self._check(psi)
         rho = self._fp64_field(rho, "rho")
         vion = self._fp64_field(vion, "vion")
@@ -314,6 +339,7 @@ class KSHamiltonian:
         Kohn-Sham potential of rho on entry).  num_electrons defaults to sum(occ); an
         orbital-sharded run passes the total over the ranks.  Returns (iterations,
         last solver residual, energies of the last update)."""
+        self.state_version += 1
         psi = self._check(psi)
         rho = self._fp64_field(rho, "rho")
         vion = self._fp64_field(vion, "vion")
@@ -365,6 +391,7 @@ class KSHamiltonian:
         """Orbital-sharded SCF: reducer(rho) must replace rho (an FP64 CUDA tensor) by
         its sum over the ranks before returning, e.g. parallel.density_reducer(group).
         None removes it."""
+        self.state_version += 1
         self._density_reducer = reducer
 
     # -- checkpoints in INQ's restart layout (operations/io.hpp, systems/electrons.hpp)
@@ -579,6 +606,7 @@ class KSHamiltonian:
         """INQB_PROJECTION_FUSED (0, "fused": inside the first tile pass, the default)
         or INQB_PROJECTION_KERNEL (1, "kernel": its own gather-and-contract kernel, on
         the tensor cores in the mixed precision)."""
+        self.state_version += 1
         m = {"fused": 0, "kernel": 1}.get(mode, mode)
         call("inqb_set_projection_mode", self._h, int(m))
 
