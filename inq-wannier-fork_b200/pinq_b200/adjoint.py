@@ -51,6 +51,7 @@ class DipolePropagation:
         self.store_powers = bool(store_powers)
         self.powers = None
         self.overlap = True  # recompute the previous segment on a second stream
+        self._tail = None  # (first step, powers) of the last segment, kept by the forward
         self._h2 = None
         self._h2_version = None
 
@@ -70,6 +71,7 @@ class DipolePropagation:
         psi = self.psi0.clone()
         cps = {}
         self.powers = None
+        self._tail = None
         if keep and self.store_powers:
             powers = self.h.powers_buffer(len(amps), self.M)
             for n in range(len(amps)):
@@ -78,14 +80,20 @@ class DipolePropagation:
             self.powers = powers
         elif keep:
             # the same term-by-term step the backward recomputes each segment with, so
-            # that the recomputed trajectory is this one exactly (one scratch row)
+            # that the recomputed trajectory is this one exactly (one scratch row); the
+            # last segment's powers are kept, since the backward walks it first
+            nsteps = len(amps)
+            last0 = ((nsteps - 1) // self.every) * self.every
             scratch = self.h.powers_buffer(1, self.M)
-            for n in range(len(amps)):
+            tail = self.h.powers_buffer(min(self.every, nsteps), self.M)
+            for n in range(nsteps):
                 if n % self.every == 0:
                     cps[n] = psi.clone()
+                row = tail[n - last0] if n >= last0 else scratch[0]
                 self.h.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)),
-                                         self._kA(self._amp(amps, n + 1)), scratch[0])
+                                         self._kA(self._amp(amps, n + 1)), row)
             del scratch
+            self._tail = (last0, tail)
         else:
             for n in range(len(amps)):
                 self.h.etrs_step_(psi, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)))
@@ -124,14 +132,18 @@ class DipolePropagation:
         seg = min(self.every, nsteps)
         store = h.powers_buffer(seg, self.M)
         for s0, s1 in segments:
-            psi = self.checkpoints[s0].clone()
-            for n in range(s0, s1):
-                h.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)),
-                                    store[n - s0])
+            if self._tail is not None and s0 == self._tail[0]:
+                buf = self._tail[1]  # the forward kept this segment's powers
+            else:
+                buf = store
+                psi = self.checkpoints[s0].clone()
+                for n in range(s0, s1):
+                    h.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)),
+                                        self._kA(self._amp(amps, n + 1)), buf[n - s0])
             for n in reversed(range(s0, s1)):
                 n2 = min(n + 1, nsteps - 1)
                 h.etrs_adjoint_step_(lam, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)),
-                                     store[n - s0], gV, gA[n], gA[n2])
+                                     buf[n - s0], gV, gA[n], gA[n2])
         del store
         return gA[:, self.direction].clone(), gV
 
@@ -153,7 +165,9 @@ class DipolePropagation:
         main = torch.cuda.current_stream(dev)
         side = torch.cuda.Stream(device=dev)
         seg = min(self.every, nsteps)
-        stores = [h.powers_buffer(seg, self.M), h.powers_buffer(seg, self.M)]
+        have_tail = self._tail is not None and segments[0][0] == self._tail[0]
+        first = self._tail[1] if have_tail else h.powers_buffer(seg, self.M)
+        stores = [first, h.powers_buffer(seg, self.M)]
         for b in stores:
             b.record_stream(side)
         ready = [torch.cuda.Event() for _ in segments]
@@ -172,7 +186,10 @@ class DipolePropagation:
                                          self._kA(self._amp(amps, n + 1)), buf[n - s0])
                 ready[i].record(side)
 
-        recompute(0)
+        if have_tail:
+            ready[0].record(main)  # the forward kept the last segment's powers
+        else:
+            recompute(0)
         for i, (s0, s1) in enumerate(segments):
             if i + 1 < len(segments):
                 recompute(i + 1)
@@ -184,6 +201,8 @@ class DipolePropagation:
                                      buf[n - s0], gV, gA[n], gA[n2])
             done[i].record(main)
         main.wait_stream(side)
+        if have_tail and len(segments) > 2:
+            self._tail = None  # its buffer held later segments' powers: recompute next time
 
 
 class _ETRSDipoleFunction(torch.autograd.Function):
