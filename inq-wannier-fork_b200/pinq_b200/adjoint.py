@@ -174,32 +174,64 @@ class DipolePropagation:
         done = [torch.cuda.Event() for _ in segments]
         side.wait_stream(main)  # the checkpoints were written on the main stream
 
+        # the recompute is enqueued by a second host thread (ctypes releases the GIL), so
+        # the two streams are fed in parallel; host flags order each event wait after
+        # the event's record
+        import threading
+
+        host_ready = [threading.Event() for _ in segments]
+        host_done = [threading.Event() for _ in segments]
+        failure = []
+        limit_s = 600.0
+
         def recompute(i):
             s0, s1 = segments[i]
             buf = stores[i % 2]
             with torch.cuda.stream(side):
                 if i >= 2:
+                    if not host_done[i - 2].wait(limit_s):
+                        raise RuntimeError("adjoint: the backward walk did not release a powers buffer")
                     side.wait_event(done[i - 2])  # the buffer's previous segment is walked back
                 psi = self.checkpoints[s0].clone()
                 for n in range(s0, s1):
                     h2.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)),
                                          self._kA(self._amp(amps, n + 1)), buf[n - s0])
                 ready[i].record(side)
+            host_ready[i].set()
+
+        def worker():
+            try:
+                torch.cuda.set_device(dev)
+                for i in range(1 if have_tail else 0, len(segments)):
+                    recompute(i)
+            except BaseException as ex:  # reported by the main thread
+                failure.append(ex)
+                for e in host_ready:
+                    e.set()
 
         if have_tail:
             ready[0].record(main)  # the forward kept the last segment's powers
-        else:
-            recompute(0)
-        for i, (s0, s1) in enumerate(segments):
-            if i + 1 < len(segments):
-                recompute(i + 1)
-            main.wait_event(ready[i])
-            buf = stores[i % 2]
-            for n in reversed(range(s0, s1)):
-                n2 = min(n + 1, nsteps - 1)
-                h.etrs_adjoint_step_(lam, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)),
-                                     buf[n - s0], gV, gA[n], gA[n2])
-            done[i].record(main)
+            host_ready[0].set()
+        thread = threading.Thread(target=worker, daemon=True)
+        thread.start()
+        try:
+            for i, (s0, s1) in enumerate(segments):
+                if not host_ready[i].wait(limit_s) or failure:
+                    raise RuntimeError("adjoint: segment recompute failed") from (failure[0] if failure else None)
+                main.wait_event(ready[i])
+                buf = stores[i % 2]
+                for n in reversed(range(s0, s1)):
+                    n2 = min(n + 1, nsteps - 1)
+                    h.etrs_adjoint_step_(lam, self.dt, self._kA(self._amp(amps, n)),
+                                         self._kA(self._amp(amps, n + 1)), buf[n - s0], gV, gA[n], gA[n2])
+                done[i].record(main)
+                host_done[i].set()
+        finally:
+            for e in host_done:
+                e.set()  # let the worker finish (or fail) on every path
+            thread.join(limit_s)
+        if failure:
+            raise RuntimeError("adjoint: segment recompute failed") from failure[0]
         main.wait_stream(side)
         if have_tail and len(segments) > 2:
             self._tail = None  # its buffer held later segments' powers: recompute next time
