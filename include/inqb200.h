@@ -385,6 +385,22 @@ int inqb_mlwf_matrices(inqb_ctx* ctx, const void* psi, int M, int ld, void* a, v
 int inqb_jade(inqb_ctx* ctx, int M, void* a, void* u, void* adiag, int maxsweep, double tol, int* sweeps,
               void* stream);
 int inqb_mlwf_rotate(inqb_ctx* ctx, void* psi, int M, int ld, const void* u, void* stream);
+/* The pieces of the TD-MLWF step over orbitals split across ranks (the reference
+ * distributes the basis instead and all-reduces the matrices over it,
+ * src/wannier/tdmlwf_trans.hpp:96-172).  The caller circulates the blocks and sums;
+ * pinq_b200.parallel.sharded_mlwf_step_ does it over torch.distributed.
+ * inqb_mlwf_gram_block: Z [3][Ma][Mb] (device complex128) = sum_p conj(a_m(p))
+ *   e^{i 2 pi r_d(p) / |a_d|} b_n(p), one block of the three weighted Gram matrices.
+ * inqb_mlwf_finish: a [6][M][M] of tdmlwf_trans::update from the summed Z [3][M][M] and
+ *   norms[M] = sum_p |psi_m|^2 (device FP64).
+ * inqb_orbital_norms: norms[M] (device FP64) of an orbital block; synchronous.
+ * inqb_mlwf_centres: centres [M][3] and spreads [M] (host) from adiag [6][M] (host
+ *   complex128), tdmlwf_trans::center / spread2 (tdmlwf_trans.hpp:196-312). */
+int inqb_mlwf_gram_block(inqb_ctx* ctx, const void* a, int Ma, int lda, const void* b, int Mb, int ldb, void* Z,
+                         void* stream);
+int inqb_mlwf_finish(inqb_ctx* ctx, int M, const void* Z, const double* norms, void* a, void* stream);
+int inqb_orbital_norms(inqb_ctx* ctx, const void* psi, int M, int ld, double* norms, void* stream);
+int inqb_mlwf_centres(inqb_ctx* ctx, int M, const double* adiag, double* centres, double* spreads);
 
 /* ---------------------------------------------------------------- launch schedules
  * (no counterpart in the reference; its kernels have fixed launch shapes).  A

@@ -1160,6 +1160,46 @@ int inqb_mlwf_matrices(inqb_ctx* ctx, const void* psi, int M, int ld, void* a, v
                           static_cast<double2*>(a), stream);
 }
 
+int inqb_mlwf_gram_block(inqb_ctx* ctx, const void* a, int Ma, int lda, const void* b, int Mb, int ldb, void* Z,
+                         void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, a, Ma, lda));
+  INQB_TRY(check_block(ctx, b, Mb, ldb));
+  if (!Z) return fail(INQB_ERR_INVALID, "null matrix buffer");
+  INQB_GUARD(ctx);
+  INQB_TRY(ctx->d_mlwf.ensure(mlwf_partial_bytes(ctx->N, Ma, Mb)));
+  return launch_mlwf_gram_block(ctx->precision, a, lda, Ma, b, ldb, Mb, ctx->N, ctx->nr, ctx->cell.lat,
+                                ctx->d_mlwf.ptr, static_cast<double2*>(Z), stream);
+}
+
+int inqb_mlwf_finish(inqb_ctx* ctx, int M, const void* Z, const double* norms, void* a, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  if (M <= 0 || !Z || !norms || !a) return fail(INQB_ERR_INVALID, "bad arguments");
+  INQB_GUARD(ctx);
+  return launch_mlwf_finish(static_cast<const double2*>(Z), M, norms, 1, static_cast<double2*>(a), stream);
+}
+
+int inqb_orbital_norms(inqb_ctx* ctx, const void* psi, int M, int ld, double* norms, void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!norms) return fail(INQB_ERR_INVALID, "null output");
+  INQB_GUARD(ctx);
+  DevBuf acc;
+  INQB_TRY(acc.ensure(sizeof(double) * 3 * (size_t)M));
+  INQB_TRY(launch_band_sums(ctx->precision, psi, psi, ld, M, ctx->N, acc.as<double>(), stream));
+  INQB_CUDA_TRY(cudaMemcpy2DAsync(norms, sizeof(double), acc.as<double>() + 2, 3 * sizeof(double), sizeof(double),
+                                  M, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  INQB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  return INQB_OK;
+}
+
+int inqb_mlwf_centres(inqb_ctx* ctx, int M, const double* adiag, double* centres, double* spreads) {
+  INQB_CHECK_CTX(ctx);
+  if (M <= 0 || !adiag) return fail(INQB_ERR_INVALID, "bad arguments");
+  mlwf_centres(ctx, M, reinterpret_cast<const double2*>(adiag), centres, spreads);
+  return INQB_OK;
+}
+
 int inqb_jade(inqb_ctx* ctx, int M, void* a, void* u, void* adiag, int maxsweep, double tol, int* sweeps,
               void* stream) {
   INQB_CHECK_CTX(ctx);

@@ -66,15 +66,15 @@ __device__ __forceinline__ void store_partial(float2* p, float x, float y) { *p 
 // grid (tiles_m * tiles_n, nslab)
 template <typename T>
 __global__ void __launch_bounds__(256, GramCfg<T>::MINB)
-    k_mlwf_gram(const cplx<T>* __restrict__ psi, long ld, int M, long N, GramGeom geo, long pts_per_slab,
-                typename GramCfg<T>::P* __restrict__ partial) {
+    k_mlwf_gram(const cplx<T>* __restrict__ pa, long lda, int Ma, const cplx<T>* __restrict__ pb, long ldb, int Mb,
+                long N, GramGeom geo, long pts_per_slab, typename GramCfg<T>::P* __restrict__ partial) {
   using R = T;
   constexpr int TMX = GramCfg<T>::TMX, TNX = GramCfg<T>::TNX, kGP = GramCfg<T>::GP;
   constexpr int TILE_M = 16 * TMX, TILE_N = 16 * TNX;
   __shared__ cplx<R> sA[kGP][TILE_M];
   __shared__ cplx<R> sB[3][kGP][TILE_N];
   __shared__ cplx<R> sW[3][kGP];
-  const int tiles_m = (M + TILE_M - 1) / TILE_M;
+  const int tiles_m = (Ma + TILE_M - 1) / TILE_M;
   const int m0 = (blockIdx.x % tiles_m) * TILE_M, n0 = (blockIdx.x / tiles_m) * TILE_N;
   const long p_beg = (long)blockIdx.y * pts_per_slab, p_end = min(N, p_beg + pts_per_slab);
   const int tm = threadIdx.x % 16, tn = threadIdx.x / 16;
@@ -113,12 +113,12 @@ __global__ void __launch_bounds__(256, GramCfg<T>::MINB)
     for (int i = threadIdx.x; i < kGP * TILE_M; i += blockDim.x) {
       const int q = i / TILE_M, j = i % TILE_M;
       const long p = pc + q;
-      sA[q][j] = (p < p_end && m0 + j < M) ? psi[p * ld + m0 + j] : mk<R>(0, 0);
+      sA[q][j] = (p < p_end && m0 + j < Ma) ? pa[p * lda + m0 + j] : mk<R>(0, 0);
     }
     for (int i = threadIdx.x; i < kGP * TILE_N; i += blockDim.x) {
       const int q = i / TILE_N, j = i % TILE_N;
       const long p = pc + q;
-      const cplx<R> vb = (p < p_end && n0 + j < M) ? psi[p * ld + n0 + j] : mk<R>(0, 0);
+      const cplx<R> vb = (p < p_end && n0 + j < Mb) ? pb[p * ldb + n0 + j] : mk<R>(0, 0);
 #pragma unroll
       for (int d = 0; d < 3; ++d) sB[d][q][j] = sW[d][q] * vb;
     }
@@ -145,8 +145,8 @@ __global__ void __launch_bounds__(256, GramCfg<T>::MINB)
     }
     __syncthreads();
   }
-  // partial[slab][d][m][n]
-  const size_t MM = (size_t)M * M;
+  // partial[slab][d][m][n], m < Ma, n < Mb
+  const size_t MM = (size_t)Ma * Mb;
 #pragma unroll
   for (int d = 0; d < 3; ++d)
 #pragma unroll
@@ -154,8 +154,8 @@ __global__ void __launch_bounds__(256, GramCfg<T>::MINB)
 #pragma unroll
       for (int b = 0; b < TNX; ++b) {
         const int m = m0 + tm + 16 * a, n = n0 + tn + 16 * b;
-        if (m < M && n < M)
-          store_partial(&partial[((size_t)blockIdx.y * 3 + d) * MM + (size_t)m * M + n], acc[d][a][b][0],
+        if (m < Ma && n < Mb)
+          store_partial(&partial[((size_t)blockIdx.y * 3 + d) * MM + (size_t)m * Mb + n], acc[d][a][b][0],
                         acc[d][a][b][1]);
       }
 }
@@ -181,8 +181,8 @@ __global__ void k_mlwf_slab_sum(const P* __restrict__ partial, int nslab, long n
 }
 
 // a[2d][m][n] = (Z + Z^H)/2, a[2d+1][m][n] = (Z - Z^H)/(2i), Z the slab sum (FP64) divided
-// by |psi_m| |psi_n| (sums[3 m + 2] = sum_p |psi_m|^2 from the band sums)
-__global__ void k_mlwf_finish(const double2* __restrict__ Z, int M, const double* __restrict__ sums,
+// by |psi_m| |psi_n|: norms[ns m + ns - 1] = sum_p |psi_m|^2 (ns = 3: the band sums; 1: plain)
+__global__ void k_mlwf_finish(const double2* __restrict__ Z, int M, const double* __restrict__ norms, int ns,
                               double2* __restrict__ a) {
   const size_t MM = (size_t)M * M;
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < 3 * (long)MM; e += (long)gridDim.x * blockDim.x) {
@@ -191,7 +191,7 @@ __global__ void k_mlwf_finish(const double2* __restrict__ Z, int M, const double
     const double2 x = Z[(size_t)d * MM + (size_t)m * M + n];
     const double2 y = Z[(size_t)d * MM + (size_t)n * M + m];
     const double zx = x.x, zy = x.y, tx = y.x, ty = y.y;
-    const double sc = 1.0 / sqrt(sums[3 * m + 2] * sums[3 * n + 2]);
+    const double sc = 1.0 / sqrt(norms[ns * m + ns - 1] * norms[ns * n + ns - 1]);
     // conj(Z[n][m]) = (tx, -ty)
     a[(2 * d) * MM + (size_t)m * M + n] = make_double2(0.5 * sc * (zx + tx), 0.5 * sc * (zy - ty));
     // (Z - conj(Z[n][m])) / (2i) = (v - i u) / 2 with u + i v = Z - conj(Z[n][m])
@@ -503,49 +503,50 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 1)
 
 namespace {
 template <typename T>
-long gram_slabs(long N, int M) {
+long gram_slabs(long N, int Ma, int Mb) {
   constexpr int TM = 16 * GramCfg<T>::TMX, TN = 16 * GramCfg<T>::TNX, kGP = GramCfg<T>::GP;
-  const long tiles = (long)((M + TM - 1) / TM) * ((M + TN - 1) / TN);
+  const long tiles = (long)((Ma + TM - 1) / TM) * ((Mb + TN - 1) / TN);
   const long chunks = (N + kGP - 1) / kGP;
   if (sizeof(T) == 4) return std::max<long>(1, (N + kSlabF32 - 1) / kSlabF32);
   return std::max<long>(1, std::min<long>(chunks, (148L * 4 + tiles - 1) / tiles));
 }
+size_t slab_bytes(long N, int Ma, int Mb) {
+  const size_t MM = (size_t)Ma * Mb;
+  return std::max((size_t)gram_slabs<double>(N, Ma, Mb) * 3 * MM * sizeof(double2),
+                  (size_t)gram_slabs<float>(N, Ma, Mb) * 3 * MM * sizeof(float2));
+}
 }  // namespace
 
-// the slabs of the larger layout, then Z [3][M][M] (FP64) at a 256-byte boundary
-size_t mlwf_partial_bytes(long N, int M) {
-  const size_t MM = (size_t)M * M;
-  const size_t slabs = std::max((size_t)gram_slabs<double>(N, M) * 3 * MM * sizeof(double2),
-                                (size_t)gram_slabs<float>(N, M) * 3 * MM * sizeof(float2));
-  return (slabs + 255) / 256 * 256 + 3 * MM * sizeof(double2);
+// the slabs of the larger layout, then Z [3][Ma][Mb] (FP64) at a 256-byte boundary
+size_t mlwf_partial_bytes(long N, int Ma, int Mb) {
+  return (slab_bytes(N, Ma, Mb) + 255) / 256 * 256 + 3 * (size_t)Ma * Mb * sizeof(double2);
 }
+size_t mlwf_partial_bytes(long N, int M) { return mlwf_partial_bytes(N, M, M); }
 
+// Z [3][Ma][Mb] = sum_p conj(a_m) e^{i theta_d} b_n (FP64 sums of the slabs), in the
+// partial buffer after the slabs; returns Z
 template <typename T>
-static int gram_impl(const void* psi, long ld, int M, long N, const GramGeom& g, const double* sums, void* partial,
-                     double2* a, cudaStream_t st) {
+static int gram_impl(const void* pa, long lda, int Ma, const void* pb, long ldb, int Mb, long N, const GramGeom& g,
+                     void* partial, double2** Zout, cudaStream_t st) {
   using P = typename GramCfg<T>::P;
   constexpr int TM = 16 * GramCfg<T>::TMX, TN = 16 * GramCfg<T>::TNX, kGP = GramCfg<T>::GP;
-  const long slabs = gram_slabs<T>(N, M);
+  const long slabs = gram_slabs<T>(N, Ma, Mb);
   const long per = ((N + slabs - 1) / slabs + kGP - 1) / kGP * kGP;
   const long nslab = (N + per - 1) / per;
-  const dim3 grid((unsigned)(((M + TM - 1) / TM) * ((M + TN - 1) / TN)), (unsigned)nslab);
-  k_mlwf_gram<T><<<grid, 256, 0, st>>>((const cplx<T>*)psi, ld, M, N, g, per, (P*)partial);
+  const dim3 grid((unsigned)(((Ma + TM - 1) / TM) * ((Mb + TN - 1) / TN)), (unsigned)nslab);
+  k_mlwf_gram<T><<<grid, 256, 0, st>>>((const cplx<T>*)pa, lda, Ma, (const cplx<T>*)pb, ldb, Mb, N, g, per,
+                                       (P*)partial);
   INQB_CUDA_TRY(cudaGetLastError());
-  const long work = 3L * M * M;
-  const size_t slab_bytes =
-      std::max((size_t)gram_slabs<double>(N, M) * 3 * (size_t)M * M * sizeof(double2),
-               (size_t)gram_slabs<float>(N, M) * 3 * (size_t)M * M * sizeof(float2));
-  double2* Z = reinterpret_cast<double2*>(static_cast<char*>(partial) + (slab_bytes + 255) / 256 * 256);
+  const long work = 3L * Ma * Mb;
+  double2* Z = reinterpret_cast<double2*>(static_cast<char*>(partial) + (slab_bytes(N, Ma, Mb) + 255) / 256 * 256);
   k_mlwf_slab_sum<P><<<(unsigned)std::min<long>((work + 255) / 256, 148L * 32), 256, 0, st>>>((const P*)partial,
                                                                                              (int)nslab, work, Z);
   INQB_CUDA_TRY(cudaGetLastError());
-  k_mlwf_finish<<<(unsigned)std::min<long>((work + 255) / 256, 148L * 8), 256, 0, st>>>(Z, M, sums, a);
-  INQB_CUDA_TRY(cudaGetLastError());
+  *Zout = Z;
   return INQB_OK;
 }
 
-int launch_mlwf_gram(int precision, const void* psi, long ld, int M, long N, const int nr[3], const double lat[3][3],
-                     const double* sums, void* partial, double2* a, void* stream) {
+static GramGeom gram_geom(const int nr[3], const double lat[3][3]) {
   GramGeom g;
   double len[3];
   for (int d = 0; d < 3; ++d) {
@@ -555,8 +556,36 @@ int launch_mlwf_gram(int precision, const void* psi, long ld, int M, long N, con
   // theta_d / pi = 2 r_d / |a_d|, r = sum_j f_j a_j
   for (int d = 0; d < 3; ++d)
     for (int j = 0; j < 3; ++j) g.frac_to_theta[d][j] = 2.0 * lat[j][d] / len[d];
-  return precision == INQB_FP64 ? gram_impl<double>(psi, ld, M, N, g, sums, partial, a, (cudaStream_t)stream)
-                                : gram_impl<float>(psi, ld, M, N, g, sums, partial, a, (cudaStream_t)stream);
+  return g;
+}
+
+int launch_mlwf_gram(int precision, const void* psi, long ld, int M, long N, const int nr[3], const double lat[3][3],
+                     const double* sums, void* partial, double2* a, void* stream) {
+  const GramGeom g = gram_geom(nr, lat);
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* Z = nullptr;
+  INQB_TRY(precision == INQB_FP64 ? gram_impl<double>(psi, ld, M, psi, ld, M, N, g, partial, &Z, st)
+                                  : gram_impl<float>(psi, ld, M, psi, ld, M, N, g, partial, &Z, st));
+  return launch_mlwf_finish(Z, M, sums, 3, a, stream);
+}
+
+int launch_mlwf_gram_block(int precision, const void* pa, long lda, int Ma, const void* pb, long ldb, int Mb, long N,
+                           const int nr[3], const double lat[3][3], void* partial, double2* Z, void* stream) {
+  const GramGeom g = gram_geom(nr, lat);
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* Zw = nullptr;
+  INQB_TRY(precision == INQB_FP64 ? gram_impl<double>(pa, lda, Ma, pb, ldb, Mb, N, g, partial, &Zw, st)
+                                  : gram_impl<float>(pa, lda, Ma, pb, ldb, Mb, N, g, partial, &Zw, st));
+  INQB_CUDA_TRY(cudaMemcpyAsync(Z, Zw, sizeof(double2) * 3 * (size_t)Ma * Mb, cudaMemcpyDeviceToDevice, st));
+  return INQB_OK;
+}
+
+int launch_mlwf_finish(const double2* Z, int M, const double* norms, int norm_stride, double2* a, void* stream) {
+  const long work = 3L * M * M;
+  k_mlwf_finish<<<(unsigned)std::min<long>((work + 255) / 256, 148L * 8), 256, 0, (cudaStream_t)stream>>>(
+      Z, M, norms, norm_stride, a);
+  INQB_CUDA_TRY(cudaGetLastError());
+  return INQB_OK;
 }
 
 int launch_identity(double2* u, int M, void* stream) {

@@ -64,6 +64,11 @@ SIGNATURES = {
     "inqb_set_projection_mode": (ctypes.c_int, [_ctxp, ctypes.c_int]),
     "inqb_device_status": (ctypes.c_int, [_ctxp, _vp]),
     "inqb_timing_passes": (ctypes.c_int, [_ctxp, _dp, _ip]),
+    "inqb_mlwf_gram_block": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
+                                            _vp, _vp]),
+    "inqb_mlwf_finish": (ctypes.c_int, [_ctxp, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "inqb_orbital_norms": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "inqb_mlwf_centres": (ctypes.c_int, [_ctxp, ctypes.c_int, _dp, _dp, _dp]),
     "inqb_overlap_block": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
                                           _vp, ctypes.c_int, _vp]),
     "inqb_cholesky_inverse": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, _vp]),

@@ -633,6 +633,43 @@ class KSHamiltonian:
         call("inqb_orthonormalize", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), self._stream())
         return psi
 
+    # -- the pieces of an orbital-sharded TD-MLWF step (parallel.sharded_mlwf_step_)
+    def mlwf_gram_block(self, a, b) -> torch.Tensor:
+        """Z [3, Ma, Mb] complex128: sum_p conj(a_m) e^{i 2 pi r_d / |a_d|} b_n."""
+        a = self._check(a)
+        b = self._check(b)
+        Z = torch.empty((3, a.shape[1], b.shape[1]), dtype=torch.complex128, device=a.device)
+        call("inqb_mlwf_gram_block", self._h, a.data_ptr(), a.shape[1], a.stride(0), b.data_ptr(), b.shape[1],
+             b.stride(0), Z.data_ptr(), self._stream())
+        return Z
+
+    def mlwf_finish(self, Z: torch.Tensor, norms: torch.Tensor) -> torch.Tensor:
+        """The six [M, M] matrices of tdmlwf_trans::update from the summed Z [3, M, M]
+        and the orbital norms sum_p |psi_m|^2 (FP64 [M])."""
+        Z = Z.contiguous()
+        norms = norms.to(torch.float64).contiguous()
+        M = Z.shape[1]
+        a = torch.empty((6, M, M), dtype=torch.complex128, device=Z.device)
+        call("inqb_mlwf_finish", self._h, M, Z.data_ptr(), norms.data_ptr(), a.data_ptr(), self._stream())
+        return a
+
+    def orbital_norms(self, psi) -> torch.Tensor:
+        """sum_p |psi_m|^2 (FP64 [M] on the device)."""
+        psi = self._check(psi)
+        out = torch.empty(psi.shape[1], dtype=torch.float64, device=psi.device)
+        call("inqb_orbital_norms", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), out.data_ptr(),
+             self._stream())
+        return out
+
+    def mlwf_centres(self, adiag):
+        """(centres [M, 3], spreads [M]) from adiag [6, M] (tdmlwf_trans::center / spread2)."""
+        ad = np.ascontiguousarray(torch.as_tensor(adiag).cpu().numpy(), np.complex128)
+        M = ad.shape[1]
+        c = np.zeros((M, 3))
+        sp = np.zeros(M)
+        call("inqb_mlwf_centres", self._h, M, dptr(ad.view(np.float64)), dptr(c), dptr(sp))
+        return c, sp
+
     # -- the pieces of an orbital-sharded orthonormalisation (parallel.sharded_orthonormalize_)
     def overlap_block(self, a, b) -> torch.Tensor:
         """dV a^H b in FP64: a [N, Ma], b [N, Mb] -> complex128 [Ma, Mb] on the device

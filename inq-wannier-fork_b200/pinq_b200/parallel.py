@@ -149,6 +149,17 @@ def sharded_orthonormalize_(ham, psi_local, group=None):
 
     S, counts = sharded_overlap(ham, psi_local, group)
     ham.cholesky_inverse_(S)
+    return _sharded_rotate_(ham, psi_local, S, counts, group)
+
+
+def _sharded_rotate_(ham, psi_local, R, counts, group=None):
+    """psi <- psi R for orbitals split in blocks (counts per rank), R [Mt, Mt] the same
+    on every rank: each rank multiplies its block by its rows of R for every rank's
+    columns, and those terms are summed on the owner (operations::rotate's
+    set-parallel branch, src/operations/rotate.hpp:100-125)."""
+    import torch
+    import torch.distributed as dist
+
     world = len(counts)
     rank = dist.get_rank(group) if world > 1 else 0
     starts = [sum(counts[:i]) for i in range(world)]
@@ -159,7 +170,7 @@ def sharded_orthonormalize_(ham, psi_local, group=None):
             continue
         cols = slice(starts[s], starts[s] + counts[s])
         if counts[rank] > 0:
-            part = ham.rotate_block(psi_local, S[r0:r1, cols])
+            part = ham.rotate_block(psi_local, R[r0:r1, cols])
         else:
             part = torch.zeros((psi_local.shape[0], counts[s]), dtype=psi_local.dtype, device=psi_local.device)
         if world > 1:
@@ -169,3 +180,44 @@ def sharded_orthonormalize_(ham, psi_local, group=None):
     if mine is not None:
         psi_local.copy_(mine)
     return psi_local
+
+
+def sharded_mlwf_step_(ham, psi_local, group=None, maxsweep=100, tol=1e-8):
+    """mlwf_properties::calculate (src/observables/mlwf_properties.hpp:28-44) for
+    orbitals split over ranks in blocks.  The three weighted Gram matrices
+    Z_d = Psi^H diag(e^{i 2 pi r_d / |a_d|}) Psi are formed block by block as the
+    orbital blocks circulate around the ranks (as sharded_overlap does), then summed
+    by an all-reduce; the norms are gathered the same way.  Every rank then forms the
+    six matrices of tdmlwf_trans::update and runs JADE on the same summed input, so
+    every rank holds the same rotation u, and Psi <- Psi u^H is summed on the owners.
+    (The reference splits the basis instead and all-reduces the matrices over it,
+    src/wannier/tdmlwf_trans.hpp:96-172.)  ham provides mlwf_gram_block, orbital_norms,
+    mlwf_finish, jade, rotate_block and mlwf_centres (KSHamiltonian does, through the C
+    ABI).  psi_local is rotated in place; returns (centres [Mt, 3], spreads [Mt], sweeps)."""
+    import torch
+    import torch.distributed as dist
+
+    counts = _block_counts(psi_local.shape[1], psi_local.device, group)
+    starts = [sum(counts[:i]) for i in range(len(counts))]
+    world = len(counts)
+    rank = dist.get_rank(group) if world > 1 else 0
+    Mt = sum(counts)
+    Z = torch.zeros((3, Mt, Mt), dtype=torch.complex128, device=psi_local.device)
+    c0, c1 = starts[rank], starts[rank] + counts[rank]
+    blk, src = psi_local, rank
+    for step in range(world):
+        if counts[src] > 0 and counts[rank] > 0:
+            Z[:, starts[src]:starts[src] + counts[src], c0:c1] = ham.mlwf_gram_block(blk, psi_local)
+        if step < world - 1:
+            src = (src - 1) % world
+            blk = _ring_shift(blk, counts[src], group)
+    allreduce_sum_(torch.view_as_real(Z), group)
+    norms = torch.zeros(Mt, dtype=torch.float64, device=psi_local.device)
+    if counts[rank] > 0:
+        norms[c0:c1] = ham.orbital_norms(psi_local)
+    allreduce_sum_(norms, group)
+    a = ham.mlwf_finish(Z, norms)
+    u, adiag, sweeps = ham.jade(a, maxsweep, tol)
+    _sharded_rotate_(ham, psi_local, u.conj().T.contiguous(), counts, group)
+    centres, spreads = ham.mlwf_centres(adiag)
+    return centres, spreads, sweeps

@@ -111,3 +111,43 @@ def test_jade_rejects_non_finite_matrices(pb):
     with pytest.raises(pb.InqbError) as e:
         h.jade(a, maxsweep=100)
     assert e.value.status == 5  # INQB_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-5)])
+def test_sharded_mlwf_pieces_equal_whole_step(pb, oracle_mod, precision, tol):
+    """The orbital-sharded TD-MLWF step's device pieces through the C ABI
+    (inqb_mlwf_gram_block, inqb_orbital_norms, inqb_mlwf_finish, inqb_jade,
+    inqb_rotate_block, inqb_mlwf_centres) with two ranks' blocks emulated in one
+    process: every (row block, column block) of the Gram matrices as the circulation
+    forms it, the rotation terms summed per owner.  Equals inqb_mlwf_step on all
+    orbitals.  The exchange itself runs over gloo in tests/test_parallel_gloo.py."""
+    o, psi, lat = gaussian_states(oracle_mod, seed=3)
+    h = _ham(pb, precision)
+    dt = torch.complex128 if precision == "fp64" else torch.complex64
+    x = torch.as_tensor(psi).to(dt).cuda()
+    whole = x.clone()
+    c_ref, s_ref, sw_ref = h.mlwf_step_(whole)
+    blocks = [x[:, :4].contiguous(), x[:, 4:].contiguous()]
+    counts = [4, 2]
+    starts = [0, 4, 6]
+    Z = torch.zeros((3, 6, 6), dtype=torch.complex128, device="cuda")
+    for q in range(2):
+        for r in range(2):
+            Z[:, starts[q]:starts[q + 1], starts[r]:starts[r + 1]] = h.mlwf_gram_block(blocks[q], blocks[r])
+    norms = torch.cat([h.orbital_norms(b) for b in blocks])
+    a = h.mlwf_finish(Z, norms)
+    u, adiag, sweeps = h.jade(a)
+    R = u.conj().T.contiguous()
+    out = []
+    for s in range(2):
+        acc = None
+        for r in range(2):
+            part = h.rotate_block(blocks[r], R[starts[r]:starts[r + 1], starts[s]:starts[s + 1]])
+            acc = part if acc is None else acc + part
+        out.append(acc)
+    got = torch.cat(out, 1)
+    centres, spreads = h.mlwf_centres(adiag)
+    assert sweeps == sw_ref
+    assert np.abs(centres - c_ref).max() < tol and np.abs(spreads - s_ref).max() < tol
+    assert rel_max(got.cpu().numpy(), whole.cpu().numpy()) < (tol if precision == "fp64" else 1e-5)
+    del counts

@@ -166,3 +166,110 @@ def test_sharded_orthonormalize_equals_whole_block(tmp_path, world, M):
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
     ovl = ops.dV * got.conj().T @ got
     assert np.abs(ovl - np.eye(M)).max() < 1e-12
+
+
+class _TorchMlwf(_TorchBlocks):
+    """The TD-MLWF block operations of KSHamiltonian that sharded_mlwf_step_ calls, in
+    torch FP64 on the CPU (the oracle's JADE and centre formulas)."""
+
+    lattice = np.diag([5.0, 6.0, 7.0])
+    nr = (6, 6, 6)
+
+    def _weights(self):
+        sym = [np.where(np.arange(n) >= (n + 1) // 2, np.arange(n) - n, np.arange(n)) / n for n in self.nr]
+        f = np.stack(np.meshgrid(*sym, indexing="ij"), -1).reshape(-1, 3)
+        L = self.lattice
+        r = f @ L
+        th = 2 * np.pi * r / np.linalg.norm(L, axis=1)[None, :]
+        return torch.tensor(np.exp(1j * th))  # [N, 3]
+
+    def mlwf_gram_block(self, a, b):
+        w = self._weights()
+        return torch.stack([a.conj().T @ (w[:, d:d + 1] * b) for d in range(3)])
+
+    def orbital_norms(self, psi):
+        return (psi.abs() ** 2).sum(0).to(torch.float64)
+
+    def mlwf_finish(self, Z, norms):
+        sc = 1.0 / torch.sqrt(norms[:, None] * norms[None, :])
+        out = []
+        for d in range(3):
+            zh = Z[d].conj().T
+            out += [0.5 * sc * (Z[d] + zh), sc * (Z[d] - zh) / 2j]
+        return torch.stack(out)
+
+    def jade(self, a, maxsweep, tol):
+        import oracle
+
+        _, u, adiag, sw = oracle.jade(a.numpy(), maxsweep, tol)
+        return torch.tensor(u), torch.tensor(adiag), sw
+
+    def mlwf_centres(self, adiag):
+        import oracle
+
+        ad = adiag.numpy()
+        M = ad.shape[1]
+        return (np.array([oracle.mlwf_center(ad, i, self.lattice) for i in range(M)]),
+                np.array([oracle.mlwf_spread(ad, i, self.lattice) for i in range(M)]))
+
+
+def _mlwf_states(M):
+    rng = np.random.default_rng(5)
+    ops = _TorchMlwf()
+    N = int(np.prod(ops.nr))
+    # Gaussians at random points, mixed by a random unitary (JADE un-mixes them)
+    sym = [np.where(np.arange(n) >= (n + 1) // 2, np.arange(n) - n, np.arange(n)) / n for n in ops.nr]
+    f = np.stack(np.meshgrid(*sym, indexing="ij"), -1).reshape(-1, 3)
+    cols = []
+    for _ in range(M):
+        c = rng.uniform(-0.5, 0.5, 3)
+        d = (f - c + 0.5) % 1.0 - 0.5
+        r2 = ((d @ ops.lattice) ** 2).sum(1)
+        cols.append(np.exp(-r2 / 2.0))
+    psi = np.stack(cols, 1).astype(complex)
+    q, _ = np.linalg.qr(rng.standard_normal((M, M)) + 1j * rng.standard_normal((M, M)))
+    return torch.tensor(psi @ q), N
+
+
+def _mlwf_main(rank, world, port, M, out_dir):
+    import datetime
+
+    import torch.distributed as dist
+
+    from pinq_b200.parallel import sharded_mlwf_step_
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        psi, _ = _mlwf_states(M)
+        first, count = orbital_range(M, world, rank)
+        mine = psi[:, first:first + count].clone()
+        c, sp, sw = sharded_mlwf_step_(_TorchMlwf(), mine, maxsweep=30)
+        np.save(os.path.join(out_dir, f"c{rank}.npy"), c)
+        np.save(os.path.join(out_dir, f"sp{rank}.npy"), sp)
+        np.save(os.path.join(out_dir, f"psi{rank}.npy"), mine.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,M", [(2, 6), (3, 4)])
+def test_sharded_mlwf_step_equals_whole_block(tmp_path, oracle_mod, world, M):
+    """The orbital-sharded TD-MLWF step (Gram blocks circulated and all-reduced, the
+    norms summed, JADE on every rank, the rotation summed on the owners) equals the step
+    on all orbitals at once: centres, spreads and rotated orbitals."""
+    from pinq_b200.parallel import sharded_mlwf_step_
+
+    mp.start_processes(_mlwf_main, args=(world, _free_port(), M, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    psi, _ = _mlwf_states(M)
+    whole = psi.clone()
+    c_ref, sp_ref, _ = sharded_mlwf_step_(_TorchMlwf(), whole, maxsweep=30)
+    parts = []
+    for r in range(world):
+        assert np.allclose(np.load(tmp_path / f"c{r}.npy"), c_ref, rtol=0, atol=1e-10)
+        # (a spread of a few-point grid can be the square root of a small negative number)
+        assert np.allclose(np.load(tmp_path / f"sp{r}.npy"), sp_ref, rtol=0, atol=1e-10, equal_nan=True)
+        parts.append(np.load(tmp_path / f"psi{r}.npy"))
+    got = np.concatenate(parts, 1)
+    assert np.abs(got - whole.numpy()).max() <= 1e-10 * np.abs(whole.numpy()).max()
