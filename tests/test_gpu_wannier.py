@@ -128,7 +128,6 @@ def test_sharded_mlwf_pieces_equal_whole_step(pb, oracle_mod, precision, tol):
     whole = x.clone()
     c_ref, s_ref, sw_ref = h.mlwf_step_(whole)
     blocks = [x[:, :4].contiguous(), x[:, 4:].contiguous()]
-    counts = [4, 2]
     starts = [0, 4, 6]
     Z = torch.zeros((3, 6, 6), dtype=torch.complex128, device="cuda")
     for q in range(2):
@@ -150,4 +149,3 @@ def test_sharded_mlwf_pieces_equal_whole_step(pb, oracle_mod, precision, tol):
     assert sweeps == sw_ref
     assert np.abs(centres - c_ref).max() < tol and np.abs(spreads - s_ref).max() < tol
     assert rel_max(got.cpu().numpy(), whole.cpu().numpy()) < (tol if precision == "fp64" else 1e-5)
-    del counts
