@@ -245,7 +245,8 @@ def _timed_ms(fn, K, W):
 
 def bench_cells(args, local):
     """cfg3: 16 uneven cells (grids 24..48^3, 8..64 orbitals, 2..16 atoms), mixed
-    precision; one CUDA graph (one branch per cell) against cell-by-cell launches."""
+    precision; one CUDA graph (one branch per cell) and one persistent launch over a
+    device work queue, against cell-by-cell launches."""
     import torch
 
     import pinq_b200 as pb
@@ -262,26 +263,38 @@ def bench_cells(args, local):
         hams.append(h)
         xs.append(x)
         ys.append(torch.empty_like(x))
-    batch = pb.CellBatch(hams)
+    batch = pb.CellBatch(hams, mode="graph")
     K = max(20, args.steps // 4)
     ms_graph = _timed_ms(lambda: batch.apply(xs, ys), K, 3)
+    # the persistent form: one kernel over (cell, pass, tiles) work items from a device queue
+    pbatch = pb.CellBatch(hams, mode="persistent")
+    ms_pers = _timed_ms(lambda: pbatch.apply(xs, ys), K, 3)
+    pbatch.status()
+    pinfo = pbatch.info()
+    pbatch.close()
 
     def seq():
         for h, x, y in zip(hams, xs, ys):
             h.apply(x, y)
 
     ms_seq = _timed_ms(seq, K, 3)
-    # the same graph with every cell's launch schedule picked by the autotuner
+    # every cell's launch schedule picked by the autotuner, then the faster launch form
     t0 = time.perf_counter()
     scheds = batch.autotune([x.shape[1] for x in xs])
+    batch.set_mode("auto")
+    form, form_ms = batch.autotune_form(xs, ys)
     tune_s = time.perf_counter() - t0
     ms_tuned = _timed_ms(lambda: batch.apply(xs, ys), K, 3)
+    batch.status()
     norb = sum(x.shape[1] for x in xs)
     return {"ncells": len(hams), "grids": [h.nr[0] for h in hams], "orbitals": norb, "steps": K,
             "graph_orbital_applies_per_s": norb * K / (ms_graph * 1e-3),
+            "persistent_orbital_applies_per_s": norb * K / (ms_pers * 1e-3),
+            "persistent_work_items": pinfo["items"], "persistent_ctas": pinfo["ctas"],
             "sequential_orbital_applies_per_s": norb * K / (ms_seq * 1e-3),
             "graph_speedup": ms_seq / ms_graph,
-            "graph_autotuned_orbital_applies_per_s": norb * K / (ms_tuned * 1e-3),
+            "autotuned_form": form, "autotuned_form_ms": form_ms,
+            "autotuned_orbital_applies_per_s": norb * K / (ms_tuned * 1e-3),
             "autotune_speedup_over_default_graph": ms_graph / ms_tuned, "autotune_s": tune_s,
             "schedules": [list(sc) for sc in scheds], "precision": "mixed"}
 

@@ -141,6 +141,35 @@ int inqb_batch_create(inqb_ctx* const* cells, int ncells, inqb_batch** out);
 int inqb_batch_destroy(inqb_batch* batch);
 int inqb_batch_apply_h(inqb_batch* batch, const void* const* psis, void* const* hpsis, const int* Ms,
                        const int* lds, void* stream);
+/* The launch form of inqb_batch_apply_h.  PERSISTENT: one launch of a persistent
+ * kernel whose CTAs take work items (cell, pass, tiles) from a device queue and wait,
+ * with a time limit, for the items each depends on; the cells (at most 64) must share
+ * one precision, have cubic grids of 16, 20, 24, 32, 40 or 48 points and use the
+ * fused projection (INQB_ERR_UNSUPPORTED otherwise).  GRAPH: the CUDA graph above.
+ * AUTO (the default): the form inqb_batch_autotune picked, GRAPH before it ran (and
+ * where the cells do not fit the persistent kernel).  Takes effect at the next apply. */
+enum inqb_batch_mode { INQB_BATCH_AUTO = 0, INQB_BATCH_GRAPH = 1, INQB_BATCH_PERSISTENT = 2 };
+int inqb_batch_set_mode(inqb_batch* batch, int mode);
+/* Times both forms on these arguments (2 untimed and 5 timed applies each, CUDA
+ * events on stream) and makes the faster the one AUTO runs.  form (optional): the
+ * pick; ms (optional, [2]): milliseconds per apply of GRAPH and PERSISTENT (-1 where
+ * the cells do not fit the persistent kernel).  Synchronous; the outputs hold H psi. */
+int inqb_batch_autotune(inqb_batch* batch, const void* const* psis, void* const* hpsis, const int* Ms,
+                        const int* lds, void* stream, int* form, double* ms);
+/* The form the last inqb_batch_apply_h set up (INQB_BATCH_GRAPH, INQB_BATCH_PERSISTENT,
+ * or 0 before the first), and for the persistent form its work items and CTAs. */
+int inqb_batch_info(inqb_batch* batch, int* form, int* nitems, int* ctas);
+/* Synchronises stream and returns INQB_ERR_TIMEOUT when a device-side wait of a
+ * persistent launch gave up since the last call (that launch stopped early and its
+ * outputs are not valid; the batch and its contexts stay usable), else INQB_OK. */
+int inqb_batch_status(inqb_batch* batch, void* stream);
+/* Time limit of one device-side wait of the persistent launch, in (0, 60] seconds
+ * (default 2). */
+int inqb_batch_set_wait_limit(inqb_batch* batch, double seconds);
+/* Test hook: when on, one work item of the next persistent plan waits for a count
+ * that no item reaches, so that wait runs out after the limit above and the launch
+ * reports INQB_ERR_TIMEOUT through inqb_batch_status. */
+int inqb_batch_test_unreachable_wait(inqb_batch* batch, int on);
 
 /* ---------------------------------------------------------------- propagation
  * operations::exponential_in_place (src/operations/exponential.hpp:21-34):

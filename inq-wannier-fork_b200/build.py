@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
               "-Xptxas", "-warn-spills", "-I" + INCLUDE, "-I" + CSRC]
 SOURCES = ["grids_144.cu", "grids_128.cu", "grids_96.cu", "grids_72.cu", "grids_64.cu", "grids_mid.cu", "grids_small.cu",
-           "hamiltonian.cu", "project.cu", "observables.cu", "adjoint.cu", "propagators.cu", "potential.cu", "checkpoint.cu", "wannier.cu", "setup.cpp", "capi.cpp"]
+           "hamiltonian.cu", "batch.cu", "project.cu", "observables.cu", "adjoint.cu", "propagators.cu", "potential.cu", "checkpoint.cu", "wannier.cu", "setup.cpp", "capi.cpp"]
 
 
 def nvcc() -> str:

@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 
+#include "batch.h"
 #include "inqb_internal.h"
 #include "broyden_host.h"
 #include "adjoint.h"
@@ -130,7 +131,8 @@ int set_kA(inqb_ctx* ctx, const double kA[3], void* stream) {
 
 // One H application: out = alpha * H in + beta * base.
 int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long ld_out, int M, const void* base,
-          long ld_base, const double alpha[2], const double beta[2], void* stream, void* fourier_out = nullptr) {
+          long ld_base, const double alpha[2], const double beta[2], void* stream, void* fourier_out = nullptr,
+          BatchCellDesc* batch_cell = nullptr) {
   INQB_TRY(reserve(ctx, M));
   if (!ctx->proj_phases_valid) {
     INQB_TRY(update_phases(ctx, stream));
@@ -154,6 +156,7 @@ int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long l
   a.beta[1] = beta[1];
   a.stream = stream;
   a.fourier_out = fourier_out;
+  a.batch_cell = batch_cell;
   a.fourier_mask = ctx->fourier_mask;
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) a.rlat[i][j] = ctx->cell.rlat[i][j];
@@ -168,7 +171,7 @@ int apply(inqb_ctx* ctx, int mode, const void* in, long ld_in, void* out, long l
     const int ys = a.ysplit > 0 ? a.ysplit : ctx->plan->ysplit;
     INQB_TRY(ctx->d_slots.ensure(sizeof(double2) * (size_t)ctx->proj.aslot.size() * ys * 4 * M));
   }
-  if (ctx->timing_on && mode == LaunchArgs::H && ctx->timing_count < ctx->timing_capacity) {
+  if (ctx->timing_on && mode == LaunchArgs::H && !batch_cell && ctx->timing_count < ctx->timing_capacity) {
     for (int i = 0; i < 6; i++) a.events[i] = ctx->timing_events[6 * ctx->timing_count + i];
     ctx->timing_count++;
   }
@@ -505,10 +508,23 @@ struct inqb_batch {
   std::vector<cudaEvent_t> events;    // [0] fork, [1..n] joins
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  // arguments the instantiated graph was built with
+  // arguments the instantiated graph or the persistent plan was built with
   std::vector<const void*> psis;
   std::vector<void*> hpsis;
   std::vector<int> Ms, lds;
+  // the persistent launch (batch.h)
+  int mode = INQB_BATCH_AUTO;
+  int tuned = INQB_BATCH_GRAPH;  // the form AUTO runs: GRAPH until inqb_batch_autotune picks
+  bool ready = false;        // a graph or a persistent plan matches the recorded arguments
+  bool persistent = false;   // the recorded arguments run as one persistent launch
+  int precision = INQB_FP64;
+  int nitems = 0, ncounters = 0, ctas = 0;
+  size_t smem = 0;
+  double wait_s = 2.0;
+  int unreachable = 0;       // test hook: one stage-C item waits for a count no item reaches
+  std::vector<unsigned char> cells_blob;  // the cells' kernel descriptors (kernel parameters)
+  size_t cell_bytes = 0;
+  inqb::DevBuf d_items, d_ctr, d_err;
 };
 
 namespace inqb {
@@ -519,6 +535,50 @@ void batch_release_graph(inqb_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
+}
+
+// The work list and device descriptors of one persistent launch for these arguments;
+// INQB_ERR_UNSUPPORTED when a cell cannot run in it (grid not compiled into the
+// kernel, projection kernel form, cells of both precisions).
+int batch_build_persistent(inqb_batch* b, const void* const* psis, void* const* hpsis, const int* Ms,
+                           const int* lds) {
+  const int n = (int)b->cells.size();
+  const int prec = b->cells[0]->precision;
+  if (n > kMaxBatchCells) return fail(INQB_ERR_UNSUPPORTED, "more cells than one persistent launch takes");
+  std::vector<BatchCellDesc> descs(n);
+  size_t smem = 0;
+  const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+  for (int i = 0; i < n; i++) {
+    if (b->cells[i]->precision != prec) return fail(INQB_ERR_UNSUPPORTED, "cells of both precisions in one batch");
+    INQB_TRY(apply(b->cells[i], LaunchArgs::H, psis[i], lds[i], hpsis[i], lds[i], Ms[i], nullptr, 0, one, zero,
+                   nullptr, nullptr, &descs[i]));
+    smem = std::max(smem, descs[i].smem);
+  }
+  int per_sm = 0, sms = 0;
+  INQB_TRY(batch_ctas_per_sm(prec, smem, &per_sm));
+  INQB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+  std::vector<BatchItem> items;
+  int nctr = 0;
+  INQB_TRY(build_batch_items(descs, per_sm * sms, items, nctr));
+  if (b->unreachable)
+    for (auto& it : items)
+      if (it.stage == kStageC) {
+        it.target += 1;
+        break;
+      }
+  const size_t csz = descs[0].bytes.size();
+  b->cell_bytes = csz;
+  b->cells_blob.assign(csz * n, 0);
+  for (int i = 0; i < n; i++) memcpy(b->cells_blob.data() + (size_t)i * csz, descs[i].bytes.data(), csz);
+  INQB_TRY(b->d_items.ensure(sizeof(BatchItem) * items.size()));
+  INQB_TRY(b->d_ctr.ensure(sizeof(unsigned) * (size_t)nctr));
+  INQB_CUDA_TRY(cudaMemcpy(b->d_items.ptr, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice));
+  b->precision = prec;
+  b->nitems = (int)items.size();
+  b->ncounters = nctr;
+  b->smem = smem;
+  b->ctas = std::min(per_sm * sms, b->nitems);
+  return INQB_OK;
 }
 
 int batch_capture(inqb_batch* b, const void* const* psis, void* const* hpsis, const int* Ms, const int* lds) {
@@ -548,10 +608,6 @@ int batch_capture(inqb_batch* b, const void* const* psis, void* const* hpsis, co
   batch_release_graph(b);
   b->graph = g;
   INQB_CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
-  b->psis.assign(psis, psis + n);
-  b->hpsis.assign(hpsis, hpsis + n);
-  b->Ms.assign(Ms, Ms + n);
-  b->lds.assign(lds, lds + n);
   return INQB_OK;
 }
 
@@ -1491,6 +1547,10 @@ int inqb_batch_create(inqb_ctx* const* cells, int ncells, inqb_batch** out) {
   auto* b = new inqb_batch();
   b->cells.assign(cells, cells + ncells);
   b->device = cells[0]->device;
+  if (b->d_err.ensure(sizeof(int)) != INQB_OK || cudaMemset(b->d_err.ptr, 0, sizeof(int)) != cudaSuccess) {
+    delete b;
+    return fail(INQB_ERR_NOMEM, "batch error word");
+  }
   for (int i = 0; i <= ncells; i++) {
     cudaStream_t s;
     cudaEvent_t e;
@@ -1529,10 +1589,12 @@ int inqb_batch_apply_h(inqb_batch* b, const void* const* psis, void* const* hpsi
   }
   DeviceGuard guard(b->device);
   if (guard.status != INQB_OK) return guard.status;
-  bool same = b->exec != nullptr;
+  bool same = b->ready;
   for (int i = 0; i < n && same; i++)
     same = b->psis[i] == psis[i] && b->hpsis[i] == hpsis[i] && b->Ms[i] == Ms[i] && b->lds[i] == lds[i];
   if (!same) {
+    b->ready = false;
+    b->persistent = false;
     // workspace, attributes and phases are set up outside the capture
     for (int i = 0; i < n; i++) {
       INQB_TRY(reserve(b->cells[i], Ms[i]));
@@ -1545,9 +1607,126 @@ int inqb_batch_apply_h(inqb_batch* b, const void* const* psis, void* const* hpsi
                      nullptr));
     }
     INQB_CUDA_TRY(cudaDeviceSynchronize());
-    INQB_TRY(batch_capture(b, psis, hpsis, Ms, lds));
+    batch_release_graph(b);
+    const int form = b->mode == INQB_BATCH_AUTO ? b->tuned : b->mode;
+    if (form == INQB_BATCH_PERSISTENT) {
+      const int st = batch_build_persistent(b, psis, hpsis, Ms, lds);
+      if (st == INQB_OK)
+        b->persistent = true;
+      else if (b->mode == INQB_BATCH_PERSISTENT || st != INQB_ERR_UNSUPPORTED)
+        return st;  // AUTO falls back to the graph where the cells do not fit the kernel
+    }
+    if (!b->persistent) INQB_TRY(batch_capture(b, psis, hpsis, Ms, lds));
+    b->psis.assign(psis, psis + n);
+    b->hpsis.assign(hpsis, hpsis + n);
+    b->Ms.assign(Ms, Ms + n);
+    b->lds.assign(lds, lds + n);
+    b->ready = true;
   }
+  if (b->persistent)
+    return launch_batch(b->precision, b->cells_blob.data(), n, b->cell_bytes, b->d_items.as<BatchItem>(), b->nitems,
+                        b->d_ctr.as<unsigned>(), b->ncounters, b->d_err.as<int>(), (long long)(b->wait_s * 1e9),
+                        b->ctas, b->smem, stream);
   INQB_CUDA_TRY(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+  return INQB_OK;
+}
+
+int inqb_batch_set_mode(inqb_batch* b, int mode) {
+  if (!b) return fail(INQB_ERR_INVALID, "null batch");
+  if (mode != INQB_BATCH_AUTO && mode != INQB_BATCH_GRAPH && mode != INQB_BATCH_PERSISTENT)
+    return fail(INQB_ERR_INVALID, "unknown batch mode");
+  b->mode = mode;
+  b->ready = false;
+  return INQB_OK;
+}
+
+int inqb_batch_autotune(inqb_batch* b, const void* const* psis, void* const* hpsis, const int* Ms, const int* lds,
+                        void* stream, int* form, double* ms) {
+  if (!b) return fail(INQB_ERR_INVALID, "null batch");
+  DeviceGuard guard(b->device);
+  if (guard.status != INQB_OK) return guard.status;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int saved = b->mode;
+  double t[2] = {-1.0, -1.0};
+  cudaEvent_t e0, e1;
+  INQB_CUDA_TRY(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(INQB_ERR_CUDA, "event creation failed");
+  }
+  int rc = INQB_OK;
+  const int forms[2] = {INQB_BATCH_GRAPH, INQB_BATCH_PERSISTENT};
+  for (int k = 0; k < 2 && rc == INQB_OK; k++) {
+    b->mode = forms[k];
+    b->ready = false;
+    int r = inqb_batch_apply_h(b, psis, hpsis, Ms, lds, stream);  // builds the form
+    if (r == INQB_ERR_UNSUPPORTED && forms[k] == INQB_BATCH_PERSISTENT) continue;
+    if (r != INQB_OK) {
+      rc = r;
+      break;
+    }
+    constexpr int kWarm = 2, kTimed = 5;
+    for (int i = 0; i < kWarm && r == INQB_OK; i++) r = inqb_batch_apply_h(b, psis, hpsis, Ms, lds, stream);
+    if (r == INQB_OK && cudaEventRecord(e0, st) != cudaSuccess) r = fail(INQB_ERR_CUDA, "event record");
+    for (int i = 0; i < kTimed && r == INQB_OK; i++) r = inqb_batch_apply_h(b, psis, hpsis, Ms, lds, stream);
+    if (r == INQB_OK && cudaEventRecord(e1, st) != cudaSuccess) r = fail(INQB_ERR_CUDA, "event record");
+    if (r == INQB_OK && cudaEventSynchronize(e1) != cudaSuccess) r = fail(INQB_ERR_CUDA, "event sync");
+    float el = 0.f;
+    if (r == INQB_OK && cudaEventElapsedTime(&el, e0, e1) != cudaSuccess) r = fail(INQB_ERR_CUDA, "elapsed time");
+    if (r == INQB_OK && forms[k] == INQB_BATCH_PERSISTENT) r = inqb_batch_status(b, stream);
+    if (r != INQB_OK) {
+      rc = r;
+      break;
+    }
+    t[k] = el / kTimed;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->mode = saved;
+  b->ready = false;
+  if (rc != INQB_OK) return rc;
+  b->tuned = (t[1] > 0.0 && t[1] < t[0]) ? INQB_BATCH_PERSISTENT : INQB_BATCH_GRAPH;
+  if (form) *form = b->tuned;
+  if (ms) {
+    ms[0] = t[0];
+    ms[1] = t[1];
+  }
+  return INQB_OK;
+}
+
+int inqb_batch_info(inqb_batch* b, int* form, int* nitems, int* ctas) {
+  if (!b) return fail(INQB_ERR_INVALID, "null batch");
+  if (form) *form = !b->ready ? 0 : (b->persistent ? INQB_BATCH_PERSISTENT : INQB_BATCH_GRAPH);
+  if (nitems) *nitems = b->persistent ? b->nitems : 0;
+  if (ctas) *ctas = b->persistent ? b->ctas : 0;
+  return INQB_OK;
+}
+
+int inqb_batch_status(inqb_batch* b, void* stream) {
+  if (!b) return fail(INQB_ERR_INVALID, "null batch");
+  DeviceGuard guard(b->device);
+  if (guard.status != INQB_OK) return guard.status;
+  cudaStream_t st = (cudaStream_t)stream;
+  int word = 0;
+  INQB_CUDA_TRY(cudaMemcpyAsync(&word, b->d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  INQB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (word == 0) return INQB_OK;
+  INQB_CUDA_TRY(cudaMemsetAsync(b->d_err.ptr, 0, sizeof(int), st));
+  INQB_CUDA_TRY(cudaStreamSynchronize(st));
+  return fail(INQB_ERR_TIMEOUT, "a device-side wait of the persistent batch launch gave up (its results are not valid)");
+}
+
+int inqb_batch_set_wait_limit(inqb_batch* b, double seconds) {
+  if (!b) return fail(INQB_ERR_INVALID, "null batch");
+  if (!(seconds > 0.0) || seconds > 60.0) return fail(INQB_ERR_INVALID, "wait limit must be in (0, 60] seconds");
+  b->wait_s = seconds;
+  return INQB_OK;
+}
+
+int inqb_batch_test_unreachable_wait(inqb_batch* b, int on) {
+  if (!b) return fail(INQB_ERR_INVALID, "null batch");
+  b->unreachable = on ? 1 : 0;
+  b->ready = false;
   return INQB_OK;
 }
 

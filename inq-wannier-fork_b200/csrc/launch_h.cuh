@@ -15,10 +15,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <tuple>
 
+#include "batch.h"
 #include "fft_tile.cuh"
 #include "inqb_internal.h"
 #include "plan.h"
@@ -73,6 +75,22 @@ struct EpiParams {
   const cplx<T>* base;      // optional [N][ld_base]
   long ld_base;
   cplx<T> alpha, beta;      // out = alpha * H in + beta * base
+};
+
+// One cell of the persistent batch launch (batch.h): every argument the three tile
+// passes of its H apply take, as launch_h_impl derives them.
+template <typename T>
+struct BatchCell {
+  const cplx<T>* in;
+  long ld_in;
+  cplx<T>* out;
+  long ld_out;
+  int M, ysplit, acc_cap, rec_cap_a, rec_cap_inv, seg_cap, vin, vio;
+  cplx<T>* tmp;
+  const cplx<T>* tw;  // x | y | z twiddles
+  ProjView<T> pj;
+  KinParams<T> kp;
+  EpiParams<T> ep;
 };
 
 }  // namespace inqb
@@ -171,6 +189,55 @@ int launch_h_impl(const LaunchArgs& a) {
     const int rec_cap_a = (TG::smem_fwd(acc_cap, rec_cap_fwd) > TG::SMEM_MAX) ? 0 : rec_cap_fwd;
     if (pj.nproj > 0 && pj.pt_stride != TG::PSTRIDE)
       return fail(INQB_ERR_INVALID, "projector tables were built for another tiling of this grid");
+    EpiParams<T> ep;
+    ep.V = (const T*)a.V;
+    ep.vshift = a.fourier_mask ? (T)(0.5 * kA2) : (T)0;
+    ep.base = (const cplx<T>*)a.base;
+    ep.ld_base = a.ld_base;
+    ep.alpha = mk<T>((T)a.alpha[0], (T)a.alpha[1]);
+    ep.beta = mk<T>((T)a.beta[0], (T)a.beta[1]);
+    // pass C stages the records in shared memory only in FP64 (where the orbital
+    // prefetch already limits it to two CTAs per SM); in FP32 the smem is worth more
+    // as a fourth CTA per SM, and the epilogue prefetches records into registers
+    int rec_cap_inv = TG::PREFETCH ? rec_cap : 0;
+    if (TG::smem_inv(rec_cap_inv, seg_cap) > TG::SMEM_MAX) rec_cap_inv = 0;
+    if (TG::smem_inv(rec_cap_inv, seg_cap) > TG::SMEM_MAX)
+      return fail(INQB_ERR_UNSUPPORTED, "tile of this grid does not fit in shared memory");
+    if (a.batch_cell) {
+      // describe the apply for the persistent batch launch instead of launching it
+      auto* d = reinterpret_cast<BatchCellDesc*>(a.batch_cell);
+      d->kind = batch_kind(NX, NY, NZ);
+      if (d->kind < 0) return fail(INQB_ERR_UNSUPPORTED, "grid not compiled into the persistent batch kernel");
+      if (sep || (pj.nproj > 0 && pj.slots == nullptr) || a.fourier_out || a.base)
+        return fail(INQB_ERR_UNSUPPORTED, "the persistent batch launch runs the fused projection only");
+      BatchCell<T> c;
+      c.in = (const cplx<T>*)a.in;
+      c.ld_in = a.ld_in;
+      c.out = (cplx<T>*)a.out;
+      c.ld_out = a.ld_out;
+      c.M = a.M;
+      c.ysplit = ysplit;
+      c.acc_cap = acc_cap;
+      c.rec_cap_a = rec_cap_a;
+      c.rec_cap_inv = rec_cap_inv;
+      c.seg_cap = seg_cap;
+      c.vin = vin;
+      c.vio = vin && vout;
+      c.tmp = tmp;
+      c.tw = tw;
+      c.pj = pj;
+      c.kp = kp;
+      c.ep = ep;
+      d->groups = tgroups;
+      d->a_per = NX * ysplit;
+      d->b_per = TG::Y2 * NZ;
+      d->c_per = NX * TG::Y1;
+      d->finish = pj.nproj > 0 ? 1 : 0;
+      d->smem = std::max({TG::smem_fwd(acc_cap, rec_cap_a), TG::SMEM_X, TG::smem_inv(rec_cap_inv, seg_cap)});
+      d->bytes.resize(sizeof(c));
+      memcpy(d->bytes.data(), &c, sizeof(c));
+      return INQB_OK;
+    }
     if (a.events[0]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[0], st));
     if (sep) {
       INQB_TRY(launch_project(sizeof(T) == 8 ? INQB_FP64 : INQB_MIXED, a.in, a.ld_in, a.M, pj.nproj, pj.L,
@@ -190,20 +257,6 @@ int launch_h_impl(const LaunchArgs& a) {
     k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out, fin, a.M,
                                                              ysplit);
     if (a.events[4]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[4], st));
-    EpiParams<T> ep;
-    ep.V = (const T*)a.V;
-    ep.vshift = a.fourier_mask ? (T)(0.5 * kA2) : (T)0;
-    ep.base = (const cplx<T>*)a.base;
-    ep.ld_base = a.ld_base;
-    ep.alpha = mk<T>((T)a.alpha[0], (T)a.alpha[1]);
-    ep.beta = mk<T>((T)a.beta[0], (T)a.beta[1]);
-    // pass C stages the records in shared memory only in FP64 (where the orbital
-    // prefetch already limits it to two CTAs per SM); in FP32 the smem is worth more
-    // as a fourth CTA per SM, and the epilogue prefetches records into registers
-    int rec_cap_inv = TG::PREFETCH ? rec_cap : 0;
-    if (TG::smem_inv(rec_cap_inv, seg_cap) > TG::SMEM_MAX) rec_cap_inv = 0;
-    if (TG::smem_inv(rec_cap_inv, seg_cap) > TG::SMEM_MAX)
-      return fail(INQB_ERR_UNSUPPORTED, "tile of this grid does not fit in shared memory");
     k_tile_inv<T, NX, NY, NZ, 1><<<ginv, thr[2], TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
         tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv, seg_cap,
         vin && vout);

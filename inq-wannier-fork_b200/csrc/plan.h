@@ -33,6 +33,9 @@ struct LaunchArgs {
   // optional, H mode: forward 3-D coefficients of `in` (before the kinetic factor) in
   // the tile layout [g][ka][kz][kx][kb][G] (groups padded to G orbitals)
   void* fourier_out = nullptr;
+  // H mode: when set (a BatchCellDesc*, batch.h), describe the apply for the
+  // persistent batch launch instead of launching it
+  void* batch_cell = nullptr;
 };
 
 // Candidate values the autotuner tries.

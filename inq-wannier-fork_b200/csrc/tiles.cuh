@@ -36,6 +36,19 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
 }
 
+// Loads of data another CTA of the same launch wrote (the Fourier intermediate, the
+// projection partial sums and results): through L2 (ld.global.cg), never a line an
+// earlier load left in this SM's L1, so one persistent launch can run the passes.
+__device__ __forceinline__ cplx<float> ld_l2(const cplx<float>* p) {
+  const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
+  return mk<float>(v.x, v.y);
+}
+__device__ __forceinline__ cplx<double> ld_l2(const cplx<double>* p) {
+  const double2 v = __ldcg(reinterpret_cast<const double2*>(p));
+  return mk<double>(v.x, v.y);
+}
+__device__ __forceinline__ double2 ld_l2(const double2* p) { return __ldcg(p); }
+
 // ---------------------------------------------------------------- geometry
 template <typename T, int NX, int NY, int NZ>
 struct TileGeom {
@@ -115,11 +128,13 @@ __device__ __forceinline__ int roff_base(const ProjView<T>& pj, int s0, bool on)
 }
 
 // ---------------------------------------------------------------- pass A
+// The body of one CTA (bx, by) of the pass; k_tile_fwd runs it at (blockIdx.x,
+// blockIdx.y), the persistent batch kernel at the coordinates of a work item.
 template <typename T, int NX, int NY, int NZ>
-__global__ void __launch_bounds__(256)
-    k_tile_fwd(const cplx<T>* __restrict__ in, long ld, int M, cplx<T>* __restrict__ tmp,
-               const cplx<T>* __restrict__ tw_y, const cplx<T>* __restrict__ tw_z, ProjView<T> pj, int acc_cap,
-               int rec_cap, int ysplit, int vec) {
+__device__ __forceinline__ void tile_fwd_body(int bx, int by, const cplx<T>* __restrict__ in, long ld, int M,
+                                              cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ tw_y,
+                                              const cplx<T>* __restrict__ tw_z, ProjView<T> pj, int acc_cap,
+                                              int rec_cap, int ysplit, int vec) {
   using TG = TileGeom<T, NX, NY, NZ>;
   using AZ = typename TG::AZ;
   constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, ZS = TG::ZS;
@@ -132,7 +147,7 @@ __global__ void __launch_bounds__(256)
 
   // ysplit CTAs share plane ix, each taking Y1 / ysplit row classes
   const int YS = ysplit, YPER = Y1 / ysplit;
-  const int grp = blockIdx.x, ix = blockIdx.y / YS, yh = blockIdx.y % YS;
+  const int grp = bx, ix = by / YS, yh = by % YS;
   const int m0 = grp * G;
   const int gcount = min(G, M - m0);
   const bool v16 = vec && gcount == G;
@@ -218,7 +233,7 @@ __global__ void __launch_bounds__(256)
             double2* d = pj.slots + (((long)(pj.plane_ptr[ix] + sl) * YS + yh) * LMAX) * M + m0 + j;
 #pragma unroll
             for (int l = 0; l < LMAX; ++l) {
-              double2 v = d[(long)l * M];
+              double2 v = ld_l2(d + (long)l * M);
               v.x += (double)a[l].x;
               v.y += (double)a[l].y;
               d[(long)l * M] = v;
@@ -296,6 +311,15 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+template <typename T, int NX, int NY, int NZ>
+__global__ void __launch_bounds__(256)
+    k_tile_fwd(const cplx<T>* __restrict__ in, long ld, int M, cplx<T>* __restrict__ tmp,
+               const cplx<T>* __restrict__ tw_y, const cplx<T>* __restrict__ tw_z, ProjView<T> pj, int acc_cap,
+               int rec_cap, int ysplit, int vec) {
+  tile_fwd_body<T, NX, NY, NZ>(blockIdx.x, blockIdx.y, in, ld, M, tmp, tw_y, tw_z, pj, acc_cap, rec_cap, ysplit,
+                               vec);
+}
+
 // ---------------------------------------------------------------- projection finish
 // proj[a][l][m] = dV ekb[a][l] sum over the atom's (plane, half) slots, in the order of
 // its planes and halves: pass A wrote one partial per slot, no atomics.  Item i =
@@ -313,7 +337,7 @@ __device__ __forceinline__ void proj_finish_item(const ProjView<T>& pj, int M, i
       v[u] = make_double2(0.0, 0.0);
       if (q < q1) {
         const long slot = (long)pj.aslot[q / ysplit] * ysplit + q % ysplit;
-        v[u] = pj.slots[(slot * LMAX + l) * M + m];
+        v[u] = ld_l2(pj.slots + (slot * LMAX + l) * M + m);
       }
     }
 #pragma unroll
@@ -333,15 +357,9 @@ __device__ __forceinline__ void proj_finish_item(const ProjView<T>& pj, int M, i
 // thread t of CTA b handles item b * blockDim + t, so the few CTAs that carry the
 // finish run beside thousands that do not.
 template <typename T, int NX, int NY, int NZ>
-__global__ void __launch_bounds__(256)
-    k_tile_x(cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ tw_x, KinParams<T> kp,
-             cplx<T>* __restrict__ fout, ProjView<T> fin, int fin_M, int fin_ysplit) {
-  if (fin.slots) {
-    const long n = (long)fin.nproj * fin.L * fin_M;
-    const long stride = (long)gridDim.x * gridDim.y * blockDim.x;
-    for (long i = ((long)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
-      proj_finish_item(fin, fin_M, fin_ysplit, i);
-  }
+__device__ __forceinline__ void tile_x_body(int bx, int by, cplx<T>* __restrict__ tmp,
+                                            const cplx<T>* __restrict__ tw_x, KinParams<T> kp,
+                                            cplx<T>* __restrict__ fout) {
   using TG = TileGeom<T, NX, NY, NZ>;
   using AX = typename TG::AX;
   constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, XS = TG::XS;
@@ -351,7 +369,7 @@ __global__ void __launch_bounds__(256)
   T* kinB = reinterpret_cast<T*>(twx + NX);  // [Y1] linear and [Y1] constant term per kb
   T* kinC = kinB + Y1;
 
-  const int kz = blockIdx.x % NZ, ka = blockIdx.x / NZ, grp = blockIdx.y;
+  const int kz = bx % NZ, ka = bx / NZ, grp = by;
   cplx<T>* blk = tmp + ((long)(grp * Y2 + ka) * NZ + kz) * TG::BLK;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) twx[i] = tw_x[i];
   // Along an x line 1/2 |G + k + A|^2 / N = kA2 n0^2 + kinB n0 + kinC with
@@ -383,7 +401,7 @@ __global__ void __launch_bounds__(256)
       if (it >= NX * G) continue;
       const int j = it % G, ix = it / G;
 #pragma unroll
-      for (int y = 0; y < Y1; ++y) u[c][y] = blk[(ix * Y1 + y) * G + j];
+      for (int y = 0; y < Y1; ++y) u[c][y] = ld_l2(blk + (ix * Y1 + y) * G + j);
     }
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
@@ -441,6 +459,19 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int y = 0; y < Y1; ++y) blk[(ix * Y1 + y) * G + j] = u[y];
   }
+}
+
+template <typename T, int NX, int NY, int NZ>
+__global__ void __launch_bounds__(256)
+    k_tile_x(cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ tw_x, KinParams<T> kp,
+             cplx<T>* __restrict__ fout, ProjView<T> fin, int fin_M, int fin_ysplit) {
+  if (fin.slots) {
+    const long n = (long)fin.nproj * fin.L * fin_M;
+    const long stride = (long)gridDim.x * gridDim.y * blockDim.x;
+    for (long i = ((long)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+      proj_finish_item(fin, fin_M, fin_ysplit, i);
+  }
+  tile_x_body<T, NX, NY, NZ>(blockIdx.x, blockIdx.y, tmp, tw_x, kp, fout);
 }
 
 // ---------------------------------------------------------------- pass B of the plain FFTs
@@ -569,12 +600,12 @@ __global__ void __launch_bounds__(256)
 // with cp.async at the start, so that read overlaps the inverse transforms.
 // MODE_H = 1: the H epilogue; 0: out = alpha * (inverse transform), the second
 // half of to_real (alpha = 1/N), reading neither orbitals, V nor projectors.
-template <typename T, int NX, int NY, int NZ, int MODE_H = 1>
-__global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
-    k_tile_inv(const cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ in, long ld_in,
-               cplx<T>* __restrict__ out, long ld_out, int M, const cplx<T>* __restrict__ tw_y,
-               const cplx<T>* __restrict__ tw_z, ProjView<T> pj, EpiParams<T> ep, int rec_cap, int seg_cap,
-               int vec) {
+template <typename T, int NX, int NY, int NZ, int MODE_H>
+__device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __restrict__ tmp,
+                                              const cplx<T>* __restrict__ in, long ld_in, cplx<T>* __restrict__ out,
+                                              long ld_out, int M, const cplx<T>* __restrict__ tw_y,
+                                              const cplx<T>* __restrict__ tw_z, const ProjView<T>& pj,
+                                              const EpiParams<T>& ep, int rec_cap, int seg_cap, int vec) {
   using TG = TileGeom<T, NX, NY, NZ>;
   using AZ = typename TG::AZ;
   constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, ZS = TG::ZS;
@@ -587,7 +618,7 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
   int* TP = reinterpret_cast<int*>(R + rec_cap);           // [PSTRIDE] point index of the tile
   cplx<T>* PT = reinterpret_cast<cplx<T>*>(TP + TG::PSTRIDE);  // [seg_cap][LMAX][G] projections
 
-  const int grp = blockIdx.x, ix = blockIdx.y / Y1, y1 = blockIdx.y % Y1;
+  const int grp = bx, ix = by / Y1, y1 = by % Y1;
   const int m0 = grp * G;
   const int gcount = min(G, M - m0);
   const bool v16 = vec && gcount == G;
@@ -635,7 +666,7 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
       const int l = i % LMAX, j = (i / LMAX) % G, ts = i / (G * LMAX);
       cplx<T> v = mk<T>(0, 0);
       if (l < pj.L && j < gcount) {
-        const double2 d = pj.proj[((long)pj.seg_atom[s0 + ts] * pj.L + l) * M + m0 + j];
+        const double2 d = ld_l2(pj.proj + ((long)pj.seg_atom[s0 + ts] * pj.L + l) * M + m0 + j);
         v = mk<T>((T)d.x, (T)d.y);
       }
       PT[i] = v;
@@ -780,7 +811,7 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
             for (int l = 0; l < LMAX; ++l) {
               cplx<T> pv = mk<T>(0, 0);
               if (l < pj.L && jb + k < gcount) {
-                const double2 d = pj.proj[((long)pj.seg_atom[s0 + re.tseg] * pj.L + l) * M + m0 + jb + k];
+                const double2 d = ld_l2(pj.proj + ((long)pj.seg_atom[s0 + re.tseg] * pj.L + l) * M + m0 + jb + k);
                 pv = mk<T>((T)d.x, (T)d.y);
               }
               t.x = fma(re.beta[l], pv.x, t.x);
@@ -811,6 +842,16 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
       }
     }
   }
+}
+
+template <typename T, int NX, int NY, int NZ, int MODE_H = 1>
+__global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
+    k_tile_inv(const cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ in, long ld_in,
+               cplx<T>* __restrict__ out, long ld_out, int M, const cplx<T>* __restrict__ tw_y,
+               const cplx<T>* __restrict__ tw_z, ProjView<T> pj, EpiParams<T> ep, int rec_cap, int seg_cap,
+               int vec) {
+  tile_inv_body<T, NX, NY, NZ, MODE_H>(blockIdx.x, blockIdx.y, tmp, in, ld_in, out, ld_out, M, tw_y, tw_z, pj, ep,
+                                       rec_cap, seg_cap, vec);
 }
 
 }  // namespace inqb

@@ -116,6 +116,13 @@ SIGNATURES = {
     "inqb_batch_destroy": (ctypes.c_int, [_vp]),
     "inqb_batch_apply_h": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), _ip,
                                           _ip, _vp]),
+    "inqb_batch_set_mode": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "inqb_batch_autotune": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                                           _ip, _ip, _vp, _ip, _dp]),
+    "inqb_batch_info": (ctypes.c_int, [_vp, _ip, _ip, _ip]),
+    "inqb_batch_status": (ctypes.c_int, [_vp, _vp]),
+    "inqb_batch_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "inqb_batch_test_unreachable_wait": (ctypes.c_int, [_vp, ctypes.c_int]),
     "inqb_timing_start": (ctypes.c_int, [_ctxp, ctypes.c_int]),
     "inqb_timing_stop": (ctypes.c_int, [_ctxp, _dp, _ip]),
 }
