@@ -285,6 +285,11 @@ int inqb_etrs_powers_size(inqb_ctx* ctx, int M, size_t* bytes);
  * Horner), like the reference's exponential. */
 int inqb_etrs_step_powers(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
                           const double kA_tdt_cov[3], void* powers, void* stream);
+/* The step of inqb_etrs_step_powers keeping nothing: the same term-by-term sums, so
+ * the same orbitals bit for bit, without writing the powers or their coefficients
+ * (the steps of a checkpointed forward pass whose powers the backward recomputes). */
+int inqb_etrs_step_terms(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                         const double kA_tdt_cov[3], void* stream);
 /* Reverse of that step for a real objective (the reference has no adjoint):
  * lambda <- U^dagger lambda, gV[p] += 2 Re sum_i conj(Xi_i) Phi_i and
  * gA_t[d], gA_tdt[d] += 2 Re sum_i <Xi_i| dH/dA_d |Phi_i> for the two half steps,

@@ -308,21 +308,36 @@ __global__ void __launch_bounds__(256)
 // part[chunk][pair][l][q][M] (the same sums as k_nl_moments).  Warps are (projector l,
 // half h); a lane holds orbital m = blockIdx.y * MW + lane % MW and walks the entry
 // stream (lane / MW) + (32 / MW) h, so that fewer than 32 orbitals still fill the warp
-// (MW = 16 for M <= 16), with four entries in flight per lane.
+// (MW = 16 for M <= 16).  The chunk's records are staged in shared memory first, and
+// a lane gathers the orbital values of B entries before it adds them up (in its entry
+// order), so B gathers are in flight instead of one record-then-gather chain.
 template <typename T, int MW>
 __global__ void __launch_bounds__(256)
-    k_nl_moments_pairs(int L, int M, EightBlocks<T> b, const int* __restrict__ chunk_atom,
+    k_nl_moments_pairs(int L, int M, const __grid_constant__ EightBlocks<T> b, const int* __restrict__ chunk_atom,
                        const int* __restrict__ chunk_beg, const int* __restrict__ atom_ptr,
                        const AdjRec<T>* __restrict__ adj, double* __restrict__ part) {
   constexpr int LM = 4, Q = 16, SUB = 32 / MW, STREAMS = 2 * SUB;
+  constexpr int B = sizeof(T) == 4 ? 8 : 4;
+  constexpr int RV = (int)(sizeof(AdjRec<T>) / 16);
+  static_assert(sizeof(AdjRec<T>) % 16 == 0, "records are copied in 16-byte pieces");
   __shared__ double red[LM][32][Q + 1];
+  __shared__ __align__(16) AdjRec<T> R[kNlChunk];
   const int c = blockIdx.x, pr = blockIdx.z;
   const int lane = threadIdx.x & 31;
   const int m = blockIdx.y * MW + (lane % MW);
   const int l = (threadIdx.x >> 5) & (LM - 1), h = threadIdx.x >> 7;
   const int stream = lane / MW + SUB * h;
   const int a = chunk_atom[c];
-  const int i0 = chunk_beg[c], i1 = min(i0 + kNlChunk, atom_ptr[a + 1]);
+  const int i0 = chunk_beg[c], n = min(kNlChunk, atom_ptr[a + 1] - i0);
+  {
+    const char* src = reinterpret_cast<const char*>(adj + i0);
+    for (int q = threadIdx.x; q < n * RV; q += blockDim.x) {
+      const unsigned d = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(R) + 16 * q);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + 16 * q) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+  }
+  __syncthreads();
   const cplx<T>* u = b.L[pr];
   const cplx<T>* w = b.P[pr];
   const long ldu = b.ldL[pr], ldw = b.ldP;
@@ -330,19 +345,30 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int q = 0; q < Q; ++q) s[q] = 0.0;
   if (m < M && l < L) {
-#pragma unroll 4
-    for (int i = i0 + stream; i < i1; i += STREAMS) {
-      const AdjRec<T> r = adj[i];
-      const cplx<T> uu = u[(long)r.pt * ldu + m], ww = w[(long)r.pt * ldw + m];
-      const double bb = (double)r.beta[l];
-      const double phr = (double)r.ph[0], phi = (double)r.ph[1];
-      const double ur = bb * (phr * uu.x - phi * uu.y), ui = bb * (phr * uu.y + phi * uu.x);
-      const double wr = bb * (phr * ww.x - phi * ww.y), wi = bb * (phr * ww.y + phi * ww.x);
-      const double x0 = r.xyz[0], x1 = r.xyz[1], x2 = r.xyz[2];
-      s[0] += ur; s[1] += ui;
-      s[2] += x0 * ur; s[3] += x0 * ui; s[4] += x1 * ur; s[5] += x1 * ui; s[6] += x2 * ur; s[7] += x2 * ui;
-      s[8] += wr; s[9] += wi;
-      s[10] += x0 * wr; s[11] += x0 * wi; s[12] += x1 * wr; s[13] += x1 * wi; s[14] += x2 * wr; s[15] += x2 * wi;
+    for (int k0 = stream; k0 < n; k0 += B * STREAMS) {
+      cplx<T> uu[B], ww[B];
+#pragma unroll
+      for (int j = 0; j < B; ++j) {
+        const int k = k0 + j * STREAMS;
+        const long pt = R[min(k, n - 1)].pt;
+        uu[j] = u[pt * ldu + m];
+        ww[j] = w[pt * ldw + m];
+      }
+#pragma unroll
+      for (int j = 0; j < B; ++j) {
+        const int k = k0 + j * STREAMS;
+        if (k >= n) continue;
+        const AdjRec<T>& r = R[k];
+        const double bb = (double)r.beta[l];
+        const double phr = (double)r.ph[0], phi = (double)r.ph[1];
+        const double ur = bb * (phr * uu[j].x - phi * uu[j].y), ui = bb * (phr * uu[j].y + phi * uu[j].x);
+        const double wr = bb * (phr * ww[j].x - phi * ww[j].y), wi = bb * (phr * ww[j].y + phi * ww[j].x);
+        const double x0 = r.xyz[0], x1 = r.xyz[1], x2 = r.xyz[2];
+        s[0] += ur; s[1] += ui;
+        s[2] += x0 * ur; s[3] += x0 * ui; s[4] += x1 * ur; s[5] += x1 * ui; s[6] += x2 * ur; s[7] += x2 * ui;
+        s[8] += wr; s[9] += wi;
+        s[10] += x0 * wr; s[11] += x0 * wi; s[12] += x1 * wr; s[13] += x1 * wi; s[14] += x2 * wr; s[15] += x2 * wi;
+      }
     }
   }
   // the SUB streams of a warp meet by shuffles (lane % MW keeps the orbital), then the
@@ -423,15 +449,18 @@ __global__ void __launch_bounds__(512)
 // these kernels read the eight blocks Lambda_0..3, Phi_0..3 once and weight them.
 
 
-// gV[p] += 2 Re sum_m sum_i conj(Xi_i) Phi_i, one warp per grid point.
-template <typename T>
+// gV[p] += 2 Re sum_m sum_i conj(Xi_i) Phi_i, one group of LPP lanes per grid point
+// (LPP = 16 where M <= 16, so no lane idles).
+template <typename T, int LPP>
 __global__ void k_vgrad8(long N, int M, EightBlocks<T> b, PairWeights pw, double* __restrict__ gV) {
-  const int lane = threadIdx.x & 31;
-  const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
-  for (long p = warp; p < N; p += nwarps) {
+  const int lane = threadIdx.x & (LPP - 1);
+  const long grp = ((long)blockIdx.x * blockDim.x + threadIdx.x) / LPP;
+  const long ngrp = ((long)gridDim.x * blockDim.x) / LPP;
+  // every lane of the warp runs the same number of iterations (the shuffles below)
+  const long pend = (N + ngrp - 1) / ngrp * ngrp;
+  for (long p = grp; p < pend; p += ngrp) {
     double re = 0.0;
-    for (int m = lane; m < M; m += 32) {
+    for (int m = lane; m < M && p < N; m += LPP) {
       double lr[4], li[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -452,29 +481,32 @@ __global__ void k_vgrad8(long N, int M, EightBlocks<T> b, PairWeights pw, double
       }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) re += __shfl_xor_sync(0xffffffffu, re, o);
-    if (lane == 0) gV[p] += 2.0 * re;
+    for (int o = LPP / 2; o > 0; o >>= 1) re += __shfl_xor_sync(0xffffffffu, re, o);
+    if (lane == 0 && p < N) gV[p] += 2.0 * re;
   }
 }
 
 // acc[2d..2d+1] += sum_{G,m} sum_i conj(Xi_i(G)) (G + kA)_d Phi_i(G) on the tile-layout
 // coefficients (b.L / b.P point at coefficient blocks, ld unused).
-template <typename T>
-__global__ void k_velocity_dot8(long nelem, int M, EightBlocks<T> b, PairWeights pw, TileFourier tf, Recip r,
+// IDX: the index type of the element arithmetic (32-bit where nelem fits: the
+// divisions below are much cheaper than in 64 bits).
+template <typename T, typename IDX>
+__global__ void k_velocity_dot8(IDX nelem, int M, EightBlocks<T> b, PairWeights pw, TileFourier tf, Recip r,
                                 double* __restrict__ acc) {
   double s[6] = {0, 0, 0, 0, 0, 0};
-  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += (long)gridDim.x * blockDim.x) {
-    long t = e / tf.G;
-    const int j0 = (int)(e - t * tf.G);
-    const int kb = (int)(t % tf.Y1);
-    t /= tf.Y1;
-    const int kx = (int)(t % r.nr[0]);
-    t /= r.nr[0];
-    const int kz = (int)(t % r.nr[2]);
-    t /= r.nr[2];
-    const int ka = (int)(t % tf.Y2);
-    const long g = t / tf.Y2;
-    if (g * tf.G + j0 >= M) continue;
+  const IDX uG = (IDX)tf.G, uY1 = (IDX)tf.Y1, uY2 = (IDX)tf.Y2, unx = (IDX)r.nr[0], unz = (IDX)r.nr[2];
+  for (IDX e = (IDX)blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += (IDX)gridDim.x * blockDim.x) {
+    IDX t = e / uG;
+    const int j0 = (int)(e - t * uG);
+    IDX t2 = t / uY1;
+    const int kb = (int)(t - t2 * uY1);
+    t = t2 / unx;
+    const int kx = (int)(t2 - t * unx);
+    t2 = t / unz;
+    const int kz = (int)(t - t2 * unz);
+    const IDX g = t2 / uY2;
+    const int ka = (int)(t2 - g * uY2);
+    if ((long)g * tf.G + j0 >= M) continue;
     const int k[3] = {kx, ka + tf.Y2 * kb, kz};
     double n[3];
     for (int c = 0; c < 3; c++) n[c] = (k[c] >= (r.nr[c] + 1) / 2) ? k[c] - r.nr[c] : k[c];
@@ -543,7 +575,8 @@ __global__ void __launch_bounds__(512)
   const int mi = threadIdx.x & 31, q = threadIdx.x >> 5;
   const int m = blockIdx.z * 32 + mi;
   const int c0 = atom_chunk_ptr[a], c1 = atom_chunk_ptr[a + 1];
-  // the four pairs' chunk sums, four loads in flight per pair (fixed order: deterministic)
+  // the four pairs' chunk sums, chunk c into accumulator (c - c0) % 4: sixteen loads in
+  // flight per thread, a fixed order (deterministic)
   double v[4][4];
 #pragma unroll
   for (int pr = 0; pr < 4; ++pr) v[pr][0] = v[pr][1] = v[pr][2] = v[pr][3] = 0.0;
@@ -552,16 +585,15 @@ __global__ void __launch_bounds__(512)
     const double* pp = part + ((long)c0 * 4 * L + l) * Q * M + (long)q * M + m;
     const long pstride = (long)L * Q * M;  // next pair of the same chunk
     int c = c0;
-    for (; c + 1 < c1; c += 2, pp += 2 * stride) {
+    for (; c + 3 < c1; c += 4, pp += 4 * stride) {
 #pragma unroll
-      for (int pr = 0; pr < 4; ++pr) {
-        v[pr][0] += pp[pr * pstride];
-        v[pr][1] += pp[pr * pstride + stride];
-      }
+      for (int pr = 0; pr < 4; ++pr)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[pr][k] += pp[pr * pstride + k * stride];
     }
-    if (c < c1)
+    for (int k = 0; c < c1; ++c, ++k, pp += stride)
 #pragma unroll
-      for (int pr = 0; pr < 4; ++pr) v[pr][2] += pp[pr * pstride];
+      for (int pr = 0; pr < 4; ++pr) v[pr][k] += pp[pr * pstride];
   }
 #pragma unroll
   for (int pr = 0; pr < 4; ++pr) mom[pr][q][mi] = (v[pr][0] + v[pr][1]) + (v[pr][2] + v[pr][3]);
@@ -638,7 +670,10 @@ static int half_grad_impl(const inqb_ctx& ctx, const void* const Lam[4], const l
   fb.ldP = 1;
   // V gradient
   const int vblocks = (int)std::min<long>((ctx.N * 32 + 255) / 256, 148L * 16);
-  k_vgrad8<T><<<vblocks, 256, 0, st>>>(ctx.N, M, b, pw, gV);
+  if (M <= 16)
+    k_vgrad8<T, 16><<<vblocks, 256, 0, st>>>(ctx.N, M, b, pw, gV);
+  else
+    k_vgrad8<T, 32><<<vblocks, 256, 0, st>>>(ctx.N, M, b, pw, gV);
   INQB_CUDA_TRY(cudaGetLastError());
   // A gradient: kinetic velocity on the coefficients, nonlocal from the pair moments
   double* acc = ctx.d_red.as<double>();
@@ -654,8 +689,13 @@ static int half_grad_impl(const inqb_ctx& ctx, const void* const Lam[4], const l
   const long nelem = (long)((M + G - 1) / G) * G * ctx.N;
   // six CTAs per SM keep enough coefficient loads in flight (the per-CTA sums end in
   // six atomics each)
-  k_velocity_dot8<T><<<(int)std::min<long>((nelem + 255) / 256, 148L * 6), 256, 0, st>>>(
-      nelem, M, fb, pw, TileFourier{G, ctx.plan->y1, ctx.plan->y2}, r, acc);
+  const int vdb = (int)std::min<long>((nelem + 255) / 256, 148L * 6);
+  if (nelem < (1L << 31) - 256L * vdb)
+    k_velocity_dot8<T, unsigned><<<vdb, 256, 0, st>>>((unsigned)nelem, M, fb, pw,
+                                                      TileFourier{G, ctx.plan->y1, ctx.plan->y2}, r, acc);
+  else
+    k_velocity_dot8<T, long><<<vdb, 256, 0, st>>>(nelem, M, fb, pw, TileFourier{G, ctx.plan->y1, ctx.plan->y2}, r,
+                                                  acc);
   INQB_CUDA_TRY(cudaGetLastError());
   const ProjTables& t = ctx.proj;
   const int nchunks = (int)t.chunk_atom.size();

@@ -1809,22 +1809,35 @@ size_t fourier_elems(const inqb_ctx* ctx, int M) {
 // One half step psi -> sum_k c_k H^k psi at the current k + A, keeping
 // P[0..3] = H^k psi (P[0] a copy of the input) and F[0..3] = their forward
 // coefficients (tile layout, written by the H applications); `out` receives the result.
+// One half step term by term: P[k] = H^k in (k < 4), out = sum_k c_k H^k in.  With
+// keep, P[0] receives a copy of in and F[k] the forward coefficients of P[k]; without,
+// P[0] is in itself and no coefficients are written (the same arithmetic).
 int half_step_powers(inqb_ctx* ctx, const void* in, long ld_in, void* const P[4], void* const F[4], void* out,
-                     long ld_out, int M, const double c[5][2], void* stream) {
+                     long ld_out, int M, const double c[5][2], void* stream, bool keep = true) {
   const long Mi = M;
   const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
   void* H4 = ctx->d_adjL.ptr;
-  {
+  const void* p0 = in;
+  long ld0 = ld_in;
+  if (keep) {
     const double a[1][2] = {{1.0, 0.0}};
     const void* x[1] = {in};
     const long ldx[1] = {ld_in};
     INQB_TRY(launch_lincomb(ctx->precision, ctx->N, M, 1, a, x, ldx, P[0], Mi, stream));
+    p0 = P[0];
+    ld0 = Mi;
   }
-  for (int k = 1; k < 4; k++)
-    INQB_TRY(apply(ctx, LaunchArgs::H, P[k - 1], Mi, P[k], Mi, M, nullptr, 0, one, zero, stream, F[k - 1]));
-  INQB_TRY(apply(ctx, LaunchArgs::H, P[3], Mi, H4, Mi, M, nullptr, 0, one, zero, stream, F[3]));
-  const void* x[5] = {P[0], P[1], P[2], P[3], H4};
-  const long ldx[5] = {Mi, Mi, Mi, Mi, Mi};
+  const void* src = p0;
+  long lds = ld0;
+  for (int k = 1; k < 4; k++) {
+    INQB_TRY(apply(ctx, LaunchArgs::H, src, lds, P[k], Mi, M, nullptr, 0, one, zero, stream,
+                   keep ? F[k - 1] : nullptr));
+    src = P[k];
+    lds = Mi;
+  }
+  INQB_TRY(apply(ctx, LaunchArgs::H, P[3], Mi, H4, Mi, M, nullptr, 0, one, zero, stream, keep ? F[3] : nullptr));
+  const void* x[5] = {p0, P[1], P[2], P[3], H4};
+  const long ldx[5] = {ld0, Mi, Mi, Mi, Mi};
   return launch_lincomb(ctx->precision, ctx->N, M, 5, c, x, ldx, out, ld_out, stream);
 }
 
@@ -1920,6 +1933,27 @@ int inqb_etrs_step_powers(inqb_ctx* ctx, void* psi, int M, int ld, double dt, co
   INQB_TRY(half_step_powers(ctx, psi, ld, P1, F1, P2[0], M, M, c, stream));
   INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
   return half_step_powers(ctx, P2[0], M, P2, F2, psi, ld, M, c, stream);
+}
+
+int inqb_etrs_step_terms(inqb_ctx* ctx, void* psi, int M, int ld, double dt, const double kA_t_cov[3],
+                         const double kA_tdt_cov[3], void* stream) {
+  INQB_CHECK_CTX(ctx);
+  INQB_TRY(check_block(ctx, psi, M, ld));
+  if (!kA_t_cov || !kA_tdt_cov || !std::isfinite(dt)) return fail(INQB_ERR_INVALID, "bad step arguments");
+  INQB_GUARD(ctx);
+  INQB_TRY(adjoint_workspace(ctx, M));
+  double c[5][2];
+  taylor_coeffs(dt, c);
+  // the adjoint workspace: block 0 takes H^4, blocks 1-3 the powers, block 4 phi
+  const size_t blk = (size_t)ctx->N * M * ctx->elem_bytes();
+  char* w = static_cast<char*>(ctx->d_adjL.ptr);
+  void* P[4] = {nullptr, w + blk, w + 2 * blk, w + 3 * blk};
+  void* const F[4] = {nullptr, nullptr, nullptr, nullptr};
+  void* phi = w + 4 * blk;
+  INQB_TRY(set_kA(ctx, kA_t_cov, stream));
+  INQB_TRY(half_step_powers(ctx, psi, ld, P, F, phi, M, M, c, stream, false));
+  INQB_TRY(set_kA(ctx, kA_tdt_cov, stream));
+  return half_step_powers(ctx, phi, M, P, F, psi, ld, M, c, stream, false);
 }
 
 int inqb_etrs_adjoint_step(inqb_ctx* ctx, void* lambda, int M, int ld, double dt, const double kA_t_cov[3],

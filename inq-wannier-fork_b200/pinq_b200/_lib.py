@@ -101,6 +101,8 @@ SIGNATURES = {
     "inqb_etrs_powers_size": (ctypes.c_int, [_ctxp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "inqb_etrs_step_powers": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
                                              _vp, _vp]),
+    "inqb_etrs_step_terms": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
+                                            _vp]),
     "inqb_etrs_adjoint_step": (ctypes.c_int, [_ctxp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, _dp, _dp,
                                               _vp, _vp, _vp, _vp, _vp]),
     "inqb_axpby": (ctypes.c_int, [_ctxp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int,

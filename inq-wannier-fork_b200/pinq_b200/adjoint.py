@@ -80,19 +80,19 @@ class DipolePropagation:
             self.powers = powers
         elif keep:
             # the same term-by-term step the backward recomputes each segment with, so
-            # that the recomputed trajectory is this one exactly (one scratch row); the
-            # last segment's powers are kept, since the backward walks it first
+            # that the recomputed trajectory is this one exactly (keeping no powers);
+            # the last segment's powers are kept, since the backward walks it first
             nsteps = len(amps)
             last0 = ((nsteps - 1) // self.every) * self.every
-            scratch = self.h.powers_buffer(1, self.M)
             tail = self.h.powers_buffer(min(self.every, nsteps), self.M)
             for n in range(nsteps):
                 if n % self.every == 0:
                     cps[n] = psi.clone()
-                row = tail[n - last0] if n >= last0 else scratch[0]
-                self.h.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)),
-                                         self._kA(self._amp(amps, n + 1)), row)
-            del scratch
+                a, b = self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1))
+                if n >= last0:
+                    self.h.etrs_step_powers_(psi, self.dt, a, b, tail[n - last0])
+                else:
+                    self.h.etrs_step_terms_(psi, self.dt, a, b)
             self._tail = (last0, tail)
         else:
             for n in range(len(amps)):
@@ -162,7 +162,11 @@ class DipolePropagation:
         h, h2 = self.h, self._recompute_context()
         amps, nsteps = self.amps, len(self.amps)
         dev = self.psi0.device
-        main = torch.cuda.current_stream(dev)
+        caller = torch.cuda.current_stream(dev)
+        # the walk is the critical path: it runs on a high-priority stream, so the block
+        # scheduler gives the recompute (default priority) only the SMs the walk leaves
+        main = torch.cuda.Stream(device=dev, priority=-1)
+        main.wait_stream(caller)
         side = torch.cuda.Stream(device=dev)
         seg = min(self.every, nsteps)
         have_tail = self._tail is not None and segments[0][0] == self._tail[0]
@@ -215,24 +219,26 @@ class DipolePropagation:
         thread = threading.Thread(target=worker, daemon=True)
         thread.start()
         try:
-            for i, (s0, s1) in enumerate(segments):
-                if not host_ready[i].wait(limit_s) or failure:
-                    raise RuntimeError("adjoint: segment recompute failed") from (failure[0] if failure else None)
-                main.wait_event(ready[i])
-                buf = stores[i % 2]
-                for n in reversed(range(s0, s1)):
-                    n2 = min(n + 1, nsteps - 1)
-                    h.etrs_adjoint_step_(lam, self.dt, self._kA(self._amp(amps, n)),
-                                         self._kA(self._amp(amps, n + 1)), buf[n - s0], gV, gA[n], gA[n2])
-                done[i].record(main)
-                host_done[i].set()
+            with torch.cuda.stream(main):
+                for i, (s0, s1) in enumerate(segments):
+                    if not host_ready[i].wait(limit_s) or failure:
+                        raise RuntimeError("adjoint: segment recompute failed") from (failure[0] if failure else None)
+                    main.wait_event(ready[i])
+                    buf = stores[i % 2]
+                    for n in reversed(range(s0, s1)):
+                        n2 = min(n + 1, nsteps - 1)
+                        h.etrs_adjoint_step_(lam, self.dt, self._kA(self._amp(amps, n)),
+                                             self._kA(self._amp(amps, n + 1)), buf[n - s0], gV, gA[n], gA[n2])
+                    done[i].record(main)
+                    host_done[i].set()
         finally:
             for e in host_done:
                 e.set()  # let the worker finish (or fail) on every path
             thread.join(limit_s)
         if failure:
             raise RuntimeError("adjoint: segment recompute failed") from failure[0]
-        main.wait_stream(side)
+        caller.wait_stream(main)
+        caller.wait_stream(side)
         if have_tail and len(segments) > 2:
             self._tail = None  # its buffer held later segments' powers: recompute next time
 

@@ -502,6 +502,15 @@ class KSHamiltonian:
              dptr(b), powers.data_ptr(), self._stream())
         return psi
 
+    def etrs_step_terms_(self, psi, dt, kA_t_cov, kA_tdt_cov):
+        """The step of etrs_step_powers_ keeping nothing: the same orbitals bit for bit."""
+        psi = self._check(psi)
+        a = np.ascontiguousarray(kA_t_cov, np.float64).reshape(3)
+        b = np.ascontiguousarray(kA_tdt_cov, np.float64).reshape(3)
+        call("inqb_etrs_step_terms", self._h, psi.data_ptr(), psi.shape[1], psi.stride(0), float(dt), dptr(a),
+             dptr(b), self._stream())
+        return psi
+
     def etrs_adjoint_step_(self, lam, dt, kA_t_cov, kA_tdt_cov, powers, gV, gA_t, gA_tdt):
         """Reverse of one ETRS step: lam <- U^dagger lam and the V / A gradients
         accumulated into gV [N] and gA_t, gA_tdt [3] (FP64 CUDA tensors)."""

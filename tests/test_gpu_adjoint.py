@@ -169,3 +169,22 @@ def test_overlapped_recompute_equals_sequential(pb, cfg2, precision):
     tol = 1e-12 if precision == "fp64" else 1e-6
     for k in range(2):
         assert np.abs(out[0][k] - out[1][k]).max() <= tol * np.abs(out[1][k]).max()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_step_terms_equals_step_powers(pb, cfg2, precision):
+    """inqb_etrs_step_terms, which keeps nothing, steps the orbitals bit for bit as
+    inqb_etrs_step_powers does (the checkpointed forward relies on it: the backward
+    recomputes its segments with the powers step), for a strided block too."""
+    prop = _prop(pb, cfg2, precision, 20)
+    h = prop.h
+    x = prop.psi0.clone()
+    wide = torch.zeros((h.N, x.shape[1] + 3), dtype=x.dtype, device="cuda")
+    y = wide[:, :x.shape[1]]
+    y.copy_(x)
+    buf = h.powers_buffer(1, x.shape[1])
+    for n in range(3):
+        a, b = prop._kA(cfg2["amps"][n]), prop._kA(cfg2["amps"][n + 1])
+        h.etrs_step_powers_(x, 0.05, a, b, buf[0])
+        h.etrs_step_terms_(y, 0.05, a, b)
+        assert torch.equal(x, y)
