@@ -86,6 +86,10 @@ class DenseHam:
         psi.copy_(self._half(float(kA2[0]), dt, phi, powers[4:8]))
         return psi
 
+    def etrs_step_terms_(self, psi, dt, kA1, kA2):
+        # the same sums as etrs_step_powers_, the powers dropped
+        return self.etrs_step_powers_(psi, dt, kA1, kA2, self.powers_buffer(1, psi.shape[1])[0])
+
     def _back(self, a, dt, lam, Phi, gV, gA):
         self.a = a
         cc = [np.conj(x) for x in self._c(dt)]
