@@ -126,24 +126,28 @@ class DipolePropagation:
                                      self.powers[n], gV, gA[n], gA[n2])
             return gA[:, self.direction].clone(), gV
         segments = [(s0, min(s0 + self.every, nsteps)) for s0 in range(0, nsteps, self.every)][::-1]
-        if self.overlap and len(segments) > 1 and self.psi0.is_cuda:
-            self._backward_overlapped(segments, lam, gV, gA)
-            return gA[:, self.direction].clone(), gV
         seg = min(self.every, nsteps)
-        store = h.powers_buffer(seg, self.M)
+        have_tail = self._tail is not None and segments[0][0] == self._tail[0]
+        if self.overlap and len(segments) > 1 and self.psi0.is_cuda:
+            # two powers buffers alternate; where the second does not fit beside the
+            # first (large cells in FP64), the segments run one after the other in one
+            second = self._try_powers_buffer(seg)
+            if second is not None:
+                self._backward_overlapped(segments, lam, gV, gA, second)
+                return gA[:, self.direction].clone(), gV
+        # one buffer: the forward's copy of the last segment's powers, reused for the
+        # recompute of every earlier segment once that segment has been walked back
+        store = self._tail[1] if have_tail else h.powers_buffer(seg, self.M)
         for s0, s1 in segments:
-            if self._tail is not None and s0 == self._tail[0]:
-                buf = self._tail[1]  # the forward kept this segment's powers
-            else:
-                buf = store
+            if not (have_tail and s0 == self._tail[0]):  # else the forward kept its powers
                 psi = self.checkpoints[s0].clone()
                 for n in range(s0, s1):
                     h.etrs_step_powers_(psi, self.dt, self._kA(self._amp(amps, n)),
-                                        self._kA(self._amp(amps, n + 1)), buf[n - s0])
+                                        self._kA(self._amp(amps, n + 1)), store[n - s0])
             for n in reversed(range(s0, s1)):
                 n2 = min(n + 1, nsteps - 1)
                 h.etrs_adjoint_step_(lam, self.dt, self._kA(self._amp(amps, n)), self._kA(self._amp(amps, n + 1)),
-                                     buf[n - s0], gV, gA[n], gA[n2])
+                                     store[n - s0], gV, gA[n], gA[n2])
         del store
         return gA[:, self.direction].clone(), gV
 
@@ -155,10 +159,18 @@ class DipolePropagation:
             self._h2_version = self.h.state_version
         return self._h2
 
-    def _backward_overlapped(self, segments, lam, gV, gA):
+    def _try_powers_buffer(self, nsteps):
+        """A powers buffer of nsteps steps, or None where the device has no room for it."""
+        try:
+            return self.h.powers_buffer(nsteps, self.M)
+        except torch.OutOfMemoryError:
+            return None
+
+    def _backward_overlapped(self, segments, lam, gV, gA, second):
         """Segments in reverse time order; segment i + 1's recompute (second context,
         second stream) overlaps segment i's backward walk.  Two powers buffers
-        alternate; events order each buffer's write after its previous read."""
+        alternate (the forward's copy of the last segment, or a new one, and `second`);
+        events order each buffer's write after its previous read."""
         h, h2 = self.h, self._recompute_context()
         amps, nsteps = self.amps, len(self.amps)
         dev = self.psi0.device
@@ -171,7 +183,7 @@ class DipolePropagation:
         seg = min(self.every, nsteps)
         have_tail = self._tail is not None and segments[0][0] == self._tail[0]
         first = self._tail[1] if have_tail else h.powers_buffer(seg, self.M)
-        stores = [first, h.powers_buffer(seg, self.M)]
+        stores = [first, second]
         for b in stores:
             b.record_stream(side)
         ready = [torch.cuda.Event() for _ in segments]

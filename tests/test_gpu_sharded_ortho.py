@@ -60,7 +60,11 @@ def test_cholesky_inverse_rejects_a_dependent_set(pb):
     s = small_system(pb, n=32, M=4, seed=22, with_proj=False)
     h = pb.KSHamiltonian(s["lattice"], s["nr"], "fp64")
     psi = torch.as_tensor(s["psi"]).to("cuda")
-    psi[:, 3] = psi[:, 1]
+    # a zero orbital: its row and column of the overlap are exactly zero, so the last
+    # pivot is exactly 0 and zpotrf's test (pivot <= 0) rejects it.  A duplicated
+    # orbital would leave a pivot of rounding size whose sign varies with the order of
+    # the overlap's sums, accepted or rejected by chance, as by zpotrf itself.
+    psi[:, 3] = 0
     S = h.overlap_block(psi, psi)
     with pytest.raises(RuntimeError, match="not positive definite"):
         h.cholesky_inverse_(S)
