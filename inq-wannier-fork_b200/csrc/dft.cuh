@@ -188,4 +188,83 @@ struct DFT<5, INV, T> {
   }
 };
 
+// ---------------------------------------------------------------- radix 8, complex64
+// Sum and difference of two complex64 values, each as one packed f32x2 instruction
+// (sm_100; round to nearest like the scalar adds, so every value is rounded once, as
+// in the scalar form).
+__device__ __forceinline__ cplx<float> padd(cplx<float> a, cplx<float> b) {
+  const float2 r = __fadd2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+  return {r.x, r.y};
+}
+__device__ __forceinline__ cplx<float> psub(cplx<float> a, cplx<float> b) {
+  unsigned long long r;
+  asm("{\n\t.reg .b64 pa, pb;\n\tmov.b64 pa, {%1, %2};\n\tmov.b64 pb, {%3, %4};\n\t"
+      "sub.rn.f32x2 %0, pa, pb;\n\t}"
+      : "=l"(r)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+  return {v.x, v.y};
+}
+__device__ __forceinline__ cplx<float> pscale(float s, cplx<float> a) {
+  const float2 r = __fmul2_rn(make_float2(s, s), make_float2(a.x, a.y));
+  return {r.x, r.y};
+}
+
+// DFT_8 of complex64 values written out as the split 8 = 2 x 4 (the generic form
+// above with the same factors): a_n = v_n + v_{n+4} gives the even outputs as a DFT_4,
+// b_n = v_n - v_{n+4} twiddled by w^n the odd ones, w = exp(-+ 2 pi i / 8).  Sums
+// and differences of values in natural (re, im) order take one packed instruction;
+// those with a factor +-i stay two scalar adds (the swap is free there).
+template <bool INV>
+struct DFT<8, INV, float> {
+  __device__ __forceinline__ static void run(cplx<float>* v) {
+    constexpr float h = 0.70710678118654752f;  // 1/sqrt(2)
+    cplx<float> a[4], b[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      a[n] = padd(v[n], v[n + 4]);
+      b[n] = psub(v[n], v[n + 4]);
+    }
+    // even outputs: DFT_4 of a
+    const cplx<float> t0 = padd(a[0], a[2]), t1 = psub(a[0], a[2]);
+    const cplx<float> t2 = padd(a[1], a[3]), t3 = psub(a[1], a[3]);
+    v[0] = padd(t0, t2);
+    v[4] = psub(t0, t2);
+    // X2 = t1 -+ i t3, X6 = t1 +- i t3 (upper signs forward)
+    if (INV) {
+      v[2] = {t1.x - t3.y, t1.y + t3.x};
+      v[6] = {t1.x + t3.y, t1.y - t3.x};
+    } else {
+      v[2] = {t1.x + t3.y, t1.y - t3.x};
+      v[6] = {t1.x - t3.y, t1.y + t3.x};
+    }
+    // odd outputs: DFT_4 of c_n = b_n w^n.  e = c0 + c2, f = c0 - c2 (c2 = -+ i b2);
+    // p1 sqrt(1/2) = c1 and p3 sqrt(1/2) = c3, so s = c1 + c3, d = c1 - c3.
+    cplx<float> e, f, p1, p3;
+    if (INV) {
+      e = {b[0].x - b[2].y, b[0].y + b[2].x};
+      f = {b[0].x + b[2].y, b[0].y - b[2].x};
+      p1 = {b[1].x - b[1].y, b[1].x + b[1].y};      // b1 (1 + i)
+      p3 = {-b[3].x - b[3].y, b[3].x - b[3].y};     // b3 (-1 + i)
+    } else {
+      e = {b[0].x + b[2].y, b[0].y - b[2].x};
+      f = {b[0].x - b[2].y, b[0].y + b[2].x};
+      p1 = {b[1].x + b[1].y, b[1].y - b[1].x};      // b1 (1 - i)
+      p3 = {b[3].y - b[3].x, -b[3].x - b[3].y};     // b3 (-1 - i)
+    }
+    const cplx<float> s = pscale(h, padd(p1, p3)), d = pscale(h, psub(p1, p3));
+    v[1] = padd(e, s);
+    v[5] = psub(e, s);
+    // X3 = f -+ i d, X7 = f +- i d
+    if (INV) {
+      v[3] = {f.x - d.y, f.y + d.x};
+      v[7] = {f.x + d.y, f.y - d.x};
+    } else {
+      v[3] = {f.x + d.y, f.y - d.x};
+      v[7] = {f.x - d.y, f.y + d.x};
+    }
+  }
+};
+
 }  // namespace inqb
