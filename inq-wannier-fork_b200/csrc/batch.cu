@@ -78,7 +78,7 @@ __device__ __forceinline__ void run_stage(const BatchCell<T>& c, int bx, int by,
     for (int t = 0; t < count; t++) {
       if (t) __syncthreads();
       tile_inv_body<T, N, N, N, 1>(bx, by + t, c.tmp, c.in, c.ld_in, c.out, c.ld_out, c.M, twy, twz, c.pj, c.ep,
-                                   c.rec_cap_inv, c.seg_cap, c.ovf_cap, c.vio);
+                                   c.rec_cap_inv, c.seg_cap, c.vio);
     }
   }
 }

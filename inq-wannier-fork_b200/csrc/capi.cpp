@@ -66,7 +66,6 @@ ProjView<T> proj_view(inqb_ctx* ctx) {
   v.max_tile_ent = t.max_tile_ent;
   v.max_tile_seg = t.max_tile_seg;
   v.pt_stride = t.pt_stride;
-  v.max_tile_ovf = t.max_tile_ovf;
   v.ent_rec = t.d_ent_rec.as<EntRec<T>>();
   v.ent_rec_pt = t.d_ent_rec_pt.as<EntRec<T>>();
   v.pt_ptr = t.d_pt_ptr.as<int>();

@@ -103,7 +103,6 @@ struct ProjTables {
   int max_tile_seg = 0;     // most atom segments in one tile
   int tile_pts = 0;         // grid points of a tile (NY / Y1 rows x NZ)
   int pt_stride = 0;        // tile stride of pt_ptr: tile_pts + 1 rounded up to 4
-  int max_tile_ovf = 0;     // most later records (a point's second and further entries) in one tile
   // host copies.  Tile (ix, y1) holds rows y = y1 + Y1 * r of plane ix; seg_ptr
   // [NX * Y1 + 1] lists its atom segments (seg_atom, seg_ent range, seg_local =
   // the atom's index among the atoms of plane ix, plane_ptr / plane_atom).
@@ -139,12 +138,8 @@ struct ProjTables {
   DevBuf d_ent_phase;               // [nent] complex, exp(+i (k+A).r), context precision
   DevBuf d_ent_rec;                 // [nent] EntRec<T>, phases filled with d_ent_phase
   // the same records in point order inside each tile (for the owner-computes
-  // nonlocal scatter): rec_pt[pt_pos[e]] is entry e.  A tile's records are the first
-  // entry of every point that has one, in point order, then the later entries (a
-  // point's second, third, ...), in point order, each point's in entry order.
-  // pt_ptr[tile * pt_stride + q] packs two counts over the tile-local points before q:
-  // bits 0-15 the points with an entry (the index of q's first record), bits 16-31 the
-  // later entries (the index of q's first later record after the first records).
+  // nonlocal scatter): rec_pt[pt_pos[e]] is entry e; pt_ptr[tile * pt_stride + q]
+  // is the first record of tile-local point q relative to the tile's first entry
   std::vector<int> pt_pos, pt_ptr;
   DevBuf d_ent_rec_pt, d_pt_pos, d_pt_ptr;
   DevBuf d_scale;                   // [nproj][L] double
@@ -155,7 +150,7 @@ struct ProjTables {
 // Kernel view of the projector tables (T = float or double).
 template <typename T>
 struct ProjView {
-  int nproj, L, max_plane_atoms, max_tile_ent, max_tile_seg, pt_stride, max_tile_ovf;
+  int nproj, L, max_plane_atoms, max_tile_ent, max_tile_seg, pt_stride;
   const int* seg_ptr;     // [NX * Y1 + 1] segments of tile (ix, y1)
   const int* seg_atom;
   const int* seg_ent;     // [nseg + 1] entry ranges

@@ -85,9 +85,7 @@ struct BatchCell {
   long ld_in;
   cplx<T>* out;
   long ld_out;
-  int M, ysplit, acc_cap, rec_cap_a, rec_cap_inv, seg_cap, ovf_cap;
-  unsigned char vin, vio;  // 16-byte vector access of the input / input and output (bytes: 64 cells of
-                           // this struct fill the kernel parameter space in FP64)
+  int M, ysplit, acc_cap, rec_cap_a, rec_cap_inv, seg_cap, vin, vio;
   cplx<T>* tmp;
   const cplx<T>* tw;  // x | y | z twiddles
   ProjView<T> pj;
@@ -205,14 +203,6 @@ int launch_h_impl(const LaunchArgs& a) {
     if (TG::smem_inv(rec_cap_inv, seg_cap) > TG::SMEM_MAX) rec_cap_inv = 0;
     if (TG::smem_inv(rec_cap_inv, seg_cap) > TG::SMEM_MAX)
       return fail(INQB_ERR_UNSUPPORTED, "tile of this grid does not fit in shared memory");
-    // without the records staged: the later records of a tile (a point's second and
-    // further entries, read inside the scatter's loop) go to shared memory where they
-    // fit without costing the pass a CTA per SM (228 KB per SM, 1 KB reserved per CTA)
-    int ovf_cap = 0;
-    if (rec_cap_inv == 0 && pj.nproj > 0) {
-      const size_t budget = std::min<size_t>(228 * 1024 / TG::INV_MIN_CTAS - 1024, TG::SMEM_MAX);
-      if (TG::smem_inv(0, seg_cap, pj.max_tile_ovf) <= budget) ovf_cap = pj.max_tile_ovf;
-    }
     if (a.batch_cell) {
       // describe the apply for the persistent batch launch instead of launching it
       auto* d = reinterpret_cast<BatchCellDesc*>(a.batch_cell);
@@ -231,7 +221,6 @@ int launch_h_impl(const LaunchArgs& a) {
       c.rec_cap_a = rec_cap_a;
       c.rec_cap_inv = rec_cap_inv;
       c.seg_cap = seg_cap;
-      c.ovf_cap = ovf_cap;
       c.vin = vin;
       c.vio = vin && vout;
       c.tmp = tmp;
@@ -244,7 +233,7 @@ int launch_h_impl(const LaunchArgs& a) {
       d->b_per = TG::Y2 * NZ;
       d->c_per = NX * TG::Y1;
       d->finish = pj.nproj > 0 ? 1 : 0;
-      d->smem = std::max({TG::smem_fwd(acc_cap, rec_cap_a), TG::SMEM_X, TG::smem_inv(rec_cap_inv, seg_cap, ovf_cap)});
+      d->smem = std::max({TG::smem_fwd(acc_cap, rec_cap_a), TG::SMEM_X, TG::smem_inv(rec_cap_inv, seg_cap)});
       d->bytes.resize(sizeof(c));
       memcpy(d->bytes.data(), &c, sizeof(c));
       return INQB_OK;
@@ -268,9 +257,9 @@ int launch_h_impl(const LaunchArgs& a) {
     k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out, fin, a.M,
                                                              ysplit);
     if (a.events[4]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[4], st));
-    k_tile_inv<T, NX, NY, NZ, 1><<<ginv, thr[2], TG::smem_inv(rec_cap_inv, seg_cap, ovf_cap), st>>>(
+    k_tile_inv<T, NX, NY, NZ, 1><<<ginv, thr[2], TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
         tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv, seg_cap,
-        ovf_cap, vin && vout);
+        vin && vout);
     if (a.events[5]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[5], st));
   } else if (a.mode == LaunchArgs::POISSON) {
     // solvers::poisson on M complex fields: forward z and inner y, then the outer y
@@ -292,7 +281,7 @@ int launch_h_impl(const LaunchArgs& a) {
     EpiParams<T> ep{};
     ep.alpha = mk<T>((T)1, (T)0);
     k_tile_inv<T, NX, NY, NZ, 0><<<ginv, thr[2], TG::smem_inv(0, 0), st>>>(
-        tmp, nullptr, 0, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, none, ep, 0, 0, 0, vout);
+        tmp, nullptr, 0, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, none, ep, 0, 0, vout);
   } else if (a.mode == LaunchArgs::FFT_FWD) {
     ProjView<T> none = pj;
     none.nproj = 0;
@@ -308,7 +297,7 @@ int launch_h_impl(const LaunchArgs& a) {
     ProjView<T> none = pj;
     none.nproj = 0;
     k_tile_inv<T, NX, NY, NZ, 0><<<ginv, thr[2], TG::smem_inv(0, 0), st>>>(
-        tmp, nullptr, 0, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, none, ep, 0, 0, 0, vout);
+        tmp, nullptr, 0, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, none, ep, 0, 0, vout);
   }
   INQB_CUDA_TRY(cudaGetLastError());
   return INQB_OK;

@@ -291,36 +291,18 @@ int build_proj_tables(const inqb_ctx& ctx, int nproj, int L, int smax, const int
     t.max_tile_ent = std::max(t.max_tile_ent, (int)by_tile[tile].size());
     t.max_tile_seg = std::max(t.max_tile_seg, t.seg_ptr[tile + 1] - t.seg_ptr[tile]);
   }
-  // point order inside each tile: the first entry of every point that has one (in
-  // point order), then the later entries (in point order, a point's in entry order, the
-  // order the scatter adds them in).  The scatter reads the first records beside the
-  // orbitals and stages the later ones in shared memory.
+  // point order inside each tile: stable sort of the tile's entries by offset
   t.tile_pts = y2n * nz;
   t.pt_stride = (t.tile_pts + 1 + 3) / 4 * 4;
   t.pt_pos.assign(total, 0);
   t.pt_ptr.assign((size_t)ntile * t.pt_stride, 0);
-  t.max_tile_ovf = 0;
-  {
-    std::vector<int> cnt(t.tile_pts), first(t.tile_pts + 1), later(t.tile_pts + 1), seen(t.tile_pts);
-    for (int tile = 0; tile < ntile; tile++) {
-      const int e0 = t.seg_ent[t.seg_ptr[tile]], e1 = t.seg_ent[t.seg_ptr[tile + 1]];
-      std::fill(cnt.begin(), cnt.end(), 0);
-      for (int e = e0; e < e1; e++) cnt[t.ent_off[e]]++;
-      for (int q = 0; q < t.tile_pts; q++) {
-        first[q + 1] = first[q] + (cnt[q] > 0 ? 1 : 0);
-        later[q + 1] = later[q] + std::max(cnt[q] - 1, 0);
-      }
-      if (first[t.tile_pts] > 0xffff || later[t.tile_pts] > 0xffff)
-        return fail(INQB_ERR_UNSUPPORTED, "more than 65535 sphere entries at the points of one tile");
-      int* tp = &t.pt_ptr[(size_t)tile * t.pt_stride];
-      for (int q = 0; q <= t.tile_pts; q++) tp[q] = first[q] | (later[q] << 16);
-      std::fill(seen.begin(), seen.end(), 0);
-      for (int e = e0; e < e1; e++) {
-        const int q = t.ent_off[e], k = seen[q]++;
-        t.pt_pos[e] = e0 + (k == 0 ? first[q] : first[t.tile_pts] + later[q] + k - 1);
-      }
-      t.max_tile_ovf = std::max(t.max_tile_ovf, later[t.tile_pts]);
-    }
+  for (int tile = 0; tile < ntile; tile++) {
+    const int e0 = t.seg_ent[t.seg_ptr[tile]], e1 = t.seg_ent[t.seg_ptr[tile + 1]];
+    int* tp = &t.pt_ptr[(size_t)tile * t.pt_stride];
+    for (int e = e0; e < e1; e++) tp[t.ent_off[e] + 1]++;
+    for (int q = 0; q < t.tile_pts; q++) tp[q + 1] += tp[q];
+    std::vector<int> fill(tp, tp + t.tile_pts);
+    for (int e = e0; e < e1; e++) t.pt_pos[e] = e0 + fill[t.ent_off[e]]++;
   }
   // grid point of every entry, in entry order
   std::vector<long> pt_of(total);

@@ -86,10 +86,10 @@ struct TileGeom {
   // pass C keeps four CTAs per SM in FP32 (64 registers a thread) and two with the
   // FP64 orbital prefetch (128 registers), where the shared memory allows them
   static constexpr int INV_MIN_CTAS = PREFETCH ? 2 : (TILE_BYTES <= 40 * 1024) ? 4 : 1;
-  static constexpr size_t smem_inv(int rec_cap, int seg_cap, int ovf_cap = 0) {
+  static constexpr size_t smem_inv(int rec_cap, int seg_cap) {
     return sizeof(cplx<T>) * ((size_t)TILE + (PREFETCH ? (size_t)PTS * G : 0) + NY + NZ) +
            sizeof(EntRec<T>) * (size_t)rec_cap + sizeof(int) * (size_t)PSTRIDE +
-           sizeof(cplx<T>) * (size_t)seg_cap * LMAX * G + sizeof(EntRec<T>) * (size_t)ovf_cap;
+           sizeof(cplx<T>) * (size_t)seg_cap * LMAX * G;
   }
   // pass A default: two CTAs per x-plane where Y1 is even
   static constexpr int YSPLIT = (Y1 % 2 == 0) ? 2 : 1;
@@ -205,8 +205,6 @@ __device__ __forceinline__ void tile_fwd_body(int bx, int by, const cplx<T>* __r
         cplx<T> a[LMAX];
 #pragma unroll
         for (int l = 0; l < LMAX; ++l) a[l] = mk<T>(0, 0);
-        // four entries' loads in flight (the sums still run in entry order)
-#pragma unroll 4
         for (int e = e0; e < e1; ++e) {
           const EntRec<T>& re = rec[e - roff];
           const int off = re.off;
@@ -607,8 +605,7 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
                                               const cplx<T>* __restrict__ in, long ld_in, cplx<T>* __restrict__ out,
                                               long ld_out, int M, const cplx<T>* __restrict__ tw_y,
                                               const cplx<T>* __restrict__ tw_z, const ProjView<T>& pj,
-                                              const EpiParams<T>& ep, int rec_cap, int seg_cap, int ovf_cap,
-                                              int vec) {
+                                              const EpiParams<T>& ep, int rec_cap, int seg_cap, int vec) {
   using TG = TileGeom<T, NX, NY, NZ>;
   using AZ = typename TG::AZ;
   constexpr int G = TG::G, PV = TG::PV, VP = TG::VP, Y1 = TG::Y1, Y2 = TG::Y2, ZS = TG::ZS;
@@ -620,7 +617,6 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
   EntRec<T>* R = reinterpret_cast<EntRec<T>*>(twz + NZ);  // [rec_cap] records in point order
   int* TP = reinterpret_cast<int*>(R + rec_cap);           // [PSTRIDE] point index of the tile
   cplx<T>* PT = reinterpret_cast<cplx<T>*>(TP + TG::PSTRIDE);  // [seg_cap][LMAX][G] projections
-  EntRec<T>* OV = reinterpret_cast<EntRec<T>*>(PT + seg_cap * LMAX * G);  // [ovf_cap] later records
 
   const int grp = bx, ix = by / Y1, y1 = by % Y1;
   const int m0 = grp * G;
@@ -639,7 +635,7 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
   cp_async_commit();
   const bool proj_on = MODE_H && pj.nproj > 0;
   const int tile = ix * Y1 + y1;
-  int roff = 0, s0 = 0, nseg = 0, nfirst = 0, nlater = 0;
+  int roff = 0, s0 = 0, nseg = 0;
   const EntRec<T>* rec = pj.ent_rec_pt;
   if (proj_on) {
     rec = stage_entries(pj, pj.ent_rec_pt, tile, rec_cap, R, roff);
@@ -648,21 +644,9 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
       cp_async16(reinterpret_cast<int4*>(TP) + q, reinterpret_cast<const int4*>(tp) + q);
     s0 = pj.seg_ptr[tile];
     nseg = pj.seg_ptr[tile + 1] - s0;
-    const int tot = tp[TG::PTS];
-    nfirst = tot & 0xffff;
-    nlater = tot >> 16;
   }
-  // the point index counts from the tile's first record: rec points there
-  if (rec != R) rec += roff_base(pj, s0, proj_on);
-  // the tile's later records (second and further entries of a point): with all its
-  // records staged (R), in shared memory (OV) when they fit, else global memory
-  const EntRec<T>* lat = rec + nfirst;
-  if (proj_on && rec != R && nlater <= ovf_cap) {
-    constexpr int V = (int)(sizeof(EntRec<T>) / 16);
-    const float4* src = reinterpret_cast<const float4*>(lat);
-    for (int q = threadIdx.x; q < nlater * V; q += blockDim.x) cp_async16(reinterpret_cast<float4*>(OV) + q, src + q);
-    lat = OV;
-  }
+  // the point index counts from the tile's first record
+  const int rbase = (rec == R) ? 0 : roff_base(pj, s0, proj_on);
   if (MODE_H && TG::PREFETCH && v16) {
     for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
       const int v = q % VP, pt = q / VP;
@@ -770,9 +754,9 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
       if (proj_on) {
         k0[b] = TP[pt];
         k1[b] = TP[pt + 1];
-        // FP32 reads the first records from global memory: start the point's now; FP64
-        // has them in shared memory already
-        if (!TG::PREFETCH && (k1[b] & 0xffff) != (k0[b] & 0xffff)) r0[b] = rec[k0[b] & 0xffff];
+        // FP32 reads records from global memory: start the first one now; FP64 has
+        // them in shared memory already
+        if (!TG::PREFETCH && k1[b] > k0[b]) r0[b] = rec[k0[b] + rbase];
       }
       vp[b] = ep.V[p] + ep.vshift;
       if (TG::PREFETCH && v16) {
@@ -798,17 +782,9 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
       cplx<T> h[PV];
 #pragma unroll
       for (int k = 0; k < PV; ++k) h[k] = S[sl + k];
-      // the point's records: its first (kk = lo - 1, when it has one), then its later
-      // ones lo .. hi - 1, the order the table lists them in
-      const int lo = k0[b] >> 16, hi = k1[b] >> 16;
-      const int kb = ((k1[b] & 0xffff) != (k0[b] & 0xffff)) ? lo - 1 : lo;
-      auto record = [&](int kk) -> EntRec<T> {
-        if (kk >= lo) return lat[kk];
-        return TG::PREFETCH ? rec[k0[b] & 0xffff] : r0[b];
-      };
       if (proj_on && pt_staged) {
-        for (int kk = kb; kk < hi; ++kk) {
-          const EntRec<T> re = record(kk);
+        for (int kk = k0[b]; kk < k1[b]; ++kk) {
+          const EntRec<T> re = (!TG::PREFETCH && kk == k0[b]) ? r0[b] : rec[kk + rbase];
           const cplx<T> ph = mk<T>(re.ph[0], re.ph[1]);
           const cplx<T>* pt = PT + (re.tseg * G + jb) * LMAX;
 #pragma unroll
@@ -825,8 +801,8 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
         }
       } else if (proj_on) {
         // more atom segments in this tile than staged: projections from global memory
-        for (int kk = kb; kk < hi; ++kk) {
-          const EntRec<T> re = record(kk);
+        for (int kk = k0[b]; kk < k1[b]; ++kk) {
+          const EntRec<T> re = (!TG::PREFETCH && kk == k0[b]) ? r0[b] : rec[kk + rbase];
           const cplx<T> ph = mk<T>(re.ph[0], re.ph[1]);
 #pragma unroll
           for (int k = 0; k < PV; ++k) {
@@ -873,9 +849,9 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
     k_tile_inv(const cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ in, long ld_in,
                cplx<T>* __restrict__ out, long ld_out, int M, const cplx<T>* __restrict__ tw_y,
                const cplx<T>* __restrict__ tw_z, ProjView<T> pj, EpiParams<T> ep, int rec_cap, int seg_cap,
-               int ovf_cap, int vec) {
+               int vec) {
   tile_inv_body<T, NX, NY, NZ, MODE_H>(blockIdx.x, blockIdx.y, tmp, in, ld_in, out, ld_out, M, tw_y, tw_z, pj, ep,
-                                       rec_cap, seg_cap, ovf_cap, vec);
+                                       rec_cap, seg_cap, vec);
 }
 
 }  // namespace inqb

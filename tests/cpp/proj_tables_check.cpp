@@ -44,29 +44,16 @@ static int check(double a, int n, int reps) {
   long tot = 0;
   for (int tile = 0; tile < ntile; tile++) {
     int e0 = t.seg_ent[t.seg_ptr[tile]], e1 = t.seg_ent[t.seg_ptr[tile + 1]];
-    // point index: bits 0-15 count the points with an entry (first records), bits
-    // 16-31 the later entries; the first records come first, then the later ones
     const int* tp = &t.pt_ptr[(size_t)tile * t.pt_stride];
-    auto first = [&](int q) { return tp[q] & 0xffff; };
-    auto later = [&](int q) { return tp[q] >> 16; };
-    const int nfirst = first(t.tile_pts);
-    if (tp[0] != 0 || nfirst + later(t.tile_pts) != e1 - e0) bad++;
-    if (later(t.tile_pts) > t.max_tile_ovf) bad++;
-    std::vector<int> seen(e1 - e0, 0), last(t.tile_pts, -1);
+    if (tp[0] != 0 || tp[t.tile_pts] != e1 - e0) bad++;
+    std::vector<int> seen(e1 - e0, 0);
     for (int e = e0; e < e1; e++) {
       int q = t.pt_pos[e] - e0;
       if (q < 0 || q >= e1 - e0) { bad++; continue; }
       seen[q]++;
       int off = t.ent_off[e];
-      if (off < 0 || off >= t.tile_pts) { bad++; continue; }
-      // a point's entries in entry order: its first record, then its later ones
-      if (last[off] < 0) {
-        if (!(first(off + 1) - first(off) == 1 && q == first(off))) bad++;
-      } else {
-        if (!(q >= nfirst + later(off) && q < nfirst + later(off + 1))) bad++;
-        if (q != (last[off] < nfirst ? nfirst + later(off) : last[off] + 1)) bad++;
-      }
-      last[off] = q;
+      if (off < 0 || off >= t.tile_pts) bad++;
+      if (!(q >= tp[off] && q < tp[off + 1])) bad++;
     }
     for (int v : seen) if (v != 1) bad++;
     for (int s = t.seg_ptr[tile]; s < t.seg_ptr[tile + 1]; s++) {
