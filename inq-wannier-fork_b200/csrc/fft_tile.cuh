@@ -36,14 +36,6 @@ struct Axis {
   __host__ __device__ static constexpr int slot_of_freq(int k) { return at(k % N1, k / N1); }
 };
 
-// Threads of the CTA running a stage loop: NT when the kernel was compiled for a fixed
-// block size (the loops' trip counts and each thread's index arithmetic then fold to
-// constants), else blockDim.x.
-template <int NT>
-__device__ __forceinline__ int nthreads() {
-  return NT > 0 ? NT : (int)blockDim.x;
-}
-
 // Twiddle table layout in shared memory: tw[k1 * N2 + j2] = exp(-2 pi i j2 k1 / N).
 template <typename A, bool INV, typename T>
 __device__ __forceinline__ cplx<T> twiddle(cplx<T> v, const cplx<T>* tw, int k1, int j2) {
@@ -52,9 +44,9 @@ __device__ __forceinline__ cplx<T> twiddle(cplx<T> v, const cplx<T>* tw, int k1,
 }
 
 // Step 1 (forward or inverse-from-natural when INV): items map to (base, es, j2).
-template <typename A, bool INV, int NT = 0, typename T, typename Map>
+template <typename A, bool INV, typename T, typename Map>
 __device__ __forceinline__ void step1(cplx<T>* S, int nitems, const cplx<T>* tw, Map map) {
-  for (int it = threadIdx.x; it < nitems; it += nthreads<NT>()) {
+  for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
     int base, es, j2;
     map(it, base, es, j2);
     cplx<T> v[A::N1];
@@ -71,10 +63,10 @@ __device__ __forceinline__ void step1(cplx<T>* S, int nitems, const cplx<T>* tw,
 }
 
 // Step 2 (forward / inverse-from-natural): items map to (base, es, k1).
-template <typename A, bool INV, int NT = 0, typename T, typename Map>
+template <typename A, bool INV, typename T, typename Map>
 __device__ __forceinline__ void step2(cplx<T>* S, int nitems, Map map) {
   if (A::N2 == 1) return;
-  for (int it = threadIdx.x; it < nitems; it += nthreads<NT>()) {
+  for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
     int base, es, k1;
     map(it, base, es, k1);
     cplx<T> v[A::N2];
@@ -89,10 +81,10 @@ __device__ __forceinline__ void step2(cplx<T>* S, int nitems, Map map) {
 // Step 2' of the inverse from transposed order: inverse DFT_N2 over k2 then the
 // conjugate twiddle; `pre` is applied to the frequency-domain values first
 // (pre(k, value) with k = k1 + N1 k2), which fuses a pointwise operator.
-template <typename A, int NT = 0, typename T, typename Map, typename Pre>
+template <typename A, typename T, typename Map, typename Pre>
 __device__ __forceinline__ void step2_inv_transposed(cplx<T>* S, int nitems, const cplx<T>* tw, Map map,
                                                      Pre pre) {
-  for (int it = threadIdx.x; it < nitems; it += nthreads<NT>()) {
+  for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
     int base, es, k1;
     map(it, base, es, k1);
     cplx<T> v[A::N2];
@@ -111,9 +103,9 @@ __device__ __forceinline__ void step2_inv_transposed(cplx<T>* S, int nitems, con
 
 // Forward step 2 fused with a pointwise operator and the inverse step 2'
 // (the kinetic multiply of H between a forward and an inverse transform).
-template <typename A, int NT = 0, typename T, typename Map, typename Op>
+template <typename A, typename T, typename Map, typename Op>
 __device__ __forceinline__ void step2_fwd_op_inv(cplx<T>* S, int nitems, const cplx<T>* tw, Map map, Op op) {
-  for (int it = threadIdx.x; it < nitems; it += nthreads<NT>()) {
+  for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
     int base, es, k1;
     map(it, base, es, k1);
     cplx<T> v[A::N2];
@@ -134,9 +126,9 @@ __device__ __forceinline__ void step2_fwd_op_inv(cplx<T>* S, int nitems, const c
 }
 
 // Step 1' of the inverse from transposed order: inverse DFT_N1 over k1, natural out.
-template <typename A, int NT = 0, typename T, typename Map>
+template <typename A, typename T, typename Map>
 __device__ __forceinline__ void step1_inv_transposed(cplx<T>* S, int nitems, Map map) {
-  for (int it = threadIdx.x; it < nitems; it += nthreads<NT>()) {
+  for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
     int base, es, j2;
     map(it, base, es, j2);
     cplx<T> v[A::N1];

@@ -30,10 +30,6 @@
 namespace inqb {
 
 constexpr int LMAX = 4;  // KB projectors per atom handled by the fused kernels
-// Block size of the H passes' second instantiation: the default schedule's, for which
-// the tile kernels are compiled with the block size fixed (other schedules run the
-// instantiation that reads blockDim)
-constexpr int kFixedThreads = 256;
 
 // ---------------------------------------------------------------- sizes
 template <int N>
@@ -123,21 +119,13 @@ int launch_h_impl(const LaunchArgs& a) {
     attr_rc = [] {
       INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_fwd<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)std::min(TG::smem_fwd(kAccAtomsMax, kRecCapMax), TG::SMEM_MAX)));
-      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_fwd<T, NX, NY, NZ, kFixedThreads>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)std::min(TG::smem_fwd(kAccAtomsMax, kRecCapMax), TG::SMEM_MAX)));
       INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x<T, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)TG::SMEM_X));
-      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x<T, NX, NY, NZ, kFixedThreads>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TG::SMEM_X));
       INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x_fft<T, NX, NY, NZ, 0>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TG::SMEM_X));
       INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_x_fft<T, NX, NY, NZ, 1>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TG::SMEM_X));
       INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_inv<T, NX, NY, NZ, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)std::min(TG::smem_inv(kRecCapMax, kAccAtomsMax), TG::SMEM_MAX)));
-      INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_inv<T, NX, NY, NZ, 1, kFixedThreads>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)std::min(TG::smem_inv(kRecCapMax, kAccAtomsMax), TG::SMEM_MAX)));
       INQB_CUDA_TRY(cudaFuncSetAttribute(k_tile_inv<T, NX, NY, NZ, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)TG::smem_inv(0, 0)));
@@ -259,32 +247,19 @@ int launch_h_impl(const LaunchArgs& a) {
     }
     if (a.events[1]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[1], st));
     if (a.events[2]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[2], st));
-    if (thr[0] == kFixedThreads)
-      k_tile_fwd<T, NX, NY, NZ, kFixedThreads><<<gfwd, thr[0], TG::smem_fwd(acc_cap, rec_cap_a), st>>>(
-          (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pjA, acc_cap, rec_cap_a, ysplit, vin);
-    else
-      k_tile_fwd<T, NX, NY, NZ><<<gfwd, thr[0], TG::smem_fwd(acc_cap, rec_cap_a), st>>>(
-          (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pjA, acc_cap, rec_cap_a, ysplit, vin);
+    k_tile_fwd<T, NX, NY, NZ><<<gfwd, thr[0], TG::smem_fwd(acc_cap, rec_cap_a), st>>>(
+        (const cplx<T>*)a.in, a.ld_in, a.M, tmp, twy, twz, pjA, acc_cap, rec_cap_a, ysplit, vin);
     if (a.events[3]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[3], st));
     // the second pass also adds the fused projection's partial sums per atom, in a
     // fixed order (its first CTAs; the third pass reads the result)
     ProjView<T> fin = pj;
     if (sep || pj.nproj == 0) fin.slots = nullptr;
-    if (thr[1] == kFixedThreads)
-      k_tile_x<T, NX, NY, NZ, kFixedThreads><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out,
-                                                                              fin, a.M, ysplit);
-    else
-      k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out, fin, a.M,
-                                                               ysplit);
+    k_tile_x<T, NX, NY, NZ><<<gx, thr[1], TG::SMEM_X, st>>>(tmp, twx, kp, (cplx<T>*)a.fourier_out, fin, a.M,
+                                                             ysplit);
     if (a.events[4]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[4], st));
-    if (thr[2] == kFixedThreads)
-      k_tile_inv<T, NX, NY, NZ, 1, kFixedThreads><<<ginv, thr[2], TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
-          tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv,
-          seg_cap, vin && vout);
-    else
-      k_tile_inv<T, NX, NY, NZ, 1><<<ginv, thr[2], TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
-          tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv,
-          seg_cap, vin && vout);
+    k_tile_inv<T, NX, NY, NZ, 1><<<ginv, thr[2], TG::smem_inv(rec_cap_inv, seg_cap), st>>>(
+        tmp, (const cplx<T>*)a.in, a.ld_in, (cplx<T>*)a.out, a.ld_out, a.M, twy, twz, pj, ep, rec_cap_inv, seg_cap,
+        vin && vout);
     if (a.events[5]) INQB_CUDA_TRY(cudaEventRecord((cudaEvent_t)a.events[5], st));
   } else if (a.mode == LaunchArgs::POISSON) {
     // solvers::poisson on M complex fields: forward z and inner y, then the outer y

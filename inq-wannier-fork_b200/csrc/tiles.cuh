@@ -91,12 +91,6 @@ struct TileGeom {
            sizeof(EntRec<T>) * (size_t)rec_cap + sizeof(int) * (size_t)PSTRIDE +
            sizeof(cplx<T>) * (size_t)seg_cap * LMAX * G;
   }
-  // CTAs per SM the first two passes are bounded for (their registers capped to match),
-  // where their shared memory holds that many: pass A three in FP32 and two in FP64,
-  // the x-line pass four in FP32 (five measured slower) and two in FP64; larger tiles
-  // leave the registers free
-  static constexpr int FWD_MIN_CTAS = TILE_BYTES > 64 * 1024 ? 1 : sizeof(T) == 4 ? 3 : 2;
-  static constexpr int X_MIN_CTAS = SMEM_X > 64 * 1024 ? 1 : sizeof(T) == 4 ? 4 : 2;
   // pass A default: two CTAs per x-plane where Y1 is even
   static constexpr int YSPLIT = (Y1 % 2 == 0) ? 2 : 1;
 };
@@ -108,7 +102,7 @@ constexpr int kRecCapMax = 1024;
 // Start the cp.async copy of tile `tile`'s entry records (from `recs`) into R
 // (cap records).  Returns the records to index with (e - roff): R when staged,
 // else global memory.
-template <int NT = 0, typename T>
+template <typename T>
 __device__ __forceinline__ const EntRec<T>* stage_entries(const ProjView<T>& pj, const EntRec<T>* recs, int tile,
                                                           int cap, EntRec<T>* R, int& roff) {
   const int e0 = pj.seg_ent[pj.seg_ptr[tile]], e1 = pj.seg_ent[pj.seg_ptr[tile + 1]];
@@ -119,7 +113,7 @@ __device__ __forceinline__ const EntRec<T>* stage_entries(const ProjView<T>& pj,
   constexpr int V = (int)(sizeof(EntRec<T>) / 16);
   const float4* src = reinterpret_cast<const float4*>(recs + e0);
   float4* dst = reinterpret_cast<float4*>(R);
-  for (int q = threadIdx.x; q < (e1 - e0) * V; q += nthreads<NT>()) cp_async16(dst + q, src + q);
+  for (int q = threadIdx.x; q < (e1 - e0) * V; q += blockDim.x) cp_async16(dst + q, src + q);
   roff = e0;
   return R;
 }
@@ -136,7 +130,7 @@ __device__ __forceinline__ int roff_base(const ProjView<T>& pj, int s0, bool on)
 // ---------------------------------------------------------------- pass A
 // The body of one CTA (bx, by) of the pass; k_tile_fwd runs it at (blockIdx.x,
 // blockIdx.y), the persistent batch kernel at the coordinates of a work item.
-template <typename T, int NX, int NY, int NZ, int NT = 0>
+template <typename T, int NX, int NY, int NZ>
 __device__ __forceinline__ void tile_fwd_body(int bx, int by, const cplx<T>* __restrict__ in, long ld, int M,
                                               cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ tw_y,
                                               const cplx<T>* __restrict__ tw_z, ProjView<T> pj, int acc_cap,
@@ -157,16 +151,16 @@ __device__ __forceinline__ void tile_fwd_body(int bx, int by, const cplx<T>* __r
   const int m0 = grp * G;
   const int gcount = min(G, M - m0);
   const bool v16 = vec && gcount == G;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = nthreads<NT>() >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const bool proj_on = pj.nproj > 0;
-  for (int i = threadIdx.x; i < NY; i += nthreads<NT>()) twy[i] = tw_y[i];
-  for (int i = threadIdx.x; i < NZ; i += nthreads<NT>()) twz[i] = tw_z[i];
+  for (int i = threadIdx.x; i < NY; i += blockDim.x) twy[i] = tw_y[i];
+  for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = tw_z[i];
   if (proj_on) {
-    for (int i = threadIdx.x; i < acc_cap * LMAX * G; i += nthreads<NT>()) acc[i] = make_double2(0.0, 0.0);
+    for (int i = threadIdx.x; i < acc_cap * LMAX * G; i += blockDim.x) acc[i] = make_double2(0.0, 0.0);
     // slots of the plane's atoms beyond the shared-memory accumulators start at zero
     if (pj.slots) {
       const int a0 = pj.plane_ptr[ix], na = pj.plane_ptr[ix + 1] - a0;
-      for (int i = threadIdx.x; i < max(0, na - acc_cap) * LMAX * G; i += nthreads<NT>()) {
+      for (int i = threadIdx.x; i < max(0, na - acc_cap) * LMAX * G; i += blockDim.x) {
         const int j = i % G, l = (i / G) % LMAX, sl = acc_cap + i / (G * LMAX);
         if (j < gcount) pj.slots[(((long)(a0 + sl) * YS + yh) * LMAX + l) * M + m0 + j] = make_double2(0.0, 0.0);
       }
@@ -176,14 +170,14 @@ __device__ __forceinline__ void tile_fwd_body(int bx, int by, const cplx<T>* __r
   for (int y1 = yh * YPER; y1 < (yh + 1) * YPER; ++y1) {
     // -- rows y1 + Y1 r of plane ix, G orbitals per point
     if (v16) {
-      for (int q = threadIdx.x; q < TG::PTS * VP; q += nthreads<NT>()) {
+      for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
         const int v = q % VP, pt = q / VP;
         const int z = pt % NZ, r = pt / NZ;
         const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
         cp_async16(S + (r * ZS + AZ::slot(z)) * G + v * PV, in + p * ld + m0 + v * PV);
       }
     } else {
-      for (int q = threadIdx.x; q < TG::PTS * G; q += nthreads<NT>()) {
+      for (int q = threadIdx.x; q < TG::PTS * G; q += blockDim.x) {
         const int j = q % G, pt = q / G;
         const int z = pt % NZ, r = pt / NZ;
         const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
@@ -191,7 +185,7 @@ __device__ __forceinline__ void tile_fwd_body(int bx, int by, const cplx<T>* __r
       }
     }
     int roff = 0;
-    const EntRec<T>* rec = proj_on ? stage_entries<NT>(pj, pj.ent_rec, ix * Y1 + y1, rec_cap, R, roff) : pj.ent_rec;
+    const EntRec<T>* rec = proj_on ? stage_entries(pj, pj.ent_rec, ix * Y1 + y1, rec_cap, R, roff) : pj.ent_rec;
     cp_async_commit();
     cp_async_wait<0>();
     __syncthreads();
@@ -261,14 +255,14 @@ __device__ __forceinline__ void tile_fwd_body(int bx, int by, const cplx<T>* __r
     }
 
     // -- z lines: (r, j), element stride G
-    step1<AZ, false, NT>(S, Y2 * G * AZ::N2, twz, [](int it, int& base, int& es, int& j2) {
+    step1<AZ, false>(S, Y2 * G * AZ::N2, twz, [](int it, int& base, int& es, int& j2) {
       const int j = it % G, rest = it / G;
       j2 = rest % AZ::N2;
       base = (rest / AZ::N2) * ZS * G + j;
       es = G;
     });
     __syncthreads();
-    step2<AZ, false, NT>(S, Y2 * G * AZ::N1, [](int it, int& base, int& es, int& k1) {
+    step2<AZ, false>(S, Y2 * G * AZ::N1, [](int it, int& base, int& es, int& k1) {
       const int j = it % G, rest = it / G;
       k1 = rest % AZ::N1;
       base = (rest / AZ::N1) * ZS * G + j;
@@ -278,7 +272,7 @@ __device__ __forceinline__ void tile_fwd_body(int bx, int by, const cplx<T>* __r
 
     // -- inner y stage: DFT_Y2 over the rows, twiddle w_NY^{y1 ka}, written straight
     // to tmp[g][ka][kz][ix][y1][G] (lanes along j write whole 64-byte runs)
-    for (int it = threadIdx.x; it < NZ * G; it += nthreads<NT>()) {
+    for (int it = threadIdx.x; it < NZ * G; it += blockDim.x) {
       const int j = it % G, kz = it / G;
       const int base = AZ::slot_of_freq(kz) * G + j;
       cplx<T> u[Y2];
@@ -300,7 +294,7 @@ __device__ __forceinline__ void tile_fwd_body(int bx, int by, const cplx<T>* __r
   if (proj_on) {
     const int a0 = pj.plane_ptr[ix];
     const int na = min(pj.plane_ptr[ix + 1] - a0, acc_cap);
-    for (int i = threadIdx.x; i < na * LMAX * G; i += nthreads<NT>()) {
+    for (int i = threadIdx.x; i < na * LMAX * G; i += blockDim.x) {
       const int j = i % G, l = (i / G) % LMAX, sl = i / (G * LMAX);
       if (j >= gcount) continue;
       const double2 v = acc[i];
@@ -317,12 +311,12 @@ __device__ __forceinline__ void tile_fwd_body(int bx, int by, const cplx<T>* __r
   }
 }
 
-template <typename T, int NX, int NY, int NZ, int NT = 0>
-__global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::FWD_MIN_CTAS)
+template <typename T, int NX, int NY, int NZ>
+__global__ void __launch_bounds__(256)
     k_tile_fwd(const cplx<T>* __restrict__ in, long ld, int M, cplx<T>* __restrict__ tmp,
                const cplx<T>* __restrict__ tw_y, const cplx<T>* __restrict__ tw_z, ProjView<T> pj, int acc_cap,
                int rec_cap, int ysplit, int vec) {
-  tile_fwd_body<T, NX, NY, NZ, NT>(blockIdx.x, blockIdx.y, in, ld, M, tmp, tw_y, tw_z, pj, acc_cap, rec_cap, ysplit,
+  tile_fwd_body<T, NX, NY, NZ>(blockIdx.x, blockIdx.y, in, ld, M, tmp, tw_y, tw_z, pj, acc_cap, rec_cap, ysplit,
                                vec);
 }
 
@@ -362,7 +356,7 @@ __device__ __forceinline__ void proj_finish_item(const ProjView<T>& pj, int M, i
 // fin.slots set, the first CTAs also finish the fused projection (pass C reads it):
 // thread t of CTA b handles item b * blockDim + t, so the few CTAs that carry the
 // finish run beside thousands that do not.
-template <typename T, int NX, int NY, int NZ, int NT = 0>
+template <typename T, int NX, int NY, int NZ>
 __device__ __forceinline__ void tile_x_body(int bx, int by, cplx<T>* __restrict__ tmp,
                                             const cplx<T>* __restrict__ tw_x, KinParams<T> kp,
                                             cplx<T>* __restrict__ fout) {
@@ -377,7 +371,7 @@ __device__ __forceinline__ void tile_x_body(int bx, int by, cplx<T>* __restrict_
 
   const int kz = bx % NZ, ka = bx / NZ, grp = by;
   cplx<T>* blk = tmp + ((long)(grp * Y2 + ka) * NZ + kz) * TG::BLK;
-  for (int i = threadIdx.x; i < NX; i += nthreads<NT>()) twx[i] = tw_x[i];
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) twx[i] = tw_x[i];
   // Along an x line 1/2 |G + k + A|^2 / N = kA2 n0^2 + kinB n0 + kinC with
   // q = n1 b1 + n2 b2 + k + A:  kA2 = |b0|^2 / 2N, kinB = b0.q / N, kinC = |q|^2 / 2N
   if (threadIdx.x < Y1) {
@@ -399,11 +393,11 @@ __device__ __forceinline__ void tile_x_body(int bx, int by, cplx<T>* __restrict_
   // outer y stage straight from HBM: a thread loads the Y1 values of its (ix, j)
   // column (lanes along j read whole 64-byte runs), DFT_Y1 over y1 -> kb, and
   // writes the column to shared memory once; two columns per thread in flight
-  for (int it0 = threadIdx.x; it0 < NX * G; it0 += 2 * nthreads<NT>()) {
+  for (int it0 = threadIdx.x; it0 < NX * G; it0 += 2 * blockDim.x) {
     cplx<T> u[2][Y1];
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-      const int it = it0 + c * nthreads<NT>();
+      const int it = it0 + c * blockDim.x;
       if (it >= NX * G) continue;
       const int j = it % G, ix = it / G;
 #pragma unroll
@@ -411,7 +405,7 @@ __device__ __forceinline__ void tile_x_body(int bx, int by, cplx<T>* __restrict_
     }
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-      const int it = it0 + c * nthreads<NT>();
+      const int it = it0 + c * blockDim.x;
       if (it >= NX * G) continue;
       const int j = it % G, ix = it / G;
       DFT<Y1, false, T>::run(u[c]);
@@ -435,12 +429,12 @@ __device__ __forceinline__ void tile_x_body(int bx, int by, cplx<T>* __restrict_
     es = XS;
   };
   const int n2 = sym_freq(kz, NZ);
-  step1<AX, false, NT>(X, Y1 * G * AX::N2, twx, map1);
+  step1<AX, false>(X, Y1 * G * AX::N2, twx, map1);
   __syncthreads();
   // fout (optional): the forward coefficients of this block, before the kinetic
   // factor, as [kx][kb][G] (the adjoint's velocity terms read them)
   cplx<T>* fblk = fout ? fout + ((long)(grp * Y2 + ka) * NZ + kz) * TG::BLK : nullptr;
-  step2_fwd_op_inv<AX, NT>(X, Y1 * G * AX::N1, twx, map2, [&](int it, int kx, cplx<T> v) {
+  step2_fwd_op_inv<AX>(X, Y1 * G * AX::N1, twx, map2, [&](int it, int kx, cplx<T> v) {
     const int kb = (it / G) / AX::N1;
     if (fblk) fblk[(kx * Y1 + kb) * G + it % G] = v;
     const int n0 = sym_freq(kx, NX);
@@ -451,11 +445,11 @@ __device__ __forceinline__ void tile_x_body(int bx, int by, cplx<T>* __restrict_
     return k * v;
   });
   __syncthreads();
-  step1_inv_transposed<AX, NT>(X, Y1 * G * AX::N2, map1);
+  step1_inv_transposed<AX>(X, Y1 * G * AX::N2, map1);
   __syncthreads();
 
   // inverse outer y stage kb -> y1, written straight back to HBM
-  for (int it = threadIdx.x; it < NX * G; it += nthreads<NT>()) {
+  for (int it = threadIdx.x; it < NX * G; it += blockDim.x) {
     const int j = it % G, ix = it / G;
     const int base = AX::slot(ix) * XS + j;
     cplx<T> u[Y1];
@@ -467,8 +461,8 @@ __device__ __forceinline__ void tile_x_body(int bx, int by, cplx<T>* __restrict_
   }
 }
 
-template <typename T, int NX, int NY, int NZ, int NT = 0>
-__global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::X_MIN_CTAS)
+template <typename T, int NX, int NY, int NZ>
+__global__ void __launch_bounds__(256)
     k_tile_x(cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ tw_x, KinParams<T> kp,
              cplx<T>* __restrict__ fout, ProjView<T> fin, int fin_M, int fin_ysplit) {
   if (fin.slots) {
@@ -477,7 +471,7 @@ __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::X_MIN_CTAS)
     for (long i = ((long)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
       proj_finish_item(fin, fin_M, fin_ysplit, i);
   }
-  tile_x_body<T, NX, NY, NZ, NT>(blockIdx.x, blockIdx.y, tmp, tw_x, kp, fout);
+  tile_x_body<T, NX, NY, NZ>(blockIdx.x, blockIdx.y, tmp, tw_x, kp, fout);
 }
 
 // ---------------------------------------------------------------- pass B of the plain FFTs
@@ -606,7 +600,7 @@ __global__ void __launch_bounds__(256)
 // with cp.async at the start, so that read overlaps the inverse transforms.
 // MODE_H = 1: the H epilogue; 0: out = alpha * (inverse transform), the second
 // half of to_real (alpha = 1/N), reading neither orbitals, V nor projectors.
-template <typename T, int NX, int NY, int NZ, int MODE_H, int NT = 0>
+template <typename T, int NX, int NY, int NZ, int MODE_H>
 __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __restrict__ tmp,
                                               const cplx<T>* __restrict__ in, long ld_in, cplx<T>* __restrict__ out,
                                               long ld_out, int M, const cplx<T>* __restrict__ tw_y,
@@ -632,7 +626,7 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
   // group 0: the (ka, kz) runs of this tile, needed first; group 1: what only the
   // epilogue reads (entry records, point index, and in FP64 the input orbitals).
   // (Reading the runs into registers for the y stage measured slower than staging.)
-  for (int q = threadIdx.x; q < TG::PTS * VP; q += nthreads<NT>()) {
+  for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
     const int v = q % VP, pt = q / VP;
     const int kz = pt % NZ, ka = pt / NZ;
     cp_async16(S + (ka * ZS + AZ::slot(kz)) * G + v * PV,
@@ -644,9 +638,9 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
   int roff = 0, s0 = 0, nseg = 0;
   const EntRec<T>* rec = pj.ent_rec_pt;
   if (proj_on) {
-    rec = stage_entries<NT>(pj, pj.ent_rec_pt, tile, rec_cap, R, roff);
+    rec = stage_entries(pj, pj.ent_rec_pt, tile, rec_cap, R, roff);
     const int* tp = pj.pt_ptr + (long)tile * TG::PSTRIDE;
-    for (int q = threadIdx.x; q < TG::PSTRIDE / 4; q += nthreads<NT>())
+    for (int q = threadIdx.x; q < TG::PSTRIDE / 4; q += blockDim.x)
       cp_async16(reinterpret_cast<int4*>(TP) + q, reinterpret_cast<const int4*>(tp) + q);
     s0 = pj.seg_ptr[tile];
     nseg = pj.seg_ptr[tile + 1] - s0;
@@ -654,7 +648,7 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
   // the point index counts from the tile's first record
   const int rbase = (rec == R) ? 0 : roff_base(pj, s0, proj_on);
   if (MODE_H && TG::PREFETCH && v16) {
-    for (int q = threadIdx.x; q < TG::PTS * VP; q += nthreads<NT>()) {
+    for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
       const int v = q % VP, pt = q / VP;
       const int z = pt % NZ, r = pt / NZ;
       const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
@@ -662,13 +656,13 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
     }
   }
   cp_async_commit();
-  for (int i = threadIdx.x; i < NY; i += nthreads<NT>()) twy[i] = tw_y[i];
-  for (int i = threadIdx.x; i < NZ; i += nthreads<NT>()) twz[i] = tw_z[i];
+  for (int i = threadIdx.x; i < NY; i += blockDim.x) twy[i] = tw_y[i];
+  for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = tw_z[i];
   // the tile's atom projections, in the tile precision, as [segment][orbital][l]
   // (a thread's orbitals read their LMAX values as whole 16-byte vectors)
   const bool pt_staged = nseg <= seg_cap;
   if (proj_on && pt_staged) {
-    for (int i = threadIdx.x; i < nseg * LMAX * G; i += nthreads<NT>()) {
+    for (int i = threadIdx.x; i < nseg * LMAX * G; i += blockDim.x) {
       const int l = i % LMAX, j = (i / LMAX) % G, ts = i / (G * LMAX);
       cplx<T> v = mk<T>(0, 0);
       if (l < pj.L && j < gcount) {
@@ -682,7 +676,7 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
   __syncthreads();
 
   // inverse inner y stage: conj twiddle, inverse DFT_Y2 over ka -> rows
-  for (int it = threadIdx.x; it < NZ * G; it += nthreads<NT>()) {
+  for (int it = threadIdx.x; it < NZ * G; it += blockDim.x) {
     const int j = it % G, zi = it / G;
     const int base = AZ::slot(zi) * G + j;
     cplx<T> u[Y2];
@@ -696,14 +690,14 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
   }
   __syncthreads();
   // inverse z from natural order: element z ends in slot_of_freq(z)
-  step1<AZ, true, NT>(S, Y2 * G * AZ::N2, twz, [](int it, int& base, int& es, int& j2) {
+  step1<AZ, true>(S, Y2 * G * AZ::N2, twz, [](int it, int& base, int& es, int& j2) {
     const int j = it % G, rest = it / G;
     j2 = rest % AZ::N2;
     base = (rest / AZ::N2) * ZS * G + j;
     es = G;
   });
   __syncthreads();
-  step2<AZ, true, NT>(S, Y2 * G * AZ::N1, [](int it, int& base, int& es, int& k1) {
+  step2<AZ, true>(S, Y2 * G * AZ::N1, [](int it, int& base, int& es, int& k1) {
     const int j = it % G, rest = it / G;
     k1 = rest % AZ::N1;
     base = (rest / AZ::N1) * ZS * G + j;
@@ -721,7 +715,7 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
   cp_async_wait<0>();
   __syncthreads();
   if (!MODE_H) {
-    for (int q = threadIdx.x; q < TG::PTS * VP; q += nthreads<NT>()) {
+    for (int q = threadIdx.x; q < TG::PTS * VP; q += blockDim.x) {
       const int v = q % VP, pt = q / VP;
       const int z = pt % NZ, r = pt / NZ;
       const long p = ((long)ix * NY + y1 + Y1 * r) * NZ + z;
@@ -742,7 +736,7 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
     }
     return;
   }
-  for (int q0 = threadIdx.x; q0 < TG::PTS * VP; q0 += BE * nthreads<NT>()) {
+  for (int q0 = threadIdx.x; q0 < TG::PTS * VP; q0 += BE * blockDim.x) {
     cplx<T> x[BE][PV];
     T vp[BE];
     // the first entry record of each point, fetched with the orbitals
@@ -750,7 +744,7 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
     int k0[BE], k1[BE];
 #pragma unroll
     for (int b = 0; b < BE; ++b) {
-      const int q = q0 + b * nthreads<NT>();
+      const int q = q0 + b * blockDim.x;
       k0[b] = k1[b] = 0;
       if (q >= TG::PTS * VP) continue;
       const int v = q % VP, pt = q / VP;
@@ -778,7 +772,7 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
     }
 #pragma unroll
     for (int b = 0; b < BE; ++b) {
-      const int q = q0 + b * nthreads<NT>();
+      const int q = q0 + b * blockDim.x;
       if (q >= TG::PTS * VP) continue;
       const int v = q % VP, pt = q / VP;
       const int z = pt % NZ, r = pt / NZ;
@@ -850,13 +844,13 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
   }
 }
 
-template <typename T, int NX, int NY, int NZ, int MODE_H = 1, int NT = 0>
+template <typename T, int NX, int NY, int NZ, int MODE_H = 1>
 __global__ void __launch_bounds__(256, TileGeom<T, NX, NY, NZ>::INV_MIN_CTAS)
     k_tile_inv(const cplx<T>* __restrict__ tmp, const cplx<T>* __restrict__ in, long ld_in,
                cplx<T>* __restrict__ out, long ld_out, int M, const cplx<T>* __restrict__ tw_y,
                const cplx<T>* __restrict__ tw_z, ProjView<T> pj, EpiParams<T> ep, int rec_cap, int seg_cap,
                int vec) {
-  tile_inv_body<T, NX, NY, NZ, MODE_H, NT>(blockIdx.x, blockIdx.y, tmp, in, ld_in, out, ld_out, M, tw_y, tw_z, pj, ep,
+  tile_inv_body<T, NX, NY, NZ, MODE_H>(blockIdx.x, blockIdx.y, tmp, in, ld_in, out, ld_out, M, tw_y, tw_z, pj, ep,
                                        rec_cap, seg_cap, vec);
 }
 
