@@ -86,10 +86,14 @@ struct TileGeom {
   // pass C keeps four CTAs per SM in FP32 (64 registers a thread) and two with the
   // FP64 orbital prefetch (128 registers), where the shared memory allows them
   static constexpr int INV_MIN_CTAS = PREFETCH ? 2 : (TILE_BYTES <= 40 * 1024) ? 4 : 1;
+  // complex values per atom segment of pass C's staged projections [l][orbital]: 64
+  // bytes of padding, so that consecutive segments start in opposite halves of the
+  // shared-memory banks
+  static constexpr int PT_STRIDE = LMAX * G + 64 / (int)sizeof(cplx<T>);
   static constexpr size_t smem_inv(int rec_cap, int seg_cap) {
     return sizeof(cplx<T>) * ((size_t)TILE + (PREFETCH ? (size_t)PTS * G : 0) + NY + NZ) +
            sizeof(EntRec<T>) * (size_t)rec_cap + sizeof(int) * (size_t)PSTRIDE +
-           sizeof(cplx<T>) * (size_t)seg_cap * LMAX * G;
+           sizeof(cplx<T>) * (size_t)seg_cap * PT_STRIDE;
   }
   // pass A default: two CTAs per x-plane where Y1 is even
   static constexpr int YSPLIT = (Y1 % 2 == 0) ? 2 : 1;
@@ -616,7 +620,7 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
   cplx<T>* twz = twy + NY;
   EntRec<T>* R = reinterpret_cast<EntRec<T>*>(twz + NZ);  // [rec_cap] records in point order
   int* TP = reinterpret_cast<int*>(R + rec_cap);           // [PSTRIDE] point index of the tile
-  cplx<T>* PT = reinterpret_cast<cplx<T>*>(TP + TG::PSTRIDE);  // [seg_cap][LMAX][G] projections
+  cplx<T>* PT = reinterpret_cast<cplx<T>*>(TP + TG::PSTRIDE);  // [seg_cap][PT_STRIDE] projections
 
   const int grp = bx, ix = by / Y1, y1 = by % Y1;
   const int m0 = grp * G;
@@ -658,18 +662,19 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
   cp_async_commit();
   for (int i = threadIdx.x; i < NY; i += blockDim.x) twy[i] = tw_y[i];
   for (int i = threadIdx.x; i < NZ; i += blockDim.x) twz[i] = tw_z[i];
-  // the tile's atom projections, in the tile precision, as [segment][orbital][l]
-  // (a thread's orbitals read their LMAX values as whole 16-byte vectors)
+  // the tile's atom projections, in the tile precision, as [segment][l][orbital] with
+  // a segment stride of PT_STRIDE: the lanes of one grid point read one contiguous run
+  // per l (a thread's PV orbitals as one 16-byte vector)
   const bool pt_staged = nseg <= seg_cap;
   if (proj_on && pt_staged) {
     for (int i = threadIdx.x; i < nseg * LMAX * G; i += blockDim.x) {
-      const int l = i % LMAX, j = (i / LMAX) % G, ts = i / (G * LMAX);
+      const int j = i % G, l = (i / G) % LMAX, ts = i / (G * LMAX);
       cplx<T> v = mk<T>(0, 0);
       if (l < pj.L && j < gcount) {
         const double2 d = ld_l2(pj.proj + ((long)pj.seg_atom[s0 + ts] * pj.L + l) * M + m0 + j);
         v = mk<T>((T)d.x, (T)d.y);
       }
-      PT[i] = v;
+      PT[ts * TG::PT_STRIDE + l * G + j] = v;
     }
   }
   cp_async_wait<1>();
@@ -786,18 +791,23 @@ __device__ __forceinline__ void tile_inv_body(int bx, int by, const cplx<T>* __r
         for (int kk = k0[b]; kk < k1[b]; ++kk) {
           const EntRec<T> re = (!TG::PREFETCH && kk == k0[b]) ? r0[b] : rec[kk + rbase];
           const cplx<T> ph = mk<T>(re.ph[0], re.ph[1]);
-          const cplx<T>* pt = PT + (re.tseg * G + jb) * LMAX;
+          const cplx<T>* pt = PT + re.tseg * TG::PT_STRIDE + jb;
+          // per orbital k, t_k = sum over l in increasing order; the PV orbitals of
+          // one l are adjacent (one 16-byte load)
+          cplx<T> t[PV];
 #pragma unroll
-          for (int k = 0; k < PV; ++k) {
-            cplx<T> t = mk<T>(0, 0);
+          for (int k = 0; k < PV; ++k) t[k] = mk<T>(0, 0);
 #pragma unroll
-            for (int l = 0; l < LMAX; ++l) {
-              const cplx<T> pv = pt[k * LMAX + l];
-              t.x = fma(re.beta[l], pv.x, t.x);
-              t.y = fma(re.beta[l], pv.y, t.y);
+          for (int l = 0; l < LMAX; ++l) {
+#pragma unroll
+            for (int k = 0; k < PV; ++k) {
+              const cplx<T> pv = pt[l * G + k];
+              t[k].x = fma(re.beta[l], pv.x, t[k].x);
+              t[k].y = fma(re.beta[l], pv.y, t[k].y);
             }
-            h[k] = h[k] + mul_conj(t, ph);
           }
+#pragma unroll
+          for (int k = 0; k < PV; ++k) h[k] = h[k] + mul_conj(t[k], ph);
         }
       } else if (proj_on) {
         // more atom segments in this tile than staged: projections from global memory
