@@ -142,3 +142,17 @@ def test_adjoint_orchestration_matches_finite_differences():
         e[p] = h
         fd = (f(amps, V + e) - f(amps, V - e)) / (2 * h)
         assert abs(fd - float(V_t.grad[p])) < 1e-7 * max(1.0, abs(fd))
+
+
+def test_recompute_overlap_follows_the_block_size():
+    """The checkpointed backward recomputes beside its walk only for small blocks
+    (grid points x orbitals up to OVERLAP_MAX_ELEMENTS); True / False force either form."""
+    limit = DipolePropagation.OVERLAP_MAX_ELEMENTS
+    for N, M, expect in ((32 ** 3, 16, True), (64 ** 3, 16, True), (64 ** 3, 128, False), (144 ** 3, 16, False)):
+        ham = DenseHam(4)
+        ham.N = N
+        prop = DipolePropagation(ham, torch.zeros((4, M), dtype=torch.complex128), np.ones(M), 0.05, 10)
+        assert prop._overlapped() is expect and (N * M <= limit) is expect
+        for forced in (True, False):
+            prop.overlap = forced
+            assert prop._overlapped() is forced
