@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <array>
+#include <cmath>
 #include <complex>
 #include <cstddef>
 #include <ostream>
@@ -173,10 +174,28 @@ inline kb_tables gaussian_kb(const std::array<double, 9>& lattice, const std::ar
 }
 
 // ks_hamiltonian<complex> on one GPU (src/hamiltonian/ks_hamiltonian.hpp:35-228).
+// exchange_operator (src/hamiltonian/exchange_operator.hpp:30-231) as every theory this
+// library runs has it: the exact-exchange coefficient is 0, so enabled() is false and
+// the operator adds nothing to H|phi> (ks_hamiltonian.hpp:147) or to the energy
+// (energy.hpp:87-91).  Exact exchange (hybrid and Hartree-Fock theories) is not
+// provided; ks_hamiltonian refuses a coefficient that INQ would treat as enabled.
+class exchange_operator {
+ public:
+  // INQ's test: |coefficient| > 1e-14 (exchange_operator.hpp:229-231)
+  static bool would_enable(double coefficient) { return std::fabs(coefficient) > 1.0e-14; }
+  bool enabled() const { return false; }
+};
+
 class ks_hamiltonian {
  public:
-  ks_hamiltonian(const std::array<double, 9>& lattice, const std::array<int, 3>& nr, precision p, int device = 0)
+  // exchange_coefficient: the theory's exact-exchange fraction (ks_hamiltonian.hpp:80);
+  // only 0 is accepted (std::invalid_argument otherwise, before any device work)
+  ks_hamiltonian(const std::array<double, 9>& lattice, const std::array<int, 3>& nr, precision p, int device = 0,
+                 double exchange_coefficient = 0.0)
       : lattice_(lattice), nr_(nr), prec_(p) {
+    if (exchange_operator::would_enable(exchange_coefficient))
+      throw std::invalid_argument("ks_hamiltonian: exact exchange is not provided (exchange coefficient " +
+                                  std::to_string(exchange_coefficient) + ", only 0 is supported)");
     check(inqb_ctx_create(lattice.data(), nr[0], nr[1], nr[2], (int)p, device, &ctx_), "inqb_ctx_create");
   }
   ks_hamiltonian(const ks_hamiltonian&) = delete;
@@ -186,6 +205,8 @@ class ks_hamiltonian {
   long basis_size() const { return (long)nr_[0] * nr_[1] * nr_[2]; }
   double volume_element() const { return inqb_volume_element(ctx_); }
   inqb_ctx* handle() const { return ctx_; }
+  // exchange() (ks_hamiltonian.hpp:206-212): never enabled here
+  const exchange_operator& exchange() const { return exchange_; }
 
   // scalar_potential() (ks_hamiltonian.hpp:200-204), one spin component
   void set_scalar_potential(const std::vector<double>& V) {
@@ -224,6 +245,7 @@ class ks_hamiltonian {
   std::array<int, 3> nr_;
   precision prec_;
   inqb_ctx* ctx_ = nullptr;
+  exchange_operator exchange_;
 };
 
 // operations::exponential_in_place (src/operations/exponential.hpp:21-34) on the

@@ -92,7 +92,18 @@ class _DeviceDoubles:
 class KSHamiltonian:
     """H|psi> and propagators for one cell/grid on one GPU (drop-in for ks_hamiltonian)."""
 
-    def __init__(self, lattice, nr, precision="fp64", device: int = 0):
+    # INQ's exchange_operator::enabled(): |coefficient| > 1e-14 (exchange_operator.hpp:229-231)
+    EXCHANGE_THRESHOLD = 1.0e-14
+
+    def __init__(self, lattice, nr, precision="fp64", device: int = 0, exchange_coefficient: float = 0.0):
+        """exchange_coefficient: the theory's exact-exchange fraction (ks_hamiltonian.hpp:80).
+        Exact exchange is not provided, so only 0 is accepted (ValueError otherwise,
+        before any device work); exchange_enabled is then False, as INQ's
+        exchange().enabled() is for these theories."""
+        if abs(float(exchange_coefficient)) > self.EXCHANGE_THRESHOLD:
+            raise ValueError(f"exact exchange is not provided (exchange coefficient {exchange_coefficient}, "
+                             "only 0 is supported)")
+        self.exchange_enabled = False
         self.lattice = _lattice(lattice).reshape(3, 3).copy()
         self.nr = tuple(int(n) for n in nr)
         self.N = int(np.prod(self.nr))
@@ -116,6 +127,7 @@ class KSHamiltonian:
         other.precision = self.precision
         other.dtype = self.dtype
         other.device = self.device
+        other.exchange_enabled = False
         h = ctypes.c_void_p()
         call("inqb_ctx_clone", self._h, ctypes.byref(h))
         other._h = h

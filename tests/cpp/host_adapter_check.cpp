@@ -44,6 +44,7 @@ int main(int argc, char** argv) {
   double diff = 0.0;
   for (long i = 0; i < N * M; i++) diff += std::abs(hphi[i] - 1.5 * w * psi[i]);
   std::printf("ho_mean_abs_diff %.12e\n", diff / (N * M));
+  std::printf("exchange_enabled %d\n", ham.exchange().enabled() ? 1 : 0);
 
   // generic exponential (HamiltonianType + axpby) vs the fused Horner exponential
   b2::device_orbitals a = phi, b = phi;

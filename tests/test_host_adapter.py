@@ -72,6 +72,7 @@ def test_host_adapter_runs(pb, oracle_mod, tmp_path):
     vals = dict(line.split() for line in r.stdout.strip().splitlines())
     assert float(vals["ho_mean_abs_diff"]) == pytest.approx(0.0051420503, rel=1.2e-5)
     assert float(vals["exp_generic_vs_fused"]) < 1e-12
+    assert vals["exchange_enabled"] == "0"  # exchange coefficient 0: INQ's operator disabled
     ref = _oracle_chain(oracle_mod)
     for key in ("scf_iterations", "cn_scf_iterations"):
         assert int(vals[key]) == ref[key], key
