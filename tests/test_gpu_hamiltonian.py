@@ -169,6 +169,21 @@ def test_apply_h_host_buffers(pb, cfg0_small):
     assert rel_max(host, dev) < 1e-14
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_apply_h_host_buffers_chunked(pb, precision):
+    """inqb_apply_h_host with more orbitals than one chunk and a ragged last chunk (77
+    orbitals: chunks of 32, 32 and 13, copied in, applied and copied out on three
+    streams) gives the device-resident apply bit for bit."""
+    s = small_system(pb, n=32, M=77, seed=31)
+    h = make_product(pb, s, precision)
+    psi = np.ascontiguousarray(s["psi"])
+    if precision == "mixed":
+        psi = psi.astype(np.complex64)
+    dev = h(torch.as_tensor(psi).to("cuda")).cpu().numpy()
+    host = h.apply_host(psi)
+    assert host.dtype == dev.dtype and np.array_equal(host, dev)
+
+
 @pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
 def test_apply_h_fourier_mask(pb, oracle_mod, cfg0_small, precision, tol):
     """INQ's zero_outside_sphere on the Laplacian term (transform.hpp:363-364), k + A != 0."""
